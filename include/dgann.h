@@ -1,0 +1,183 @@
+/*
+ * dgann.h -- C ABI of libdgann, the B200 (sm_100a) search hot path of
+ * pydiskann_b200: batched Vamana/DiskANN beam search (FP32 / BF16 storage,
+ * PQ, int8 SQ, F16 and RaBitQ codes with an exact FP32 rerank), label-filtered
+ * beam search and SPFresh posting-list scans.
+ *
+ * The entry points replace the search surface of diskann-rs 0.5.0 (paths
+ * relative to the crate root; each declaration names what it stands in for).
+ * Conventions:
+ *   - every call returns a DgStatus; DG_OK is 0.  On failure the thread-local
+ *     message of dg_last_error() says why.  Nothing panics or throws across
+ *     the ABI (the reference asserts on a dimension mismatch,
+ *     src/lib.rs:684-690; here that is DG_EINVAL).
+ *   - ids are u32 node ids (u64 for SPFresh); result rows are k-strided and
+ *     padded with DG_PAD / +inf; the true count of each row is in out_counts
+ *     (the reference returns min(k, found), tests/correctness.rs:58-66).
+ *   - the caller owns every input; dg_*_create copies what it needs into HBM.
+ *     Query and output pointers are host memory unless DG_FLAG_DEVICE_PTRS is
+ *     set, in which case they are device pointers on the handle's device.
+ *   - a handle may be searched from several host threads; calls on one handle
+ *     are serialised internally.  `stream` (a cudaStream_t, may be NULL for the
+ *     handle's own stream) orders the work; with host pointers the call
+ *     returns after the results are in host memory.
+ */
+#ifndef DGANN_H
+#define DGANN_H
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DG_API __attribute__((visibility("default")))
+#else
+#define DG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DG_PAD 0xFFFFFFFFu
+#define DG_PAD64 0xFFFFFFFFFFFFFFFFull
+#define DGANN_VERSION 1
+
+typedef enum {
+  DG_OK = 0,
+  DG_EINVAL = 1,   /* bad shape, dimension mismatch, bad parameter */
+  DG_ENOMEM = 2,   /* HBM budget exceeded / allocation failed */
+  DG_ETIMEOUT = 3, /* a bounded device wait expired */
+  DG_EDEVICE = 4,  /* CUDA error (message in dg_last_error) */
+  DG_ENOTSUP = 5   /* combination not implemented */
+} DgStatus;
+
+/* Metrics (src/metric.rs:16-39; the Python binding's "l2" is squared L2,
+ * python/src/lib.rs:13,28). */
+typedef enum { DG_L2SQ = 0, DG_L2 = 1, DG_COSINE = 2, DG_DOT = 3 } DgMetric;
+
+/* Where the beam search takes its distances from. */
+typedef enum {
+  DG_TRAVERSE_F32 = 0,  /* full vectors (DiskANN::distance_to, src/lib.rs:726-733) */
+  DG_TRAVERSE_BF16 = 1, /* BF16 copy of the vectors, FP32 accumulate */
+  DG_TRAVERSE_CODES = 2 /* quantized codes (QuantizedDiskANN, src/quantized.rs:13-54) */
+} DgTraversal;
+
+typedef enum { DG_Q_NONE = 0, DG_Q_PQ = 1, DG_Q_INT8 = 2, DG_Q_RABITQ = 3, DG_Q_F16 = 4 } DgQuantizer;
+
+/* Filter::matches as a postfix program (src/filtered.rs:61-135). Leaves test
+ * labels[field] (a missing field never matches); AND/OR pop `field` results. */
+typedef enum {
+  DG_F_TRUE = 0, DG_F_EQ = 1, DG_F_IN = 2, DG_F_LT = 3, DG_F_GT = 4,
+  DG_F_RANGE = 5, DG_F_AND = 6, DG_F_OR = 7
+} DgFilterOpCode;
+typedef struct {
+  uint32_t op;
+  uint32_t field; /* label field of a leaf; child count of AND/OR */
+  uint64_t a;     /* value (EQ/LT/GT), min (RANGE), offset into the value pool (IN) */
+  uint64_t b;     /* max (RANGE), value count (IN) */
+} DgFilterOp;
+
+#define DG_FLAG_DEVICE_PTRS 1u /* queries / outputs are device pointers */
+
+typedef struct DgIndex DgIndex;
+
+/* Graph index: replaces DiskANN<D> (src/lib.rs:305-330) once built/opened. */
+typedef struct {
+  uint32_t dim;
+  uint32_t max_degree; /* R; adjacency rows are R slots padded with DG_PAD */
+  uint64_t num_vectors;
+  uint32_t medoid;     /* entry point (src/lib.rs:748-768) */
+  int32_t metric;      /* DgMetric */
+  const float *vectors;      /* host f32[num_vectors*dim] */
+  const uint32_t *adjacency; /* host u32[num_vectors*max_degree] */
+  int32_t device;            /* CUDA device ordinal */
+  uint64_t hbm_budget_bytes; /* 0 = no limit; creation fails with DG_ENOMEM beyond it */
+} DgIndexDesc;
+
+/* DiskANN::build_index / open -> a device-resident index. */
+DG_API DgStatus dg_index_create(const DgIndexDesc *desc, DgIndex **out);
+DG_API DgStatus dg_index_destroy(DgIndex *idx);
+
+/* Adds a BF16 copy of the vectors for DG_TRAVERSE_BF16 (FP32 accumulate). */
+DG_API DgStatus dg_index_enable_bf16(DgIndex *idx);
+
+/* QuantizedDiskANN::from_pq (src/quantized.rs:210-222): codebooks
+ * [M][K][dim/M] f32, codes u8[n*M].  Pass codes = NULL to encode on the GPU
+ * with ProductQuantizer::encode semantics (src/pq.rs:122-149). */
+DG_API DgStatus dg_index_attach_pq(DgIndex *idx, uint32_t M, uint32_t K, const float *codebooks,
+                            const uint8_t *codes);
+/* QuantizedDiskANN::from_int8 (src/quantized.rs:252-265): global scale/offset
+ * (src/sq.rs:128-157); codes = NULL encodes on the GPU (src/sq.rs:208-220). */
+DG_API DgStatus dg_index_attach_int8(DgIndex *idx, float scale, float offset, const uint8_t *codes);
+/* QuantizedDiskANN::from_f16 (src/quantized.rs:225-236). */
+DG_API DgStatus dg_index_attach_f16(DgIndex *idx);
+/* QuantizedDiskANN::from_rabitq (src/quantized.rs:239-249): padded dim,
+ * centroid f32[dim], signs f32[3*padded] (src/rabitq.rs:78-107); codes of
+ * padded/8+8 bytes or NULL to encode on the GPU (src/rabitq.rs:218-256). */
+DG_API DgStatus dg_index_attach_rabitq(DgIndex *idx, uint32_t padded, const float *centroid,
+                                const float *signs, const uint8_t *codes);
+/* FilteredDiskANN labels (src/filtered.rs:140-160): u64[n*num_fields]. */
+DG_API DgStatus dg_index_attach_labels(DgIndex *idx, uint32_t num_fields, const uint64_t *labels);
+
+typedef struct {
+  uint32_t k;
+  uint32_t beam_width;  /* L (search_with_dists' beam_width) */
+  uint32_t rerank_size; /* QuantizedConfig::rerank_size (src/quantized.rs:133-143) */
+  int32_t traversal;    /* DgTraversal */
+  /* Filter: ops[filter_offsets[q] .. filter_offsets[q+1]) is query q's
+   * program when filter_offsets != NULL; otherwise ops[0..filter_nops) applies
+   * to every query; no ops = Filter::None. Host pointers. */
+  const DgFilterOp *filter_ops;
+  uint32_t filter_nops;
+  const uint32_t *filter_offsets;
+  const uint64_t *filter_pool;
+  uint32_t filter_pool_len;
+  const uint32_t *per_query_beam; /* optional u32[nq] host array of per-query L */
+  uint32_t flags;                 /* DG_FLAG_* */
+  void *stream;                   /* cudaStream_t or NULL */
+} DgSearchParams;
+
+/* Batched search.  Stands in for DiskANN::search_with_dists (src/lib.rs:683-714),
+ * QuantizedDiskANN::search_with_dists / search_batch /
+ * search_filtered_with_dists (src/quantized.rs:300-398) and
+ * FilteredDiskANN::search_filtered_with_dists / search_filtered_batch
+ * (src/filtered.rs:436-480).  queries f32[nq*dim]; out_ids u32[nq*k];
+ * out_dists f32[nq*k]; out_counts u32[nq]; out_stats (optional) u32[nq*2] =
+ * (expansions, distance evaluations) per query. */
+DG_API DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *queries, uint32_t nq,
+                         uint32_t *out_ids, float *out_dists, uint32_t *out_counts,
+                         uint32_t *out_stats);
+
+/* FilteredDiskANN::count_matching (src/filtered.rs:508-510). */
+DG_API DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
+                           const uint64_t *pool, uint32_t pool_len, uint64_t *out_count);
+
+/* ---------------------------------------------------------- index building */
+/* calculate_medoid (src/lib.rs:748-768) on the GPU. X is host f32[n*dim]. */
+DG_API DgStatus dg_medoid(const float *X, uint64_t n, uint32_t dim, int32_t metric, int32_t device,
+                   uint32_t *out_medoid);
+/* build_vamana_graph (src/lib.rs:774-917) on the GPU: bootstrap, two
+ * search+prune passes with symmetrisation, counter-based random draws from
+ * `seed`.  X host f32[n*dim]; adjacency out host u32[n*R]. */
+DG_API DgStatus dg_build_vamana(const float *X, uint64_t n, uint32_t dim, int32_t metric, uint32_t R,
+                         uint32_t build_beam, float alpha, uint64_t seed, uint32_t medoid,
+                         int32_t device, uint32_t *out_adjacency);
+/* ProductQuantizer::train (src/pq.rs:51-119): Lloyd iterations on the GPU
+ * from `seed`; codebooks out host f32[M*K*(dim/M)]. */
+DG_API DgStatus dg_pq_train(const float *X, uint64_t n, uint32_t dim, uint32_t M, uint32_t K,
+                     uint32_t iterations, uint64_t sample, uint64_t seed, int32_t device,
+                     float *out_codebooks);
+/* ProductQuantizer::encode (src/pq.rs:122-149) on the GPU. */
+DG_API DgStatus dg_pq_encode(const float *X, uint64_t n, uint32_t dim, uint32_t M, uint32_t K,
+                      const float *codebooks, int32_t device, uint8_t *out_codes);
+/* Exact k nearest neighbours (brute force, FP64 accumulation) on the GPU. */
+DG_API DgStatus dg_exact_knn(const float *X, uint64_t n, uint32_t dim, const float *Q, uint32_t nq,
+                      uint32_t k, int32_t metric, int32_t device, uint32_t *out_ids,
+                      float *out_dists);
+
+DG_API const char *dg_last_error(void);
+DG_API int32_t dg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

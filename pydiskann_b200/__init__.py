@@ -1,0 +1,597 @@
+"""pydiskann_b200 -- the pydiskann search surface on one NVIDIA B200.
+
+Class and method names, defaults and error types follow the reference Python
+binding (pydiskann 0.5.5, python/src/lib.rs):
+  * ``metric="l2"`` is squared L2, ``"cosine"`` is 1 - cos, ``"dot"`` is 1 - a.b;
+  * ``search`` returns ids, ``search_with_dists`` (id, distance) pairs,
+    ``search_batch`` one id list per query;
+  * bad metric / quantizer names raise ValueError, library errors
+    RuntimeError, out-of-range ids IndexError.
+Every search runs in libdgann.so (hand-written sm_100a kernels); there is no
+CPU path.  Index construction (Vamana graph, PQ codebooks, codes) also runs
+on the GPU.  ``path`` arguments are accepted for signature compatibility;
+on-disk persistence is not part of this package.
+
+Batched array entry points (``search_arrays``) take numpy arrays or CUDA
+tensors and return arrays, for callers that keep queries and results in HBM.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import PAD, check, lib, ptr
+
+__all__ = [
+    "DiskANN", "QuantizedDiskANN", "FilteredDiskANN", "Filter", "build_graph", "medoid",
+    "pq_train", "pq_encode", "exact_knn", "read_fvecs", "write_fvecs", "read_ivecs",
+]
+
+_METRICS = {"l2": _lib.L2SQ, "cosine": _lib.COSINE, "dot": _lib.DOT, "euclidean": _lib.L2}
+
+
+def _metric(m: str) -> int:
+    try:
+        return _METRICS[m]
+    except KeyError:
+        raise ValueError(f"unknown metric: {m}") from None
+
+
+def _f32(x, dim=None) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    if a.ndim == 1 and dim is not None:
+        a = a.reshape(1, -1)
+    return a
+
+
+# ---------------------------------------------------------------- builders
+def medoid(vectors, metric: str = "l2", device: int = 0) -> int:
+    """calculate_medoid (src/lib.rs:748-768) on the GPU."""
+    X = _f32(vectors)
+    out = C.c_uint32()
+    check(lib().dg_medoid(ptr(X), X.shape[0], X.shape[1], _metric(metric), device, C.byref(out)))
+    return out.value
+
+
+def build_graph(vectors, max_degree=64, build_beam_width=128, alpha=1.2, metric="l2", seed=0,
+                medoid_id=None, device=0):
+    """build_vamana_graph (src/lib.rs:774-917) on the GPU -> (adjacency u32[n,R], medoid)."""
+    X = _f32(vectors)
+    if X.ndim != 2 or X.shape[0] == 0:
+        raise RuntimeError("Index error: No vectors provided")
+    m = _metric(metric)
+    if medoid_id is None:
+        medoid_id = medoid(X, metric, device)
+    adj = np.empty((X.shape[0], max_degree), dtype=np.uint32)
+    check(lib().dg_build_vamana(ptr(X), X.shape[0], X.shape[1], m, max_degree, build_beam_width,
+                                float(alpha), seed, medoid_id, device, ptr(adj)))
+    return adj, medoid_id
+
+
+def pq_train(vectors, num_subspaces=8, num_centroids=256, kmeans_iterations=20,
+             training_sample_size=50_000, seed=0, device=0) -> np.ndarray:
+    """ProductQuantizer::train (src/pq.rs:51-119) -> codebooks f32[M, K, dim/M]."""
+    X = _f32(vectors)
+    M, K = num_subspaces, num_centroids
+    if X.shape[0] == 0:
+        raise RuntimeError("Index error: No vectors to train on")
+    cb = np.empty((M, K, X.shape[1] // max(M, 1)), dtype=np.float32)
+    check(lib().dg_pq_train(ptr(X), X.shape[0], X.shape[1], M, K, kmeans_iterations,
+                            training_sample_size, seed, device, ptr(cb)))
+    return cb
+
+
+def pq_encode(vectors, codebooks, device=0) -> np.ndarray:
+    """ProductQuantizer::encode (src/pq.rs:122-149) on the GPU -> u8[n, M]."""
+    X = _f32(vectors)
+    cb = _f32(codebooks)
+    M, K, _ = cb.shape
+    codes = np.empty((X.shape[0], M), dtype=np.uint8)
+    check(lib().dg_pq_encode(ptr(X), X.shape[0], X.shape[1], M, K, ptr(cb), device, ptr(codes)))
+    return codes
+
+
+def exact_knn(vectors, queries, k=10, metric="l2", device=0):
+    """Brute-force k nearest neighbours (FP64 accumulation) -> (ids, dists)."""
+    X = _f32(vectors)
+    Q = _f32(queries).reshape(-1, X.shape[1])
+    ids = np.empty((Q.shape[0], k), dtype=np.uint32)
+    ds = np.empty((Q.shape[0], k), dtype=np.float32)
+    check(lib().dg_exact_knn(ptr(X), X.shape[0], X.shape[1], ptr(Q), Q.shape[0], k, _metric(metric),
+                             device, ptr(ids), ptr(ds)))
+    return ids, ds
+
+
+# ------------------------------------------------------------------ filter
+class Filter:
+    """Filter predicate over a vector's label fields (src/filtered.rs:61-135).
+
+    Compiled to the postfix DgFilterOp program the kernels evaluate.
+    """
+
+    __slots__ = ("_kind", "_args")
+
+    def __init__(self, kind, args=()):
+        self._kind = kind
+        self._args = args
+
+    @staticmethod
+    def none():
+        return Filter("none")
+
+    @staticmethod
+    def eq(field: int, value: int):
+        return Filter("eq", (field, value))
+
+    @staticmethod
+    def in_(field: int, values: Iterable[int]):
+        return Filter("in", (field, frozenset(int(v) for v in values)))
+
+    @staticmethod
+    def lt(field: int, value: int):
+        return Filter("lt", (field, value))
+
+    @staticmethod
+    def gt(field: int, value: int):
+        return Filter("gt", (field, value))
+
+    @staticmethod
+    def range(field: int, min: int, max: int):  # noqa: A002 - reference argument names
+        return Filter("range", (field, min, max))
+
+    @staticmethod
+    def and_(filters: Sequence["Filter"]):
+        return Filter("and", tuple(filters))
+
+    @staticmethod
+    def or_(filters: Sequence["Filter"]):
+        return Filter("or", tuple(filters))
+
+    def is_none(self) -> bool:
+        return self._kind == "none"
+
+    def matches(self, labels: Sequence[int]) -> bool:
+        k, a = self._kind, self._args
+        if k == "none":
+            return True
+        if k in ("and", "or"):
+            res = (f.matches(labels) for f in a)
+            return all(res) if k == "and" else any(res)
+        field = a[0]
+        if field >= len(labels):
+            return False
+        v = labels[field]
+        if k == "eq":
+            return v == a[1]
+        if k == "in":
+            return v in a[1]
+        if k == "lt":
+            return v < a[1]
+        if k == "gt":
+            return v > a[1]
+        return a[1] <= v <= a[2]
+
+    def compile(self, ops: list, pool: list):
+        """Append this filter's postfix program to ops (FilterOp tuples)."""
+        k, a = self._kind, self._args
+        if k == "none":
+            return
+        if k in ("and", "or"):
+            for f in a:
+                if f.is_none():
+                    ops.append((_lib.F_TRUE, 0, 0, 0))
+                else:
+                    f.compile(ops, pool)
+            ops.append((_lib.F_AND if k == "and" else _lib.F_OR, len(a), 0, 0))
+            return
+        field = a[0]
+        if k == "eq":
+            ops.append((_lib.F_EQ, field, a[1], 0))
+        elif k == "lt":
+            ops.append((_lib.F_LT, field, a[1], 0))
+        elif k == "gt":
+            ops.append((_lib.F_GT, field, a[1], 0))
+        elif k == "range":
+            ops.append((_lib.F_RANGE, field, a[1], a[2]))
+        else:
+            vals = sorted(a[1])
+            ops.append((_lib.F_IN, field, len(pool), len(vals)))
+            pool.extend(vals)
+
+    def program(self):
+        ops, pool = [], []
+        self.compile(ops, pool)
+        return ops, pool
+
+    def __repr__(self):
+        return f"Filter.{self._kind}{self._args!r}"
+
+
+def _pack_programs(progs):
+    """[(ops, pool)] per query -> (FilterOp array, offsets u32[nq+1], pool u64)."""
+    all_ops, offs, pool = [], [0], []
+    for ops, p in progs:
+        base = len(pool)
+        for (op, field, a, b) in ops:
+            if op == _lib.F_IN:
+                a += base
+            all_ops.append((op, field, a, b))
+        pool.extend(p)
+        offs.append(len(all_ops))
+    arr = (_lib.FilterOp * max(len(all_ops), 1))()
+    for i, (op, field, a, b) in enumerate(all_ops):
+        arr[i] = _lib.FilterOp(op, field, a, b)
+    return arr, np.asarray(offs, dtype=np.uint32), np.asarray(pool if pool else [0], dtype=np.uint64), len(pool)
+
+
+# ------------------------------------------------------------------- index
+class _Index:
+    """A device-resident graph index (one libdgann DgIndex handle)."""
+
+    def __init__(self, vectors, adjacency, medoid_id, metric="l2", device=0, hbm_budget_bytes=0):
+        X = _f32(vectors)
+        adj = np.ascontiguousarray(adjacency, dtype=np.uint32)
+        if X.ndim != 2 or X.shape[0] == 0:
+            raise RuntimeError("Index error: No vectors provided")
+        self._X = X
+        self._metric_name = metric
+        self._metric = _metric(metric)
+        self.device = device
+        d = _lib.IndexDesc()
+        d.dim, d.max_degree, d.num_vectors = X.shape[1], adj.shape[1], X.shape[0]
+        d.medoid, d.metric = int(medoid_id), self._metric
+        d.vectors, d.adjacency = ptr(X), ptr(adj)
+        d.device, d.hbm_budget_bytes = device, hbm_budget_bytes
+        h = C.c_void_p()
+        check(lib().dg_index_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.adjacency = adj
+        self.medoid_id = int(medoid_id)
+        self._bf16 = False
+        self._quant = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dg_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- properties
+    @property
+    def num_vectors(self) -> int:
+        return self._X.shape[0]
+
+    @property
+    def dim(self) -> int:
+        return self._X.shape[1]
+
+    @property
+    def max_degree(self) -> int:
+        return self.adjacency.shape[1]
+
+    def get_vector(self, id: int):  # noqa: A002
+        if id < 0 or id >= self.num_vectors:
+            raise IndexError(id)
+        return self._X[id].tolist()
+
+    def enable_bf16(self):
+        if not self._bf16:
+            check(lib().dg_index_enable_bf16(self._h))
+            self._bf16 = True
+
+    # -- the batched entry point
+    def search_arrays(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32,
+                      rerank_size=0, filters=None, per_query_beam=None, out=None, stream=None,
+                      with_stats=False):
+        """Batched search over numpy arrays (host) or CUDA tensors (device).
+
+        Returns (ids u32[nq,k], dists f32[nq,k], counts u32[nq]) of the same
+        kind as `queries`; rows are padded with PAD / +inf past counts.
+        `filters` is one Filter for all queries or a list of one per query.
+        """
+        dev = hasattr(queries, "data_ptr") and getattr(queries, "is_cuda", False)
+        p = _lib.SearchParams()
+        p.k, p.beam_width, p.rerank_size, p.traversal = k, beam_width, rerank_size, traversal
+        keep = []
+        if dev:
+            import torch
+
+            Q = queries.contiguous()
+            nq = Q.shape[0]
+            if Q.dtype != torch.float32 or Q.shape[1] != self.dim:
+                raise ValueError(f"Query dim {Q.shape[1]} != index dim {self.dim}")
+            if out is None:
+                out = (torch.empty((nq, k), dtype=torch.int32, device=Q.device),
+                       torch.empty((nq, k), dtype=torch.float32, device=Q.device),
+                       torch.empty((nq,), dtype=torch.int32, device=Q.device))
+            stats = torch.empty((nq, 2), dtype=torch.int32, device=Q.device) if with_stats else None
+            p.flags = _lib.FLAG_DEVICE_PTRS
+            p.stream = stream if stream is not None else torch.cuda.current_stream(Q.device).cuda_stream
+        else:
+            Q = _f32(queries)
+            if Q.ndim == 1:
+                Q = Q.reshape(1, -1)
+            nq = Q.shape[0]
+            if Q.shape[1] != self.dim:
+                raise ValueError(f"Query dim {Q.shape[1]} != index dim {self.dim}")
+            if out is None:
+                out = (np.empty((nq, k), dtype=np.uint32), np.empty((nq, k), dtype=np.float32),
+                       np.empty((nq,), dtype=np.uint32))
+            stats = np.empty((nq, 2), dtype=np.uint32) if with_stats else None
+            if stream is not None:
+                p.stream = stream
+        if filters is not None:
+            if isinstance(filters, Filter):
+                if not filters.is_none():
+                    arr, offs, pool, plen = _pack_programs([filters.program()])
+                    keep += [arr, pool]
+                    p.filter_ops, p.filter_nops = C.cast(arr, C.c_void_p), int(offs[-1])
+                    p.filter_pool, p.filter_pool_len = ptr(pool), plen
+            else:
+                if len(filters) != nq:
+                    raise ValueError("one filter per query expected")
+                arr, offs, pool, plen = _pack_programs([f.program() for f in filters])
+                keep += [arr, offs, pool]
+                p.filter_ops, p.filter_offsets = C.cast(arr, C.c_void_p), ptr(offs)
+                p.filter_pool, p.filter_pool_len = ptr(pool), plen
+        if per_query_beam is not None:
+            pl = np.ascontiguousarray(per_query_beam, dtype=np.uint32)
+            keep.append(pl)
+            p.per_query_beam = ptr(pl)
+        check(lib().dg_search_batch(self._h, C.byref(p), ptr(Q), nq, ptr(out[0]), ptr(out[1]),
+                                    ptr(out[2]), ptr(stats)))
+        if with_stats:
+            return out[0], out[1], out[2], stats
+        return out
+
+    # -- reference-shaped helpers
+    def _rows(self, ids, dists, cnt):
+        return [[(int(ids[i, j]), float(dists[i, j])) for j in range(int(cnt[i]))] for i in range(len(cnt))]
+
+
+class DiskANN(_Index):
+    """DiskANN<D> (src/lib.rs) search surface: plain FP32 Vamana beam search.
+
+    ``traversal="bf16"`` reads a BF16 copy of the vectors during the beam
+    search (FP32 accumulation) and ``rerank_size`` then re-scores the best
+    candidates with the FP32 rows.
+    """
+
+    @staticmethod
+    def build(vectors, path=None, metric="l2", max_degree=64, build_beam_width=128, alpha=1.2,
+              seed=0, device=0):
+        X = _f32(vectors)
+        if X.ndim != 2 or X.shape[0] == 0:
+            raise RuntimeError("Index error: No vectors provided")
+        adj, med = build_graph(X, max_degree, build_beam_width, alpha, metric, seed, None, device)
+        return DiskANN(X, adj, med, metric, device)
+
+    @staticmethod
+    def from_graph(vectors, adjacency, medoid_id, metric="l2", device=0, hbm_budget_bytes=0):
+        return DiskANN(vectors, adjacency, medoid_id, metric, device, hbm_budget_bytes)
+
+    def search_with_dists(self, query, k=10, beam_width=128):
+        ids, ds, cnt = self.search_arrays(_f32(query).reshape(1, -1), k, beam_width)
+        return self._rows(ids, ds, cnt)[0]
+
+    def search(self, query, k=10, beam_width=128):
+        return [i for i, _ in self.search_with_dists(query, k, beam_width)]
+
+    def search_batch(self, queries, k=10, beam_width=128):
+        ids, ds, cnt = self.search_arrays(_f32(queries).reshape(-1, self.dim), k, beam_width)
+        return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
+
+
+class QuantizedDiskANN(_Index):
+    """QuantizedDiskANN<D> (src/quantized.rs): beam search on codes + exact rerank."""
+
+    def __init__(self, vectors, adjacency, medoid_id, metric="l2", device=0, rerank_size=0,
+                 hbm_budget_bytes=0):
+        super().__init__(vectors, adjacency, medoid_id, metric, device, hbm_budget_bytes)
+        self.rerank_size = rerank_size
+
+    @staticmethod
+    def build(vectors, path=None, quantizer="f16", metric="l2", rerank_size=0, pq_subspaces=8,
+              max_degree=64, build_beam_width=128, alpha=1.2, seed=0, device=0):
+        if quantizer not in ("f16", "int8", "pq", "rabitq"):
+            raise ValueError(f"unknown quantizer: {quantizer}")
+        _metric(metric)
+        X = _f32(vectors)
+        if X.ndim != 2 or X.shape[0] == 0:
+            raise RuntimeError("Index error: No vectors provided")
+        adj, med = build_graph(X, max_degree, build_beam_width, alpha, metric, seed, None, device)
+        q = QuantizedDiskANN(X, adj, med, metric, device, rerank_size)
+        if quantizer == "f16":
+            q.attach_f16()
+        elif quantizer == "int8":
+            q.attach_int8(*int8_params(X))
+        elif quantizer == "pq":
+            q.attach_pq(pq_train(X, pq_subspaces, 256, 20, 50_000, seed, device))
+        else:
+            cen, signs = rabitq_params(X, seed)
+            q.attach_rabitq(cen, signs)
+        return q
+
+    def attach_pq(self, codebooks, codes=None):
+        cb = _f32(codebooks)
+        M, K, ds = cb.shape
+        if ds * M != self.dim:
+            raise RuntimeError(f"Index error: Dimension {self.dim} not divisible by num_subspaces {M}")
+        c = None if codes is None else np.ascontiguousarray(codes, dtype=np.uint8)
+        check(lib().dg_index_attach_pq(self._h, M, K, ptr(cb), ptr(c)))
+        self._quant = ("pq", cb)
+
+    def attach_int8(self, scale, offset, codes=None):
+        c = None if codes is None else np.ascontiguousarray(codes, dtype=np.uint8)
+        check(lib().dg_index_attach_int8(self._h, float(scale), float(offset), ptr(c)))
+        self._quant = ("int8", (scale, offset))
+
+    def attach_f16(self):
+        check(lib().dg_index_attach_f16(self._h))
+        self._quant = ("f16", None)
+
+    def attach_rabitq(self, centroid, signs, codes=None):
+        cen, sg = _f32(centroid), _f32(signs)
+        padded = sg.size // 3
+        c = None if codes is None else np.ascontiguousarray(codes, dtype=np.uint8)
+        check(lib().dg_index_attach_rabitq(self._h, padded, ptr(cen), ptr(sg), ptr(c)))
+        self._quant = ("rabitq", (cen, sg))
+
+    def search_arrays(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_CODES,
+                      rerank_size=None, **kw):
+        rr = self.rerank_size if rerank_size is None else rerank_size
+        return super().search_arrays(queries, k, beam_width, traversal, rr, **kw)
+
+    def search_with_dists(self, query, k=10, beam_width=128):
+        ids, ds, cnt = self.search_arrays(_f32(query).reshape(1, -1), k, beam_width)
+        return self._rows(ids, ds, cnt)[0]
+
+    def search(self, query, k=10, beam_width=128):
+        return [i for i, _ in self.search_with_dists(query, k, beam_width)]
+
+    def search_batch(self, queries, k=10, beam_width=128):
+        ids, ds, cnt = self.search_arrays(_f32(queries).reshape(-1, self.dim), k, beam_width)
+        return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
+
+    def search_filtered_with_dists(self, query, k, beam_width, labels, filter):  # noqa: A002
+        """QuantizedDiskANN::search_filtered_with_dists (src/quantized.rs:350-398)."""
+        if not getattr(self, "_labels_attached", False):
+            self.attach_labels(labels)
+        ids, ds, cnt = self.search_arrays(_f32(query).reshape(1, -1), k, beam_width, filters=filter)
+        return self._rows(ids, ds, cnt)[0]
+
+    def attach_labels(self, labels):
+        lab = np.ascontiguousarray(labels, dtype=np.uint64)
+        if lab.shape[0] != self.num_vectors:
+            raise ValueError(f"Labels count {lab.shape[0]} != index vectors {self.num_vectors}")
+        check(lib().dg_index_attach_labels(self._h, lab.shape[1], ptr(lab)))
+        self._labels = lab
+        self._labels_attached = True
+
+
+class FilteredDiskANN(_Index):
+    """FilteredDiskANN<D> (src/filtered.rs): label-filtered beam search."""
+
+    def __init__(self, vectors, adjacency, medoid_id, labels, metric="l2", device=0,
+                 hbm_budget_bytes=0):
+        lab = np.ascontiguousarray(labels, dtype=np.uint64)
+        X = _f32(vectors)
+        if lab.ndim != 2 or lab.shape[0] != X.shape[0]:
+            raise RuntimeError(
+                f"Index error: vectors.len() ({X.shape[0]}) != labels.len() ({lab.shape[0] if lab.ndim else 0})")
+        super().__init__(X, adjacency, medoid_id, metric, device, hbm_budget_bytes)
+        check(lib().dg_index_attach_labels(self._h, lab.shape[1], ptr(lab)))
+        self._labels = lab
+
+    @staticmethod
+    def build(vectors, labels, path=None, metric="l2", max_degree=64, build_beam_width=128,
+              alpha=1.2, seed=0, device=0):
+        lab = [list(map(int, l)) for l in labels]
+        nf = len(lab[0]) if lab else 0
+        for i, l in enumerate(lab):
+            if len(l) != nf:
+                raise RuntimeError(f"Index error: Label {i} has {len(l)} fields, expected {nf}")
+        X = _f32(vectors)
+        if len(lab) != X.shape[0]:
+            raise RuntimeError(f"Index error: vectors.len() ({X.shape[0]}) != labels.len() ({len(lab)})")
+        adj, med = build_graph(X, max_degree, build_beam_width, alpha, metric, seed, None, device)
+        arr = np.asarray(lab, dtype=np.uint64).reshape(X.shape[0], nf)
+        return FilteredDiskANN(X, adj, med, arr, metric, device)
+
+    @property
+    def num_fields(self) -> int:
+        return self._labels.shape[1]
+
+    def get_labels(self, id: int):  # noqa: A002
+        if id < 0 or id >= self.num_vectors:
+            return None
+        return self._labels[id].astype(np.int64).tolist()
+
+    def count_matching(self, filter: Filter) -> int:  # noqa: A002
+        ops, pool = filter.program()
+        arr, offs, pl, plen = _pack_programs([(ops, pool)])
+        out = C.c_uint64()
+        check(lib().dg_count_matching(self._h, C.cast(arr, C.c_void_p), len(ops), ptr(pl), plen,
+                                      C.byref(out)))
+        return out.value
+
+    def search(self, query, k=10, beam_width=128):
+        ids, ds, cnt = self.search_arrays(_f32(query).reshape(1, -1), k, beam_width)
+        return ids[0, : cnt[0]].astype(np.int64).tolist()
+
+    def search_filtered_with_dists(self, query, filter, k=10, beam_width=128):  # noqa: A002
+        ids, ds, cnt = self.search_arrays(_f32(query).reshape(1, -1), k, beam_width, filters=filter)
+        return self._rows(ids, ds, cnt)[0]
+
+    def search_filtered(self, query, filter, k=10, beam_width=128):  # noqa: A002
+        return [i for i, _ in self.search_filtered_with_dists(query, filter, k, beam_width)]
+
+    def search_filtered_batch(self, queries, filter, k=10, beam_width=128):  # noqa: A002
+        ids, ds, cnt = self.search_arrays(_f32(queries).reshape(-1, self.dim), k, beam_width,
+                                          filters=filter)
+        return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
+
+
+# --------------------------------------------------------- quantizer params
+def int8_params(vectors):
+    """Int8Quantizer::train (src/sq.rs:128-157): one global (scale, offset)."""
+    X = _f32(vectors)
+    lo, hi = np.float32(X.min()), np.float32(X.max())
+    rng = np.float32(hi - lo)
+    scale = np.float32(1.0) if abs(rng) < np.finfo(np.float32).eps else np.float32(rng / np.float32(255.0))
+    return float(scale), float(lo)
+
+
+def rabitq_padded(dim: int) -> int:
+    """src/rabitq.rs:83: next_power_of_two(max(dim, 64))."""
+    return 1 << max(6, math.ceil(math.log2(max(dim, 1))))
+
+
+def rabitq_params(vectors, seed=0):
+    """RaBitQ::train (src/rabitq.rs:78-107): centroid and 3 rounds of +-1/sqrt(padded) signs.
+
+    The reference draws the signs from StdRng(0x7ab17); callers holding a
+    trained reference quantizer pass its signs to attach_rabitq instead.
+    """
+    X = _f32(vectors)
+    cen = (X.astype(np.float64).sum(axis=0) / X.shape[0]).astype(np.float32)
+    P = rabitq_padded(X.shape[1])
+    scale = np.float32(1.0) / np.float32(math.sqrt(P))
+    bits = np.random.default_rng([seed, 0x7AB17]).integers(0, 2, size=3 * P)
+    signs = np.where(bits == 1, scale, -scale).astype(np.float32)
+    return cen, signs
+
+
+# ----------------------------------------------------------------- formats
+def read_fvecs(path):
+    """fvecs reader (src/formats.rs:7-47)."""
+    raw = np.fromfile(path, dtype=np.int32)
+    if raw.size == 0:
+        return []
+    d = raw[0]
+    return raw.reshape(-1, d + 1)[:, 1:].view(np.float32).tolist()
+
+
+def read_ivecs(path):
+    raw = np.fromfile(path, dtype=np.int32)
+    if raw.size == 0:
+        return []
+    d = raw[0]
+    return raw.reshape(-1, d + 1)[:, 1:].tolist()
+
+
+def write_fvecs(path, vectors):
+    X = _f32(vectors)
+    out = np.empty((X.shape[0], X.shape[1] + 1), dtype=np.int32)
+    out[:, 0] = X.shape[1]
+    out[:, 1:] = X.view(np.int32)
+    out.tofile(path)

@@ -1,0 +1,117 @@
+"""ctypes binding of libdgann.so (include/dgann.h).
+
+The library is the only compute path: importing this module without a built
+libdgann.so raises, and there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdgann.so")
+
+DG_OK, DG_EINVAL, DG_ENOMEM, DG_ETIMEOUT, DG_EDEVICE, DG_ENOTSUP = range(6)
+L2SQ, L2, COSINE, DOT = 0, 1, 2, 3
+TRAVERSE_F32, TRAVERSE_BF16, TRAVERSE_CODES = 0, 1, 2
+Q_NONE, Q_PQ, Q_INT8, Q_RABITQ, Q_F16 = 0, 1, 2, 3, 4
+F_TRUE, F_EQ, F_IN, F_LT, F_GT, F_RANGE, F_AND, F_OR = range(8)
+FLAG_DEVICE_PTRS = 1
+PAD = 0xFFFFFFFF
+PAD64 = 0xFFFFFFFFFFFFFFFF
+
+
+class DgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(msg)
+        self.status = status
+
+
+class FilterOp(C.Structure):
+    _fields_ = [("op", C.c_uint32), ("field", C.c_uint32), ("a", C.c_uint64), ("b", C.c_uint64)]
+
+
+class IndexDesc(C.Structure):
+    _fields_ = [
+        ("dim", C.c_uint32), ("max_degree", C.c_uint32), ("num_vectors", C.c_uint64),
+        ("medoid", C.c_uint32), ("metric", C.c_int32), ("vectors", C.c_void_p),
+        ("adjacency", C.c_void_p), ("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
+    ]
+
+
+class SearchParams(C.Structure):
+    _fields_ = [
+        ("k", C.c_uint32), ("beam_width", C.c_uint32), ("rerank_size", C.c_uint32),
+        ("traversal", C.c_int32), ("filter_ops", C.c_void_p), ("filter_nops", C.c_uint32),
+        ("filter_offsets", C.c_void_p), ("filter_pool", C.c_void_p),
+        ("filter_pool_len", C.c_uint32), ("per_query_beam", C.c_void_p), ("flags", C.c_uint32),
+        ("stream", C.c_void_p),
+    ]
+
+
+# Every symbol include/dgann.h declares, with its ctypes signature.
+def _signatures():
+    vp, u32, u64, i32, f32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float
+    st = C.c_int
+    return {
+        "dg_index_create": (st, [vp, vp]),
+        "dg_index_destroy": (st, [vp]),
+        "dg_index_enable_bf16": (st, [vp]),
+        "dg_index_attach_pq": (st, [vp, u32, u32, vp, vp]),
+        "dg_index_attach_int8": (st, [vp, f32, f32, vp]),
+        "dg_index_attach_f16": (st, [vp]),
+        "dg_index_attach_rabitq": (st, [vp, u32, vp, vp, vp]),
+        "dg_index_attach_labels": (st, [vp, u32, vp]),
+        "dg_search_batch": (st, [vp, vp, vp, u32, vp, vp, vp, vp]),
+        "dg_count_matching": (st, [vp, vp, u32, vp, u32, vp]),
+        "dg_medoid": (st, [vp, u64, u32, i32, i32, vp]),
+        "dg_build_vamana": (st, [vp, u64, u32, i32, u32, u32, f32, u64, u32, i32, vp]),
+        "dg_pq_train": (st, [vp, u64, u32, u32, u32, u32, u64, u64, i32, vp]),
+        "dg_pq_encode": (st, [vp, u64, u32, u32, u32, vp, i32, vp]),
+        "dg_exact_knn": (st, [vp, u64, u32, vp, u32, u32, i32, i32, vp, vp]),
+        "dg_last_error": (C.c_char_p, []),
+        "dg_version": (i32, []),
+    }
+
+
+EXPORTED = tuple(_signatures().keys())
+
+_lib = None
+
+
+def lib():
+    """Load libdgann.so; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"libdgann.so not found at {LIB_PATH}; build it with `python -m pydiskann_b200.build`"
+            )
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _signatures().items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != DG_OK:
+        msg = lib().dg_last_error().decode(errors="replace")
+        if status == DG_EINVAL:
+            raise ValueError(msg)
+        raise DgError(status, msg)
+
+
+def ptr(a):
+    """Address of a numpy array, torch tensor, or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(C.c_void_p)
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    raise TypeError(type(a))

@@ -1,0 +1,512 @@
+// dg_abi.cu -- the extern "C" surface of libdgann (declared in include/dgann.h).
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "dg_index.h"
+#include "dg_launch.cuh"
+
+namespace dg {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+DgStatus fail(DgStatus st, const std::string &msg) {
+  g_err = msg;
+  return st;
+}
+DgStatus cuda_fail(cudaError_t e, const char *what) {
+  g_err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? DG_ENOMEM : DG_EDEVICE;
+}
+
+// Rows are padded to a multiple of 32 dimensions: every 16-byte chunk
+// geometry of the gather kernels then divides the row exactly.
+uint32_t dpad_of(uint32_t d) { return (d + 31u) & ~31u; }
+
+DgStatus dev_alloc(DgIndex *idx, void **p, size_t bytes) {
+  if (idx->hbm_budget && idx->hbm_used + bytes > idx->hbm_budget)
+    return fail(DG_ENOMEM, "index exceeds its HBM budget (" + std::to_string(idx->hbm_budget) + " bytes)");
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  idx->hbm_used += bytes;
+  idx->allocations.push_back(q);
+  *p = q;
+  return DG_OK;
+}
+
+DgStatus buf_reserve(DgIndex::Buf &b, size_t bytes) {
+  if (bytes <= b.cap) return DG_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  size_t want = std::max<size_t>(bytes, 256);
+  DG_CUDA(cudaMalloc(&b.p, want));
+  b.cap = want;
+  return DG_OK;
+}
+
+DgStatus to_device(DgIndex *idx, void **dst, const void *src, size_t bytes) {
+  DgStatus s = dev_alloc(idx, dst, bytes);
+  if (s != DG_OK) return s;
+  DG_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, idx->stream));
+  return DG_OK;
+}
+
+DgStatus upload_rows_f32(const float *host, uint64_t n, uint32_t d, uint32_t dpad, float *dev,
+                         cudaStream_t st) {
+  if (d == dpad) {
+    DG_CUDA(cudaMemcpyAsync(dev, host, n * d * sizeof(float), cudaMemcpyHostToDevice, st));
+    return DG_OK;
+  }
+  DG_CUDA(cudaMemsetAsync(dev, 0, n * dpad * sizeof(float), st));
+  DG_CUDA(cudaMemcpy2DAsync(dev, dpad * sizeof(float), host, d * sizeof(float), d * sizeof(float), n,
+                            cudaMemcpyHostToDevice, st));
+  return DG_OK;
+}
+
+static int met_kind(int32_t metric) {
+  return metric == DG_DOT ? MET_DOT : metric == DG_COSINE ? MET_COS : MET_L2;
+}
+
+// Lanes per row for a row of `chunks` 16-byte chunks.
+static int lanes_per_row(uint32_t chunks) {
+  if (chunks % 8 == 0) return 8;
+  if (chunks % 4 == 0) return 4;
+  return 2;
+}
+
+}  // namespace dg
+
+using namespace dg;
+
+extern "C" {
+
+const char *dg_last_error(void) { return g_err.c_str(); }
+int32_t dg_version(void) { return DGANN_VERSION; }
+
+DgStatus dg_index_create(const DgIndexDesc *desc, DgIndex **out) {
+  if (!desc || !out) return fail(DG_EINVAL, "null argument");
+  *out = nullptr;
+  if (desc->dim == 0 || desc->num_vectors == 0)
+    return fail(DG_EINVAL, "index needs at least one vector of dimension >= 1");
+  if (desc->num_vectors >= (1ull << 31)) return fail(DG_EINVAL, "num_vectors must be < 2^31");
+  if (desc->max_degree == 0 || desc->max_degree > (uint32_t)kStageCap)
+    return fail(DG_EINVAL, "max_degree must be in [1, 256]");
+  if (desc->medoid >= desc->num_vectors) return fail(DG_EINVAL, "medoid out of range");
+  if (desc->metric < DG_L2SQ || desc->metric > DG_DOT) return fail(DG_EINVAL, "unknown metric");
+  if (!desc->vectors || !desc->adjacency) return fail(DG_EINVAL, "vectors and adjacency are required");
+  DG_CUDA(cudaSetDevice(desc->device));
+  DgIndex *idx = new (std::nothrow) DgIndex();
+  if (!idx) return fail(DG_ENOMEM, "host allocation failed");
+  idx->device = desc->device;
+  idx->n = desc->num_vectors;
+  idx->d = desc->dim;
+  idx->dpad = dpad_of(desc->dim);
+  idx->R = desc->max_degree;
+  idx->medoid = desc->medoid;
+  idx->metric = desc->metric;
+  idx->hbm_budget = desc->hbm_budget_bytes;
+  DgStatus s = DG_OK;
+  auto bail = [&](DgStatus st) {
+    dg_index_destroy(idx);
+    return st;
+  };
+  if (cudaStreamCreateWithFlags(&idx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(DG_EDEVICE, "stream creation failed"));
+  if ((s = dev_alloc(idx, (void **)&idx->vec, idx->n * idx->dpad * 4)) != DG_OK) return bail(s);
+  if ((s = upload_rows_f32(desc->vectors, idx->n, idx->d, idx->dpad, idx->vec, idx->stream)) != DG_OK)
+    return bail(s);
+  if ((s = to_device(idx, (void **)&idx->adj, desc->adjacency, idx->n * idx->R * 4)) != DG_OK) return bail(s);
+  for (auto &sl : idx->slots) {
+    if (cudaMalloc(&sl.counter, 4) != cudaSuccess) return bail(fail(DG_ENOMEM, "counter allocation"));
+    if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess)
+      return bail(fail(DG_EDEVICE, "event creation"));
+  }
+  if (cudaStreamSynchronize(idx->stream) != cudaSuccess) return bail(fail(DG_EDEVICE, "upload failed"));
+  *out = idx;
+  return DG_OK;
+}
+
+DgStatus dg_index_destroy(DgIndex *idx) {
+  if (!idx) return DG_OK;
+  cudaSetDevice(idx->device);
+  if (idx->stream) cudaStreamSynchronize(idx->stream);
+  for (auto &sl : idx->slots) {
+    if (sl.done) {
+      cudaEventSynchronize(sl.done);
+      cudaEventDestroy(sl.done);
+    }
+    for (DgIndex::Buf *b : {&sl.q, &sl.ids, &sl.dists, &sl.cnt, &sl.stats, &sl.fops, &sl.foffs,
+                            &sl.fpool, &sl.perl})
+      if (b->p) cudaFree(b->p);
+    if (sl.counter) cudaFree(sl.counter);
+  }
+  for (void *p : idx->allocations) cudaFree(p);
+  if (idx->stream) cudaStreamDestroy(idx->stream);
+  delete idx;
+  return DG_OK;
+}
+
+DgStatus dg_index_enable_bf16(DgIndex *idx) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  if (idx->bf16) return DG_OK;
+  DgStatus s = dev_alloc(idx, (void **)&idx->bf16, idx->n * idx->dpad * 2);
+  if (s != DG_OK) return s;
+  if ((s = encode_bf16_device(idx->vec, idx->n, idx->dpad, idx->bf16, idx->stream)) != DG_OK) return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+static DgStatus attach_codes_common(DgIndex *idx, int quant, uint32_t code_size) {
+  if (idx->quant != DG_Q_NONE) return fail(DG_EINVAL, "a quantizer is already attached");
+  idx->quant = quant;
+  idx->code_size = code_size;
+  idx->code_stride = (code_size + 15u) & ~15u;
+  DgStatus s = dev_alloc(idx, (void **)&idx->codes, idx->n * idx->code_stride);
+  if (s != DG_OK) return s;
+  DG_CUDA(cudaMemsetAsync(idx->codes, 0, idx->n * idx->code_stride, idx->stream));
+  return DG_OK;
+}
+
+static DgStatus upload_code_rows(DgIndex *idx, const uint8_t *codes) {
+  DG_CUDA(cudaMemcpy2DAsync(idx->codes, idx->code_stride, codes, idx->code_size, idx->code_size,
+                            idx->n, cudaMemcpyHostToDevice, idx->stream));
+  return DG_OK;
+}
+
+DgStatus dg_index_attach_pq(DgIndex *idx, uint32_t M, uint32_t K, const float *codebooks,
+                            const uint8_t *codes) {
+  if (!idx || !codebooks) return fail(DG_EINVAL, "null argument");
+  if (M == 0 || idx->d % M != 0)
+    return fail(DG_EINVAL, "Dimension " + std::to_string(idx->d) + " not divisible by num_subspaces " +
+                               std::to_string(M));
+  if (K == 0 || K > 256) return fail(DG_EINVAL, "num_centroids must be in [1, 256] (codes are u8)");
+  if (codes && K < 256) {  // every code indexes a K-entry table row
+    for (uint64_t i = 0; i < idx->n * M; ++i)
+      if (codes[i] >= K) return fail(DG_EINVAL, "PQ code " + std::to_string(codes[i]) + " >= num_centroids");
+  }
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  DgStatus s = attach_codes_common(idx, DG_Q_PQ, M);
+  if (s != DG_OK) return s;
+  idx->pq_M = M;
+  idx->pq_K = K;
+  const size_t cbb = (size_t)M * K * (idx->d / M) * 4;
+  if ((s = to_device(idx, (void **)&idx->pq_cb, codebooks, cbb)) != DG_OK) return s;
+  if (codes) s = upload_code_rows(idx, codes);
+  else s = encode_pq_device(idx->vec, idx->n, idx->d, idx->dpad, M, K, idx->pq_cb, idx->codes,
+                            idx->code_stride, idx->stream);
+  if (s != DG_OK) return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+DgStatus dg_index_attach_int8(DgIndex *idx, float scale, float offset, const uint8_t *codes) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  if (!(scale > 0.0f)) return fail(DG_EINVAL, "int8 scale must be positive");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  DgStatus s = attach_codes_common(idx, DG_Q_INT8, idx->dpad);
+  if (s != DG_OK) return s;
+  idx->code_size = idx->d;
+  idx->i8_scale = scale;
+  idx->i8_offset = offset;
+  if (codes) s = upload_code_rows(idx, codes);
+  else s = encode_int8_device(idx->vec, idx->n, idx->d, idx->dpad, scale, offset, idx->codes,
+                              idx->code_stride, idx->stream);
+  if (s != DG_OK) return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+DgStatus dg_index_attach_f16(DgIndex *idx) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  DgStatus s = attach_codes_common(idx, DG_Q_F16, idx->dpad * 2);
+  if (s != DG_OK) return s;
+  idx->code_size = idx->d * 2;
+  if ((s = encode_f16_device(idx->vec, idx->n, idx->dpad, (uint16_t *)idx->codes, idx->stream)) != DG_OK)
+    return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+DgStatus dg_index_attach_rabitq(DgIndex *idx, uint32_t padded, const float *centroid,
+                                const float *signs, const uint8_t *codes) {
+  if (!idx || !centroid || !signs) return fail(DG_EINVAL, "null argument");
+  uint32_t want = 1;
+  while (want < std::max(idx->d, 64u)) want <<= 1;
+  if (padded != want) return fail(DG_EINVAL, "RaBitQ padded dim must be next_pow2(max(dim, 64))");
+  if (padded > 4096) return fail(DG_ENOTSUP, "RaBitQ padded dim above 4096");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  DgStatus s = attach_codes_common(idx, DG_Q_RABITQ, padded / 8 + 8);
+  if (s != DG_OK) return s;
+  idx->rq_padded = padded;
+  if ((s = to_device(idx, (void **)&idx->rq_centroid, centroid, idx->d * 4)) != DG_OK) return s;
+  if ((s = to_device(idx, (void **)&idx->rq_signs, signs, 3ull * padded * 4)) != DG_OK) return s;
+  if (codes) s = upload_code_rows(idx, codes);
+  else s = encode_rabitq_device(idx->vec, idx->n, idx->d, idx->dpad, padded, idx->rq_centroid,
+                                idx->rq_signs, idx->codes, idx->code_stride, idx->stream);
+  if (s != DG_OK) return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+DgStatus dg_index_attach_labels(DgIndex *idx, uint32_t num_fields, const uint64_t *labels) {
+  if (!idx || (!labels && num_fields)) return fail(DG_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  if (idx->labels) return fail(DG_EINVAL, "labels are already attached");
+  idx->nf = num_fields;
+  DgStatus s = to_device(idx, (void **)&idx->labels, labels ? (const void *)labels : (const void *)"",
+                         std::max<size_t>(idx->n * num_fields * 8, 8));
+  if (s != DG_OK) return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+// Stack depth a postfix program needs; -1 if it is malformed.
+static int program_depth(const DgFilterOp *ops, uint32_t n, uint64_t pool_len) {
+  int sp = 0, mx = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const DgFilterOp &o = ops[i];
+    if (o.op > DG_F_OR) return -1;
+    if (o.op == DG_F_AND || o.op == DG_F_OR) {
+      if ((int)o.field > sp) return -1;
+      sp -= (int)o.field;
+    } else if (o.op == DG_F_IN && (o.a > pool_len || o.b > pool_len - o.a)) {
+      return -1;
+    }
+    ++sp;
+    mx = std::max(mx, sp);
+  }
+  if (n > 0 && sp != 1) return -1;
+  return mx;
+}
+
+static DgStatus stage_copy(DgIndex::Buf &b, const void *src, size_t bytes, cudaStream_t st) {
+  DgStatus s = buf_reserve(b, bytes);
+  if (s != DG_OK) return s;
+  if (bytes) DG_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st));
+  return DG_OK;
+}
+
+DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *queries, uint32_t nq,
+                         uint32_t *out_ids, float *out_dists, uint32_t *out_counts,
+                         uint32_t *out_stats) {
+  if (!idx || !p) return fail(DG_EINVAL, "null argument");
+  if (nq == 0) return DG_OK;
+  if (!queries || !out_ids || !out_dists || !out_counts) return fail(DG_EINVAL, "null buffer");
+  if (p->k == 0) return fail(DG_EINVAL, "k must be >= 1");
+  const bool devptr = (p->flags & DG_FLAG_DEVICE_PTRS) != 0;
+  // traversal kind
+  int trav;
+  switch (p->traversal) {
+    case DG_TRAVERSE_F32: trav = TRAV_F32; break;
+    case DG_TRAVERSE_BF16:
+      if (!idx->bf16) return fail(DG_EINVAL, "BF16 traversal needs dg_index_enable_bf16");
+      trav = TRAV_BF16;
+      break;
+    case DG_TRAVERSE_CODES:
+      switch (idx->quant) {
+        case DG_Q_PQ: trav = TRAV_PQ; break;
+        case DG_Q_INT8: trav = TRAV_INT8; break;
+        case DG_Q_RABITQ: trav = TRAV_RABITQ; break;
+        case DG_Q_F16: trav = TRAV_F16; break;
+        default: return fail(DG_EINVAL, "code traversal needs an attached quantizer");
+      }
+      break;
+    default: return fail(DG_EINVAL, "unknown traversal");
+  }
+  // per-query beams and filters
+  uint32_t maxL = p->beam_width;
+  if (p->per_query_beam) {
+    maxL = 0;
+    for (uint32_t i = 0; i < nq; ++i) maxL = std::max(maxL, p->per_query_beam[i]);
+    for (uint32_t i = 0; i < nq; ++i)
+      if (p->per_query_beam[i] == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
+  }
+  if (maxL == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
+  const uint32_t total_ops = p->filter_offsets ? p->filter_offsets[nq] : p->filter_nops;
+  bool any_filter = false;
+  if (p->filter_offsets) {
+    if (p->filter_offsets[0] != 0) return fail(DG_EINVAL, "filter_offsets[0] must be 0");
+    for (uint32_t i = 0; i < nq; ++i) {
+      if (p->filter_offsets[i + 1] < p->filter_offsets[i]) return fail(DG_EINVAL, "filter_offsets not monotone");
+      const uint32_t c = p->filter_offsets[i + 1] - p->filter_offsets[i];
+      if (c) {
+        any_filter = true;
+        int dep = program_depth(p->filter_ops + p->filter_offsets[i], c, p->filter_pool_len);
+        if (dep < 0 || dep > kFilterStack) return fail(DG_EINVAL, "malformed filter program");
+      }
+    }
+  } else if (p->filter_nops) {
+    any_filter = true;
+    int dep = program_depth(p->filter_ops, p->filter_nops, p->filter_pool_len);
+    if (dep < 0 || dep > kFilterStack) return fail(DG_EINVAL, "malformed filter program");
+  }
+  if (any_filter && !p->filter_ops) return fail(DG_EINVAL, "filter ops missing");
+  if (any_filter && !idx->labels) return fail(DG_EINVAL, "filtered search needs attached labels");
+  const bool reranked = trav != TRAV_F32 && p->rerank_size > 0;
+  const uint32_t search_k = reranked ? std::max(p->rerank_size, p->k) : p->k;
+  uint64_t need = maxL;
+  if (any_filter) need = std::max<uint64_t>({(uint64_t)maxL * 4, (uint64_t)p->k * 10, search_k});
+  int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
+  if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
+  if (reranked && !any_filter && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
+  uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
+  if (const char *e = std::getenv("DG_HBITS")) hbits = (uint32_t)std::max(6, std::min(14, atoi(e)));
+
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  cudaStream_t st = p->stream ? (cudaStream_t)p->stream : idx->stream;
+  DgIndex::Slot &sl = idx->slots[idx->next_slot];
+  idx->next_slot = (idx->next_slot + 1) % DgIndex::kSlots;
+  if (sl.pending) {
+    DG_CUDA(cudaEventSynchronize(sl.done));
+    sl.pending = false;
+  }
+  DgStatus s;
+  SearchArgs a{};
+  a.n = idx->n;
+  a.d = idx->d;
+  a.dpad = idx->dpad;
+  a.R = idx->R;
+  a.medoid = idx->medoid;
+  a.metric = idx->metric;
+  a.vec_f32 = idx->vec;
+  a.vec_bf16 = idx->bf16;
+  a.adj = idx->adj;
+  a.codes = idx->codes;
+  a.code_stride = idx->code_stride;
+  a.pq_M = idx->pq_M;
+  a.pq_K = idx->pq_K;
+  a.pq_ds = idx->pq_M ? idx->d / idx->pq_M : 0;
+  a.pq_cb = idx->pq_cb;
+  a.i8_scale = idx->i8_scale;
+  a.i8_offset = idx->i8_offset;
+  a.rq_padded = idx->rq_padded;
+  a.rq_centroid = idx->rq_centroid;
+  a.rq_signs = idx->rq_signs;
+  a.labels = idx->labels;
+  a.nf = idx->nf;
+  a.nq = nq;
+  a.k = p->k;
+  a.L = p->beam_width;
+  a.rerank = p->rerank_size;
+  a.hbits = hbits;
+  if (any_filter) {
+    if ((s = stage_copy(sl.fops, p->filter_ops, (size_t)total_ops * sizeof(DgFilterOp), st)) != DG_OK) return s;
+    a.fops = (const DgFilterOp *)sl.fops.p;
+    a.fnops = p->filter_offsets ? 0 : p->filter_nops;
+    if (p->filter_offsets) {
+      if ((s = stage_copy(sl.foffs, p->filter_offsets, (size_t)(nq + 1) * 4, st)) != DG_OK) return s;
+      a.foffs = (const uint32_t *)sl.foffs.p;
+    }
+    if ((s = stage_copy(sl.fpool, p->filter_pool, (size_t)p->filter_pool_len * 8, st)) != DG_OK) return s;
+    a.fpool = (const uint64_t *)sl.fpool.p;
+  }
+  if (p->per_query_beam) {
+    if ((s = stage_copy(sl.perl, p->per_query_beam, (size_t)nq * 4, st)) != DG_OK) return s;
+    a.perL = (const uint32_t *)sl.perl.p;
+  }
+  const size_t kq = (size_t)nq * p->k;
+  if (devptr) {
+    a.Q = queries;
+    a.out_ids = out_ids;
+    a.out_d = out_dists;
+    a.out_cnt = out_counts;
+    a.out_stats = out_stats;
+  } else {
+    if ((s = stage_copy(sl.q, queries, (size_t)nq * idx->d * 4, st)) != DG_OK) return s;
+    if ((s = buf_reserve(sl.ids, kq * 4)) != DG_OK) return s;
+    if ((s = buf_reserve(sl.dists, kq * 4)) != DG_OK) return s;
+    if ((s = buf_reserve(sl.cnt, (size_t)nq * 4)) != DG_OK) return s;
+    a.Q = (const float *)sl.q.p;
+    a.out_ids = (uint32_t *)sl.ids.p;
+    a.out_d = (float *)sl.dists.p;
+    a.out_cnt = (uint32_t *)sl.cnt.p;
+    if (out_stats) {
+      if ((s = buf_reserve(sl.stats, (size_t)nq * 8)) != DG_OK) return s;
+      a.out_stats = (uint32_t *)sl.stats.p;
+    }
+  }
+  a.counter = sl.counter;
+  DG_CUDA(cudaMemsetAsync(sl.counter, 0, 4, st));
+
+  const int met = met_kind(idx->metric);
+  int lpr = 1;
+  if (trav == TRAV_F32) lpr = 8;
+  else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
+  else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
+  const WarpLayout Ly = warp_layout(trav, lcap, any_filter, hbits, idx->dpad, idx->pq_M, idx->pq_K,
+                                    idx->rq_padded);
+  LaunchInfo info;
+  switch (trav) {
+    case TRAV_F32: s = launch_search_f32(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
+    case TRAV_BF16: s = launch_search_bf16(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
+    case TRAV_F16: s = launch_search_f16(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
+    case TRAV_INT8: s = launch_search_int8(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
+    case TRAV_PQ: s = launch_search_pq(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
+    default: s = launch_search_rabitq(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
+  }
+  if (s != DG_OK) return s;
+  if (!devptr) {
+    DG_CUDA(cudaMemcpyAsync(out_ids, a.out_ids, kq * 4, cudaMemcpyDeviceToHost, st));
+    DG_CUDA(cudaMemcpyAsync(out_dists, a.out_d, kq * 4, cudaMemcpyDeviceToHost, st));
+    DG_CUDA(cudaMemcpyAsync(out_counts, a.out_cnt, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
+    if (out_stats) DG_CUDA(cudaMemcpyAsync(out_stats, a.out_stats, (size_t)nq * 8, cudaMemcpyDeviceToHost, st));
+  }
+  DG_CUDA(cudaEventRecord(sl.done, st));
+  sl.pending = true;
+  if (!devptr) {
+    DG_CUDA(cudaEventSynchronize(sl.done));
+    sl.pending = false;
+  }
+  return DG_OK;
+}
+
+DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
+                           const uint64_t *pool, uint32_t pool_len, uint64_t *out_count) {
+  if (!idx || !out_count) return fail(DG_EINVAL, "null argument");
+  if (nops == 0) {
+    *out_count = idx->n;
+    return DG_OK;
+  }
+  if (!idx->labels) return fail(DG_EINVAL, "count_matching needs attached labels");
+  int dep = program_depth(ops, nops, pool_len);
+  if (dep < 0 || dep > kFilterStack) return fail(DG_EINVAL, "malformed filter program");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  DgIndex::Slot &sl = idx->slots[idx->next_slot];
+  idx->next_slot = (idx->next_slot + 1) % DgIndex::kSlots;
+  if (sl.pending) {
+    DG_CUDA(cudaEventSynchronize(sl.done));
+    sl.pending = false;
+  }
+  DgStatus s;
+  if ((s = stage_copy(sl.fops, ops, (size_t)nops * sizeof(DgFilterOp), idx->stream)) != DG_OK) return s;
+  if ((s = stage_copy(sl.fpool, pool, (size_t)pool_len * 8, idx->stream)) != DG_OK) return s;
+  if ((s = buf_reserve(sl.cnt, 8)) != DG_OK) return s;
+  DG_CUDA(cudaMemsetAsync(sl.cnt.p, 0, 8, idx->stream));
+  if ((s = count_matching_device(idx->labels, idx->n, idx->nf, (const DgFilterOp *)sl.fops.p, nops,
+                                 (const uint64_t *)sl.fpool.p, (unsigned long long *)sl.cnt.p,
+                                 idx->stream)) != DG_OK)
+    return s;
+  unsigned long long c = 0;
+  DG_CUDA(cudaMemcpyAsync(&c, sl.cnt.p, 8, cudaMemcpyDeviceToHost, idx->stream));
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  *out_count = c;
+  return DG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+// dg_index.h -- the device-resident index behind a DgIndex handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <vector>
+
+#include "dg_common.cuh"
+
+struct DgIndex {
+  int device = 0;
+  uint64_t n = 0;
+  uint32_t d = 0, dpad = 0, R = 0, medoid = 0;
+  int32_t metric = DG_L2SQ;
+  // HBM layout: every row starts on a 128-byte boundary when dpad*4 >= 128.
+  float *vec = nullptr;       // [n][dpad] f32, zero padded
+  uint16_t *bf16 = nullptr;   // [n][dpad] bf16 copy (optional)
+  uint32_t *adj = nullptr;    // [n][R]
+  int32_t quant = DG_Q_NONE;
+  uint8_t *codes = nullptr;   // [n][code_stride]
+  uint32_t code_size = 0, code_stride = 0;
+  uint32_t pq_M = 0, pq_K = 0;
+  float *pq_cb = nullptr;     // [M][K][d/M]
+  float i8_scale = 1.0f, i8_offset = 0.0f;
+  uint32_t rq_padded = 0;
+  float *rq_centroid = nullptr, *rq_signs = nullptr;
+  uint64_t *labels = nullptr; // [n][nf]
+  uint32_t nf = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t hbm_budget = 0, hbm_used = 0;
+  std::mutex mu;
+  // Per-call resources.  A call takes the next slot of a ring; a slot is reused
+  // only after the event recorded at the end of its previous call completed,
+  // so calls on different streams may overlap on the device.
+  struct Buf {
+    void *p = nullptr;
+    size_t cap = 0;
+  };
+  struct Slot {
+    Buf q, ids, dists, cnt, stats, fops, foffs, fpool, perl;
+    uint32_t *counter = nullptr;  // work counter of the persistent grid
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+  };
+  static constexpr int kSlots = 16;
+  Slot slots[kSlots];
+  int next_slot = 0;
+  std::vector<void *> allocations;
+};
+
+namespace dg {
+uint32_t dpad_of(uint32_t d);
+DgStatus dev_alloc(DgIndex *idx, void **p, size_t bytes);
+DgStatus buf_reserve(DgIndex::Buf &b, size_t bytes);
+DgStatus to_device(DgIndex *idx, void **dst, const void *src, size_t bytes);
+// Rows of d floats from the host into [n][dpad] device rows, zero padded.
+DgStatus upload_rows_f32(const float *host, uint64_t n, uint32_t d, uint32_t dpad, float *dev,
+                         cudaStream_t st);
+// Kernels used by the attach/encode entry points (dg_build.cu).
+DgStatus encode_pq_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint32_t M,
+                          uint32_t K, const float *cb, uint8_t *codes, uint32_t stride,
+                          cudaStream_t st);
+DgStatus encode_int8_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, float scale,
+                            float offset, uint8_t *codes, uint32_t stride, cudaStream_t st);
+DgStatus encode_f16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_t *codes,
+                           cudaStream_t st);
+DgStatus encode_bf16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_t *out,
+                            cudaStream_t st);
+DgStatus encode_rabitq_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint32_t P,
+                              const float *centroid, const float *signs, uint8_t *codes,
+                              uint32_t stride, cudaStream_t st);
+DgStatus count_matching_device(const uint64_t *labels, uint64_t n, uint32_t nf,
+                               const DgFilterOp *ops, uint32_t nops, const uint64_t *pool,
+                               unsigned long long *count, cudaStream_t st);
+}  // namespace dg

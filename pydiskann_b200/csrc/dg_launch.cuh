@@ -1,0 +1,90 @@
+// dg_launch.cuh -- host-side launch of the beam-search kernel instantiations.
+#pragma once
+#include <mutex>
+#include <unordered_map>
+
+#include "dg_search_kernel.cuh"
+
+namespace dg {
+
+struct LaunchInfo {
+  int grid = 0;
+  int blocks_per_sm = 0;
+  uint32_t smem = 0;
+};
+
+// Launch geometry: 4 warps per block, as many resident blocks as shared memory
+// allows on every SM, never more warps than queries.
+template <typename K>
+DgStatus launch_persistent(K kernel, const SearchArgs &a, const WarpLayout &Ly, cudaStream_t st,
+                           LaunchInfo *info) {
+  const uint32_t smem = Ly.total * 4;
+  int dev = 0;
+  DG_CUDA(cudaGetDevice(&dev));
+  int max_optin = 0, sms = 0;
+  DG_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (smem > (uint32_t)max_optin)
+    return fail(DG_ENOTSUP, "search state does not fit in shared memory (beam/quantizer too large)");
+  DG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int nb = 0;
+  DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, 128, smem));
+  if (nb <= 0) return fail(DG_ENOTSUP, "search kernel cannot be resident on an SM");
+  int grid = nb * sms;
+  const int need = (int)((a.nq + 3) / 4);
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  kernel<<<grid, 128, smem, st>>>(a, Ly);
+  DG_CUDA(cudaGetLastError());
+  if (info) {
+    info->grid = grid;
+    info->blocks_per_sm = nb;
+    info->smem = smem;
+  }
+  return DG_OK;
+}
+
+template <int TRAV, int MET, int LPR>
+DgStatus launch_trav(const SearchArgs &a, const WarpLayout &Ly, int lcap, bool filt, cudaStream_t st,
+                     LaunchInfo *info) {
+  constexpr int F = 8;  // lanes per FP32 row in the rerank gather
+  switch (lcap) {
+    case 64:
+      return filt ? launch_persistent(beam_search_kernel<TRAV, MET, LPR, F, 64, true>, a, Ly, st, info)
+                  : launch_persistent(beam_search_kernel<TRAV, MET, LPR, F, 64, false>, a, Ly, st, info);
+    case 256:
+      return filt ? launch_persistent(beam_search_kernel<TRAV, MET, LPR, F, 256, true>, a, Ly, st, info)
+                  : launch_persistent(beam_search_kernel<TRAV, MET, LPR, F, 256, false>, a, Ly, st, info);
+    case 1024:
+      return filt ? launch_persistent(beam_search_kernel<TRAV, MET, LPR, F, 1024, true>, a, Ly, st, info)
+                  : launch_persistent(beam_search_kernel<TRAV, MET, LPR, F, 1024, false>, a, Ly, st, info);
+    default:
+      return fail(DG_EINVAL, "unsupported working-set capacity");
+  }
+}
+
+template <int TRAV, int LPR>
+DgStatus launch_met(const SearchArgs &a, const WarpLayout &Ly, int met, int lcap, bool filt,
+                    cudaStream_t st, LaunchInfo *info) {
+  switch (met) {
+    case MET_L2: return launch_trav<TRAV, MET_L2, LPR>(a, Ly, lcap, filt, st, info);
+    case MET_DOT: return launch_trav<TRAV, MET_DOT, LPR>(a, Ly, lcap, filt, st, info);
+    default: return launch_trav<TRAV, MET_COS, LPR>(a, Ly, lcap, filt, st, info);
+  }
+}
+
+// One entry per traversal kind, defined in its own translation unit.
+DgStatus launch_search_f32(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
+                           bool filt, cudaStream_t st, LaunchInfo *info);
+DgStatus launch_search_bf16(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
+                            bool filt, cudaStream_t st, LaunchInfo *info);
+DgStatus launch_search_f16(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
+                           bool filt, cudaStream_t st, LaunchInfo *info);
+DgStatus launch_search_int8(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
+                            bool filt, cudaStream_t st, LaunchInfo *info);
+DgStatus launch_search_pq(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
+                          bool filt, cudaStream_t st, LaunchInfo *info);
+DgStatus launch_search_rabitq(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
+                              bool filt, cudaStream_t st, LaunchInfo *info);
+
+}  // namespace dg

@@ -1,0 +1,509 @@
+// dg_search.cuh -- warp-per-query best-first beam search (sm_100a).
+//
+// Restates beam_search (diskann-rs src/lib.rs:198-303) for one query per warp:
+//   * the working set `w` is a sorted shared-memory array of 64-bit keys
+//     ((distance, id) order, bit 0 = "expanded");  the reference's frontier
+//     min-heap is the first unexpanded entry of that array, because an entry
+//     the reference evicts from `w` is never smaller than the current worst of
+//     `w` and therefore only ever ends the search;
+//   * one expansion gathers the adjacency row, drops visited ids, computes all
+//     new distances in one batch and merges them into `w` with a warp-wide
+//     bitonic sort and a merge-path scatter.  Processing a row as one batch
+//     keeps exactly the L smallest (distance, id) pairs, which is what the
+//     reference's sequential insert-if-smaller loop keeps;
+//   * the visited set is a direct-mapped, overwrite-on-collision table in
+//     shared memory.  It never reports an unvisited id as visited; an id it
+//     forgets is recomputed and removed again by the duplicate check of the
+//     merge (a forgotten id that is not in `w` any more cannot re-enter it,
+//     since `w`'s worst entry only decreases), so results do not depend on the
+//     table size;
+//   * filtered search keeps the insertion-sorted result list, the iteration cap
+//     and the early-termination factor of the reference's filtered branch;
+//   * quantized search (src/quantized.rs:68-124) traverses on codes, then
+//     reranks the first max(rerank, k) entries with exact FP32 distances in
+//     their code-distance order (a stable sort by exact distance).
+// Warps take queries from a global counter, so uneven beams, k and filters
+// balance across the persistent grid.
+#pragma once
+#include "dg_common.cuh"
+
+namespace dg {
+
+// ------------------------------------------------------------ launch args
+struct SearchArgs {
+  uint64_t n;
+  uint32_t d, dpad, R, medoid;
+  int32_t metric;
+  const float *vec_f32;   // [n][dpad] exact rows (rerank and FP32 traversal)
+  const uint16_t *vec_bf16;  // [n][dpad] BF16 traversal rows (may be null)
+  const uint32_t *adj;    // [n][R]
+  // quantized codes
+  const uint8_t *codes;
+  uint32_t code_stride;   // bytes per code row (multiple of 16)
+  uint32_t pq_M, pq_K, pq_ds;
+  const float *pq_cb;     // [M][K][ds]
+  float i8_scale, i8_offset;
+  uint32_t rq_padded;
+  const float *rq_centroid;  // [d]
+  const float *rq_signs;     // [3][padded]
+  // labels / filter
+  const uint64_t *labels;
+  uint32_t nf;
+  const DgFilterOp *fops;
+  const uint32_t *foffs;  // per-query program offsets (nq+1) or null
+  uint32_t fnops;
+  const uint64_t *fpool;
+  // queries and parameters
+  const float *Q;  // [nq][d]
+  uint32_t nq, k, L, rerank;
+  const uint32_t *perL;  // per-query L or null
+  uint32_t hbits;        // log2 of the visited-table slots
+  // outputs
+  uint32_t *out_ids;
+  float *out_d;
+  uint32_t *out_cnt;
+  uint32_t *out_stats;
+  uint32_t *counter;  // work counter, zero at launch
+};
+
+enum TravKind { TRAV_F32 = 0, TRAV_BF16 = 1, TRAV_PQ = 2, TRAV_INT8 = 3, TRAV_RABITQ = 4, TRAV_F16 = 5 };
+enum MetKind { MET_L2 = 0, MET_DOT = 1, MET_COS = 2 };
+
+constexpr int kStageCap = 256;  // max adjacency degree
+
+// Per-warp shared-memory carve-up (byte offsets), computed on host and device.
+struct WarpLayout {
+  uint32_t w0, w1, res, cstage, stage, hash, qf, prov, total;
+};
+__host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
+__host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool filt, uint32_t hbits,
+                                                  uint32_t dpad, uint32_t pq_M, uint32_t pq_K,
+                                                  uint32_t rq_padded) {
+  WarpLayout L{};
+  uint32_t o = 0;
+  L.w0 = o; o += lcap * 8;
+  L.w1 = o; o += lcap * 8;
+  L.res = o; o += filt ? lcap * 8 : 0;
+  L.cstage = o; o += 32 * 8;
+  L.stage = o; o += kStageCap * 4;
+  L.hash = o; o += (1u << hbits) * 4;
+  L.qf = o; o += align16(dpad * 4);
+  L.prov = o;
+  uint32_t p = 0;
+  if (trav == TRAV_PQ) p = pq_M * pq_K * 4;
+  else if (trav == TRAV_INT8) p = align16(dpad);
+  else if (trav == TRAV_RABITQ) p = 4 * (rq_padded / 64) * 8 + 32 + align16(rq_padded * 4);
+  else if (trav == TRAV_F16) p = align16(dpad * 4);
+  o += align16(p);
+  L.total = align16(o);
+  return L;
+}
+
+// ------------------------------------------------------- small warp helpers
+__device__ __forceinline__ uint32_t lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+// number of keys in a[0..n) that are < key (a sorted ascending)
+__device__ __forceinline__ int lower_bound_smem(const uint64_t *a, int n, uint64_t key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Merge the nc sorted keys of cst[] into sorted src[0..size) -> dst (capacity
+// cap).  Keys must be distinct nodes.  Returns the new size.
+__device__ __forceinline__ int merge_keys(const uint64_t *src, int size, uint64_t *dst, int cap,
+                                          const uint64_t *cst, int nc, int lane) {
+  if (lane < nc) {
+    uint64_t ck = cst[lane];
+    int np = lower_bound_smem(src, size, ck) + lane;
+    if (np < cap) dst[np] = ck;
+  }
+  for (int i = lane; i < size; i += 32) {
+    uint64_t w = src[i];
+    int np = i + lower_bound_smem(cst, nc, w);
+    if (np < cap) dst[np] = w;
+  }
+  __syncwarp();
+  return min(cap, size + nc);
+}
+
+// Given one candidate key per lane (kKeyInvalid = none), sort, drop
+// duplicates within the batch and against list[0..size), drop keys that cannot
+// enter a full list of capacity cap, and compact the survivors into
+// cst[0..return) in ascending order.
+__device__ __forceinline__ int prepare_batch(uint64_t key, const uint64_t *list, int size, int cap,
+                                             uint64_t *cst, int lane) {
+  key = warp_sort_keys(key, lane);
+  const uint64_t prev = shfl64(key, lane > 0 ? lane - 1 : 0);
+  bool ok = key != kKeyInvalid;
+  if (ok && lane > 0 && prev == key) ok = false;  // duplicate id within the batch
+  if (ok) {
+    int pos = lower_bound_smem(list, size, key);
+    if (pos < size && strip_flag(list[pos]) == key) ok = false;  // already listed
+    if (size >= cap && key > strip_flag(list[cap - 1])) ok = false;  // cannot enter
+  }
+  const uint32_t m = __ballot_sync(kFull, ok);
+  if (ok) cst[__popc(m & lanemask_lt(lane))] = key;
+  __syncwarp();
+  return __popc(m);
+}
+
+// Ascending bitonic sort of a[0..n) in shared memory by one warp (n <= 2048).
+__device__ __forceinline__ void warp_sort_smem(uint64_t *a, int n, int lane) {
+  int p2 = 1;
+  while (p2 < n) p2 <<= 1;
+  for (int i = n + lane; i < p2; i += 32) a[i] = kKeyInvalid;
+  __syncwarp();
+  for (int k = 2; k <= p2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < p2; i += 32) {
+        int l = i ^ j;
+        if (l > i) {
+          uint64_t x = a[i], y = a[l];
+          bool up = (i & k) == 0;
+          if ((x > y) == up) {
+            a[i] = y;
+            a[l] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------- row-gather distances
+// Rows are split into 16-byte chunks; LPR lanes cooperate on one row, RPI =
+// 32/LPR rows are read per warp instruction (fully coalesced), LOADS chunks
+// per lane per row.  Partial sums are transposed-reduced so lane j ends up
+// with candidate j's distance.
+template <int ELEM>  // 0 = f32, 1 = bf16, 2 = f16
+struct Chunk;
+template <> struct Chunk<0> {
+  static constexpr int EPC = 4;
+  __device__ static void unpack(uint4 v, float (&x)[4]) {
+    x[0] = __uint_as_float(v.x); x[1] = __uint_as_float(v.y);
+    x[2] = __uint_as_float(v.z); x[3] = __uint_as_float(v.w);
+  }
+};
+template <> struct Chunk<1> {
+  static constexpr int EPC = 8;
+  __device__ static void unpack(uint4 v, float (&x)[8]) {
+    x[0] = __uint_as_float(v.x << 16); x[1] = __uint_as_float(v.x & 0xffff0000u);
+    x[2] = __uint_as_float(v.y << 16); x[3] = __uint_as_float(v.y & 0xffff0000u);
+    x[4] = __uint_as_float(v.z << 16); x[5] = __uint_as_float(v.z & 0xffff0000u);
+    x[6] = __uint_as_float(v.w << 16); x[7] = __uint_as_float(v.w & 0xffff0000u);
+  }
+};
+template <> struct Chunk<2> {
+  static constexpr int EPC = 8;
+  __device__ static void unpack(uint4 v, float (&x)[8]) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      x[2 * i] = __half2float(__ushort_as_half((unsigned short)(w[i] & 0xffffu)));
+      x[2 * i + 1] = __half2float(__ushort_as_half((unsigned short)(w[i] >> 16)));
+    }
+  }
+};
+
+__device__ __forceinline__ float finish_metric(int met, bool sqrt_l2, float a, float b, float qq) {
+  if (met == MET_L2) return sqrt_l2 ? sqrtf(a) : a;
+  if (met == MET_DOT) return 1.0f - a;
+  // angular (numkong): a = q.x, b = x.x, qq = q.q
+  if (qq == 0.0f && b == 0.0f) return 0.0f;
+  if (a == 0.0f) return 1.0f;
+  float r = 1.0f - a / (sqrtf(qq) * sqrtf(b));
+  return r > 0.0f ? r : 0.0f;
+}
+
+// Distance of lane j's candidate `cand` (valid when j < cnt) against the
+// query held in shared memory (qs, f32, dpad long).  rows: base pointer, row
+// stride in bytes; chunks = row bytes / 16.
+template <int LPR, int ELEM, int MET>
+__device__ __forceinline__ float rows_distance(const uint8_t *__restrict__ rows, uint32_t stride,
+                                               int loads, const float *qs, uint32_t cand, int cnt,
+                                               int lane, bool sqrt_l2, float qq) {
+  constexpr int RPI = 32 / LPR;
+  constexpr int EPC = Chunk<ELEM>::EPC;
+  const int g = lane / LPR, r = lane % LPR;
+  float pa[LPR], pb[LPR];
+#pragma unroll
+  for (int i = 0; i < LPR; ++i) { pa[i] = 0.0f; pb[i] = 0.0f; }
+  for (int t = 0; t < loads; ++t) {
+    const int chunk = r + LPR * t;
+    float qv[EPC];
+#pragma unroll
+    for (int e = 0; e < EPC; ++e) qv[e] = qs[chunk * EPC + e];
+#pragma unroll
+    for (int i = 0; i < LPR; ++i) {
+      if (i * RPI < cnt) {  // warp-uniform
+        const int c = i * RPI + g;
+        const uint32_t id = __shfl_sync(kFull, cand, c & 31);
+        if (c < cnt) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(rows + (size_t)id * stride) + chunk);
+          float x[EPC];
+          Chunk<ELEM>::unpack(v, x);
+#pragma unroll
+          for (int e = 0; e < EPC; ++e) {
+            if (MET == MET_L2) {
+              float df = x[e] - qv[e];
+              pa[i] = fmaf(df, df, pa[i]);
+            } else {
+              pa[i] = fmaf(x[e], qv[e], pa[i]);
+              if (MET == MET_COS) pb[i] = fmaf(x[e], x[e], pb[i]);
+            }
+          }
+        }
+      }
+    }
+  }
+  float a = transpose_reduce<LPR>(pa, lane);
+  float b = 0.0f;
+  if (MET == MET_COS) b = transpose_reduce<LPR>(pb, lane);
+  // lane l holds candidate (l % LPR) * RPI + l / LPR; route candidate j to lane j
+  const int srcl = (lane % RPI) * LPR + lane / RPI;
+  a = __shfl_sync(kFull, a, srcl);
+  if (MET == MET_COS) b = __shfl_sync(kFull, b, srcl);
+  return finish_metric(MET, sqrt_l2, a, b, qq);
+}
+
+// int8 codes: exact integer squared distance (src/sq.rs:168-172).
+template <int LPR>
+__device__ __forceinline__ uint32_t int8_l2_group(const uint8_t *__restrict__ codes, uint32_t stride,
+                                                  int loads, const uint8_t *qcode, uint32_t cand,
+                                                  int cnt, int lane) {
+  constexpr int RPI = 32 / LPR;
+  const int g = lane / LPR, r = lane % LPR;
+  uint32_t p[LPR];
+#pragma unroll
+  for (int i = 0; i < LPR; ++i) p[i] = 0;
+  for (int t = 0; t < loads; ++t) {
+    const int chunk = r + LPR * t;
+    const uint4 qv = *reinterpret_cast<const uint4 *>(qcode + chunk * 16);
+#pragma unroll
+    for (int i = 0; i < LPR; ++i) {
+      if (i * RPI < cnt) {
+        const int c = i * RPI + g;
+        const uint32_t id = __shfl_sync(kFull, cand, c & 31);
+        if (c < cnt) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(codes + (size_t)id * stride) + chunk);
+          uint32_t a0 = __vabsdiffu4(v.x, qv.x), a1 = __vabsdiffu4(v.y, qv.y);
+          uint32_t a2 = __vabsdiffu4(v.z, qv.z), a3 = __vabsdiffu4(v.w, qv.w);
+          p[i] = __dp4a(a0, a0, p[i]);
+          p[i] = __dp4a(a1, a1, p[i]);
+          p[i] = __dp4a(a2, a2, p[i]);
+          p[i] = __dp4a(a3, a3, p[i]);
+        }
+      }
+    }
+  }
+  uint32_t s = transpose_reduce<LPR>(p, lane);
+  const int srcl = (lane % RPI) * LPR + lane / RPI;
+  return __shfl_sync(kFull, s, srcl);
+}
+
+// int8 codes decoded for non-L2 metrics (src/quantized.rs:28-36): c*scale+offset.
+template <int LPR, int MET>
+__device__ __forceinline__ float int8_decode_group(const uint8_t *__restrict__ codes, uint32_t stride,
+                                                   int loads, const float *qs, float scale,
+                                                   float offset, uint32_t dlim, uint32_t cand,
+                                                   int cnt, int lane, float qq) {
+  constexpr int RPI = 32 / LPR;
+  const int g = lane / LPR, r = lane % LPR;
+  float pa[LPR], pb[LPR];
+#pragma unroll
+  for (int i = 0; i < LPR; ++i) { pa[i] = 0.0f; pb[i] = 0.0f; }
+  for (int t = 0; t < loads; ++t) {
+    const int chunk = r + LPR * t;
+#pragma unroll
+    for (int i = 0; i < LPR; ++i) {
+      if (i * RPI < cnt) {
+        const int c = i * RPI + g;
+        const uint32_t id = __shfl_sync(kFull, cand, c & 31);
+        if (c < cnt) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(codes + (size_t)id * stride) + chunk);
+          const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            // padding columns beyond the dimension decode to nothing
+            float x = (uint32_t)(chunk * 16 + e) < dlim
+                          ? __fadd_rn(__fmul_rn((float)((w[e >> 2] >> (8 * (e & 3))) & 0xffu), scale), offset)
+                          : 0.0f;
+            pa[i] = fmaf(x, qs[chunk * 16 + e], pa[i]);
+            if (MET == MET_COS) pb[i] = fmaf(x, x, pb[i]);
+          }
+        }
+      }
+    }
+  }
+  float a = transpose_reduce<LPR>(pa, lane);
+  float b = 0.0f;
+  if (MET == MET_COS) b = transpose_reduce<LPR>(pb, lane);
+  const int srcl = (lane % RPI) * LPR + lane / RPI;
+  a = __shfl_sync(kFull, a, srcl);
+  if (MET == MET_COS) b = __shfl_sync(kFull, b, srcl);
+  return finish_metric(MET, false, a, b, qq);
+}
+
+// ------------------------------------------------------------ quantizers
+// PQ lookup table (src/pq.rs:181-198): lut[m][c] = sequential f32 sum of
+// squared differences over the subspace, rounded like the oracle.
+__device__ __forceinline__ void build_pq_lut(const SearchArgs &a, const float *qs, float *lut, int lane) {
+  const uint32_t total = a.pq_M * a.pq_K;
+  for (uint32_t e = lane; e < total; e += 32) {
+    const uint32_t m = e / a.pq_K;
+    const float *cen = a.pq_cb + (size_t)e * a.pq_ds;
+    const float *qq = qs + m * a.pq_ds;
+    float acc = 0.0f;
+    for (uint32_t j = 0; j < a.pq_ds; ++j) {
+      float t = __fsub_rn(qq[j], __ldg(cen + j));
+      acc = __fadd_rn(acc, __fmul_rn(t, t));
+    }
+    lut[e] = acc;
+  }
+}
+// src/pq.rs:202-209: sequential f32 sum over subspaces.
+__device__ __forceinline__ float pq_adc(const SearchArgs &a, const float *lut, uint32_t id) {
+  const uint8_t *row = a.codes + (size_t)id * a.code_stride;
+  float d = 0.0f;
+  const uint32_t K = a.pq_K;
+  uint32_t m = 0;
+  for (uint32_t c = 0; m < a.pq_M; ++c) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(row) + c);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+      if (m < a.pq_M) {
+        const uint32_t code = (w[b >> 2] >> (8 * (b & 3))) & 0xffu;
+        d = __fadd_rn(d, lut[m * K + code]);
+        ++m;
+      }
+    }
+  }
+  return d;
+}
+
+// int8 query encoding (src/sq.rs:208-220): x*(1/scale) + (-offset/scale),
+// rounded to nearest even and saturated.
+__device__ __forceinline__ uint8_t int8_code(float x, float inv, float beta) {
+  float t = __fadd_rn(__fmul_rn(x, inv), beta);
+  if (!(t == t)) return 0;
+  t = rintf(t);
+  if (t < 0.0f) return 0;
+  if (t > 255.0f) return 255;
+  return (uint8_t)t;
+}
+
+// RaBitQ query preparation (src/rabitq.rs:136-187) by one warp in shared
+// memory: residual, norm, normalisation, 3 rounds of sign flip + FHT, 4-bit
+// quantisation into bit planes and the estimator constants.
+__device__ inline void rabitq_prepare(const float *q, uint32_t d, uint32_t P, const float *cen,
+                               const float *signs, float *r, uint64_t *planes, float *k5,
+                               int lane) {
+  for (uint32_t i = lane; i < P; i += 32) r[i] = i < d ? __fsub_rn(q[i], cen[i]) : 0.0f;
+  __syncwarp();
+  float s = 0.0f;  // sequential sum of squares, as the oracle
+  if (lane == 0)
+    for (uint32_t i = 0; i < P; ++i) s = __fadd_rn(s, __fmul_rn(r[i], r[i]));
+  const float nq = __shfl_sync(kFull, __fsqrt_rn(s), 0);
+  if (nq > 0.0f)
+    for (uint32_t i = lane; i < P; i += 32) r[i] = __fdiv_rn(r[i], nq);
+  __syncwarp();
+  for (int rd = 0; rd < 3; ++rd) {
+    for (uint32_t i = lane; i < P; i += 32) r[i] = __fmul_rn(r[i], signs[rd * P + i]);
+    __syncwarp();
+    for (uint32_t h = 1; h < P; h *= 2) {
+      for (uint32_t t = lane; t < P / 2; t += 32) {
+        const uint32_t blk = t / h, off = t % h;
+        const uint32_t j = blk * 2 * h + off;
+        const float x = r[j], y = r[j + h];
+        r[j] = __fadd_rn(x, y);
+        r[j + h] = __fsub_rn(x, y);
+      }
+      __syncwarp();
+    }
+  }
+  float lo = 3.402823466e38f, hi = -3.402823466e38f;
+  for (uint32_t i = lane; i < P; i += 32) {
+    lo = fminf(lo, r[i]);
+    hi = fmaxf(hi, r[i]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(kFull, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(kFull, hi, o));
+  }
+  const float delta = __fdiv_rn(__fsub_rn(hi, lo), 15.0f);
+  const float inv = delta > 0.0f ? __fdiv_rn(1.0f, delta) : 0.0f;
+  const uint32_t words = P / 64;
+  uint32_t sum_u = 0;
+  for (uint32_t wd = 0; wd < words; ++wd) {
+    // each lane handles 2 coordinates of this 64-bit word
+    uint64_t pl[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int h2 = 0; h2 < 2; ++h2) {
+      const uint32_t bit = lane + 32 * h2;
+      const uint32_t i = wd * 64 + bit;
+      float t = roundf(__fmul_rn(__fsub_rn(r[i], lo), inv));
+      uint32_t u = t <= 0.0f ? 0u : (uint32_t)t;
+      u = min(u, 15u);
+      sum_u += u;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if ((u >> j) & 1u) pl[j] |= 1ull << bit;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      uint32_t lo32 = (uint32_t)pl[j], hi32 = (uint32_t)(pl[j] >> 32);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo32 |= __shfl_xor_sync(kFull, lo32, o);
+        hi32 |= __shfl_xor_sync(kFull, hi32, o);
+      }
+      if (lane == 0) planes[j * words + wd] = ((uint64_t)hi32 << 32) | lo32;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum_u += __shfl_xor_sync(kFull, sum_u, o);
+  if (lane == 0) {
+    const float sd = __fsqrt_rn((float)P);
+    k5[0] = __fmul_rn(nq, nq);
+    k5[1] = __fmul_rn(2.0f, nq);
+    k5[2] = __fdiv_rn(__fmul_rn(2.0f, delta), sd);
+    k5[3] = __fdiv_rn(__fmul_rn(2.0f, lo), sd);
+    k5[4] = __fdiv_rn(-__fadd_rn(__fmul_rn(delta, (float)sum_u), __fmul_rn((float)P, lo)), sd);
+  }
+  __syncwarp();
+}
+
+// src/rabitq.rs:191-197 for one code row.
+__device__ __forceinline__ float rabitq_est(const uint8_t *code, uint32_t P, const uint64_t *planes,
+                                            const float *k5) {
+  const uint32_t words = P / 64;
+  uint32_t S = 0, C = 0;
+  for (uint32_t i = 0; i < words; i += 2) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(code) + (i >> 1));
+    const uint64_t b0 = ((uint64_t)v.y << 32) | v.x;
+    const uint64_t b1 = ((uint64_t)v.w << 32) | v.z;
+    C += __popcll(b0);
+    S += __popcll(b0 & planes[i]) + (__popcll(b0 & planes[words + i]) << 1) +
+         (__popcll(b0 & planes[2 * words + i]) << 2) + (__popcll(b0 & planes[3 * words + i]) << 3);
+    if (i + 1 < words) {
+      C += __popcll(b1);
+      S += __popcll(b1 & planes[i + 1]) + (__popcll(b1 & planes[words + i + 1]) << 1) +
+           (__popcll(b1 & planes[2 * words + i + 1]) << 2) +
+           (__popcll(b1 & planes[3 * words + i + 1]) << 3);
+    }
+  }
+  const float2 nf = __ldg(reinterpret_cast<const float2 *>(code + P / 8));
+  const float inner = __fadd_rn(__fadd_rn(__fmul_rn(k5[2], (float)S), __fmul_rn(k5[3], (float)C)), k5[4]);
+  const float e = __fsub_rn(__fadd_rn(nf.x, k5[0]), __fmul_rn(__fmul_rn(k5[1], nf.y), inner));
+  return fmaxf(e, 0.0f);
+}
+
+}  // namespace dg

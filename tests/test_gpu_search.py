@@ -1,0 +1,235 @@
+"""GPU beam search vs the CPU oracle, through the C ABI.
+
+The seeded data is integer valued, so every FP32 (and BF16 / F16) distance is
+exact in any summation order: ids, counts and distances must be bit-identical
+to the oracle's.  Non-integer data (cosine) is compared within 1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+import pydiskann_b200 as dg
+from pydiskann_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_same(g, o):
+    gi, gd, gc = g
+    oi, od, oc = o
+    assert (np.asarray(gc) == oc).all(), np.nonzero(np.asarray(gc) != oc)
+    bad = np.nonzero((np.asarray(gi) != oi).any(1))[0]
+    assert len(bad) == 0, (bad[:5], np.asarray(gi)[bad[:2]], oi[bad[:2]])
+    assert np.array_equal(np.asarray(gd), od)
+
+
+@pytest.fixture(scope="module")
+def gindex(small_data, small_graph):
+    X, _ = small_data
+    adj, med = small_graph
+    idx = dg.DiskANN.from_graph(X, adj, med)
+    yield idx
+    idx.close()
+
+
+@pytest.fixture(scope="module")
+def oindex(oracle, small_data, small_graph):
+    X, _ = small_data
+    adj, med = small_graph
+    return oracle.OracleIndex(X, adj, med)
+
+
+@pytest.mark.parametrize("L", [1, 16, 64, 200, 700])
+@pytest.mark.parametrize("k", [1, 10])
+def test_fp32_matches_oracle(gindex, oindex, small_data, L, k):
+    _, Q = small_data
+    assert_same(gindex.search_arrays(Q, k, L), oindex.search(Q, k, L))
+
+
+def test_bf16_traversal_matches_oracle(gindex, oindex, small_data):
+    """Integer data is exact in BF16: the BF16 traversal equals the FP32 one, and
+    the FP32 rerank of its whole working set returns the same distances."""
+    _, Q = small_data
+    gindex.enable_bf16()
+    assert_same(gindex.search_arrays(Q, 10, 64, traversal=_lib.TRAVERSE_BF16), oindex.search(Q, 10, 64))
+    assert_same(gindex.search_arrays(Q, 10, 64, traversal=_lib.TRAVERSE_BF16, rerank_size=64),
+                oindex.search(Q, 10, 64))
+
+
+def test_stats_and_uneven_beams(gindex, oindex, small_data):
+    _, Q = small_data
+    L = np.random.default_rng(1).integers(8, 257, size=len(Q)).astype(np.uint32)
+    gi, gd, gc, st = gindex.search_arrays(Q, 10, 64, per_query_beam=L, with_stats=True)
+    oi, od, oc, ost = oindex.search(Q, 10, 64, per_query_L=L, with_stats=True)
+    assert_same((gi, gd, gc), (oi, od, oc))
+    assert (st[:, 0] == ost[:, 0]).all()  # same number of expansions
+    assert (st[:, 1] >= ost[:, 1]).all()  # forgotten visits are re-evaluated, never skipped
+
+
+def test_device_pointer_path(gindex, oindex, small_data):
+    import torch
+
+    _, Q = small_data
+    Qd = torch.from_numpy(Q).cuda()
+    ids, ds, cnt = gindex.search_arrays(Qd, 10, 64)
+    torch.cuda.synchronize()
+    oi, od, oc = oindex.search(Q, 10, 64)
+    assert_same((ids.cpu().numpy().view(np.uint32), ds.cpu().numpy(), cnt.cpu().numpy().view(np.uint32)),
+                (oi, od, oc))
+
+
+def test_pq_codes_and_search_match_oracle(oracle, small_data, small_graph):
+    X, Q = small_data
+    adj, med = small_graph
+    cb = dg.pq_train(X, num_subspaces=16, num_centroids=256, kmeans_iterations=8, training_sample_size=3000, seed=4)
+    codes = oracle.pq_encode(X, cb)
+    assert np.array_equal(dg.pq_encode(X, cb), codes)
+    q = dg.QuantizedDiskANN(X, adj, med)
+    q.attach_pq(cb)  # encodes on the GPU
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_pq(cb, codes)
+    for L, rr in ((32, 0), (64, 64), (128, 20)):
+        assert_same(q.search_arrays(Q, 10, L, rerank_size=rr), o.search(Q, 10, L, rerank=rr, use_codes=True))
+    q.close()
+
+
+def test_int8_codes_and_search_match_oracle(oracle, small_data, small_graph):
+    X, Q = small_data
+    adj, med = small_graph
+    s, off = dg.int8_params(X)
+    assert (s, off) == oracle.int8_train(X)
+    codes = oracle.int8_encode(X, s, off)
+    q = dg.QuantizedDiskANN(X, adj, med)
+    q.attach_int8(s, off)
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_int8(s, off, codes)
+    for L, rr in ((48, 0), (64, 32)):
+        assert_same(q.search_arrays(Q, 10, L, rerank_size=rr), o.search(Q, 10, L, rerank=rr, use_codes=True))
+    q.close()
+
+
+def test_f16_search_matches_oracle(oracle, small_data, small_graph):
+    X, Q = small_data
+    adj, med = small_graph
+    q = dg.QuantizedDiskANN(X, adj, med)
+    q.attach_f16()
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_f16(oracle.f16_encode(X))
+    assert_same(q.search_arrays(Q, 10, 64), o.search(Q, 10, 64, use_codes=True))
+    q.close()
+
+
+def test_rabitq_codes_and_search_match_oracle(oracle, small_data, small_graph):
+    X, Q = small_data
+    adj, med = small_graph
+    cen, signs = dg.rabitq_params(X, seed=3)
+    P = dg.rabitq_padded(X.shape[1])
+    codes = oracle.rabitq_encode(X, P, cen, signs)
+    q = dg.QuantizedDiskANN(X, adj, med)
+    q.attach_rabitq(cen, signs)
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_rabitq(P, cen, signs, codes)
+    for L, rr in ((64, 0), (64, 64)):
+        assert_same(q.search_arrays(Q, 10, L, rerank_size=rr), o.search(Q, 10, L, rerank=rr, use_codes=True))
+    q.close()
+
+
+def _labels(n, seed=2):
+    rng = np.random.default_rng(seed)
+    return np.stack([np.arange(n) % 5, rng.integers(0, 100, n), rng.integers(0, 7, n)], 1).astype(np.uint64)
+
+
+FILTERS = [
+    dg.Filter.eq(0, 3),
+    dg.Filter.range(1, 10, 30),
+    dg.Filter.and_([dg.Filter.eq(0, 1), dg.Filter.gt(1, 50)]),
+    dg.Filter.or_([dg.Filter.eq(2, 6), dg.Filter.in_(1, [1, 2, 3, 99])]),
+    dg.Filter.lt(1, 2),
+]
+
+
+@pytest.mark.parametrize("fi", range(len(FILTERS)))
+def test_filtered_matches_oracle(oracle, small_data, small_graph, fi):
+    X, Q = small_data
+    adj, med = small_graph
+    lab = _labels(len(X))
+    f = FILTERS[fi]
+    g = dg.FilteredDiskANN(X, adj, med, lab)
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_labels(lab)
+    ops, pool = f.program()
+    for k, L in ((10, 32), (10, 64), (5, 16)):
+        assert_same(g.search_arrays(Q, k, L, filters=f), o.search(Q, k, L, filter_ops=ops, filter_pool=pool))
+    assert g.count_matching(f) == sum(f.matches(list(map(int, r))) for r in lab)
+    g.close()
+
+
+def test_per_query_filters_match_oracle(oracle, small_data, small_graph):
+    X, Q = small_data
+    adj, med = small_graph
+    lab = _labels(len(X))
+    g = dg.FilteredDiskANN(X, adj, med, lab)
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_labels(lab)
+    fl = [FILTERS[i % len(FILTERS)] if i % 7 else dg.Filter.none() for i in range(len(Q))]
+    gi, gd, gc = g.search_arrays(Q, 10, 40, filters=fl)
+    for i, f in enumerate(fl):
+        ops, pool = f.program()
+        oi, od, oc = o.search(Q[i:i + 1], 10, 40, filter_ops=ops or None, filter_pool=pool)
+        assert gc[i] == oc[0] and (gi[i] == oi[0]).all() and np.array_equal(gd[i], od[0]), i
+    g.close()
+
+
+def test_quantized_filtered_matches_oracle(oracle, small_data, small_graph):
+    X, Q = small_data
+    adj, med = small_graph
+    lab = _labels(len(X))
+    s, off = dg.int8_params(X)
+    q = dg.QuantizedDiskANN(X, adj, med)
+    q.attach_int8(s, off)
+    q.attach_labels(lab)
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_int8(s, off, oracle.int8_encode(X, s, off))
+    o.set_labels(lab)
+    f = FILTERS[3]
+    ops, pool = f.program()
+    assert_same(q.search_arrays(Q, 10, 32, rerank_size=16, filters=f),
+                o.search(Q, 10, 32, rerank=16, use_codes=True, filter_ops=ops, filter_pool=pool))
+    q.close()
+
+
+def test_cosine_within_tolerance(oracle):
+    from pydiskann_b200 import synth
+
+    X, Q = synth.cosine(3000, 50, 96, seed=5)
+    adj, med = oracle.build_vamana(X, 24, 48, 1.2, seed=3, metric=oracle.COSINE)
+    g = dg.DiskANN.from_graph(X, adj, med, metric="cosine")
+    o = oracle.OracleIndex(X, adj, med, oracle.COSINE)
+    gi, gd, gc = g.search_arrays(Q, 10, 64)
+    oi, od, oc = o.search(Q, 10, 64)
+    same = np.mean([len(set(gi[i]) & set(oi[i])) / 10 for i in range(len(Q))])
+    assert same >= 0.98
+    for i in range(len(Q)):
+        for j in range(10):
+            if gi[i, j] == oi[i, j]:
+                assert abs(gd[i, j] - od[i, j]) <= 1e-5 * max(1e-3, abs(od[i, j])) + 1e-6
+    g.close()
+
+
+def test_edge_cases():
+    X = np.array([[1.0, 2.0, 3.0]], dtype=np.float32)
+    idx = dg.DiskANN.build(X)
+    assert idx.search([1.0, 2.0, 3.0], 1, 8) == [0]
+    assert idx.search([0.0, 0.0, 0.0], 10, 8) == [0]
+    with pytest.raises(ValueError):
+        idx.search([1.0, 2.0], 1, 8)
+    with pytest.raises(RuntimeError):
+        dg.DiskANN.build(np.zeros((0, 4), dtype=np.float32))
+    with pytest.raises(ValueError):
+        dg.DiskANN.build(X, metric="manhattan")
+    Y = np.tile(np.array([[1.0, 2.0, 3.0]], dtype=np.float32), (10, 1))
+    r = dg.DiskANN.build(Y).search_with_dists([1.0, 2.0, 3.0], 5, 8)
+    assert len(r) == 5 and all(d < 1e-6 for _, d in r)
+    rng = np.random.default_rng(201)
+    Z = rng.random((50, 16), dtype=np.float32)
+    r = dg.DiskANN.build(Z).search_with_dists(Z[0], 1, 1)
+    assert len(r) == 1 and r[0][1] >= 0.0
