@@ -350,15 +350,16 @@ __global__ void __launch_bounds__(kPruneThreads) k_prune(PruneArgs a) {
     const float alpha = fmaxf(a.alpha, 1.0f);
     float cur_alpha = 1.0f;
     uint32_t np = 0;
+    // Every thread takes the same decisions from S/O: the flag of the entry
+    // being decided is written only after the barrier that ends its selection,
+    // and each pass ends with a barrier, so no thread can read a flag in the
+    // middle of its update and skip a barrier the others wait at.
     while (cur_alpha <= alpha && np < a.R) {
       for (uint32_t i = 0; i < m; ++i) {
         if (np >= a.R) break;
         if (S[i] || O[i] > cur_alpha) continue;
         const uint32_t idi = key_id(K[i]);
-        if (tid == 0) {
-          S[i] = 1;
-          s_out[np] = idi;
-        }
+        if (tid == 0) s_out[np] = idi;
         ++np;
         for (uint32_t j = i + 1 + tid; j < m; j += blockDim.x) {
           if (S[j] || O[j] > alpha) continue;
@@ -367,7 +368,9 @@ __global__ void __launch_bounds__(kPruneThreads) k_prune(PruneArgs a) {
           O[j] = djk == 0.0f ? __int_as_float(0x7f800000) : fmaxf(O[j], __fdiv_rn(key_dist(kj), djk));
         }
         __syncthreads();
+        if (tid == 0) S[i] = 1;
       }
+      __syncthreads();
       cur_alpha = __fmul_rn(cur_alpha, 1.2f);
     }
     if (tid == 0) {
