@@ -1,0 +1,499 @@
+#!/usr/bin/env python
+"""QPS at recall@10 >= 0.95 on the 1M x 128 PQ workload, on one B200 (or N replicas).
+
+Workload: 1M x 128 FP32 base vectors from a 256-centre clipped Gaussian mixture
+(seeded synthetic data with the configuration's shapes and value distribution),
+10k queries per batch, Vamana graph R=64, L_build=128, alpha=1.2 (built on the
+GPU), PQ M=16 x K=256 trained with 25 Lloyd iterations on a 100k sample, k=10.
+A step is one batched search of the 10k queries.  Three variants are swept over
+the beam width L and each is timed at the smallest L whose recall@10 against
+the exact FP64 ground truth reaches 0.95:
+  fp32       -- plain FP32 beam search (DiskANN::search)
+  bf16_rerank-- BF16 rows during the search, FP32 rerank of the top L
+  int8_rerank-- int8 SQ codes (global scale/offset, src/sq.rs) during the
+                search, FP32 rerank of the top L
+  pq_rerank  -- PQ ADC during the search, FP32 rerank of the top L
+The headline `value` is the fastest variant at recall >= 0.95; a variant that
+does not reach it within the swept beams is reported with its best recall.
+
+`--impl reference` times the CPU restatement of the reference search (the
+oracle, all host threads) on the same graph, codes and queries.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+CACHE = os.environ.get("DGANN_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "dgann_bench_cache"))
+R, L_BUILD, ALPHA, M, K_PQ, PQ_ITERS, PQ_SAMPLE, K = 64, 128, 1.2, 16, 256, 25, 100_000, 10
+L_SWEEP = (16, 24, 32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256, 384, 512, 768, 1024)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--nq", type=int, default=10_000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--target-recall", type=float, default=0.95)
+    ap.add_argument("--variants", default="fp32,bf16_rerank,int8_rerank,pq_rerank")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ setup
+def workload(args, device=0, build=True):
+    """Data (regenerated), graph, codebooks and ground truth (cached on disk)."""
+    from pydiskann_b200 import synth
+
+    t0 = time.time()
+    X, Q = synth.pq_config(args.n, args.nq, 128, args.seed)
+    log(f"[setup] data {X.shape} + {Q.shape} in {time.time() - t0:.1f}s")
+    key = f"pq_n{args.n}_q{args.nq}_R{R}_L{L_BUILD}_a{ALPHA}_M{M}_s{args.seed}"
+    d = os.path.join(CACHE, key)
+    files = {k: os.path.join(d, k + ".npy") for k in ("adj", "meta", "cb", "codes", "gt")}
+    if all(os.path.exists(f) for f in files.values()):
+        adj = np.load(files["adj"])
+        med = int(np.load(files["meta"])[0])
+        cb = np.load(files["cb"])
+        codes = np.load(files["codes"])
+        gt = np.load(files["gt"])
+        log(f"[setup] graph/codebooks/ground truth from cache {d}")
+        return X, Q, adj, med, (cb, codes), gt, {"cached": True}
+    if not build:
+        return None
+    import pydiskann_b200 as dg
+
+    times = {}
+    t0 = time.time()
+    med = dg.medoid(X, device=device)
+    times["medoid_s"] = time.time() - t0
+    t0 = time.time()
+    adj, _ = dg.build_graph(X, R, L_BUILD, ALPHA, seed=args.seed, medoid_id=med, device=device)
+    times["graph_build_s"] = time.time() - t0
+    log(f"[setup] GPU Vamana build {times['graph_build_s']:.1f}s")
+    t0 = time.time()
+    cb = dg.pq_train(X, M, K_PQ, PQ_ITERS, PQ_SAMPLE, seed=args.seed, device=device)
+    times["pq_train_s"] = time.time() - t0
+    codes = dg.pq_encode(X, cb, device=device)
+    t0 = time.time()
+    gt, _ = dg.exact_knn(X, Q, K, device=device)
+    times["ground_truth_s"] = time.time() - t0
+    log(f"[setup] PQ train {times['pq_train_s']:.1f}s, exact kNN {times['ground_truth_s']:.1f}s")
+    os.makedirs(d, exist_ok=True)
+    for k, v in (("adj", adj), ("meta", np.array([med])), ("cb", cb), ("codes", codes), ("gt", gt)):
+        tmp = files[k] + f".tmp{os.getpid()}.npy"
+        np.save(tmp, v)
+        os.replace(tmp, files[k])
+    return X, Q, adj, med, (cb, codes), gt, times
+
+
+def recall(ids, gt, k=K):
+    ids = np.asarray(ids)[:, :k]
+    hits = sum(len(set(ids[i].tolist()) & set(gt[i, :k].tolist())) for i in range(len(gt)))
+    return hits / (len(gt) * k)
+
+
+# ------------------------------------------------------------ clock probe
+class Clocks:
+    """Samples SM clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx.append(float(p[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.remove(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ GPU timing
+VARIANTS = {
+    # name: (traversal, rerank = L?)
+    "fp32": ("f32", False),
+    "bf16_rerank": ("bf16", True),
+    "int8_rerank": ("int8", True),
+    "pq_rerank": ("codes", True),
+}
+
+
+def run_variant(idx, qidx, name, Qd, L, out=None, with_stats=False, stream=None):
+    """idx: the FP32/BF16 index; qidx: {"pq": QuantizedDiskANN, "int8": ...}."""
+    from pydiskann_b200 import _lib
+
+    trav, rr = VARIANTS[name]
+    t = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES,
+         "int8": _lib.TRAVERSE_CODES}[trav]
+    target = qidx["pq"] if trav == "codes" else qidx["int8"] if trav == "int8" else idx
+    return target.search_arrays(Qd, K, L, traversal=t, rerank_size=L if rr else 0, out=out,
+                                with_stats=with_stats, stream=stream)
+
+
+def algorithmic_bytes(name, stats, L, d=128):
+    """Bytes the algorithm must read per launch: adjacency rows, distance
+    operands, rerank rows, queries and results (SURVEY 8(d) per-query terms)."""
+    E = stats[:, 0].astype(np.float64).sum()
+    N = stats[:, 1].astype(np.float64).sum()
+    nq = stats.shape[0]
+    adj = E * 4 * R
+    if name == "fp32":
+        dist, rr = N * 4 * d, 0.0
+    elif name == "bf16_rerank":
+        dist, rr = N * 2 * d, nq * L * 4 * d
+    elif name == "int8_rerank":
+        dist, rr = N * d, nq * L * 4 * d
+    else:
+        dist, rr = N * M, nq * L * 4 * d
+    return adj + dist + rr + nq * 4 * d + nq * K * 8, {"expansions_per_query": E / nq, "dist_evals_per_query": N / nq}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import pydiskann_b200 as dg
+
+    # rank 0 fills the cache, the others read it (no data-path collective)
+    wl = None
+    if rank == 0:
+        wl = workload(args, local)
+    if dist is not None:
+        dist.barrier()
+    if wl is None:
+        wl = workload(args, local)
+    X, Q, adj, med, (cb, codes), gt, setup_times = wl
+    t0 = time.time()
+    wanted = args.variants.split(",")
+    idx, qidx = None, {}
+    if "fp32" in wanted or "bf16_rerank" in wanted:
+        idx = dg.DiskANN.from_graph(X, adj, med, device=local)
+        if "bf16_rerank" in wanted:
+            idx.enable_bf16()
+    if "pq_rerank" in wanted:
+        qidx["pq"] = dg.QuantizedDiskANN(X, adj, med, device=local)
+        qidx["pq"].attach_pq(cb, codes)
+    if "int8_rerank" in wanted:
+        qidx["int8"] = dg.QuantizedDiskANN(X, adj, med, device=local)
+        qidx["int8"].attach_int8(*dg.int8_params(X))
+    log(f"[setup] index upload + encodes {time.time() - t0:.1f}s")
+    Qd = torch.from_numpy(Q).to(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- recall sweep: smallest L reaching the target for each variant
+    chosen, curves = {}, {}
+    for name in args.variants.split(","):
+        curves[name] = []
+        for L in L_SWEEP:
+            ids, _, _ = run_variant(idx, qidx, name, Qd, L)
+            torch.cuda.synchronize()
+            rec = recall(ids.cpu().numpy().view(np.uint32), gt)
+            curves[name].append((L, round(rec, 4)))
+            if rec >= args.target_recall:
+                chosen[name] = (L, rec)
+                break
+        log(f"[sweep] {name}: {chosen.get(name)} curve {curves[name]}")
+
+    # ---- timing per variant (device-resident queries and results)
+    results = {}
+    for name, (L, rec) in chosen.items():
+        out = run_variant(idx, qidx, name, Qd, L)
+        for _ in range(args.warmup):
+            run_variant(idx, qidx, name, Qd, L, out=out)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        with Clocks(local) as ck:
+            torch.cuda.synchronize()
+            t_start = torch.cuda.Event(enable_timing=True)
+            t_end = torch.cuda.Event(enable_timing=True)
+            t_start.record(stream)
+            for s in range(args.steps):
+                ev[s][0].record(stream)
+                run_variant(idx, qidx, name, Qd, L, out=out)
+                ev[s][1].record(stream)
+            t_end.record(stream)
+            torch.cuda.synchronize()
+        total_ms = t_start.elapsed_time(t_end)
+        steps_ms = np.array([a.elapsed_time(b) for a, b in ev])
+        if dist is not None:
+            tt = torch.tensor([total_ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            total_ms = float(tt.item())
+        _, _, _, st = run_variant(idx, qidx, name, Qd, L, with_stats=True)
+        stats = st.cpu().numpy().view(np.uint32)
+        alg_bytes, work = algorithmic_bytes(name, stats, L)
+        results[name] = {
+            "L": L, "recall_at_10": round(rec, 4), "qps": world * args.nq * args.steps / (total_ms / 1e3),
+            "ms_per_step": total_ms / args.steps, "p50_ms": float(np.percentile(steps_ms, 50)),
+            "p99_ms": float(np.percentile(steps_ms, 99)), "launch_ms": float(steps_ms.mean()),
+            "alg_bytes_per_launch": alg_bytes, **work, "clocks": ck.summary(),
+        }
+        log(f"[time] {name}: {json.dumps(results[name])}")
+
+    head = max(results, key=lambda n: results[n]["qps"]) if results else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    line = {
+        "metric": "QPS @ recall@10=0.95, plain FP32 vs BF16+FP32-rerank, 1 B200; p99 ms",
+        "value": results[head]["qps"] if head else None,
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": results[head]["ms_per_step"] if head else None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": {"fp32": "f32", "bf16_rerank": "bf16+f32", "int8_rerank": "u8+f32"}.get(head, "u8-pq+f32"),
+        "data": "synthetic (seeded 256-centre Gaussian mixture, 1M x 128, 10k queries)",
+        "config": {"workload": f"pq-1Mx128 M={M} R={R} L_build={L_BUILD} alpha={ALPHA} k={K} "
+                               f"nq={args.nq} n={args.n}", "variant": head,
+                   "L": results[head]["L"] if head else None, "global_batch": args.nq * world,
+                   "parallelism": f"replicas{world}", "l2_policy": "inputs larger than L2 (768 MB index)"},
+        "variants": results,
+        "recall_curves": curves,
+        "p99_ms": results[head]["p99_ms"] if head else None,
+        "setup": setup_times,
+    }
+    if head:
+        r = results[head]
+        ach = r["alg_bytes_per_launch"] / (r["launch_ms"] / 1e3) / 1e9
+        line["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                            "frac": round(ach / hbm, 4), "traffic": None,
+                            "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650"}
+        line["clocks"] = r["clocks"]
+        line["gpu_launches"] = args.steps
+        line["e2e"] = e2e(args, idx, qidx, head, r["L"], Q, gt, dist, world, dev)
+        if "fp32" in results:
+            line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
+    if rank == 0 and head and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, X, Q, adj, med, (cb, codes), head, results[head]["L"])
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if idx is not None:
+        idx.close()
+    for q in qidx.values():
+        q.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def e2e(args, idx, qidx, name, L, Q, gt, dist, world, dev):
+    """The same search through the public API with host buffers: the queries
+    are copied from pinned host memory and the results read back every step."""
+    import torch
+
+    Qh = torch.from_numpy(Q).pin_memory()
+    Qn = Qh.numpy()
+    outs = (torch.empty((args.nq, K), dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+            torch.empty((args.nq, K), dtype=torch.float32).pin_memory().numpy(),
+            torch.empty((args.nq,), dtype=torch.int32).pin_memory().numpy().view(np.uint32))
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        run_variant(idx, qidx, name, Qn, L, out=outs, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        run_variant(idx, qidx, name, Qn, L, out=outs, stream=stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    rec = recall(outs[0], gt)
+    return {"value": world * args.nq * args.steps / (ms / 1e3), "unit": "queries/s",
+            "h2d_bytes_per_step": int(Q.nbytes), "d2h_bytes_per_step": int(args.nq * (K * 8 + 4)),
+            "recall_at_10": round(rec, 4)}
+
+
+# ------------------------------------------------------------ CPU legs
+def _oracle_index(X, adj, med, pq, name):
+    import oracle
+
+    o = oracle.OracleIndex(X, adj, med)
+    if name == "pq_rerank":
+        o.set_pq(*pq)
+    elif name == "int8_rerank":
+        import pydiskann_b200 as dg
+
+        sc, off = dg.int8_params(X)
+        o.set_int8(sc, off, oracle.int8_encode(X, sc, off))
+    return o
+
+
+def _oracle_run(o, name, Qs, L, threads):
+    # bf16_rerank runs as its FP32 equivalent on the CPU: the BF16 copy of
+    # integer-valued rows is exact, so both give the same ids and distances
+    if name in ("fp32", "bf16_rerank"):
+        return o.search(Qs, K, L, threads=threads)
+    return o.search(Qs, K, L, rerank=L, use_codes=True, threads=threads)
+
+
+def cpu_baseline(args, X, Q, adj, med, pq, name, L, threads=None):
+    threads = threads or os.cpu_count() or 1
+    o = _oracle_index(X, adj, med, pq, name)
+    t0 = time.time()
+    _oracle_run(o, name, Q[:200], L, threads)
+    rate = 200 / max(time.time() - t0, 1e-6)
+    ns = int(min(len(Q), max(200, rate * args.cpu_seconds)))
+    t0 = time.time()
+    _oracle_run(o, name, Q[:ns], L, threads)
+    dt = time.time() - t0
+    return {"value": ns / dt, "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"{ns} of the {len(Q)} queries, variant {name} at L={L}, same graph/codes",
+            "seconds": round(dt, 2)}
+
+
+def reference_arm(args):
+    """The reference's plain search (DiskANN::search, CPU restatement, all host
+    threads) at the smallest beam reaching the recall target, on the workload
+    of the GPU arm.  Under torchrun only rank 0 works."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = workload(args, 0, build=False)
+    if wl is None:
+        # the graph and codebooks are inputs of the search; they are built once
+        # with the GPU builder and cached for both arms
+        wl = workload(args, 0, build=True)
+    X, Q, adj, med, pq, gt, _ = wl
+    threads = os.cpu_count() or 1
+    name = "fp32"
+    o = _oracle_index(X, adj, med, pq, name)
+    # beam sweep on a 1000-query sample
+    ns = min(1000, len(Q))
+    L = L_SWEEP[-1]
+    for Lc in L_SWEEP:
+        ids, _, _ = _oracle_run(o, name, Q[:ns], Lc, threads)
+        if recall(ids, gt[:ns]) >= args.target_recall:
+            L = Lc
+            break
+    t0 = time.time()
+    _oracle_run(o, name, Q[:200], L, threads)
+    rate = 200 / max(time.time() - t0, 1e-6)
+    per_step = int(min(len(Q), max(100, rate * 6.0)))
+    for _ in range(args.warmup):
+        _oracle_run(o, name, Q[:min(per_step, 200)], L, threads)
+    t0 = time.time()
+    ids_all = []
+    for s in range(args.steps):
+        lo = (s * per_step) % len(Q)
+        qs = Q[lo:lo + per_step]
+        ids, _, _ = _oracle_run(o, name, qs, L, threads)
+        ids_all.append((lo, ids))
+    dt = time.time() - t0
+    nq_done = sum(len(ids) for _, ids in ids_all)
+    qps = nq_done / dt
+    rec = float(np.mean([recall(ids, gt[lo:lo + len(ids)]) for lo, ids in ids_all]))
+    line = {
+        "impl": "reference",
+        "metric": "QPS @ recall@10=0.95, plain FP32 vs BF16+FP32-rerank, 1 B200; p99 ms",
+        "value": qps, "unit": "queries/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 256-centre Gaussian mixture, 1M x 128, 10k queries)",
+        "config": {"workload": f"pq-1Mx128 M={M} R={R} L_build={L_BUILD} alpha={ALPHA} k={K} "
+                               f"nq={args.nq} n={args.n}", "variant": name, "L": L,
+                   "recall_at_10": round(rec, 4)},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"{per_step} queries per step, plain FP32 beam search (CPU restatement "
+                                   f"of the reference search, OpenMP over queries)"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main() or 0)

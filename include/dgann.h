@@ -77,6 +77,7 @@ typedef struct {
 } DgFilterOp;
 
 #define DG_FLAG_DEVICE_PTRS 1u /* queries / outputs are device pointers */
+#define DG_FLAG_STREAM 2u      /* run on `stream` as given; NULL = the legacy default stream */
 
 typedef struct DgIndex DgIndex;
 
@@ -133,7 +134,7 @@ typedef struct {
   uint32_t filter_pool_len;
   const uint32_t *per_query_beam; /* optional u32[nq] host array of per-query L */
   uint32_t flags;                 /* DG_FLAG_* */
-  void *stream;                   /* cudaStream_t or NULL */
+  void *stream;                   /* cudaStream_t; without DG_FLAG_STREAM, NULL = the handle's stream */
 } DgSearchParams;
 
 /* Batched search.  Stands in for DiskANN::search_with_dists (src/lib.rs:683-714),

@@ -314,7 +314,8 @@ class _Index:
                        torch.empty((nq, k), dtype=torch.float32, device=Q.device),
                        torch.empty((nq,), dtype=torch.int32, device=Q.device))
             stats = torch.empty((nq, 2), dtype=torch.int32, device=Q.device) if with_stats else None
-            p.flags = _lib.FLAG_DEVICE_PTRS
+            # ordered on the caller's torch stream (handle 0 is the legacy default stream)
+            p.flags = _lib.FLAG_DEVICE_PTRS | _lib.FLAG_STREAM
             p.stream = stream if stream is not None else torch.cuda.current_stream(Q.device).cuda_stream
         else:
             Q = _f32(queries)
@@ -328,6 +329,7 @@ class _Index:
                        np.empty((nq,), dtype=np.uint32))
             stats = np.empty((nq, 2), dtype=np.uint32) if with_stats else None
             if stream is not None:
+                p.flags = _lib.FLAG_STREAM
                 p.stream = stream
         if filters is not None:
             if isinstance(filters, Filter):

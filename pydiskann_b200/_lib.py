@@ -19,6 +19,7 @@ TRAVERSE_F32, TRAVERSE_BF16, TRAVERSE_CODES = 0, 1, 2
 Q_NONE, Q_PQ, Q_INT8, Q_RABITQ, Q_F16 = 0, 1, 2, 3, 4
 F_TRUE, F_EQ, F_IN, F_LT, F_GT, F_RANGE, F_AND, F_OR = range(8)
 FLAG_DEVICE_PTRS = 1
+FLAG_STREAM = 2
 PAD = 0xFFFFFFFF
 PAD64 = 0xFFFFFFFFFFFFFFFF
 

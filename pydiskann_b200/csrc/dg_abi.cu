@@ -368,7 +368,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
 
   std::lock_guard<std::mutex> lk(idx->mu);
   DG_CUDA(cudaSetDevice(idx->device));
-  cudaStream_t st = p->stream ? (cudaStream_t)p->stream : idx->stream;
+  cudaStream_t st = (p->flags & DG_FLAG_STREAM) || p->stream ? (cudaStream_t)p->stream : idx->stream;
   DgIndex::Slot &sl = idx->slots[idx->next_slot];
   idx->next_slot = (idx->next_slot + 1) % DgIndex::kSlots;
   if (sl.pending) {
