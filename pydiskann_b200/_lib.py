@@ -11,7 +11,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdgann.so")
+# DGANN_LIBRARY points at a libdgann.so built elsewhere (e.g. another tuning)
+LIB_PATH = os.environ.get("DGANN_LIBRARY", os.path.join(HERE, "libdgann.so"))
 
 DG_OK, DG_EINVAL, DG_ENOMEM, DG_ETIMEOUT, DG_EDEVICE, DG_ENOTSUP = range(6)
 L2SQ, L2, COSINE, DOT = 0, 1, 2, 3

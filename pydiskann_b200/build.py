@@ -50,22 +50,30 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False, defines=(),
+          obj_dir: str | None = None, lib_path: str | None = None) -> str:
+    """Compile every csrc/*.cu and link the library (only stale objects rebuild).
+
+    `defines` adds -D flags (tuning knobs such as DG_SEARCH_MIN_BLOCKS);
+    obj_dir / lib_path place an alternative build elsewhere.
+    """
+    OBJ_ = obj_dir or OBJ
+    LIB_ = lib_path or LIB
+    os.makedirs(OBJ_, exist_ok=True)
     nvcc = _nvcc()
     hdrs = _headers()
     srcs = _sources()
     objs = []
     todo = []
     for s in srcs:
-        o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
+        o = os.path.join(OBJ_, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             todo.append((s, o))
 
     def compile_one(so):
         s, o = so
-        cmd = [nvcc] + NVCC_FLAGS + ["-c", s, "-o", o]
+        cmd = [nvcc] + NVCC_FLAGS + [f"-D{d}" for d in defines] + ["-c", s, "-o", o]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {s}:\n{r.stderr[-6000:]}")
@@ -77,12 +85,12 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         jobs = jobs or min(len(todo), os.cpu_count() or 4)
         with cf.ThreadPoolExecutor(jobs) as ex:
             list(ex.map(compile_one, todo))
-    if force or todo or _stale(LIB, objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if force or todo or _stale(LIB_, objs):
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB_] + objs + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
-    return LIB
+    return LIB_
 
 
 if __name__ == "__main__":
@@ -90,5 +98,8 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-j", type=int, default=None)
     ap.add_argument("-v", action="store_true")
+    ap.add_argument("-D", action="append", default=[], help="extra preprocessor define")
+    ap.add_argument("--obj-dir", default=None)
+    ap.add_argument("--lib", default=None)
     a = ap.parse_args()
-    print(build(a.force, a.j, a.v))
+    print(build(a.force, a.j, a.v, a.D, a.obj_dir, a.lib))

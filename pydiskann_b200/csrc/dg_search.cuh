@@ -152,6 +152,55 @@ __device__ __forceinline__ int prepare_batch(uint64_t key, const uint64_t *list,
   return __popc(m);
 }
 
+// Inserts one batch of candidate keys (one per lane, kKeyInvalid = none) into
+// the sorted double-buffered list bufs[cur][0..size) of capacity cap.
+// Keys at or above the worst entry of a full list are dropped before any
+// sorting (late in a search almost every candidate is), a handful of
+// survivors are ranked with shuffles, larger batches go through the warp
+// bitonic sort.  Duplicates (within the batch or already listed) are dropped.
+// Same result as prepare_batch + merge_keys; returns the number inserted.
+__device__ __forceinline__ int insert_batch(uint64_t key, uint64_t *const bufs[2], int &cur, int &size,
+                                            int cap, uint64_t *cst, int lane) {
+  const uint64_t *list = bufs[cur];
+  const uint64_t thr = size >= cap ? strip_flag(list[cap - 1]) : kKeyInvalid;
+  const bool surv = key < thr;
+  const uint32_t m = __ballot_sync(kFull, surv);
+  if (!m) return 0;
+  const int s = __popc(m);
+  int nc;
+  if (s <= 8) {
+    if (surv) cst[__popc(m & lanemask_lt(lane))] = key;
+    __syncwarp();
+    const uint64_t k = lane < s ? cst[lane] : kKeyInvalid;
+    bool alive = lane < s;
+    if (alive) {
+      const int pos = lower_bound_smem(list, size, k);
+      if (pos < size && strip_flag(list[pos]) == k) alive = false;
+    }
+    for (int i = 0; i < s; ++i) {
+      const uint64_t o = shfl64(k, i);
+      if (i < lane && o == k) alive = false;
+    }
+    const uint32_t am = __ballot_sync(kFull, alive);
+    int rank = 0;
+    for (int i = 0; i < s; ++i) {
+      const uint64_t o = shfl64(k, i);
+      if (((am >> i) & 1u) && o < k) ++rank;
+    }
+    __syncwarp();
+    if (alive) cst[rank] = k;
+    __syncwarp();
+    nc = __popc(am);
+  } else {
+    nc = prepare_batch(surv ? key : kKeyInvalid, list, size, cap, cst, lane);
+  }
+  if (nc > 0) {
+    size = merge_keys(list, size, bufs[cur ^ 1], cap, cst, nc, lane);
+    cur ^= 1;
+  }
+  return nc;
+}
+
 // Ascending bitonic sort of a[0..n) in shared memory by one warp (n <= 2048).
 __device__ __forceinline__ void warp_sort_smem(uint64_t *a, int n, int lane) {
   int p2 = 1;
@@ -223,7 +272,9 @@ __device__ __forceinline__ float finish_metric(int met, bool sqrt_l2, float a, f
 
 // Distance of lane j's candidate `cand` (valid when j < cnt) against the
 // query held in shared memory (qs, f32, dpad long).  rows: base pointer, row
-// stride in bytes; chunks = row bytes / 16.
+// stride in bytes; chunks = row bytes / 16.  Each round issues the loads of
+// all LPR row slots before any arithmetic, so a warp keeps LPR 16-byte loads
+// per lane in flight.
 template <int LPR, int ELEM, int MET>
 __device__ __forceinline__ float rows_distance(const uint8_t *__restrict__ rows, uint32_t stride,
                                                int loads, const float *qs, uint32_t cand, int cnt,
@@ -232,31 +283,37 @@ __device__ __forceinline__ float rows_distance(const uint8_t *__restrict__ rows,
   constexpr int EPC = Chunk<ELEM>::EPC;
   const int g = lane / LPR, r = lane % LPR;
   float pa[LPR], pb[LPR];
+  uint32_t ids[LPR];  // DG_PAD marks an empty slot
 #pragma unroll
-  for (int i = 0; i < LPR; ++i) { pa[i] = 0.0f; pb[i] = 0.0f; }
+  for (int i = 0; i < LPR; ++i) {
+    pa[i] = 0.0f;
+    pb[i] = 0.0f;
+    const int c = i * RPI + g;
+    const uint32_t id = __shfl_sync(kFull, cand, c & 31);
+    ids[i] = c < cnt ? id : DG_PAD;
+  }
   for (int t = 0; t < loads; ++t) {
     const int chunk = r + LPR * t;
+    uint4 v[LPR];
+#pragma unroll
+    for (int i = 0; i < LPR; ++i)
+      if (ids[i] != DG_PAD) v[i] = __ldg(reinterpret_cast<const uint4 *>(rows + (size_t)ids[i] * stride) + chunk);
     float qv[EPC];
 #pragma unroll
     for (int e = 0; e < EPC; ++e) qv[e] = qs[chunk * EPC + e];
 #pragma unroll
     for (int i = 0; i < LPR; ++i) {
-      if (i * RPI < cnt) {  // warp-uniform
-        const int c = i * RPI + g;
-        const uint32_t id = __shfl_sync(kFull, cand, c & 31);
-        if (c < cnt) {
-          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(rows + (size_t)id * stride) + chunk);
-          float x[EPC];
-          Chunk<ELEM>::unpack(v, x);
+      if (ids[i] != DG_PAD) {
+        float x[EPC];
+        Chunk<ELEM>::unpack(v[i], x);
 #pragma unroll
-          for (int e = 0; e < EPC; ++e) {
-            if (MET == MET_L2) {
-              float df = x[e] - qv[e];
-              pa[i] = fmaf(df, df, pa[i]);
-            } else {
-              pa[i] = fmaf(x[e], qv[e], pa[i]);
-              if (MET == MET_COS) pb[i] = fmaf(x[e], x[e], pb[i]);
-            }
+        for (int e = 0; e < EPC; ++e) {
+          if (MET == MET_L2) {
+            float df = x[e] - qv[e];
+            pa[i] = fmaf(df, df, pa[i]);
+          } else {
+            pa[i] = fmaf(x[e], qv[e], pa[i]);
+            if (MET == MET_COS) pb[i] = fmaf(x[e], x[e], pb[i]);
           }
         }
       }
@@ -280,25 +337,30 @@ __device__ __forceinline__ uint32_t int8_l2_group(const uint8_t *__restrict__ co
   constexpr int RPI = 32 / LPR;
   const int g = lane / LPR, r = lane % LPR;
   uint32_t p[LPR];
+  uint32_t ids[LPR];  // DG_PAD marks an empty slot
 #pragma unroll
-  for (int i = 0; i < LPR; ++i) p[i] = 0;
+  for (int i = 0; i < LPR; ++i) {
+    p[i] = 0;
+    const int c = i * RPI + g;
+    const uint32_t id = __shfl_sync(kFull, cand, c & 31);
+    ids[i] = c < cnt ? id : DG_PAD;
+  }
   for (int t = 0; t < loads; ++t) {
     const int chunk = r + LPR * t;
+    uint4 v[LPR];
+#pragma unroll
+    for (int i = 0; i < LPR; ++i)
+      if (ids[i] != DG_PAD) v[i] = __ldg(reinterpret_cast<const uint4 *>(codes + (size_t)ids[i] * stride) + chunk);
     const uint4 qv = *reinterpret_cast<const uint4 *>(qcode + chunk * 16);
 #pragma unroll
     for (int i = 0; i < LPR; ++i) {
-      if (i * RPI < cnt) {
-        const int c = i * RPI + g;
-        const uint32_t id = __shfl_sync(kFull, cand, c & 31);
-        if (c < cnt) {
-          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(codes + (size_t)id * stride) + chunk);
-          uint32_t a0 = __vabsdiffu4(v.x, qv.x), a1 = __vabsdiffu4(v.y, qv.y);
-          uint32_t a2 = __vabsdiffu4(v.z, qv.z), a3 = __vabsdiffu4(v.w, qv.w);
-          p[i] = __dp4a(a0, a0, p[i]);
-          p[i] = __dp4a(a1, a1, p[i]);
-          p[i] = __dp4a(a2, a2, p[i]);
-          p[i] = __dp4a(a3, a3, p[i]);
-        }
+      if (ids[i] != DG_PAD) {
+        const uint32_t a0 = __vabsdiffu4(v[i].x, qv.x), a1 = __vabsdiffu4(v[i].y, qv.y);
+        const uint32_t a2 = __vabsdiffu4(v[i].z, qv.z), a3 = __vabsdiffu4(v[i].w, qv.w);
+        p[i] = __dp4a(a0, a0, p[i]);
+        p[i] = __dp4a(a1, a1, p[i]);
+        p[i] = __dp4a(a2, a2, p[i]);
+        p[i] = __dp4a(a3, a3, p[i]);
       }
     }
   }
@@ -316,27 +378,33 @@ __device__ __forceinline__ float int8_decode_group(const uint8_t *__restrict__ c
   constexpr int RPI = 32 / LPR;
   const int g = lane / LPR, r = lane % LPR;
   float pa[LPR], pb[LPR];
+  uint32_t ids[LPR];  // DG_PAD marks an empty slot
 #pragma unroll
-  for (int i = 0; i < LPR; ++i) { pa[i] = 0.0f; pb[i] = 0.0f; }
+  for (int i = 0; i < LPR; ++i) {
+    pa[i] = 0.0f;
+    pb[i] = 0.0f;
+    const int c = i * RPI + g;
+    const uint32_t id = __shfl_sync(kFull, cand, c & 31);
+    ids[i] = c < cnt ? id : DG_PAD;
+  }
   for (int t = 0; t < loads; ++t) {
     const int chunk = r + LPR * t;
+    uint4 v[LPR];
+#pragma unroll
+    for (int i = 0; i < LPR; ++i)
+      if (ids[i] != DG_PAD) v[i] = __ldg(reinterpret_cast<const uint4 *>(codes + (size_t)ids[i] * stride) + chunk);
 #pragma unroll
     for (int i = 0; i < LPR; ++i) {
-      if (i * RPI < cnt) {
-        const int c = i * RPI + g;
-        const uint32_t id = __shfl_sync(kFull, cand, c & 31);
-        if (c < cnt) {
-          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(codes + (size_t)id * stride) + chunk);
-          const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+      if (ids[i] != DG_PAD) {
+        const uint32_t w[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
 #pragma unroll
-          for (int e = 0; e < 16; ++e) {
-            // padding columns beyond the dimension decode to nothing
-            float x = (uint32_t)(chunk * 16 + e) < dlim
-                          ? __fadd_rn(__fmul_rn((float)((w[e >> 2] >> (8 * (e & 3))) & 0xffu), scale), offset)
-                          : 0.0f;
-            pa[i] = fmaf(x, qs[chunk * 16 + e], pa[i]);
-            if (MET == MET_COS) pb[i] = fmaf(x, x, pb[i]);
-          }
+        for (int e = 0; e < 16; ++e) {
+          // padding columns beyond the dimension decode to nothing
+          float x = (uint32_t)(chunk * 16 + e) < dlim
+                        ? __fadd_rn(__fmul_rn((float)((w[e >> 2] >> (8 * (e & 3))) & 0xffu), scale), offset)
+                        : 0.0f;
+          pa[i] = fmaf(x, qs[chunk * 16 + e], pa[i]);
+          if (MET == MET_COS) pb[i] = fmaf(x, x, pb[i]);
         }
       }
     }

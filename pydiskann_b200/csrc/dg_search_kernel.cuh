@@ -201,11 +201,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
       uint64_t key = lane < cnt ? make_key(d, cand) : kKeyInvalid;
       bool match = false;
       if (filtered && lane < cnt) match = allow(cand);
-      const int nc = prepare_batch(key, W[cur], wsize, (int)working, cst, lane);
-      if (nc > 0) {
-        wsize = merge_keys(W[cur], wsize, W[cur ^ 1], (int)working, cst, nc, lane);
-        cur ^= 1;
-      }
+      insert_batch(key, W, cur, wsize, (int)working, cst, lane);
       if (filtered) {
         // result list: every visited match, kept as the search_k smallest
         uint64_t mk = (lane < cnt && match) ? make_key(d, cand) : kKeyInvalid;
@@ -265,8 +261,13 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
   __syncwarp();
 }
 
+// Resident blocks per SM the register allocation is sized for (4 warps each).
+#ifndef DG_SEARCH_MIN_BLOCKS
+#define DG_SEARCH_MIN_BLOCKS 6
+#endif
+
 template <int TRAV, int MET, int LPR, int LPRF, int LCAP, bool FILT>
-__global__ void __launch_bounds__(128) beam_search_kernel(SearchArgs a, WarpLayout Ly) {
+__global__ void __launch_bounds__(128, DG_SEARCH_MIN_BLOCKS) beam_search_kernel(SearchArgs a, WarpLayout Ly) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t *wsm = smem + (size_t)warp * Ly.total;

@@ -189,11 +189,7 @@ __global__ void __launch_bounds__(128) k_build_search(BuildArgs a, WarpLayout Ly
               ELEM == 1 ? a.dpad * 2 : a.dpad * 4, ELEM == 1 ? (a.dpad / 8) / LPR : (a.dpad / 4) / LPR,
               qs, c, cnt, lane, a.metric == DG_L2, qq);
           const uint64_t key = lane < cnt ? make_key(dd, c) : kKeyInvalid;
-          const int nc = prepare_batch(key, W[cur], wsize, (int)a.Lb, cst, lane);
-          if (nc > 0) {
-            wsize = merge_keys(W[cur], wsize, W[cur ^ 1], (int)a.Lb, cst, nc, lane);
-            cur ^= 1;
-          }
+          insert_batch(key, W, cur, wsize, (int)a.Lb, cst, lane);
         }
       }
       for (int i = lane; i < wsize; i += 32) out[nout + i] = strip_flag(W[cur][i]);
