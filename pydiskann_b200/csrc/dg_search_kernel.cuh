@@ -64,6 +64,267 @@ __device__ __forceinline__ uint32_t vhash(uint32_t id, uint32_t hbits) {
   return (id * 2654435761u) >> (32 - hbits);
 }
 
+// Per-query quantizer state (QuantizerState::prepare, src/quantized.rs:167-174).
+template <int TRAV>
+__device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm, const WarpLayout &Ly,
+                                              const float *qs, int lane) {
+  if (TRAV == TRAV_PQ) {
+    build_pq_lut(a, qs, reinterpret_cast<float *>(wsm + Ly.prov), lane);
+  } else if (TRAV == TRAV_INT8) {
+    uint8_t *qc8 = wsm + Ly.prov;
+    const float inv = __fdiv_rn(1.0f, a.i8_scale);
+    const float beta = __fdiv_rn(-a.i8_offset, a.i8_scale);
+    for (uint32_t i = lane; i < a.dpad; i += 32) qc8[i] = i < a.d ? int8_code(qs[i], inv, beta) : 0;
+  } else if (TRAV == TRAV_F16) {
+    float *qh = reinterpret_cast<float *>(wsm + Ly.prov);
+    for (uint32_t i = lane; i < a.dpad; i += 32) qh[i] = __half2float(__float2half_rn(qs[i]));
+  } else if (TRAV == TRAV_RABITQ) {
+    uint8_t *p = wsm + Ly.prov;
+    uint64_t *planes = reinterpret_cast<uint64_t *>(p);
+    float *k5 = reinterpret_cast<float *>(p + 4 * (a.rq_padded / 64) * 8);
+    float *rbuf = reinterpret_cast<float *>(p + 4 * (a.rq_padded / 64) * 8 + 32);
+    rabitq_prepare(qs, a.d, a.rq_padded, a.rq_centroid, a.rq_signs, rbuf, planes, k5, lane);
+  }
+  __syncwarp();
+}
+
+// Writes a query's results: the first k of src (sorted keys), or, with
+// rerank, the first max(rerank, k) reranked with exact FP32 distances in
+// their traversal order (a stable sort by exact distance, src/quantized.rs:110-121).
+template <int TRAV, int MET, int LPRF>
+__device__ inline void emit_results(const SearchArgs &a, uint32_t q, const uint64_t *src, int have,
+                                    bool use_rerank, uint32_t search_k, uint64_t *tmp, const float *qs,
+                                    float qq, uint32_t n_exp, uint32_t n_dist, int lane) {
+  const uint32_t k = a.k;
+  uint32_t *oid = a.out_ids + (size_t)q * k;
+  float *od = a.out_d + (size_t)q * k;
+  int count;
+  if (use_rerank) {
+    const int nr = min(have, (int)search_k);
+    for (int g0 = 0; g0 < nr; g0 += 32) {
+      const int cnt = min(32, nr - g0);
+      const uint32_t cand = lane < cnt ? key_id(src[g0 + lane]) : 0u;
+      const float d = exact_distance<MET, LPRF>(a, qs, cand, cnt, lane, qq);
+      if (lane < cnt) tmp[g0 + lane] = make_key_payload(d, (uint32_t)(g0 + lane));
+    }
+    __syncwarp();
+    warp_sort_smem(tmp, nr, lane);
+    count = min(nr, (int)k);
+    for (int i = lane; i < count; i += 32) {
+      const uint64_t kk = tmp[i];
+      oid[i] = key_id(src[key_id(kk)]);
+      od[i] = key_dist(kk);
+    }
+  } else {
+    count = min(have, (int)k);
+    for (int i = lane; i < count; i += 32) {
+      oid[i] = key_id(src[i]);
+      od[i] = key_dist(src[i]);
+    }
+  }
+  for (int i = count + lane; i < (int)k; i += 32) {
+    oid[i] = DG_PAD;
+    od[i] = __int_as_float(0x7f800000);
+  }
+  if (lane == 0) {
+    a.out_cnt[q] = (uint32_t)count;
+    if (a.out_stats) {
+      a.out_stats[2 * q] = n_exp;
+      a.out_stats[2 * q + 1] = n_dist;
+    }
+  }
+  __syncwarp();
+}
+
+// Inserts the ns keys of skeys[] into a register-resident sorted list of at
+// most 64 entries (entry i in lane i % 32: w0 for i < 32, w1 above) with
+// capacity cap.  Keys not below a full list's worst entry, keys already listed
+// and repeats within the batch are dropped.
+__device__ __forceinline__ void reg_insert(const uint64_t *skeys, int ns, uint64_t &w0, uint64_t &w1,
+                                           int &wsize, int cap, uint64_t *scat, uint64_t *cst, int lane) {
+  for (int b0 = 0; b0 < ns; b0 += 32) {
+    const int cnt = min(32, ns - b0);
+    uint64_t kk = lane < cnt ? skeys[b0 + lane] : kKeyInvalid;
+    if (wsize >= cap) {
+      const uint64_t thr = strip_flag(shfl64(cap - 1 < 32 ? w0 : w1, (cap - 1) & 31));
+      if (!(kk < thr)) kk = kKeyInvalid;
+    }
+    const uint32_t vm = __ballot_sync(kFull, kk != kKeyInvalid);
+    const int s = __popc(vm);
+    if (s == 0) continue;
+    // survivors sorted ascending into lanes 0..s-1, repeats flagged dead
+    uint64_t ck;
+    bool alive;
+    if (s > 8) {
+      ck = warp_sort_keys(kk, lane);
+      const uint64_t prev = shfl64(ck, lane > 0 ? lane - 1 : 0);
+      alive = lane < s && !(lane > 0 && prev == ck);
+    } else {
+      if (kk != kKeyInvalid) cst[__popc(vm & lanemask_lt(lane))] = kk;
+      __syncwarp();
+      const uint64_t u = lane < s ? cst[lane] : kKeyInvalid;
+      bool al = lane < s;
+      int rank = 0;
+      for (int i = 0; i < s; ++i) {
+        const uint64_t o = shfl64(u, i);
+        if (o < u) ++rank;
+        if (i < lane && o == u) al = false;
+      }
+      __syncwarp();
+      if (al) cst[rank] = u;  // distinct keys: ranks are a permutation of the alive ones
+      const uint32_t am = __ballot_sync(kFull, al);
+      __syncwarp();
+      const int na = __popc(am);
+      ck = lane < na ? cst[lane] : kKeyInvalid;
+      alive = lane < na;
+      __syncwarp();
+    }
+    // rank of every survivor in the list, listed duplicates, and the shift
+    // of every list entry
+    const uint64_t s0 = strip_flag(w0), s1 = strip_flag(w1);
+    int mypos = 0, c0 = 0, c1 = 0;
+    bool myalive = false;
+    const int sn = __popc(__ballot_sync(kFull, lane < 32 && (alive || lane < s)));
+    for (int t = 0; t < sn; ++t) {
+      const uint64_t kt = shfl64(ck, t);
+      const bool at = __shfl_sync(kFull, alive, t);
+      if (!at) continue;  // uniform
+      const uint32_t lt0 = __ballot_sync(kFull, s0 < kt), lt1 = __ballot_sync(kFull, s1 < kt);
+      const bool dup = __any_sync(kFull, s0 == kt || s1 == kt);
+      if (lane == t) {
+        mypos = __popc(lt0) + __popc(lt1);
+        myalive = !dup;
+      }
+      if (!dup) {
+        c0 += kt < s0;
+        c1 += kt < s1;
+      }
+    }
+    const uint32_t am = __ballot_sync(kFull, myalive);
+    const int nc = __popc(am);
+    if (nc == 0) continue;
+    if (myalive) {
+      const int np = mypos + __popc(am & lanemask_lt(lane));
+      if (np < cap) scat[np] = ck;
+    }
+    if (lane < wsize && lane + c0 < cap) scat[lane + c0] = w0;
+    if (lane + 32 < wsize && lane + 32 + c1 < cap) scat[lane + 32 + c1] = w1;
+    __syncwarp();
+    wsize = min(cap, wsize + nc);
+    w0 = lane < wsize ? scat[lane] : kKeyInvalid;
+    w1 = lane + 32 < wsize ? scat[lane + 32] : kKeyInvalid;
+    __syncwarp();
+  }
+}
+
+// Unfiltered search with beams up to 64: the working list lives in registers,
+// entry i in lane i % 32 (w0 for i < 32, w1 above), so finding the frontier,
+// the threshold and insertion ranks are ballots and shuffles instead of
+// shared-memory binary searches.  Results are identical to search_one.
+template <int TRAV, int MET, int LPR, int LPRF>
+__device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *wsm, const WarpLayout &Ly,
+                                      int lane) {
+  uint64_t *scat = reinterpret_cast<uint64_t *>(wsm + Ly.w0);  // scatter buffer, 64 keys
+  uint64_t *skeys = reinterpret_cast<uint64_t *>(wsm + Ly.w1) ; // survivors of one expansion (<= 64)
+  uint64_t *cst = reinterpret_cast<uint64_t *>(wsm + Ly.cstage);
+  uint32_t *stage = reinterpret_cast<uint32_t *>(wsm + Ly.stage);
+  uint32_t *hash = reinterpret_cast<uint32_t *>(wsm + Ly.hash);
+  float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
+  const uint32_t hsz = 1u << a.hbits;
+  const int L = (int)(a.perL ? a.perL[q] : a.L);
+  const uint32_t k = a.k;
+  const bool use_rerank = TRAV != TRAV_F32 && a.rerank > 0;
+  const uint32_t search_k = use_rerank ? max(a.rerank, k) : k;
+
+  const float *qg = a.Q + (size_t)q * a.d;
+  for (uint32_t i = lane; i < a.dpad; i += 32) qs[i] = i < a.d ? qg[i] : 0.0f;
+  for (uint32_t i = lane; i < hsz; i += 32) hash[i] = DG_PAD;
+  __syncwarp();
+  float qq = 0.0f;
+  if (MET == MET_COS) {
+    for (uint32_t i = lane; i < a.dpad; i += 32) qq = fmaf(qs[i], qs[i], qq);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) qq += __shfl_xor_sync(kFull, qq, o);
+  }
+  prepare_query<TRAV>(a, wsm, Ly, qs, lane);
+
+  uint64_t w0 = kKeyInvalid, w1 = kKeyInvalid;
+  int wsize = 1;
+  uint32_t n_exp = 0, n_dist = 1;
+  {
+    const uint32_t cand = a.medoid;
+    float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, 1, lane, qq);
+    d = __shfl_sync(kFull, d, 0);
+    if (lane == 0) {
+      w0 = make_key(d, cand);
+      hash[vhash(cand, a.hbits)] = cand;
+    }
+    __syncwarp();
+  }
+  while (true) {
+    const uint32_t m0 = __ballot_sync(kFull, lane < wsize && !key_expanded(w0));
+    const uint32_t m1 = __ballot_sync(kFull, lane + 32 < wsize && !key_expanded(w1));
+    const int idx = m0 ? __ffs(m0) - 1 : (m1 ? 31 + __ffs(m1) : -1);
+    if (idx < 0) break;
+    const uint64_t best = shfl64(idx < 32 ? w0 : w1, idx & 31);
+    uint64_t thr = kKeyInvalid;
+    if (wsize >= L) {
+      const uint64_t worst = shfl64(L - 1 < 32 ? w0 : w1, (L - 1) & 31);
+      if (key_dist(best) >= key_dist(worst)) break;  // src/lib.rs:253-259
+      thr = strip_flag(worst);
+    }
+    if (lane == (idx & 31)) {
+      if (idx < 32) w0 |= 1ull;
+      else w1 |= 1ull;
+    }
+    ++n_exp;
+    // stage unvisited neighbours
+    const uint32_t *row = a.adj + (size_t)key_id(best) * a.R;
+    int ns = 0;
+    for (uint32_t j0 = 0; j0 < a.R; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      const uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
+      bool ok = nb != DG_PAD && nb < a.n;
+      if (ok) ok = hash[vhash(nb, a.hbits)] != nb;
+      const uint32_t m = __ballot_sync(kFull, ok);
+      if (ok) {
+        stage[ns + __popc(m & lanemask_lt(lane))] = nb;
+        hash[vhash(nb, a.hbits)] = nb;
+      }
+      ns += __popc(m);
+    }
+    __syncwarp();
+    n_dist += ns;
+    // distances; keep only keys below the current worst (the rest cannot enter)
+    int nsurv = 0;
+    for (int g0 = 0; g0 < ns; g0 += 32) {
+      if (nsurv > 32) {  // the 64-key survivor buffer could overflow: insert what it holds
+        __syncwarp();
+        reg_insert(skeys, nsurv, w0, w1, wsize, L, scat, cst, lane);
+        nsurv = 0;
+        thr = wsize >= L ? strip_flag(shfl64(L - 1 < 32 ? w0 : w1, (L - 1) & 31)) : kKeyInvalid;
+      }
+      const int cnt = min(32, ns - g0);
+      const uint32_t cand = lane < cnt ? stage[g0 + lane] : DG_PAD;
+      const float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, cnt, lane, qq);
+      const uint64_t key = lane < cnt ? make_key(d, cand) : kKeyInvalid;
+      const bool sv = key < thr;
+      const uint32_t m = __ballot_sync(kFull, sv);
+      if (sv) skeys[nsurv + __popc(m & lanemask_lt(lane))] = key;
+      nsurv += __popc(m);
+    }
+    __syncwarp();
+    if (nsurv) reg_insert(skeys, nsurv, w0, w1, wsize, L, scat, cst, lane);
+  }
+  // emit through the shared-memory path
+  uint64_t *Wm = scat;
+  if (lane < wsize) Wm[lane] = w0;
+  if (lane + 32 < wsize) Wm[lane + 32] = w1;
+  __syncwarp();
+  emit_results<TRAV, MET, LPRF>(a, q, Wm, wsize, use_rerank, search_k, reinterpret_cast<uint64_t *>(wsm + Ly.w1),
+                                qs, qq, n_exp, n_dist, lane);
+}
+
 template <int TRAV, int MET, int LPR, int LPRF, int LCAP, bool FILT>
 __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm, const WarpLayout &Ly,
                            int lane) {
@@ -105,25 +366,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) qq += __shfl_xor_sync(kFull, qq, o);
   }
-  // ---- per-query quantizer state (QuantizerState::prepare, src/quantized.rs:167-174)
-  if (TRAV == TRAV_PQ) {
-    build_pq_lut(a, qs, reinterpret_cast<float *>(wsm + Ly.prov), lane);
-  } else if (TRAV == TRAV_INT8) {
-    uint8_t *qc8 = wsm + Ly.prov;
-    const float inv = __fdiv_rn(1.0f, a.i8_scale);
-    const float beta = __fdiv_rn(-a.i8_offset, a.i8_scale);
-    for (uint32_t i = lane; i < a.dpad; i += 32) qc8[i] = i < a.d ? int8_code(qs[i], inv, beta) : 0;
-  } else if (TRAV == TRAV_F16) {
-    float *qh = reinterpret_cast<float *>(wsm + Ly.prov);
-    for (uint32_t i = lane; i < a.dpad; i += 32) qh[i] = __half2float(__float2half_rn(qs[i]));
-  } else if (TRAV == TRAV_RABITQ) {
-    uint8_t *p = wsm + Ly.prov;
-    uint64_t *planes = reinterpret_cast<uint64_t *>(p);
-    float *k5 = reinterpret_cast<float *>(p + 4 * (a.rq_padded / 64) * 8);
-    float *rbuf = reinterpret_cast<float *>(p + 4 * (a.rq_padded / 64) * 8 + 32);
-    rabitq_prepare(qs, a.d, a.rq_padded, a.rq_centroid, a.rq_signs, rbuf, planes, k5, lane);
-  }
-  __syncwarp();
+  prepare_query<TRAV>(a, wsm, Ly, qs, lane);
 
   const uint64_t *labels = a.labels;
   auto allow = [&](uint32_t id) -> bool {
@@ -218,47 +461,8 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
   }
 
   // ---- emit
-  const uint64_t *src = filtered ? RES : W[cur];
-  const int have = filtered ? rsize : wsize;
-  uint32_t *oid = a.out_ids + (size_t)q * k;
-  float *od = a.out_d + (size_t)q * k;
-  int count;
-  if (use_rerank) {
-    const int nr = min(have, (int)search_k);
-    uint64_t *tmp = W[cur ^ 1];
-    for (int g0 = 0; g0 < nr; g0 += 32) {
-      const int cnt = min(32, nr - g0);
-      const uint32_t cand = lane < cnt ? key_id(src[g0 + lane]) : 0u;
-      const float d = exact_distance<MET, LPRF>(a, qs, cand, cnt, lane, qq);
-      if (lane < cnt) tmp[g0 + lane] = make_key_payload(d, (uint32_t)(g0 + lane));
-    }
-    __syncwarp();
-    warp_sort_smem(tmp, nr, lane);
-    count = min(nr, (int)k);
-    for (int i = lane; i < count; i += 32) {
-      const uint64_t kk = tmp[i];
-      oid[i] = key_id(src[key_id(kk)]);
-      od[i] = key_dist(kk);
-    }
-  } else {
-    count = min(have, (int)k);
-    for (int i = lane; i < count; i += 32) {
-      oid[i] = key_id(src[i]);
-      od[i] = key_dist(src[i]);
-    }
-  }
-  for (int i = count + lane; i < (int)k; i += 32) {
-    oid[i] = DG_PAD;
-    od[i] = __int_as_float(0x7f800000);
-  }
-  if (lane == 0) {
-    a.out_cnt[q] = (uint32_t)count;
-    if (a.out_stats) {
-      a.out_stats[2 * q] = n_exp;
-      a.out_stats[2 * q + 1] = n_dist;
-    }
-  }
-  __syncwarp();
+  emit_results<TRAV, MET, LPRF>(a, q, filtered ? RES : W[cur], filtered ? rsize : wsize, use_rerank, search_k,
+                                W[cur ^ 1], qs, qq, n_exp, n_dist, lane);
 }
 
 // Resident blocks per SM the register allocation is sized for (4 warps each).
@@ -276,7 +480,10 @@ __global__ void __launch_bounds__(128, DG_SEARCH_MIN_BLOCKS) beam_search_kernel(
     if (lane == 0) q = atomicAdd(a.counter, 1u);
     q = __shfl_sync(kFull, q, 0);
     if (q >= a.nq) break;
-    search_one<TRAV, MET, LPR, LPRF, LCAP, FILT>(a, q, wsm, Ly, lane);
+    if (LCAP == 64 && !FILT)
+      search_one_reg<TRAV, MET, LPR, LPRF>(a, q, wsm, Ly, lane);
+    else
+      search_one<TRAV, MET, LPR, LPRF, LCAP, FILT>(a, q, wsm, Ly, lane);
   }
 }
 
