@@ -363,8 +363,13 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
   if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
   if (reranked && !any_filter && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
+  // visited table: 2^hbits words of two 16-bit tags (about 3 tags per
+  // visited node at these beams); DG_HBITS overrides for tuning
   uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
   if (const char *e = std::getenv("DG_HBITS")) hbits = (uint32_t)std::max(6, std::min(14, atoi(e)));
+  uint32_t hB = 1;
+  while (hB < 32 && (1ull << hB) < idx->n) ++hB;
+  hB = std::max(hB, hbits);
 
   std::lock_guard<std::mutex> lk(idx->mu);
   DG_CUDA(cudaSetDevice(idx->device));
@@ -404,6 +409,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   a.L = p->beam_width;
   a.rerank = p->rerank_size;
   a.hbits = hbits;
+  a.hB = hB;
   if (any_filter) {
     if ((s = stage_copy(sl.fops, p->filter_ops, (size_t)total_ops * sizeof(DgFilterOp), st)) != DG_OK) return s;
     a.fops = (const DgFilterOp *)sl.fops.p;

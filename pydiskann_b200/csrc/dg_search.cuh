@@ -11,8 +11,8 @@
 //     bitonic sort and a merge-path scatter.  Processing a row as one batch
 //     keeps exactly the L smallest (distance, id) pairs, which is what the
 //     reference's sequential insert-if-smaller loop keeps;
-//   * the visited set is a direct-mapped, overwrite-on-collision table in
-//     shared memory.  It never reports an unvisited id as visited; an id it
+//   * the visited set is a small exact-tag table in shared memory (struct
+//     Visited).  It never reports an unvisited id as visited; an id it
 //     forgets is recomputed and removed again by the duplicate check of the
 //     merge (a forgotten id that is not in `w` any more cannot re-enter it,
 //     since `w`'s worst entry only decreases), so results do not depend on the
@@ -57,7 +57,8 @@ struct SearchArgs {
   const float *Q;  // [nq][d]
   uint32_t nq, k, L, rerank;
   const uint32_t *perL;  // per-query L or null
-  uint32_t hbits;        // log2 of the visited-table slots
+  uint32_t hbits;        // log2 of the visited-table words
+  uint32_t hB;           // id bits mixed by the visited table (n <= 2^hB)
   // outputs
   uint32_t *out_ids;
   float *out_d;
@@ -101,6 +102,45 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
 
 // ------------------------------------------------------- small warp helpers
 __device__ __forceinline__ uint32_t lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+// ------------------------------------------------------------ visited set
+// A per-query table of 2^bbits 32-bit words in shared memory.  Ids are mixed
+// by a multiply with an odd constant modulo 2^B (a bijection on the B-bit ids,
+// n <= 2^B); the top bbits bits of the mix pick a word, the remaining B-bbits
+// bits (+1, 0 = empty) form a 16-bit tag, and each word holds the two most
+// recent tags of its bucket.  (word, tag) identifies an id uniquely, so the
+// table never reports an unvisited id as visited; it may forget an id when a
+// bucket overflows, which only costs a recomputed distance.  When B-bbits
+// exceeds 15 bits the words hold whole ids instead (direct mapped).
+struct Visited {
+  uint32_t *w;
+  uint32_t bbits, B;
+  __device__ __forceinline__ bool tagged() const { return B - bbits <= 15; }
+  __device__ __forceinline__ uint32_t mix(uint32_t id) const {
+    const uint32_t h = id * 0x9E3779B1u;
+    return B >= 32 ? h : (h & ((1u << B) - 1u));
+  }
+  __device__ __forceinline__ void clear(int lane) const {
+    const uint32_t words = 1u << bbits, empty = tagged() ? 0u : 0xFFFFFFFFu;
+    for (uint32_t i = lane; i < words; i += 32) w[i] = empty;
+  }
+  // True when `id` is recorded; otherwise records it.
+  __device__ __forceinline__ bool test_and_set(uint32_t id) const {
+    if (tagged()) {
+      const uint32_t h = mix(id);
+      const uint32_t slot = h >> (B - bbits);
+      const uint32_t tag = (h & ((1u << (B - bbits)) - 1u)) + 1u;
+      const uint32_t v = w[slot];
+      if ((v & 0xffffu) == tag || (v >> 16) == tag) return true;
+      w[slot] = (v << 16) | tag;
+      return false;
+    }
+    const uint32_t slot = (id * 0x9E3779B1u) >> (32 - bbits);
+    if (w[slot] == id) return true;
+    w[slot] = id;
+    return false;
+  }
+};
 
 // number of keys in a[0..n) that are < key (a sorted ascending)
 __device__ __forceinline__ int lower_bound_smem(const uint64_t *a, int n, uint64_t key) {

@@ -60,10 +60,6 @@ __device__ __forceinline__ float exact_distance(const SearchArgs &a, const float
                                      (a.dpad / 4) / LPRF, qs, cand, cnt, lane, a.metric == DG_L2, qq);
 }
 
-__device__ __forceinline__ uint32_t vhash(uint32_t id, uint32_t hbits) {
-  return (id * 2654435761u) >> (32 - hbits);
-}
-
 // Per-query quantizer state (QuantizerState::prepare, src/quantized.rs:167-174).
 template <int TRAV>
 __device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm, const WarpLayout &Ly,
@@ -228,9 +224,8 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
   uint64_t *skeys = reinterpret_cast<uint64_t *>(wsm + Ly.w1) ; // survivors of one expansion (<= 64)
   uint64_t *cst = reinterpret_cast<uint64_t *>(wsm + Ly.cstage);
   uint32_t *stage = reinterpret_cast<uint32_t *>(wsm + Ly.stage);
-  uint32_t *hash = reinterpret_cast<uint32_t *>(wsm + Ly.hash);
+  const Visited vt{reinterpret_cast<uint32_t *>(wsm + Ly.hash), a.hbits, a.hB};
   float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
-  const uint32_t hsz = 1u << a.hbits;
   const int L = (int)(a.perL ? a.perL[q] : a.L);
   const uint32_t k = a.k;
   const bool use_rerank = TRAV != TRAV_F32 && a.rerank > 0;
@@ -238,7 +233,7 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
 
   const float *qg = a.Q + (size_t)q * a.d;
   for (uint32_t i = lane; i < a.dpad; i += 32) qs[i] = i < a.d ? qg[i] : 0.0f;
-  for (uint32_t i = lane; i < hsz; i += 32) hash[i] = DG_PAD;
+  vt.clear(lane);
   __syncwarp();
   float qq = 0.0f;
   if (MET == MET_COS) {
@@ -257,7 +252,7 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
     d = __shfl_sync(kFull, d, 0);
     if (lane == 0) {
       w0 = make_key(d, cand);
-      hash[vhash(cand, a.hbits)] = cand;
+      vt.test_and_set(cand);
     }
     __syncwarp();
   }
@@ -285,12 +280,9 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
       const uint32_t j = j0 + lane;
       const uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
       bool ok = nb != DG_PAD && nb < a.n;
-      if (ok) ok = hash[vhash(nb, a.hbits)] != nb;
+      if (ok) ok = !vt.test_and_set(nb);
       const uint32_t m = __ballot_sync(kFull, ok);
-      if (ok) {
-        stage[ns + __popc(m & lanemask_lt(lane))] = nb;
-        hash[vhash(nb, a.hbits)] = nb;
-      }
+      if (ok) stage[ns + __popc(m & lanemask_lt(lane))] = nb;
       ns += __popc(m);
     }
     __syncwarp();
@@ -332,9 +324,8 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
   uint64_t *RES = reinterpret_cast<uint64_t *>(wsm + Ly.res);
   uint64_t *cst = reinterpret_cast<uint64_t *>(wsm + Ly.cstage);
   uint32_t *stage = reinterpret_cast<uint32_t *>(wsm + Ly.stage);
-  uint32_t *hash = reinterpret_cast<uint32_t *>(wsm + Ly.hash);
+  const Visited vt{reinterpret_cast<uint32_t *>(wsm + Ly.hash), a.hbits, a.hB};
   float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
-  const uint32_t hsz = 1u << a.hbits;
 
   const uint32_t L = a.perL ? a.perL[q] : a.L;
   const uint32_t k = a.k;
@@ -358,7 +349,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
   // ---- query into shared memory (zero padded), norms, visited table
   const float *qg = a.Q + (size_t)q * a.d;
   for (uint32_t i = lane; i < a.dpad; i += 32) qs[i] = i < a.d ? qg[i] : 0.0f;
-  for (uint32_t i = lane; i < hsz; i += 32) hash[i] = DG_PAD;
+  vt.clear(lane);
   __syncwarp();
   float qq = 0.0f;
   if (MET == MET_COS) {
@@ -382,7 +373,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     d = __shfl_sync(kFull, d, 0);
     if (lane == 0) {
       W[0][0] = make_key(d, cand);
-      hash[vhash(cand, a.hbits)] = cand;
+      vt.test_and_set(cand);
       if (filtered && allow(cand)) RES[0] = make_key(d, cand);
     }
     wsize = 1;
@@ -423,14 +414,11 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     int ns = 0;
     for (uint32_t j0 = 0; j0 < a.R; j0 += 32) {
       const uint32_t j = j0 + lane;
-      uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
+      const uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
       bool ok = nb != DG_PAD && nb < a.n;
-      if (ok) ok = hash[vhash(nb, a.hbits)] != nb;
+      if (ok) ok = !vt.test_and_set(nb);
       const uint32_t m = __ballot_sync(kFull, ok);
-      if (ok) {
-        stage[ns + __popc(m & lanemask_lt(lane))] = nb;
-        hash[vhash(nb, a.hbits)] = nb;
-      }
+      if (ok) stage[ns + __popc(m & lanemask_lt(lane))] = nb;
       ns += __popc(m);
     }
     __syncwarp();

@@ -65,7 +65,7 @@ struct BuildArgs {
   const float *vf;      // [n][dpad]
   const uint16_t *vb;   // [n][dpad] bf16 (only when every value is bf16-exact)
   const uint32_t *graph;  // snapshot [n][R]
-  uint32_t hbits;
+  uint32_t hbits, hB;     // visited table: log2 words, id bits
   uint64_t u0, u1;        // node range of this chunk
   uint32_t cw;            // candidate slots per node (R + 3*Lb)
   uint64_t *cand;         // [(u1-u0)][cw]
@@ -92,9 +92,8 @@ __global__ void __launch_bounds__(128) k_build_search(BuildArgs a, WarpLayout Ly
   uint64_t *W[2] = {reinterpret_cast<uint64_t *>(wsm + Ly.w0), reinterpret_cast<uint64_t *>(wsm + Ly.w1)};
   uint64_t *cst = reinterpret_cast<uint64_t *>(wsm + Ly.cstage);
   uint32_t *stage = reinterpret_cast<uint32_t *>(wsm + Ly.stage);
-  uint32_t *hash = reinterpret_cast<uint32_t *>(wsm + Ly.hash);
+  const Visited vt{reinterpret_cast<uint32_t *>(wsm + Ly.hash), a.hbits, a.hB};
   float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
-  const uint32_t hsz = 1u << a.hbits;
   const uint64_t gw = blockIdx.x * (uint64_t)(blockDim.x >> 5) + warp;
   const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
   for (uint64_t u = a.u0 + gw; u < a.u1; u += nw) {
@@ -134,7 +133,7 @@ __global__ void __launch_bounds__(128) k_build_search(BuildArgs a, WarpLayout Ly
     const uint32_t seeds[3] = {a.medoid, (uint32_t)range_of(rand4(a.seed, a.pass + 1, u, 0), a.n),
                                (uint32_t)range_of(rand4(a.seed, a.pass + 1, u, 1), a.n)};
     for (int s = 0; s < 3; ++s) {
-      for (uint32_t i = lane; i < hsz; i += 32) hash[i] = DG_PAD;
+      vt.clear(lane);
       __syncwarp();
       int cur = 0, wsize = 1;
       {
@@ -146,7 +145,7 @@ __global__ void __launch_bounds__(128) k_build_search(BuildArgs a, WarpLayout Ly
         dd = __shfl_sync(kFull, dd, 0);
         if (lane == 0) {
           W[0][0] = make_key(dd, c);
-          hash[(c * 2654435761u) >> (32 - a.hbits)] = c;
+          vt.test_and_set(c);
         }
         __syncwarp();
       }
@@ -171,13 +170,9 @@ __global__ void __launch_bounds__(128) k_build_search(BuildArgs a, WarpLayout Ly
           const uint32_t j = j0 + lane;
           const uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
           bool ok = nb != DG_PAD && nb < a.n;
-          const uint32_t h = (nb * 2654435761u) >> (32 - a.hbits);
-          if (ok) ok = hash[h] != nb;
+          if (ok) ok = !vt.test_and_set(nb);
           const uint32_t m = __ballot_sync(kFull, ok);
-          if (ok) {
-            stage[ns + __popc(m & ((1u << lane) - 1u))] = nb;
-            hash[h] = nb;
-          }
+          if (ok) stage[ns + __popc(m & ((1u << lane) - 1u))] = nb;
           ns += __popc(m);
         }
         __syncwarp();
@@ -455,6 +450,12 @@ __global__ void k_bf16_exact(const float *v, uint64_t total, unsigned int *flag)
   }
 }
 
+static uint32_t id_bits(uint64_t n) {
+  uint32_t b = 1;
+  while (b < 32 && (1ull << b) < n) ++b;
+  return b;
+}
+
 template <int ELEM, int MET>
 static DgStatus run_build(const BuildArgs &base, float *vf, uint16_t *vb, uint32_t *g0, uint32_t *g1,
                           float alpha, cudaStream_t st, uint32_t **result) {
@@ -483,7 +484,7 @@ static DgStatus run_build(const BuildArgs &base, float *vf, uint16_t *vb, uint32
   DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pblocks, prune_k, kPruneThreads, psmem));
   const int pgrid = std::max(1, pblocks) * sms;
   // search kernel geometry
-  const uint32_t hbits = 10;
+  const uint32_t hbits = base.Lb <= 64 ? 10 : base.Lb <= 128 ? 11 : 12;
   const WarpLayout Ly = warp_layout(ELEM == 1 ? TRAV_BF16 : TRAV_F32, lcap, false, hbits, dpad, 0, 0, 0);
   void (*sk)(BuildArgs, WarpLayout) = lcap == 64 ? k_build_search<ELEM, MET, LPR, 64>
                                     : lcap == 256 ? k_build_search<ELEM, MET, LPR, 256>
@@ -518,6 +519,7 @@ static DgStatus run_build(const BuildArgs &base, float *vf, uint16_t *vb, uint32
     a.pass = pass;
     a.graph = cur;
     a.hbits = hbits;
+    a.hB = std::max(id_bits(n), hbits);
     a.cw = cw;
     a.cand = cand;
     a.cand_cnt = ccnt;
