@@ -148,6 +148,25 @@ DG_API DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const flo
                          uint32_t *out_ids, float *out_dists, uint32_t *out_counts,
                          uint32_t *out_stats);
 
+/* dg_search_batch for callers that cannot have device memory allocated for
+ * them (hosts whose device memory belongs to a separate pool manager,
+ * latency-critical threads that must not pay cudaMalloc's implicit device
+ * synchronisation).  No counterpart in the reference: it is an addition of
+ * this library.  It allocates nothing: its scratch (the search's work counter
+ * and copies of the filter programs and per-query beams) lives in a
+ * file-scope device array of 256 KiB that every GPU loading the library keeps
+ * until the process exits.  Requires DG_FLAG_DEVICE_PTRS (queries and outputs
+ * in device memory, no host staging) and returns after enqueueing on the
+ * stream.  Per-call parameters larger than the array (about 10k filter ops or
+ * 60k per-query beams) are rejected with DG_EINVAL.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  Every call reuses the same array, so
+ * calls that overlap on the GPU (any device, any stream, any handle) race:
+ * order them on one stream or wait between them.  out_stats is not written. */
+DG_API DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p, const float *queries,
+                                       uint32_t nq, uint32_t *out_ids, float *out_dists,
+                                       uint32_t *out_counts);
+
 /* FilteredDiskANN::count_matching (src/filtered.rs:508-510). */
 DG_API DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
                            const uint64_t *pool, uint32_t pool_len, uint64_t *out_count);

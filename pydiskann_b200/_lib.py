@@ -67,6 +67,7 @@ def _signatures():
         "dg_index_attach_rabitq": (st, [vp, u32, vp, vp, vp]),
         "dg_index_attach_labels": (st, [vp, u32, vp]),
         "dg_search_batch": (st, [vp, vp, vp, u32, vp, vp, vp, vp]),
+        "dg_search_batch_static": (st, [vp, vp, vp, u32, vp, vp, vp]),
         "dg_count_matching": (st, [vp, vp, u32, vp, u32, vp]),
         "dg_medoid": (st, [vp, u64, u32, i32, i32, vp]),
         "dg_build_vamana": (st, [vp, u64, u32, i32, u32, u32, f32, u64, u32, i32, vp]),

@@ -516,3 +516,200 @@ DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Search without any device allocation.
+//
+// Some callers cannot have device memory allocated on their behalf: hosts
+// whose device memory is owned by a separate pool manager, and
+// latency-critical request threads that must not pay cudaMalloc's implicit
+// device-wide synchronisation.  dg_search_batch_static serves them: its only
+// scratch memory (the work counter of the persistent grid and copies of the
+// per-call filter programs and beams) lives in the file-scope array below,
+// which every GPU that loads the library holds until the process exits.
+namespace dg {
+
+constexpr size_t kStaticScratchBytes = 256 * 1024;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_static_mu;
+static void *g_static_addr[kMaxDevices];
+
+// Device address of g_static_scratch on `device` (the current device).  In host
+// code the array's name only stands in for the symbol, so the address is asked
+// for once per device, with that device current, and kept.
+static DgStatus static_scratch(int device, unsigned char **out) {
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (device < 0 || device >= kMaxDevices) return fail(DG_EINVAL, "device ordinal out of range");
+  if (!g_static_addr[device]) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+    g_static_addr[device] = ptr;
+  }
+  *out = static_cast<unsigned char *>(g_static_addr[device]);
+  return DG_OK;
+}
+
+}  // namespace dg
+
+extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p, const float *queries,
+                                           uint32_t nq, uint32_t *out_ids, float *out_dists,
+                                           uint32_t *out_counts) {
+  if (!idx || !p) return fail(DG_EINVAL, "null argument");
+  if (nq == 0) return DG_OK;
+  if (!queries || !out_ids || !out_dists || !out_counts) return fail(DG_EINVAL, "null buffer");
+  if (!(p->flags & DG_FLAG_DEVICE_PTRS))
+    return fail(DG_EINVAL, "dg_search_batch_static needs device pointers (DG_FLAG_DEVICE_PTRS)");
+  if (p->k == 0) return fail(DG_EINVAL, "k must be >= 1");
+  int trav;
+  switch (p->traversal) {
+    case DG_TRAVERSE_F32: trav = TRAV_F32; break;
+    case DG_TRAVERSE_BF16:
+      if (!idx->bf16) return fail(DG_EINVAL, "BF16 traversal needs dg_index_enable_bf16");
+      trav = TRAV_BF16;
+      break;
+    case DG_TRAVERSE_CODES:
+      switch (idx->quant) {
+        case DG_Q_PQ: trav = TRAV_PQ; break;
+        case DG_Q_INT8: trav = TRAV_INT8; break;
+        case DG_Q_RABITQ: trav = TRAV_RABITQ; break;
+        case DG_Q_F16: trav = TRAV_F16; break;
+        default: return fail(DG_EINVAL, "code traversal needs an attached quantizer");
+      }
+      break;
+    default: return fail(DG_EINVAL, "unknown traversal");
+  }
+  uint32_t maxL = p->beam_width;
+  if (p->per_query_beam) {
+    maxL = 0;
+    for (uint32_t i = 0; i < nq; ++i) {
+      if (p->per_query_beam[i] == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
+      maxL = std::max(maxL, p->per_query_beam[i]);
+    }
+  }
+  if (maxL == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
+  const uint32_t total_ops = p->filter_offsets ? p->filter_offsets[nq] : p->filter_nops;
+  bool any_filter = false;
+  if (p->filter_offsets) {
+    if (p->filter_offsets[0] != 0) return fail(DG_EINVAL, "filter_offsets[0] must be 0");
+    for (uint32_t i = 0; i < nq; ++i) {
+      if (p->filter_offsets[i + 1] < p->filter_offsets[i]) return fail(DG_EINVAL, "filter_offsets not monotone");
+      const uint32_t c = p->filter_offsets[i + 1] - p->filter_offsets[i];
+      if (c) {
+        any_filter = true;
+        const int dep = program_depth(p->filter_ops + p->filter_offsets[i], c, p->filter_pool_len);
+        if (dep < 0 || dep > kFilterStack) return fail(DG_EINVAL, "malformed filter program");
+      }
+    }
+  } else if (p->filter_nops) {
+    any_filter = true;
+    const int dep = program_depth(p->filter_ops, p->filter_nops, p->filter_pool_len);
+    if (dep < 0 || dep > kFilterStack) return fail(DG_EINVAL, "malformed filter program");
+  }
+  if (any_filter && !p->filter_ops) return fail(DG_EINVAL, "filter ops missing");
+  if (any_filter && !idx->labels) return fail(DG_EINVAL, "filtered search needs attached labels");
+  const bool reranked = trav != TRAV_F32 && p->rerank_size > 0;
+  const uint32_t search_k = reranked ? std::max(p->rerank_size, p->k) : p->k;
+  uint64_t need = maxL;
+  if (any_filter) need = std::max<uint64_t>({(uint64_t)maxL * 4, (uint64_t)p->k * 10, search_k});
+  const int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
+  if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
+  if (reranked && !any_filter && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
+  uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
+  uint32_t hB = 1;
+  while (hB < 32 && (1ull << hB) < idx->n) ++hB;
+  hB = std::max(hB, hbits);
+
+  // scratch layout: [0, 256) work counter | filter ops | offsets | pool | beams
+  auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+  const size_t o_ops = 256;
+  const size_t o_offs = o_ops + up16(any_filter ? (size_t)total_ops * sizeof(DgFilterOp) : 0);
+  const size_t o_pool = o_offs + up16(any_filter && p->filter_offsets ? (size_t)(nq + 1) * 4 : 0);
+  const size_t o_beam = o_pool + up16(any_filter ? (size_t)p->filter_pool_len * 8 : 0);
+  const size_t used = o_beam + up16(p->per_query_beam ? (size_t)nq * 4 : 0);
+  if (used > kStaticScratchBytes)
+    return fail(DG_EINVAL, "per-call parameters need " + std::to_string(used) + " bytes; the static scratch holds " +
+                               std::to_string(kStaticScratchBytes) + " (fewer filter ops or per-query beams per call)");
+
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  unsigned char *scratch = nullptr;
+  DgStatus s = static_scratch(idx->device, &scratch);
+  if (s != DG_OK) return s;
+  cudaStream_t st = (p->flags & DG_FLAG_STREAM) || p->stream ? (cudaStream_t)p->stream : idx->stream;
+
+  SearchArgs a{};
+  a.n = idx->n;
+  a.d = idx->d;
+  a.dpad = idx->dpad;
+  a.R = idx->R;
+  a.medoid = idx->medoid;
+  a.metric = idx->metric;
+  a.vec_f32 = idx->vec;
+  a.vec_bf16 = idx->bf16;
+  a.adj = idx->adj;
+  a.codes = idx->codes;
+  a.code_stride = idx->code_stride;
+  a.pq_M = idx->pq_M;
+  a.pq_K = idx->pq_K;
+  a.pq_ds = idx->pq_M ? idx->d / idx->pq_M : 0;
+  a.pq_cb = idx->pq_cb;
+  a.i8_scale = idx->i8_scale;
+  a.i8_offset = idx->i8_offset;
+  a.rq_padded = idx->rq_padded;
+  a.rq_centroid = idx->rq_centroid;
+  a.rq_signs = idx->rq_signs;
+  a.labels = idx->labels;
+  a.nf = idx->nf;
+  a.nq = nq;
+  a.k = p->k;
+  a.L = p->beam_width;
+  a.rerank = p->rerank_size;
+  a.hbits = hbits;
+  a.hB = hB;
+  // every call reuses the array: the counter must start at zero again
+  DG_CUDA(cudaMemsetAsync(scratch, 0, 4, st));
+  a.counter = reinterpret_cast<uint32_t *>(scratch);
+  if (any_filter) {
+    DG_CUDA(cudaMemcpyAsync(scratch + o_ops, p->filter_ops, (size_t)total_ops * sizeof(DgFilterOp),
+                            cudaMemcpyHostToDevice, st));
+    a.fops = reinterpret_cast<const DgFilterOp *>(scratch + o_ops);
+    a.fnops = p->filter_offsets ? 0 : p->filter_nops;
+    if (p->filter_offsets) {
+      DG_CUDA(cudaMemcpyAsync(scratch + o_offs, p->filter_offsets, (size_t)(nq + 1) * 4, cudaMemcpyHostToDevice, st));
+      a.foffs = reinterpret_cast<const uint32_t *>(scratch + o_offs);
+    }
+    if (p->filter_pool_len)
+      DG_CUDA(cudaMemcpyAsync(scratch + o_pool, p->filter_pool, (size_t)p->filter_pool_len * 8,
+                              cudaMemcpyHostToDevice, st));
+    a.fpool = reinterpret_cast<const uint64_t *>(scratch + o_pool);
+  }
+  if (p->per_query_beam) {
+    DG_CUDA(cudaMemcpyAsync(scratch + o_beam, p->per_query_beam, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
+    a.perL = reinterpret_cast<const uint32_t *>(scratch + o_beam);
+  }
+  a.Q = queries;
+  a.out_ids = out_ids;
+  a.out_d = out_dists;
+  a.out_cnt = out_counts;
+  a.out_stats = nullptr;
+
+  const int met = met_kind(idx->metric);
+  int lpr = 1;
+  if (trav == TRAV_F32) lpr = 8;
+  else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
+  else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
+  const WarpLayout Ly = warp_layout(trav, lcap, any_filter, hbits, idx->dpad, idx->pq_M, idx->pq_K,
+                                    idx->rq_padded);
+  LaunchInfo info;
+  switch (trav) {
+    case TRAV_F32: return launch_search_f32(a, Ly, met, lpr, lcap, any_filter, st, &info);
+    case TRAV_BF16: return launch_search_bf16(a, Ly, met, lpr, lcap, any_filter, st, &info);
+    case TRAV_F16: return launch_search_f16(a, Ly, met, lpr, lcap, any_filter, st, &info);
+    case TRAV_INT8: return launch_search_int8(a, Ly, met, lpr, lcap, any_filter, st, &info);
+    case TRAV_PQ: return launch_search_pq(a, Ly, met, lpr, lcap, any_filter, st, &info);
+    default: return launch_search_rabitq(a, Ly, met, lpr, lcap, any_filter, st, &info);
+  }
+}
