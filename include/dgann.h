@@ -171,6 +171,66 @@ DG_API DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p, co
 DG_API DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
                            const uint64_t *pool, uint32_t pool_len, uint64_t *out_count);
 
+/* ------------------------------------------------------------------ SPFresh */
+/* Posting lists of an SPFresh index (src/spfresh.rs:62-111,250-281): posting
+ * slot b has a centroid, a live flag and block_len[b] entries (id, code) out
+ * of block_cap; codes are the raw f32 vector (quantizer DG_Q_NONE), F16, int8,
+ * PQ or RaBitQ residual codes against the posting centroid.  The raw store
+ * holds every vector by id for the rerank.  Ids stay below 2^31. */
+typedef struct DgSpfresh DgSpfresh;
+typedef struct {
+  uint32_t dim;
+  int32_t metric;             /* DgMetric */
+  int32_t device;
+  uint32_t num_blocks;        /* posting slots, live or free */
+  uint32_t block_cap;         /* entries per slot (2 * max_posting_size) */
+  const float *centroids;     /* f32[num_blocks*dim] */
+  const uint8_t *block_live;  /* u8[num_blocks] */
+  const uint32_t *block_len;  /* u32[num_blocks] */
+  const uint64_t *entry_ids;  /* u64[num_blocks*block_cap] */
+  const uint8_t *entry_codes; /* [num_blocks*block_cap][code_size] */
+  uint32_t code_size;         /* 4*dim raw, 2*dim F16, dim int8, M for PQ, padded/8+8 RaBitQ */
+  int32_t quantizer;          /* DgQuantizer */
+  uint32_t pq_M, pq_K;
+  const float *pq_codebooks;  /* [M][K][dim/M] */
+  float int8_scale, int8_offset;
+  uint32_t rq_padded;
+  const float *rq_signs;      /* f32[3*padded] */
+  uint64_t id_capacity;       /* every id < id_capacity */
+  uint64_t num_raw;           /* rows of `raw` given now (ids 0..num_raw-1) */
+  const float *raw;           /* f32[num_raw*dim] */
+  const uint8_t *deleted;     /* optional u8[id_capacity] tombstones */
+} DgSpfreshDesc;
+
+typedef struct {
+  uint32_t k;
+  uint32_t nprobe;      /* n_probe of SPFresh::search (src/spfresh.rs:886-895) */
+  uint32_t rerank_size; /* SPFreshConfig::rerank_size (quantized postings) */
+  float probe_ratio;    /* SPFreshConfig::probe_ratio (inf = off) */
+  uint32_t flags;       /* DG_FLAG_* */
+  void *stream;
+} DgSpfreshParams;
+
+/* SPFresh::build / open -> device-resident posting lists. */
+DG_API DgStatus dg_spfresh_create(const DgSpfreshDesc *desc, DgSpfresh **out);
+DG_API DgStatus dg_spfresh_destroy(DgSpfresh *s);
+/* Replaces whole posting slots after host-side insert / split / merge
+ * (Inner::rewrite / push, src/spfresh.rs:294-320): centroids f32[n*dim],
+ * live u8[n], lens u32[n], ids u64[n*block_cap], codes [n*block_cap][code_size]. */
+DG_API DgStatus dg_spfresh_update_blocks(DgSpfresh *s, const uint32_t *blocks, uint32_t n,
+                                         const float *centroids, const uint8_t *live,
+                                         const uint32_t *lens, const uint64_t *entry_ids,
+                                         const uint8_t *entry_codes);
+/* Raw vectors of ids first_id .. first_id+n-1 (the raw store, src/spfresh.rs:283-286). */
+DG_API DgStatus dg_spfresh_put_raw(DgSpfresh *s, uint64_t first_id, const float *vectors, uint64_t n);
+/* SPFresh::delete tombstones (src/spfresh.rs:863-871); deleted = 0 clears. */
+DG_API DgStatus dg_spfresh_set_deleted(DgSpfresh *s, const uint64_t *ids, uint64_t n, int32_t deleted);
+/* SPFresh::search_with_dists / search_batch (src/spfresh.rs:671-770,886-908):
+ * out_ids u64[nq*k] (DG_PAD64 padded), out_dists f32[nq*k], out_counts u32[nq]. */
+DG_API DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const float *queries,
+                                        uint32_t nq, uint64_t *out_ids, float *out_dists,
+                                        uint32_t *out_counts);
+
 /* ---------------------------------------------------------- index building */
 /* calculate_medoid (src/lib.rs:748-768) on the GPU. X is host f32[n*dim]. */
 DG_API DgStatus dg_medoid(const float *X, uint64_t n, uint32_t dim, int32_t metric, int32_t device,

@@ -27,7 +27,7 @@ from . import _lib
 from ._lib import PAD, check, lib, ptr
 
 __all__ = [
-    "DiskANN", "QuantizedDiskANN", "FilteredDiskANN", "Filter", "build_graph", "medoid",
+    "DiskANN", "QuantizedDiskANN", "FilteredDiskANN", "SPFresh", "Filter", "build_graph", "medoid",
     "pq_train", "pq_encode", "exact_knn", "read_fvecs", "write_fvecs", "read_ivecs",
 ]
 
@@ -597,3 +597,6 @@ def write_fvecs(path, vectors):
     out[:, 0] = X.shape[1]
     out[:, 1:] = X.view(np.int32)
     out.tofile(path)
+
+
+from .spfresh import SPFresh  # noqa: E402  (uses the helpers above)

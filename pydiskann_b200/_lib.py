@@ -53,6 +53,23 @@ class SearchParams(C.Structure):
     ]
 
 
+class SpfreshDesc(C.Structure):
+    _fields_ = [
+        ("dim", C.c_uint32), ("metric", C.c_int32), ("device", C.c_int32), ("num_blocks", C.c_uint32),
+        ("block_cap", C.c_uint32), ("centroids", C.c_void_p), ("block_live", C.c_void_p),
+        ("block_len", C.c_void_p), ("entry_ids", C.c_void_p), ("entry_codes", C.c_void_p),
+        ("code_size", C.c_uint32), ("quantizer", C.c_int32), ("pq_M", C.c_uint32), ("pq_K", C.c_uint32),
+        ("pq_codebooks", C.c_void_p), ("int8_scale", C.c_float), ("int8_offset", C.c_float),
+        ("rq_padded", C.c_uint32), ("rq_signs", C.c_void_p), ("id_capacity", C.c_uint64),
+        ("num_raw", C.c_uint64), ("raw", C.c_void_p), ("deleted", C.c_void_p),
+    ]
+
+
+class SpfreshParams(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("nprobe", C.c_uint32), ("rerank_size", C.c_uint32),
+                ("probe_ratio", C.c_float), ("flags", C.c_uint32), ("stream", C.c_void_p)]
+
+
 # Every symbol include/dgann.h declares, with its ctypes signature.
 def _signatures():
     vp, u32, u64, i32, f32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float
@@ -69,6 +86,12 @@ def _signatures():
         "dg_search_batch": (st, [vp, vp, vp, u32, vp, vp, vp, vp]),
         "dg_search_batch_static": (st, [vp, vp, vp, u32, vp, vp, vp]),
         "dg_count_matching": (st, [vp, vp, u32, vp, u32, vp]),
+        "dg_spfresh_create": (st, [vp, vp]),
+        "dg_spfresh_destroy": (st, [vp]),
+        "dg_spfresh_update_blocks": (st, [vp, vp, u32, vp, vp, vp, vp, vp]),
+        "dg_spfresh_put_raw": (st, [vp, u64, vp, u64]),
+        "dg_spfresh_set_deleted": (st, [vp, vp, u64, i32]),
+        "dg_spfresh_search_batch": (st, [vp, vp, vp, u32, vp, vp, vp]),
         "dg_medoid": (st, [vp, u64, u32, i32, i32, vp]),
         "dg_build_vamana": (st, [vp, u64, u32, i32, u32, u32, f32, u64, u32, i32, vp]),
         "dg_pq_train": (st, [vp, u64, u32, u32, u32, u32, u64, u64, i32, vp]),

@@ -1,0 +1,682 @@
+// dg_spfresh.cu -- SPFresh posting-list search on the GPU (diskann-rs
+// src/spfresh.rs:344-378, 671-770).
+//
+// One warp per query, persistent grid with a work counter:
+//   1. routing: the distance from the query to every live posting centroid,
+//      each summed sequentially by one lane in the order the oracle sums it,
+//      kept as the nprobe smallest (distance, posting) keys (nearest,
+//      src/spfresh.rs:358-378; brute force at every posting count);
+//   2. the probe_ratio cut (:683-687);
+//   3. the scan of every probed posting: tombstoned ids skipped, the
+//      distance of each entry's code (raw f32, PQ, int8, F16) inserted into
+//      the `want` smallest (distance, id) keys (:702-717), then the exact FP32
+//      rerank from the raw store (:719-723);
+//   4. RaBitQ codes with an L2 metric follow search_rabitq (:731-770): a
+//      per-posting residual query, and an exact distance only for entries whose
+//      lower bound est - err beats the current k-th exact distance.  The
+//      threshold changes after every insertion, so the warp computes a batch of
+//      candidates in parallel and replays the decisions entry by entry.
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dg_index.h"
+#include "dg_search.cuh"
+
+struct DgSpfresh {
+  int device = 0;
+  uint32_t d = 0, dpad = 0, nblocks = 0, cap = 0;
+  int32_t metric = DG_L2SQ;
+  int32_t quant = DG_Q_NONE;
+  uint32_t code_size = 0, code_stride = 0;
+  float *centroids = nullptr;  // [nblocks][dpad]
+  uint8_t *live = nullptr;     // [nblocks]
+  uint32_t *len = nullptr;     // [nblocks]
+  uint32_t *ids = nullptr;     // [nblocks][cap]
+  uint8_t *codes = nullptr;    // [nblocks][cap][code_stride]
+  uint64_t id_cap = 0;
+  uint32_t *deleted = nullptr; // bitmap over ids
+  float *raw = nullptr;        // [id_cap][dpad]
+  uint32_t pq_M = 0, pq_K = 0;
+  float *pq_cb = nullptr;
+  float i8_scale = 1.0f, i8_offset = 0.0f;
+  uint32_t rq_padded = 0;
+  float *rq_signs = nullptr;
+  uint32_t *counter = nullptr;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  std::vector<void *> allocs;
+  DgIndex::Buf q, oids, od, ocnt;
+};
+
+namespace dg {
+
+struct SpfArgs {
+  uint32_t d, dpad, nblocks, cap;
+  int32_t metric;
+  const float *centroids;
+  const uint8_t *live;
+  const uint32_t *len;
+  const uint32_t *ids;
+  const uint8_t *codes;
+  uint32_t code_stride;
+  const uint32_t *deleted;
+  const float *raw;
+  uint32_t pq_M, pq_K, pq_ds;
+  const float *pq_cb;
+  float i8_scale, i8_offset;
+  uint32_t rq_padded;
+  const float *rq_signs;
+  const float *Q;
+  uint32_t nq, k, nprobe, rerank;
+  float probe_ratio;
+  uint64_t *out_ids;
+  float *out_d;
+  uint32_t *out_cnt;
+  uint32_t *counter;
+};
+
+enum SpfKind { SPF_RAW = 0, SPF_PQ = 1, SPF_INT8 = 2, SPF_F16 = 3, SPF_RABITQ = 4 };
+
+// metric_eval of the oracle with its rounding (sequential sums).
+__device__ __forceinline__ float seq_metric(const float *q, const float *x, uint32_t d, int metric) {
+  if (metric == DG_L2SQ || metric == DG_L2) {
+    float acc = 0.0f;
+    for (uint32_t i = 0; i < d; ++i) {
+      const float t = __fsub_rn(q[i], __ldg(x + i));
+      acc = __fadd_rn(acc, __fmul_rn(t, t));
+    }
+    return metric == DG_L2 ? __fsqrt_rn(acc) : acc;
+  }
+  float ab = 0.0f, aa = 0.0f, bb = 0.0f;
+  for (uint32_t i = 0; i < d; ++i) {
+    const float xv = __ldg(x + i);
+    ab = __fadd_rn(ab, __fmul_rn(q[i], xv));
+    aa = __fadd_rn(aa, __fmul_rn(q[i], q[i]));
+    bb = __fadd_rn(bb, __fmul_rn(xv, xv));
+  }
+  if (metric == DG_DOT) return __fsub_rn(1.0f, ab);
+  if (aa == 0.0f && bb == 0.0f) return 0.0f;
+  if (ab == 0.0f) return 1.0f;
+  const float r = __fsub_rn(1.0f, __fdiv_rn(ab, __fmul_rn(__fsqrt_rn(aa), __fsqrt_rn(bb))));
+  return r > 0.0f ? r : 0.0f;
+}
+
+struct SpfLayout {
+  uint32_t p0, p1, r0, r1, cst, qf, prov, total;
+};
+__host__ __device__ inline SpfLayout spf_layout(uint32_t pcap, uint32_t rcap, uint32_t dpad, int kind,
+                                                uint32_t pq_M, uint32_t pq_K, uint32_t P) {
+  SpfLayout L{};
+  uint32_t o = 0;
+  L.p0 = o; o += pcap * 8;
+  L.p1 = o; o += pcap * 8;
+  L.r0 = o; o += rcap * 8;
+  L.r1 = o; o += rcap * 8;
+  L.cst = o; o += 64 * 8;
+  L.qf = o; o += align16(dpad * 4);
+  L.prov = o;
+  uint32_t p = 0;
+  if (kind == SPF_PQ) p = pq_M * pq_K * 4;
+  else if (kind == SPF_INT8) p = align16(dpad);
+  else if (kind == SPF_F16) p = align16(dpad * 4);
+  else if (kind == SPF_RABITQ) p = 4 * (P / 64) * 8 + 32 + align16(P * 4);
+  o += align16(p);
+  L.total = align16(o);
+  return L;
+}
+
+__device__ __forceinline__ bool is_deleted(const uint32_t *bm, uint32_t id) {
+  return (__ldg(bm + (id >> 5)) >> (id & 31)) & 1u;
+}
+
+// Distances of lane j's entry (row index `row` into the code array, valid for
+// j < cnt) by the posting's code kind (quantized_distance_from_codes).
+template <int KIND, int MET>
+__device__ __forceinline__ float entry_distance(const SpfArgs &a, uint8_t *wsm, const SpfLayout &Ly, uint32_t row,
+                                                int cnt, int lane, float qq) {
+  const float *qs = reinterpret_cast<const float *>(wsm + Ly.qf);
+  const bool sq = a.metric == DG_L2;
+  if (KIND == SPF_RAW) {
+    // code = the f32 vector: dist.eval(query, code)
+    return rows_distance<8, 0, MET>(a.codes, a.code_stride, (a.code_stride / 16) / 8, qs, row, cnt, lane, sq, qq);
+  } else if (KIND == SPF_F16) {
+    const float *qx = MET == MET_L2 ? reinterpret_cast<const float *>(wsm + Ly.prov) : qs;
+    const int ch = a.code_stride / 16;
+    return ch % 8 == 0 ? rows_distance<8, 2, MET>(a.codes, a.code_stride, ch / 8, qx, row, cnt, lane, sq, qq)
+                       : rows_distance<4, 2, MET>(a.codes, a.code_stride, ch / 4, qx, row, cnt, lane, sq, qq);
+  } else if (KIND == SPF_INT8) {
+    const int ch = a.code_stride / 16;
+    if (MET == MET_L2) {
+      const uint8_t *qc = wsm + Ly.prov;
+      const uint32_t s = ch % 8 == 0 ? int8_l2_group<8>(a.codes, a.code_stride, ch / 8, qc, row, cnt, lane)
+                         : ch % 4 == 0 ? int8_l2_group<4>(a.codes, a.code_stride, ch / 4, qc, row, cnt, lane)
+                                       : int8_l2_group<2>(a.codes, a.code_stride, ch / 2, qc, row, cnt, lane);
+      const float dd = __fmul_rn(__fmul_rn(__uint2float_rn(s), a.i8_scale), a.i8_scale);
+      return sq ? __fsqrt_rn(dd) : dd;
+    }
+    return ch % 8 == 0 ? int8_decode_group<8, MET>(a.codes, a.code_stride, ch / 8, qs, a.i8_scale, a.i8_offset, a.d,
+                                                   row, cnt, lane, qq)
+         : ch % 4 == 0 ? int8_decode_group<4, MET>(a.codes, a.code_stride, ch / 4, qs, a.i8_scale, a.i8_offset, a.d,
+                                                   row, cnt, lane, qq)
+                       : int8_decode_group<2, MET>(a.codes, a.code_stride, ch / 2, qs, a.i8_scale, a.i8_offset, a.d,
+                                                   row, cnt, lane, qq);
+  } else {  // PQ (L2 metrics only)
+    const float *lut = reinterpret_cast<const float *>(wsm + Ly.prov);
+    float dd = 0.0f;
+    if (lane < cnt) {
+      const uint8_t *crow = a.codes + (size_t)row * a.code_stride;
+      const uint32_t K = a.pq_K;
+      for (uint32_t m = 0; m < a.pq_M; ++m) dd = __fadd_rn(dd, lut[m * K + __ldg(crow + m)]);
+    }
+    return sq ? __fsqrt_rn(dd) : dd;
+  }
+}
+
+template <int KIND, int MET>
+__global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly, uint32_t pcap, uint32_t rcap) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t *wsm = smem + (size_t)warp * Ly.total;
+  uint64_t *const P[2] = {reinterpret_cast<uint64_t *>(wsm + Ly.p0), reinterpret_cast<uint64_t *>(wsm + Ly.p1)};
+  uint64_t *const Rl[2] = {reinterpret_cast<uint64_t *>(wsm + Ly.r0), reinterpret_cast<uint64_t *>(wsm + Ly.r1)};
+  uint64_t *cst = reinterpret_cast<uint64_t *>(wsm + Ly.cst);
+  float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
+  while (true) {
+    uint32_t q = 0;
+    if (lane == 0) q = atomicAdd(a.counter, 1u);
+    q = __shfl_sync(kFull, q, 0);
+    if (q >= a.nq) break;
+    const float *qg = a.Q + (size_t)q * a.d;
+    for (uint32_t i = lane; i < a.dpad; i += 32) qs[i] = i < a.d ? qg[i] : 0.0f;
+    __syncwarp();
+    float qq = 0.0f;
+    if (MET == MET_COS) {
+      for (uint32_t i = lane; i < a.dpad; i += 32) qq = fmaf(qs[i], qs[i], qq);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) qq += __shfl_xor_sync(kFull, qq, o);
+    }
+    // ---- 1. routing
+    const int nprobe = (int)max(a.nprobe, 1u);
+    int pcur = 0, psize = 0;
+    for (uint32_t b0 = 0; b0 < a.nblocks; b0 += 32) {
+      const uint32_t b = b0 + lane;
+      uint64_t key = kKeyInvalid;
+      if (b < a.nblocks && a.live[b]) key = make_key(seq_metric(qs, a.centroids + (size_t)b * a.dpad, a.d, a.metric), b);
+      insert_batch(key, P, pcur, psize, nprobe, cst, lane);
+    }
+    // ---- 2. probe_ratio cut
+    int np = psize;
+    if (np > 0 && isfinite(a.probe_ratio)) {
+      const float d0 = key_dist(P[pcur][0]);
+      if (d0 >= 0.0f) {
+        const float lim = __fmul_rn(d0, fmaxf(a.probe_ratio, 1.0f));
+        int first_out = psize;
+        for (int i = lane; i < psize; i += 32)
+          if (key_dist(P[pcur][i]) > lim) first_out = min(first_out, i);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) first_out = min(first_out, __shfl_xor_sync(kFull, first_out, o));
+        np = first_out;
+      }
+    }
+    // ---- per-query code state
+    if (KIND == SPF_PQ) {
+      SearchArgs sa{};
+      sa.pq_M = a.pq_M;
+      sa.pq_K = a.pq_K;
+      sa.pq_ds = a.pq_ds;
+      sa.pq_cb = a.pq_cb;
+      build_pq_lut(sa, qs, reinterpret_cast<float *>(wsm + Ly.prov), lane);
+    } else if (KIND == SPF_INT8) {
+      uint8_t *qc8 = wsm + Ly.prov;
+      const float inv = __fdiv_rn(1.0f, a.i8_scale);
+      const float beta = __fdiv_rn(-a.i8_offset, a.i8_scale);
+      for (uint32_t i = lane; i < a.dpad; i += 32) qc8[i] = i < a.d ? int8_code(qs[i], inv, beta) : 0;
+    } else if (KIND == SPF_F16) {
+      float *qh = reinterpret_cast<float *>(wsm + Ly.prov);
+      for (uint32_t i = lane; i < a.dpad; i += 32) qh[i] = __half2float(__float2half_rn(qs[i]));
+    }
+    __syncwarp();
+    const uint32_t k = a.k;
+    int rcur = 0, rsize = 0;
+    uint32_t *oids32 = nullptr;
+    (void)oids32;
+    if (KIND == SPF_RABITQ) {
+      // ---- 4. search_rabitq: heap of the k smallest exact distances
+      const int kk = (int)k;
+      uint8_t *pv = wsm + Ly.prov;
+      uint64_t *planes = reinterpret_cast<uint64_t *>(pv);
+      float *k5 = reinterpret_cast<float *>(pv + 4 * (a.rq_padded / 64) * 8);
+      float *rbuf = reinterpret_cast<float *>(pv + 4 * (a.rq_padded / 64) * 8 + 32);
+      const uint32_t P2 = a.rq_padded;
+      for (int pi = 0; pi < np; ++pi) {
+        const uint32_t b = key_id(P[pcur][pi]);
+        rabitq_prepare(qs, a.d, P2, a.centroids + (size_t)b * a.dpad, a.rq_signs, rbuf, planes, k5, lane);
+        const uint32_t n_e = a.len[b];
+        for (uint32_t e0 = 0; e0 < n_e; e0 += 32) {
+          const uint32_t e = e0 + lane;
+          const uint32_t row = b * a.cap + e;
+          bool valid = e < n_e;
+          uint32_t id = valid ? __ldg(a.ids + row) : 0u;
+          if (valid && is_deleted(a.deleted, id)) valid = false;
+          float est = 0.0f, err = 0.0f;
+          if (valid) {
+            const uint8_t *code = a.codes + (size_t)row * a.code_stride;
+            est = rabitq_est(code, P2, planes, k5);
+            const float2 nf = __ldg(reinterpret_cast<const float2 *>(code + P2 / 8));
+            const float ip = nf.y > 0.0f ? __fdiv_rn(__fsqrt_rn(nf.x), nf.y) : 0.0f;
+            err = ip > 0.0f ? __fmul_rn(__fmul_rn(__fmul_rn(k5[1], nf.y), 1.9f),
+                                        __fsqrt_rn(__fdiv_rn(fmaxf(__fsub_rn(1.0f, __fmul_rn(ip, ip)), 0.0f),
+                                                             __fsub_rn((float)P2, 1.0f))))
+                            : __int_as_float(0x7f800000);
+          }
+          // candidates that pass against the threshold at the start of the batch
+          // (the threshold only falls, so nothing else can pass later)
+          const float kth0 = rsize < kk ? __int_as_float(0x7f800000) : key_dist(Rl[rcur][kk - 1]);
+          const bool maybe = valid && __fsub_rn(est, err) < kth0;
+          const uint32_t mm = __ballot_sync(kFull, maybe);
+          if (!mm) continue;
+          // exact squared distances of those, computed together
+          uint32_t *stage = reinterpret_cast<uint32_t *>(cst);
+          if (maybe) stage[__popc(mm & lanemask_lt(lane))] = id;
+          __syncwarp();
+          const int cnt = __popc(mm);
+          const uint32_t cid = lane < cnt ? stage[lane] : 0u;
+          const float ex = rows_distance<8, 0, MET_L2>(reinterpret_cast<const uint8_t *>(a.raw), a.dpad * 4,
+                                                       (a.dpad / 4) / 8, qs, cid, cnt, lane, false, 0.0f);
+          __syncwarp();
+          // replay in entry order against the running threshold
+          int slot = 0;
+          for (int j = 0; j < 32; ++j) {
+            if (!((mm >> j) & 1u)) continue;
+            const float ej = __shfl_sync(kFull, __fsub_rn(est, err), j);
+            const float xj = __shfl_sync(kFull, ex, slot);
+            const uint32_t ij = __shfl_sync(kFull, id, j);
+            ++slot;
+            const float kth = rsize < kk ? __int_as_float(0x7f800000) : key_dist(Rl[rcur][kk - 1]);
+            if (ej < kth) insert_batch(lane == 0 ? make_key(xj, ij) : kKeyInvalid, Rl, rcur, rsize, kk, cst + 32, lane);
+          }
+        }
+      }
+      // sqrt for DistL2, then (distance, id) order
+      uint64_t *tmp = Rl[rcur ^ 1];
+      for (int i = lane; i < rsize; i += 32) {
+        const uint64_t kv = Rl[rcur][i];
+        const float dd = key_dist(kv);
+        tmp[i] = make_key(a.metric == DG_L2 ? __fsqrt_rn(dd) : dd, key_id(kv));
+      }
+      __syncwarp();
+      warp_sort_smem(tmp, rsize, lane);
+      const int count = min(rsize, kk);
+      for (int i = lane; i < (int)k; i += 32) {
+        a.out_ids[(size_t)q * k + i] = i < count ? (uint64_t)key_id(tmp[i]) : DG_PAD64;
+        a.out_d[(size_t)q * k + i] = i < count ? key_dist(tmp[i]) : __int_as_float(0x7f800000);
+      }
+      if (lane == 0) a.out_cnt[q] = (uint32_t)count;
+      __syncwarp();
+      continue;
+    }
+    // ---- 3. scan (src/spfresh.rs:702-717)
+    const bool rerank = KIND != SPF_RAW && a.rerank > 0;
+    const int want = (int)(rerank ? max(k, a.rerank) : k);
+    for (int pi = 0; pi < np; ++pi) {
+      const uint32_t b = key_id(P[pcur][pi]);
+      const uint32_t n_e = a.len[b];
+      for (uint32_t e0 = 0; e0 < n_e; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        const int cnt = (int)min(32u, n_e - e0);
+        const uint32_t row = b * a.cap + min(e, n_e - 1);
+        const uint32_t id = __ldg(a.ids + row);
+        const float dd = entry_distance<KIND, MET>(a, wsm, Ly, row, cnt, lane, qq);
+        const bool ok = e < n_e && !is_deleted(a.deleted, id);
+        insert_batch(ok ? make_key(dd, id) : kKeyInvalid, Rl, rcur, rsize, want, cst, lane);
+      }
+    }
+    // rerank from the raw store (src/spfresh.rs:719-723), then (distance, id) order
+    uint64_t *src = Rl[rcur];
+    uint64_t *tmp = Rl[rcur ^ 1];
+    if (rerank) {
+      for (int g0 = 0; g0 < rsize; g0 += 32) {
+        const int cnt = min(32, rsize - g0);
+        const uint32_t cid = lane < cnt ? key_id(src[g0 + lane]) : 0u;
+        float ex = 0.0f;
+        if (MET == MET_L2)
+          ex = rows_distance<8, 0, MET_L2>(reinterpret_cast<const uint8_t *>(a.raw), a.dpad * 4, (a.dpad / 4) / 8, qs,
+                                           cid, cnt, lane, a.metric == DG_L2, qq);
+        else
+          ex = rows_distance<8, 0, MET>(reinterpret_cast<const uint8_t *>(a.raw), a.dpad * 4, (a.dpad / 4) / 8, qs,
+                                        cid, cnt, lane, false, qq);
+        if (lane < cnt) tmp[g0 + lane] = make_key(ex, cid);
+      }
+      __syncwarp();
+      warp_sort_smem(tmp, rsize, lane);
+      src = tmp;
+    }
+    const int count = min(rsize, (int)k);
+    for (int i = lane; i < (int)k; i += 32) {
+      a.out_ids[(size_t)q * k + i] = i < count ? (uint64_t)key_id(src[i]) : DG_PAD64;
+      a.out_d[(size_t)q * k + i] = i < count ? key_dist(src[i]) : __int_as_float(0x7f800000);
+    }
+    if (lane == 0) a.out_cnt[q] = (uint32_t)count;
+    __syncwarp();
+  }
+}
+
+template <int KIND, int MET>
+static DgStatus spf_launch(const SpfArgs &a, uint32_t pcap, uint32_t rcap, cudaStream_t st) {
+  const SpfLayout Ly = spf_layout(pcap, rcap, a.dpad, KIND, a.pq_M, a.pq_K, a.rq_padded);
+  auto kern = spfresh_kernel<KIND, MET>;
+  const uint32_t smem = Ly.total * 4;
+  int dev = 0, sms = 0, optin = 0;
+  DG_CUDA(cudaGetDevice(&dev));
+  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem > (uint32_t)optin) return fail(DG_ENOTSUP, "SPFresh search state does not fit in shared memory");
+  DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int nb = 0;
+  DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 128, smem));
+  if (nb < 1) return fail(DG_ENOTSUP, "SPFresh kernel cannot be resident");
+  const int grid = std::max(1, std::min(nb * sms, (int)((a.nq + 3) / 4)));
+  kern<<<grid, 128, smem, st>>>(a, Ly, pcap, rcap);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+template <int KIND>
+static DgStatus spf_launch_met(const SpfArgs &a, int met, uint32_t pcap, uint32_t rcap, cudaStream_t st) {
+  if (met == MET_L2) return spf_launch<KIND, MET_L2>(a, pcap, rcap, st);
+  if (KIND == SPF_PQ || KIND == SPF_RABITQ) return fail(DG_ENOTSUP, "this code kind supports l2 metrics only");
+  if (met == MET_DOT) return spf_launch<KIND, MET_DOT>(a, pcap, rcap, st);
+  return spf_launch<KIND, MET_COS>(a, pcap, rcap, st);
+}
+
+static DgStatus spf_alloc(DgSpfresh *s, void **p, size_t bytes) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  s->allocs.push_back(q);
+  *p = q;
+  return DG_OK;
+}
+
+}  // namespace dg
+
+using namespace dg;
+
+extern "C" {
+
+DgStatus dg_spfresh_destroy(DgSpfresh *s) {
+  if (!s) return DG_OK;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (void *p : s->allocs) cudaFree(p);
+  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt})
+    if (b->p) cudaFree(b->p);
+  if (s->counter) cudaFree(s->counter);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return DG_OK;
+}
+
+DgStatus dg_spfresh_create(const DgSpfreshDesc *desc, DgSpfresh **out) {
+  if (!desc || !out) return fail(DG_EINVAL, "null argument");
+  *out = nullptr;
+  if (desc->dim == 0 || desc->num_blocks == 0 || desc->block_cap == 0)
+    return fail(DG_EINVAL, "SPFresh needs dim, num_blocks and block_cap >= 1");
+  if (desc->id_capacity >= (1ull << 31)) return fail(DG_EINVAL, "SPFresh ids must stay below 2^31");
+  if ((uint64_t)desc->num_blocks * desc->block_cap >= (1ull << 32)) return fail(DG_EINVAL, "too many posting slots");
+  if (desc->metric < DG_L2SQ || desc->metric > DG_DOT) return fail(DG_EINVAL, "unknown metric");
+  if (!desc->centroids || !desc->block_live || !desc->block_len || !desc->entry_ids || !desc->raw)
+    return fail(DG_EINVAL, "centroids, block arrays, entry ids and raw vectors are required");
+  const uint32_t d = desc->dim, dpad = dpad_of(d);
+  uint32_t code_size = 0;
+  switch (desc->quantizer) {
+    case DG_Q_NONE: code_size = d * 4; break;
+    case DG_Q_F16: code_size = d * 2; break;
+    case DG_Q_INT8: code_size = d; break;
+    case DG_Q_PQ:
+      if (!desc->pq_codebooks || desc->pq_M == 0 || d % desc->pq_M || desc->pq_K == 0 || desc->pq_K > 256)
+        return fail(DG_EINVAL, "bad PQ parameters");
+      code_size = desc->pq_M;
+      break;
+    case DG_Q_RABITQ: {
+      uint32_t want = 1;
+      while (want < std::max(d, 64u)) want <<= 1;
+      if (desc->rq_padded != want || !desc->rq_signs) return fail(DG_EINVAL, "bad RaBitQ parameters");
+      code_size = want / 8 + 8;
+      break;
+    }
+    default: return fail(DG_EINVAL, "unknown quantizer");
+  }
+  if (desc->code_size != code_size)
+    return fail(DG_EINVAL, "code_size must be " + std::to_string(code_size) + " for this quantizer and dimension");
+  if (!desc->entry_codes) return fail(DG_EINVAL, "entry codes are required");
+  DG_CUDA(cudaSetDevice(desc->device));
+  DgSpfresh *s = new (std::nothrow) DgSpfresh();
+  if (!s) return fail(DG_ENOMEM, "host allocation failed");
+  auto bail = [&](DgStatus st) {
+    dg_spfresh_destroy(s);
+    return st;
+  };
+  s->device = desc->device;
+  s->d = d;
+  s->dpad = dpad;
+  s->nblocks = desc->num_blocks;
+  s->cap = desc->block_cap;
+  s->metric = desc->metric;
+  s->quant = desc->quantizer;
+  s->code_size = code_size;
+  // raw codes are rows of the padded dimension so they share the FP32 gather
+  s->code_stride = desc->quantizer == DG_Q_NONE ? dpad * 4
+                   : desc->quantizer == DG_Q_F16 ? dpad * 2
+                   : desc->quantizer == DG_Q_INT8 ? dpad
+                                                  : ((code_size + 15u) & ~15u);
+  s->id_cap = desc->id_capacity;
+  s->pq_M = desc->pq_M;
+  s->pq_K = desc->pq_K;
+  s->i8_scale = desc->int8_scale;
+  s->i8_offset = desc->int8_offset;
+  s->rq_padded = desc->rq_padded;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(DG_EDEVICE, "stream creation failed"));
+  DgStatus st;
+  const size_t nb = s->nblocks, slots = nb * s->cap;
+  if ((st = spf_alloc(s, (void **)&s->centroids, nb * dpad * 4)) != DG_OK) return bail(st);
+  if ((st = spf_alloc(s, (void **)&s->live, nb)) != DG_OK) return bail(st);
+  if ((st = spf_alloc(s, (void **)&s->len, nb * 4)) != DG_OK) return bail(st);
+  if ((st = spf_alloc(s, (void **)&s->ids, slots * 4)) != DG_OK) return bail(st);
+  if ((st = spf_alloc(s, (void **)&s->codes, slots * s->code_stride)) != DG_OK) return bail(st);
+  if ((st = spf_alloc(s, (void **)&s->deleted, ((s->id_cap + 31) / 32 + 1) * 4)) != DG_OK) return bail(st);
+  if ((st = spf_alloc(s, (void **)&s->raw, std::max<uint64_t>(s->id_cap, 1) * dpad * 4)) != DG_OK) return bail(st);
+  if (cudaMalloc(&s->counter, 4) != cudaSuccess) return bail(fail(DG_ENOMEM, "counter allocation"));
+  cudaStream_t ss = s->stream;
+  if ((st = upload_rows_f32(desc->centroids, nb, d, dpad, s->centroids, ss)) != DG_OK) return bail(st);
+  DG_CUDA(cudaMemcpyAsync(s->live, desc->block_live, nb, cudaMemcpyHostToDevice, ss));
+  DG_CUDA(cudaMemcpyAsync(s->len, desc->block_len, nb * 4, cudaMemcpyHostToDevice, ss));
+  {
+    std::vector<uint32_t> ids32(slots);
+    for (size_t i = 0; i < slots; ++i) {
+      const uint64_t v = desc->entry_ids[i];
+      if (v != DG_PAD64 && v >= s->id_cap) return bail(fail(DG_EINVAL, "entry id beyond id_capacity"));
+      ids32[i] = v == DG_PAD64 ? 0u : (uint32_t)v;
+    }
+    for (size_t b = 0; b < nb; ++b)
+      if (desc->block_len[b] > s->cap) return bail(fail(DG_EINVAL, "block_len above block_cap"));
+    DG_CUDA(cudaMemcpyAsync(s->ids, ids32.data(), slots * 4, cudaMemcpyHostToDevice, ss));
+    DG_CUDA(cudaStreamSynchronize(ss));
+  }
+  DG_CUDA(cudaMemsetAsync(s->codes, 0, slots * s->code_stride, ss));
+  DG_CUDA(cudaMemcpy2DAsync(s->codes, s->code_stride, desc->entry_codes, code_size, code_size, slots,
+                            cudaMemcpyHostToDevice, ss));
+  DG_CUDA(cudaMemsetAsync(s->deleted, 0, ((s->id_cap + 31) / 32 + 1) * 4, ss));
+  if (desc->deleted) {
+    std::vector<uint32_t> bm((s->id_cap + 31) / 32 + 1, 0u);
+    for (uint64_t i = 0; i < s->id_cap; ++i)
+      if (desc->deleted[i]) bm[i >> 5] |= 1u << (i & 31);
+    DG_CUDA(cudaMemcpyAsync(s->deleted, bm.data(), bm.size() * 4, cudaMemcpyHostToDevice, ss));
+    DG_CUDA(cudaStreamSynchronize(ss));
+  }
+  if ((st = upload_rows_f32(desc->raw, desc->num_raw, d, dpad, s->raw, ss)) != DG_OK) return bail(st);
+  if (desc->quantizer == DG_Q_PQ) {
+    const size_t cbb = (size_t)s->pq_M * s->pq_K * (d / s->pq_M) * 4;
+    if ((st = spf_alloc(s, (void **)&s->pq_cb, cbb)) != DG_OK) return bail(st);
+    DG_CUDA(cudaMemcpyAsync(s->pq_cb, desc->pq_codebooks, cbb, cudaMemcpyHostToDevice, ss));
+  }
+  if (desc->quantizer == DG_Q_RABITQ) {
+    if ((st = spf_alloc(s, (void **)&s->rq_signs, 3ull * s->rq_padded * 4)) != DG_OK) return bail(st);
+    DG_CUDA(cudaMemcpyAsync(s->rq_signs, desc->rq_signs, 3ull * s->rq_padded * 4, cudaMemcpyHostToDevice, ss));
+  }
+  if (cudaStreamSynchronize(ss) != cudaSuccess) return bail(fail(DG_EDEVICE, "upload failed"));
+  *out = s;
+  return DG_OK;
+}
+
+DgStatus dg_spfresh_update_blocks(DgSpfresh *s, const uint32_t *blocks, uint32_t nupd, const float *centroids,
+                                  const uint8_t *live, const uint32_t *lens, const uint64_t *entry_ids,
+                                  const uint8_t *entry_codes) {
+  if (!s || (nupd && (!blocks || !centroids || !live || !lens || !entry_ids || !entry_codes)))
+    return fail(DG_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  DG_CUDA(cudaSetDevice(s->device));
+  cudaStream_t ss = s->stream;
+  std::vector<uint32_t> ids32(s->cap);
+  for (uint32_t u = 0; u < nupd; ++u) {
+    const uint32_t b = blocks[u];
+    if (b >= s->nblocks) return fail(DG_EINVAL, "block index out of range");
+    if (lens[u] > s->cap) return fail(DG_EINVAL, "block_len above block_cap");
+    for (uint32_t i = 0; i < s->cap; ++i) {
+      const uint64_t v = entry_ids[(size_t)u * s->cap + i];
+      if (i < lens[u] && v >= s->id_cap) return fail(DG_EINVAL, "entry id beyond id_capacity");
+      ids32[i] = i < lens[u] ? (uint32_t)v : 0u;
+    }
+    DG_CUDA(cudaMemcpyAsync(s->ids + (size_t)b * s->cap, ids32.data(), s->cap * 4, cudaMemcpyHostToDevice, ss));
+    DgStatus st = upload_rows_f32(centroids + (size_t)u * s->d, 1, s->d, s->dpad, s->centroids + (size_t)b * s->dpad, ss);
+    if (st != DG_OK) return st;
+    DG_CUDA(cudaMemcpyAsync(s->live + b, live + u, 1, cudaMemcpyHostToDevice, ss));
+    DG_CUDA(cudaMemcpyAsync(s->len + b, lens + u, 4, cudaMemcpyHostToDevice, ss));
+    uint8_t *dst = s->codes + (size_t)b * s->cap * s->code_stride;
+    DG_CUDA(cudaMemsetAsync(dst, 0, (size_t)s->cap * s->code_stride, ss));
+    DG_CUDA(cudaMemcpy2DAsync(dst, s->code_stride, entry_codes + (size_t)u * s->cap * s->code_size, s->code_size,
+                              s->code_size, s->cap, cudaMemcpyHostToDevice, ss));
+    DG_CUDA(cudaStreamSynchronize(ss));  // ids32 is reused for the next block
+  }
+  return DG_OK;
+}
+
+DgStatus dg_spfresh_put_raw(DgSpfresh *s, uint64_t first_id, const float *vectors, uint64_t n) {
+  if (!s || (n && !vectors)) return fail(DG_EINVAL, "null argument");
+  if (first_id + n > s->id_cap) return fail(DG_EINVAL, "raw rows beyond id_capacity");
+  std::lock_guard<std::mutex> lk(s->mu);
+  DG_CUDA(cudaSetDevice(s->device));
+  DgStatus st = upload_rows_f32(vectors, n, s->d, s->dpad, s->raw + first_id * s->dpad, s->stream);
+  if (st != DG_OK) return st;
+  DG_CUDA(cudaStreamSynchronize(s->stream));
+  return DG_OK;
+}
+
+DgStatus dg_spfresh_set_deleted(DgSpfresh *s, const uint64_t *ids, uint64_t n, int32_t deleted) {
+  if (!s || (n && !ids)) return fail(DG_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  DG_CUDA(cudaSetDevice(s->device));
+  const size_t words = (s->id_cap + 31) / 32 + 1;
+  std::vector<uint32_t> bm(words);
+  DG_CUDA(cudaMemcpyAsync(bm.data(), s->deleted, words * 4, cudaMemcpyDeviceToHost, s->stream));
+  DG_CUDA(cudaStreamSynchronize(s->stream));
+  for (uint64_t i = 0; i < n; ++i) {
+    if (ids[i] >= s->id_cap) return fail(DG_EINVAL, "id beyond id_capacity");
+    if (deleted) bm[ids[i] >> 5] |= 1u << (ids[i] & 31);
+    else bm[ids[i] >> 5] &= ~(1u << (ids[i] & 31));
+  }
+  DG_CUDA(cudaMemcpyAsync(s->deleted, bm.data(), words * 4, cudaMemcpyHostToDevice, s->stream));
+  DG_CUDA(cudaStreamSynchronize(s->stream));
+  return DG_OK;
+}
+
+DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const float *queries, uint32_t nq,
+                                 uint64_t *out_ids, float *out_dists, uint32_t *out_counts) {
+  if (!s || !p) return fail(DG_EINVAL, "null argument");
+  if (nq == 0) return DG_OK;
+  if (!queries || !out_ids || !out_dists || !out_counts) return fail(DG_EINVAL, "null buffer");
+  if (p->k == 0) return fail(DG_EINVAL, "k must be >= 1");
+  const uint32_t nprobe = std::max(p->nprobe, 1u);
+  const bool rq = s->quant == DG_Q_RABITQ && (s->metric == DG_L2 || s->metric == DG_L2SQ);
+  const bool rerank = s->quant != DG_Q_NONE && !rq && p->rerank_size > 0;
+  const uint32_t want = rerank ? std::max(p->k, p->rerank_size) : p->k;
+  auto cap_of = [](uint32_t x) -> uint32_t { return x <= 64 ? 64 : x <= 256 ? 256 : x <= 1024 ? 1024 : 0; };
+  const uint32_t pcap = cap_of(nprobe), rcap = cap_of(want);
+  if (!pcap) return fail(DG_ENOTSUP, "n_probe above 1024");
+  if (!rcap) return fail(DG_ENOTSUP, "k / rerank_size above 1024");
+  if (s->quant == DG_Q_RABITQ && !rq) return fail(DG_ENOTSUP, "RaBitQ postings support l2 metrics only");
+  if (s->quant == DG_Q_PQ && s->metric != DG_L2 && s->metric != DG_L2SQ)
+    return fail(DG_ENOTSUP, "PQ postings support l2 metrics only");
+  const bool devptr = (p->flags & DG_FLAG_DEVICE_PTRS) != 0;
+  std::lock_guard<std::mutex> lk(s->mu);
+  DG_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (p->flags & DG_FLAG_STREAM) || p->stream ? (cudaStream_t)p->stream : s->stream;
+  SpfArgs a{};
+  a.d = s->d;
+  a.dpad = s->dpad;
+  a.nblocks = s->nblocks;
+  a.cap = s->cap;
+  a.metric = s->metric;
+  a.centroids = s->centroids;
+  a.live = s->live;
+  a.len = s->len;
+  a.ids = s->ids;
+  a.codes = s->codes;
+  a.code_stride = s->code_stride;
+  a.deleted = s->deleted;
+  a.raw = s->raw;
+  a.pq_M = s->pq_M;
+  a.pq_K = s->pq_K;
+  a.pq_ds = s->pq_M ? s->d / s->pq_M : 0;
+  a.pq_cb = s->pq_cb;
+  a.i8_scale = s->i8_scale;
+  a.i8_offset = s->i8_offset;
+  a.rq_padded = s->rq_padded;
+  a.rq_signs = s->rq_signs;
+  a.nq = nq;
+  a.k = p->k;
+  a.nprobe = nprobe;
+  a.rerank = rerank ? p->rerank_size : 0;
+  a.probe_ratio = p->probe_ratio;
+  a.counter = s->counter;
+  DgStatus r;
+  const size_t kq = (size_t)nq * p->k;
+  if (devptr) {
+    a.Q = queries;
+    a.out_ids = out_ids;
+    a.out_d = out_dists;
+    a.out_cnt = out_counts;
+  } else {
+    if ((r = buf_reserve(s->q, (size_t)nq * s->d * 4)) != DG_OK) return r;
+    if ((r = buf_reserve(s->oids, kq * 8)) != DG_OK) return r;
+    if ((r = buf_reserve(s->od, kq * 4)) != DG_OK) return r;
+    if ((r = buf_reserve(s->ocnt, (size_t)nq * 4)) != DG_OK) return r;
+    DG_CUDA(cudaMemcpyAsync(s->q.p, queries, (size_t)nq * s->d * 4, cudaMemcpyHostToDevice, st));
+    a.Q = (const float *)s->q.p;
+    a.out_ids = (uint64_t *)s->oids.p;
+    a.out_d = (float *)s->od.p;
+    a.out_cnt = (uint32_t *)s->ocnt.p;
+  }
+  DG_CUDA(cudaMemsetAsync(s->counter, 0, 4, st));
+  const int met = s->metric == DG_DOT ? MET_DOT : s->metric == DG_COSINE ? MET_COS : MET_L2;
+  switch (s->quant) {
+    case DG_Q_NONE: r = spf_launch_met<SPF_RAW>(a, met, pcap, rcap, st); break;
+    case DG_Q_PQ: r = spf_launch_met<SPF_PQ>(a, met, pcap, rcap, st); break;
+    case DG_Q_INT8: r = spf_launch_met<SPF_INT8>(a, met, pcap, rcap, st); break;
+    case DG_Q_F16: r = spf_launch_met<SPF_F16>(a, met, pcap, rcap, st); break;
+    default: r = spf_launch_met<SPF_RABITQ>(a, met, pcap, rcap, st); break;
+  }
+  if (r != DG_OK) return r;
+  if (!devptr) {
+    DG_CUDA(cudaMemcpyAsync(out_ids, a.out_ids, kq * 8, cudaMemcpyDeviceToHost, st));
+    DG_CUDA(cudaMemcpyAsync(out_dists, a.out_d, kq * 4, cudaMemcpyDeviceToHost, st));
+    DG_CUDA(cudaMemcpyAsync(out_counts, a.out_cnt, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
+    DG_CUDA(cudaStreamSynchronize(st));
+  }
+  return DG_OK;
+}
+
+}  // extern "C"

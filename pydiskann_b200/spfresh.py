@@ -1,0 +1,573 @@
+"""SPFresh (diskann-rs src/spfresh.rs): posting lists searched on the GPU,
+maintained on the host.
+
+Search runs in libdgann (dg_spfresh_search_batch): routing to the nprobe
+nearest live postings, the probe_ratio cut, the scan with tombstones and the
+FP32 rerank, or the RaBitQ error-bound scan.  This module holds the host side
+of the index the way the reference keeps it -- posting slots with
+(id, code) entries, centroids, a raw vector store, tombstones -- and restates
+its update path: insert (nearest posting, push, split when full,
+src/spfresh.rs:416-476), drain / split with 2-means and neighbourhood
+reassignment (:122-162, 502-611), relocate (:538-573) and gc (:613-643).
+Routing is brute force over the live centroids at every size (the reference
+switches to a centroid graph above 4096 postings, :358-378; that graph is
+rebuilt non-deterministically, so exact routing is used instead).  Changed
+posting slots are uploaded to the device after each call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr
+
+_METRICS = {"l2": _lib.L2SQ, "cosine": _lib.COSINE, "dot": _lib.DOT, "euclidean": _lib.L2}
+CHUNK = 4096
+
+
+def _dist_rows(metric, v, C_):
+    """metric_eval(v, row) for every row of C_ (float64 accumulation)."""
+    v = v.astype(np.float64)
+    Cm = C_.astype(np.float64)
+    if metric in (_lib.L2SQ, _lib.L2):
+        d = ((Cm - v) ** 2).sum(1)
+        return np.sqrt(d) if metric == _lib.L2 else d
+    ab = Cm @ v
+    if metric == _lib.DOT:
+        return 1.0 - ab
+    aa, bb = float(v @ v), (Cm * Cm).sum(1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = 1.0 - ab / (np.sqrt(aa) * np.sqrt(bb))
+    r = np.where((aa == 0) & (bb == 0), 0.0, np.where(ab == 0, 1.0, r))
+    return np.maximum(r, 0.0)
+
+
+def _fht(v):
+    """Unnormalised fast Walsh-Hadamard transform along the last axis (src/rabitq.rs:31-43)."""
+    v = v.copy()
+    n = v.shape[-1]
+    h = 1
+    while h < n:
+        a = v.reshape(*v.shape[:-1], n // (2 * h), 2, h)
+        x, y = a[..., 0, :].copy(), a[..., 1, :].copy()
+        a[..., 0, :] = x + y
+        a[..., 1, :] = x - y
+        h *= 2
+    return v
+
+
+class _Codec:
+    """Code of a vector stored in a posting (Inner::encode, src/spfresh.rs:328-339)."""
+
+    def __init__(self, kind, dim, params):
+        self.kind, self.dim, self.p = kind, dim, params
+        if kind is None:
+            self.size = 4 * dim
+        elif kind == "f16":
+            self.size = 2 * dim
+        elif kind == "int8":
+            self.size = dim
+        elif kind == "pq":
+            self.size = params["codebooks"].shape[0]
+        else:
+            self.size = params["padded"] // 8 + 8
+
+    @property
+    def residual(self):
+        return self.kind == "rabitq"
+
+    def encode(self, V, centroid=None):
+        V = np.atleast_2d(np.asarray(V, dtype=np.float32))
+        if self.kind is None:
+            return V.view(np.uint8).reshape(len(V), -1).copy()
+        if self.kind == "f16":
+            return V.astype(np.float16).view(np.uint8).reshape(len(V), -1).copy()
+        if self.kind == "int8":
+            s, o = np.float32(self.p["scale"]), np.float32(self.p["offset"])
+            t = V * (np.float32(1.0) / s) + (-o / s)
+            return np.clip(np.rint(t), 0, 255).astype(np.uint8)
+        if self.kind == "pq":
+            cb = self.p["codebooks"]
+            M, K, ds = cb.shape
+            out = np.empty((len(V), M), dtype=np.uint8)
+            for m in range(M):
+                sub = V[:, m * ds:(m + 1) * ds]
+                d = ((sub[:, None, :] - cb[m][None]) ** 2).sum(-1, dtype=np.float32)
+                out[:, m] = d.argmin(1)
+            return out
+        # RaBitQ residual code against the posting centroid (src/rabitq.rs:218-256)
+        P, signs = self.p["padded"], self.p["signs"].reshape(3, -1)
+        r = np.zeros((len(V), P), dtype=np.float32)
+        r[:, : self.dim] = V - centroid
+        norm = np.sqrt((r * r).sum(1, dtype=np.float32)).astype(np.float32)
+        nz = norm > 0
+        r[nz] /= norm[nz, None]
+        for rd in range(3):
+            r = _fht(r * signs[rd])
+        bits = np.packbits(r > 0, axis=1, bitorder="little")
+        ip = np.abs(r).sum(1, dtype=np.float32) / np.float32(math.sqrt(P))
+        fac = np.where(ip > 0, norm / np.where(ip > 0, ip, 1), 0).astype(np.float32)
+        tail = np.stack([norm * norm, fac], 1).astype(np.float32).view(np.uint8)
+        return np.concatenate([bits, tail], 1)
+
+
+def kmeans2(vs, metric):
+    """2-means on raw vectors with an index split when degenerate (src/spfresh.rs:122-162)."""
+    n = len(vs)
+
+    def means(side):
+        out = []
+        for k in (False, True):
+            sel = vs[side == k]
+            cnt = max(len(sel), 1)
+            out.append((sel.sum(0, dtype=np.float32) / np.float32(cnt)).astype(np.float32))
+        return out
+
+    d0 = _dist_rows(metric, vs[0], vs[1:]) if n > 1 else np.zeros(0)
+    far = int(np.argmax(d0)) + 1 if n > 1 else 0
+    c = [vs[0].copy(), vs[far].copy()]
+    side = np.zeros(n, dtype=bool)
+    for _ in range(5):
+        side = _dist_rows(metric, c[1], vs) < _dist_rows(metric, c[0], vs)
+        if side.all() or not side.any():
+            break
+        c = means(side)
+    if side.all() or not side.any():
+        side = np.arange(n) >= n // 2
+        c = means(side)
+    return c[0], c[1], side
+
+
+class SPFresh:
+    """SPFresh<D> (src/spfresh.rs:774-936) with GPU posting scans."""
+
+    def __init__(self, dim, metric="l2", quantizer=None, qparams=None, rerank_size=0, max_posting_size=128,
+                 min_posting_size=16, reassign_neighbors=16, probe_ratio=float("inf"), device=0):
+        if metric not in _METRICS:
+            raise ValueError(f"unknown metric: {metric}")
+        self.dim, self.metric_name, self.metric = dim, metric, _METRICS[metric]
+        self.codec = _Codec(quantizer, dim, qparams or {})
+        self.rerank_size, self.max_posting, self.min_posting = rerank_size, max_posting_size, min_posting_size
+        self.reassign_neighbors, self.probe_ratio, self.device = reassign_neighbors, probe_ratio, device
+        self.cap = 2 * max_posting_size  # block layout, src/spfresh.rs:109-111
+        self.cent = np.zeros((0, dim), dtype=np.float32)
+        self.live_b = np.zeros(0, dtype=bool)
+        self.ids = []      # per slot: np.uint64 array of entry ids
+        self.codes = []    # per slot: u8 [len, code_size]
+        self.free = []
+        self.raw = np.zeros((0, dim), dtype=np.float32)
+        self.next_id = 0
+        self.deleted = set()
+        self.live = 0
+        self.created = []
+        self._h = None
+        self._dirty = set()
+        self._dev_blocks = 0
+        self._dev_ids = 0
+        self._raw_synced = 0
+        self._del_synced = set()
+
+    # ------------------------------------------------------------ building
+    @staticmethod
+    def build(vectors, path=None, metric="l2", quantizer=None, rerank_size=0, pq_subspaces=8,
+              max_posting_size=128, min_posting_size=16, reassign_neighbors=16, probe_ratio=float("inf"),
+              seed=0, device=0):
+        """SPFresh::build (src/spfresh.rs:801-817): n / (max_posting/2) postings seeded
+        from random vectors, then every vector inserted."""
+        X = np.ascontiguousarray(vectors, dtype=np.float32)
+        if X.ndim != 2 or len(X) == 0:
+            raise RuntimeError("Index error: No vectors provided")
+        if quantizer not in (None, "f16", "int8", "pq", "rabitq"):
+            raise ValueError(f"unknown quantizer: {quantizer}")
+        import pydiskann_b200 as dg
+
+        qp = {}
+        if quantizer == "pq" and device is None:
+            raise ValueError("PQ training runs on the GPU; give a device")
+        if quantizer == "int8":
+            qp["scale"], qp["offset"] = dg.int8_params(X)
+        elif quantizer == "pq":
+            qp["codebooks"] = dg.pq_train(X, pq_subspaces, 256, 20, 50_000, seed, device)
+        elif quantizer == "rabitq":
+            _, signs = dg.rabitq_params(X, seed)
+            qp["padded"], qp["signs"] = dg.rabitq_padded(X.shape[1]), signs
+        s = SPFresh(X.shape[1], metric, quantizer, qp, rerank_size, max_posting_size, min_posting_size,
+                    reassign_neighbors, probe_ratio, device)
+        k = max(1, len(X) // max(max_posting_size // 2, 1))
+        rng = np.random.default_rng([seed, 0x5EED])
+        for i in rng.choice(len(X), size=min(k, len(X)), replace=False):
+            s._new_posting(X[i].copy())
+        s._insert(X)
+        s._sync()
+        return s
+
+    # ------------------------------------------------------------ host state
+    def _len(self, b):
+        return len(self.ids[b])
+
+    def _is_live(self, b):
+        return 0 <= b < len(self.live_b) and bool(self.live_b[b])
+
+    def _live_entries(self, b):
+        ids, codes = self.ids[b], self.codes[b]
+        keep = np.array([int(i) not in self.deleted for i in ids], dtype=bool) if len(ids) else np.zeros(0, bool)
+        return ids[keep], codes[keep]
+
+    def _new_posting(self, centroid):
+        if self.free:
+            b = self.free.pop()
+            self.cent[b] = centroid
+        else:
+            b = len(self.live_b)
+            self.cent = np.vstack([self.cent, centroid[None].astype(np.float32)])
+            self.live_b = np.append(self.live_b, False)
+            self.ids.append(np.zeros(0, dtype=np.uint64))
+            self.codes.append(np.zeros((0, self.codec.size), dtype=np.uint8))
+        self.live_b[b] = True
+        self.ids[b] = np.zeros(0, dtype=np.uint64)
+        self.codes[b] = np.zeros((0, self.codec.size), dtype=np.uint8)
+        self.created.append(b)
+        self._dirty.add(b)
+        return b
+
+    def _free_posting(self, b):
+        self.live_b[b] = False
+        self.ids[b] = np.zeros(0, dtype=np.uint64)
+        self.codes[b] = np.zeros((0, self.codec.size), dtype=np.uint8)
+        self.free.append(b)
+        self._dirty.add(b)
+
+    def _rewrite(self, b, ids, codes):
+        self.ids[b], self.codes[b] = np.asarray(ids, dtype=np.uint64), np.asarray(codes, dtype=np.uint8).reshape(-1, self.codec.size)
+        self._dirty.add(b)
+
+    def _push(self, b, id_, code):
+        self.ids[b] = np.append(self.ids[b], np.uint64(id_))
+        self.codes[b] = np.vstack([self.codes[b], np.asarray(code, dtype=np.uint8).reshape(1, -1)])
+        self._dirty.add(b)
+
+    def _encode(self, v, b):
+        return self.codec.encode(v, self.cent[b] if self.codec.residual else None)[0]
+
+    def _nearest(self, v, n):
+        """Live postings by (distance to centroid, slot), closest first (src/spfresh.rs:358-378)."""
+        live = np.nonzero(self.live_b)[0]
+        if len(live) == 0:
+            return []
+        d = _dist_rows(self.metric, v, self.cent[live]).astype(np.float32)
+        order = np.lexsort((live, d))[: max(n, 0)]
+        return [(int(live[i]), float(d[i])) for i in order]
+
+    def _dist(self, v, b):
+        return float(_dist_rows(self.metric, v, self.cent[b:b + 1])[0])
+
+    # --------------------------------------------------------------- updates
+    def insert(self, vectors):
+        """Inner::insert (src/spfresh.rs:416-476); returns the new ids."""
+        X = np.ascontiguousarray(vectors, dtype=np.float32)
+        if X.size == 0:
+            X = X.reshape(0, self.dim)
+        if X.ndim != 2 or X.shape[1] != self.dim:
+            raise RuntimeError(f"Index error: Vector dim {X.shape[-1]} != index dim {self.dim}")
+        ids = self._insert(X)
+        self._sync()
+        return ids
+
+    def _insert(self, X):
+        first = self.next_id
+        ids = list(range(first, first + len(X)))
+        if first + len(X) > len(self.raw):
+            grow = np.zeros((max(first + len(X), 2 * len(self.raw)) - len(self.raw), self.dim), dtype=np.float32)
+            self.raw = np.vstack([self.raw, grow])
+        self.raw[first:first + len(X)] = X
+        self.next_id += len(X)
+        self.live += len(X)
+        for c0 in range(0, len(X), CHUNK):
+            chunk = X[c0:c0 + CHUNK]
+            self.created = []
+            live = np.nonzero(self.live_b)[0]
+            targets = []
+            if len(live):
+                Cm = self.cent[live].astype(np.float64)
+                for v in chunk:
+                    d = _dist_rows(self.metric, v, Cm).astype(np.float32)
+                    targets.append(int(live[np.lexsort((live, d))[0]]))
+            else:
+                targets = [None] * len(chunk)
+            for j, v in enumerate(chunk):
+                id_ = first + c0 + j
+                t = targets[j]
+                best = (t, self._dist(v, t)) if t is not None and self._is_live(t) else None
+                if best is None:
+                    nn = self._nearest(v, 1)
+                    best = nn[0] if nn else None
+                for c in list(self.created):
+                    if self._is_live(c):
+                        dc = self._dist(v, c)
+                        if best is None or dc < best[1]:
+                            best = (c, dc)
+                b = best[0] if best is not None else self._new_posting(v.copy())
+                self._push(b, id_, self._encode(v, b))
+                if self._len(b) >= self.max_posting:
+                    self._drain([b])
+        return ids
+
+    def _neighbourhood(self, p):
+        return [b for b, _ in self._nearest(self.cent[p], self.reassign_neighbors + 2)]
+
+    def _local_moves(self, p, cands):
+        ids, _ = self._live_entries(p)
+        cands = [t for t in cands if t != p and self._is_live(t)]
+        moves = []
+        if not cands:
+            return moves
+        for id_ in ids:
+            v = self.raw[int(id_)]
+            dp = self._dist(v, p)
+            d = _dist_rows(self.metric, v, self.cent[cands])
+            i = int(np.argmin(d))
+            if d[i] < dp:
+                moves.append((int(id_), cands[i]))
+        return moves
+
+    def _drain(self, queue):
+        while queue:
+            b = queue.pop()
+            if not self._is_live(b):
+                continue
+            if self._len(b) >= self.max_posting:
+                self._split(b, queue)
+            else:
+                self._relocate(b, self._local_moves(b, self._neighbourhood(b)), queue)
+
+    def _relocate(self, frm, moves, queue):
+        if not moves:
+            return
+        mv = dict(moves)
+        ids, codes = self._live_entries(frm)
+        keep = np.array([int(i) not in mv for i in ids], dtype=bool)
+        self._rewrite(frm, ids[keep], codes[keep])
+        for id_, code in zip(ids[~keep], codes[~keep]):
+            t = mv[int(id_)]
+            if not (self._is_live(t) and self._len(t) < 2 * self.max_posting):
+                if frm not in queue:
+                    queue.insert(0, frm)
+                if self._is_live(t):
+                    queue.append(t)
+                t = frm
+            if self.codec.residual:
+                code = self._encode(self.raw[int(id_)], t)
+            self._push(t, int(id_), code)
+            if self._len(t) >= self.max_posting:
+                queue.append(t)
+
+    def _split(self, b, queue):
+        # Splits converge for metric distances; a score such as 1 - dot on
+        # unnormalised data routes every vector to the largest centroid and
+        # keeps splitting, which shows as more postings than vectors.
+        if int(self.live_b.sum()) > max(64, self.next_id):
+            raise RuntimeError("Index error: SPFresh splits did not converge "
+                               "(more postings than vectors; a non-metric score on unnormalised data?)")
+        ids, codes = self._live_entries(b)
+        if len(ids) < 2:
+            self._rewrite(b, ids, codes)
+            return
+        vs = self.raw[ids.astype(np.int64)]
+        c1, c2, side = kmeans2(vs, self.metric)
+        self._free_posting(b)
+        nb = [self._new_posting(c1), self._new_posting(c2)]
+        for id_, code, sd in zip(ids, codes, side):
+            t = nb[int(sd)]
+            if self.codec.residual:
+                code = self._encode(self.raw[int(id_)], t)
+            self._push(t, int(id_), code)
+        around = sorted({q for p in nb for q in self._neighbourhood(p)})
+        for p in nb:
+            self._relocate(p, self._local_moves(p, around), queue)
+        for q in around:
+            if q in nb or not self._is_live(q):
+                continue
+            self._relocate(q, self._local_moves(q, nb), queue)
+        for p in nb:
+            if self._len(p) >= self.max_posting:
+                queue.append(p)
+
+    def delete(self, ids):
+        """SPFresh::delete (src/spfresh.rs:863-871): tombstones."""
+        for i in ids:
+            i = int(i)
+            if i < self.next_id and i not in self.deleted:
+                self.deleted.add(i)
+                self.live -= 1
+        self._sync()
+
+    def is_deleted(self, id):  # noqa: A002
+        return int(id) in self.deleted
+
+    def get_vector(self, id):  # noqa: A002
+        id = int(id)  # noqa: A001
+        return None if id >= self.next_id or id in self.deleted else self.raw[id].tolist()
+
+    def gc(self):
+        """Inner::gc (src/spfresh.rs:613-643): purge tombstones, merge small postings."""
+        queue = []
+        for b in range(len(self.live_b)):
+            if not self._is_live(b):
+                continue
+            ids, codes = self._live_entries(b)
+            if len(ids) < self.min_posting and int(self.live_b.sum()) > 1:
+                self._free_posting(b)
+                for id_, code in zip(ids, codes):
+                    v = self.raw[int(id_)]
+                    nn = self._nearest(v, 1)
+                    t = nn[0][0] if nn else int(np.nonzero(self.live_b)[0][0])
+                    if self.codec.residual:
+                        code = self._encode(v, t)
+                    self._push(t, int(id_), code)
+                    if self._len(t) >= self.max_posting:
+                        queue.append(t)
+                        self._drain(queue)
+            elif len(ids) != self._len(b):
+                self._rewrite(b, ids, codes)
+        self._drain(queue)
+        self._sync()
+
+    def stats(self):
+        sizes = [self._len(b) for b in range(len(self.live_b)) if self._is_live(b)]
+        return {"live": self.live, "deleted": len(self.deleted), "postings": int(self.live_b.sum()),
+                "max_posting": max(sizes) if sizes else 0}
+
+    # ------------------------------------------------------------ device side
+    def host_arrays(self, nblocks=None):
+        """Posting slots as the flat arrays of DgSpfreshDesc."""
+        nb = nblocks or max(len(self.live_b), 1)
+        cent = np.zeros((nb, self.dim), dtype=np.float32)
+        cent[: len(self.cent)] = self.cent
+        live = np.zeros(nb, dtype=np.uint8)
+        live[: len(self.live_b)] = self.live_b
+        lens = np.zeros(nb, dtype=np.uint32)
+        ids = np.full((nb, self.cap), np.uint64(_lib.PAD64), dtype=np.uint64)
+        codes = np.zeros((nb, self.cap, self.codec.size), dtype=np.uint8)
+        for b in range(len(self.live_b)):
+            n = self._len(b)
+            lens[b] = n
+            ids[b, :n] = self.ids[b]
+            codes[b, :n] = self.codes[b]
+        return cent, live, lens, ids, codes
+
+    def _sync(self):
+        if self.device is None:  # host-only instance (update logic without a GPU mirror)
+            return
+        if self._h is None or len(self.live_b) > self._dev_blocks or self.next_id > self._dev_ids:
+            self._create_device()
+            return
+        if self._dirty:
+            blocks = np.array(sorted(self._dirty), dtype=np.uint32)
+            cent, live, lens, ids, codes = self.host_arrays(self._dev_blocks)
+            check(lib().dg_spfresh_update_blocks(
+                self._h, ptr(blocks), len(blocks), ptr(np.ascontiguousarray(cent[blocks])),
+                ptr(np.ascontiguousarray(live[blocks])), ptr(np.ascontiguousarray(lens[blocks])),
+                ptr(np.ascontiguousarray(ids[blocks])), ptr(np.ascontiguousarray(codes[blocks]))))
+            self._dirty.clear()
+        if self.next_id > self._raw_synced:
+            rows = np.ascontiguousarray(self.raw[self._raw_synced:self.next_id])
+            check(lib().dg_spfresh_put_raw(self._h, self._raw_synced, ptr(rows), len(rows)))
+            self._raw_synced = self.next_id
+        new_del = self.deleted - self._del_synced
+        if new_del:
+            arr = np.array(sorted(new_del), dtype=np.uint64)
+            check(lib().dg_spfresh_set_deleted(self._h, ptr(arr), len(arr), 1))
+            self._del_synced |= new_del
+
+    def _create_device(self):
+        if self._h is not None:
+            lib().dg_spfresh_destroy(self._h)
+            self._h = None
+        nb = max(2 * len(self.live_b), 16)
+        id_cap = max(2 * self.next_id, 1024)
+        cent, live, lens, ids, codes = self.host_arrays(nb)
+        raw = np.ascontiguousarray(self.raw[: self.next_id])
+        dele = np.zeros(id_cap, dtype=np.uint8)
+        for i in self.deleted:
+            dele[i] = 1
+        d = _lib.SpfreshDesc()
+        d.dim, d.metric, d.device, d.num_blocks, d.block_cap = self.dim, self.metric, self.device, nb, self.cap
+        keep = [cent, live, lens, ids, codes, raw, dele]
+        d.centroids, d.block_live, d.block_len = ptr(cent), ptr(live), ptr(lens)
+        d.entry_ids, d.entry_codes, d.code_size = ptr(ids), ptr(codes), self.codec.size
+        kinds = {None: _lib.Q_NONE, "f16": _lib.Q_F16, "int8": _lib.Q_INT8, "pq": _lib.Q_PQ, "rabitq": _lib.Q_RABITQ}
+        d.quantizer = kinds[self.codec.kind]
+        if self.codec.kind == "pq":
+            cb = np.ascontiguousarray(self.codec.p["codebooks"], dtype=np.float32)
+            keep.append(cb)
+            d.pq_M, d.pq_K, d.pq_codebooks = cb.shape[0], cb.shape[1], ptr(cb)
+        if self.codec.kind == "int8":
+            d.int8_scale, d.int8_offset = self.codec.p["scale"], self.codec.p["offset"]
+        if self.codec.kind == "rabitq":
+            sg = np.ascontiguousarray(self.codec.p["signs"], dtype=np.float32)
+            keep.append(sg)
+            d.rq_padded, d.rq_signs = self.codec.p["padded"], ptr(sg)
+        d.id_capacity, d.num_raw, d.raw, d.deleted = id_cap, self.next_id, ptr(raw), ptr(dele)
+        h = C.c_void_p()
+        check(lib().dg_spfresh_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self._dev_blocks, self._dev_ids = nb, id_cap
+        self._dirty.clear()
+        self._raw_synced = self.next_id
+        self._del_synced = set(self.deleted)
+
+    def close(self):
+        if self._h is not None:
+            lib().dg_spfresh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ----------------------------------------------------------------- search
+    def search_arrays(self, queries, k=10, n_probe=8, stream=None):
+        """Batched search: numpy in -> numpy out (ids u64, dists f32, counts u32),
+        or CUDA tensors in -> tensors out."""
+        if self._h is None:
+            raise RuntimeError("Index error: this SPFresh instance has no device mirror (device=None)")
+        dev = hasattr(queries, "data_ptr") and getattr(queries, "is_cuda", False)
+        p = _lib.SpfreshParams()
+        p.k, p.nprobe, p.rerank_size, p.probe_ratio = k, n_probe, self.rerank_size, self.probe_ratio
+        if dev:
+            import torch
+
+            Q = queries.contiguous()
+            nq = Q.shape[0]
+            out = (torch.empty((nq, k), dtype=torch.int64, device=Q.device),
+                   torch.empty((nq, k), dtype=torch.float32, device=Q.device),
+                   torch.empty((nq,), dtype=torch.int32, device=Q.device))
+            p.flags = _lib.FLAG_DEVICE_PTRS | _lib.FLAG_STREAM
+            p.stream = stream if stream is not None else torch.cuda.current_stream(Q.device).cuda_stream
+        else:
+            Q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, self.dim)
+            nq = Q.shape[0]
+            out = (np.empty((nq, k), dtype=np.uint64), np.empty((nq, k), dtype=np.float32),
+                   np.empty(nq, dtype=np.uint32))
+        if Q.shape[1] != self.dim:
+            raise ValueError(f"Query dim {Q.shape[1]} != index dim {self.dim}")
+        check(lib().dg_spfresh_search_batch(self._h, C.byref(p), ptr(Q), nq, ptr(out[0]), ptr(out[1]),
+                                            ptr(out[2])))
+        return out
+
+    def search_with_dists(self, query, k=10, n_probe=8):
+        ids, ds, cnt = self.search_arrays(np.asarray(query, dtype=np.float32).reshape(1, -1), k, n_probe)
+        return [(int(ids[0, j]), float(ds[0, j])) for j in range(int(cnt[0]))]
+
+    def search(self, query, k=10, n_probe=8):
+        return [i for i, _ in self.search_with_dists(query, k, n_probe)]
+
+    def search_batch(self, queries, k=10, n_probe=8):
+        ids, ds, cnt = self.search_arrays(queries, k, n_probe)
+        return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
+

@@ -1,0 +1,112 @@
+"""SPFresh posting scans on the GPU vs the oracle's restatement of
+Inner::search / search_rabitq (src/spfresh.rs:671-770) on the same posting
+lists, after inserts and deletes.  Integer-valued data: distances are exact,
+so ids, counts and distances must match bit for bit (cosine within 1e-5)."""
+import numpy as np
+import pytest
+
+import pydiskann_b200 as dg
+from pydiskann_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_view(oracle, s):
+    cent, live, lens, ids, codes = s.host_arrays(len(s.live_b))
+    dele = np.zeros(max(s.next_id, 1), dtype=np.uint8)
+    for i in s.deleted:
+        dele[i] = 1
+    raw = np.ascontiguousarray(s.raw[: s.next_id])
+    v = oracle.Spfresh()
+    keep = [cent, live, lens, ids, codes, dele, raw]
+    p = oracle._p
+    v.d, v.metric, v.num_blocks, v.block_cap = s.dim, s.metric, len(live), s.cap
+    v.block_live, v.centroids, v.block_len, v.entry_ids = p(live), p(cent), p(lens), p(ids)
+    v.entry_codes, v.code_size, v.deleted, v.next_id, v.raw = p(codes), s.codec.size, p(dele), s.next_id, p(raw)
+    q = {None: oracle.Q_NONE, "f16": oracle.Q_F16, "int8": oracle.Q_INT8, "pq": oracle.Q_PQ, "rabitq": oracle.Q_RABITQ}
+    v.quant = q[s.codec.kind]
+    if s.codec.kind == "pq":
+        cb = np.ascontiguousarray(s.codec.p["codebooks"], dtype=np.float32)
+        keep.append(cb)
+        v.pq_M, v.pq_K, v.pq_codebooks = cb.shape[0], cb.shape[1], p(cb)
+    if s.codec.kind == "int8":
+        v.int8_scale, v.int8_offset = s.codec.p["scale"], s.codec.p["offset"]
+    if s.codec.kind == "rabitq":
+        sg = np.ascontiguousarray(s.codec.p["signs"], dtype=np.float32)
+        keep.append(sg)
+        v.rq_padded, v.rq_signs = s.codec.p["padded"], p(sg)
+    v.probe_ratio, v.rerank_size = s.probe_ratio, s.rerank_size
+    return v, keep
+
+
+CASES = [
+    (None, "l2", 0, float("inf")),
+    (None, "euclidean", 0, 1.5),
+    ("int8", "l2", 20, float("inf")),
+    ("int8", "l2", 0, float("inf")),
+    ("f16", "l2", 15, 2.0),
+    ("pq", "l2", 30, float("inf")),
+    ("rabitq", "l2", 0, float("inf")),
+    ("rabitq", "euclidean", 0, float("inf")),
+]
+
+
+@pytest.mark.parametrize("quant,metric,rerank,ratio", CASES)
+def test_spfresh_scan_matches_oracle(oracle, quant, metric, rerank, ratio):
+    X = synth.mixture(4000, 32, 40, seed=12, clip=False)
+    s = dg.SPFresh.build(X, metric=metric, quantizer=quant, rerank_size=rerank, pq_subspaces=8, max_posting_size=40,
+                         min_posting_size=8, probe_ratio=ratio, seed=2)
+    s.insert(synth.mixture(500, 32, 40, seed=13, clip=False))
+    s.delete(list(range(0, 4500, 9)))
+    Q = synth.mixture(120, 32, 40, seed=12, stream=synth.STREAM_QUERY, clip=False)
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 1), (10, 6), (7, 40)):
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc), (k, nprobe)
+        assert np.array_equal(gi, oi), (k, nprobe, np.nonzero((gi != oi).any(1))[0][:5])
+        assert np.array_equal(gd, od), (k, nprobe)
+    s.close()
+
+
+def test_spfresh_cosine_within_tolerance(oracle):
+    X = synth.mixture(3000, 32, 30, seed=14, clip=False)
+    s = dg.SPFresh.build(X, metric="cosine", max_posting_size=40, seed=3)
+    Q = synth.mixture(80, 32, 30, seed=14, stream=synth.STREAM_QUERY, clip=False)
+    view, keep = oracle_view(oracle, s)
+    gi, gd, gc = s.search_arrays(Q, 10, 8)
+    oi, od, oc = oracle.spfresh_search(view, Q, 10, 8)
+    assert np.array_equal(gc, oc)
+    assert np.mean([len(set(gi[i]) & set(oi[i])) / 10 for i in range(len(Q))]) >= 0.98
+    same = gi == oi
+    assert np.allclose(gd[same], od[same], rtol=1e-5, atol=1e-6)
+    s.close()
+
+
+def test_exhaustive_probe_is_exact_knn(oracle):
+    """python/tests/test_spfresh.py:84-90: probing every posting returns the
+    brute-force neighbours of the live vectors."""
+    X = synth.mixture(3000, 32, 20, seed=15, clip=False)
+    s = dg.SPFresh.build(X, max_posting_size=60, seed=4)
+    s.delete(list(range(5, 3000, 11)))
+    Q = synth.mixture(50, 32, 20, seed=15, stream=synth.STREAM_QUERY, clip=False)
+    gi, gd, gc = s.search_arrays(Q, 10, 1024)
+    live = np.array([i for i in range(3000) if i not in s.deleted])
+    ei, ed = oracle.exact_knn(X[live], Q, 10)
+    assert np.array_equal(gi.astype(np.int64), live[ei.astype(np.int64)])
+    assert np.array_equal(gd, ed.astype(np.float32))
+    # batch equals single (python/tests/test_spfresh.py:246-249)
+    batch = s.search_batch(Q[:10], 10, 16)
+    assert all(s.search(Q[i], 10, 16) == batch[i] for i in range(10))
+    s.close()
+
+
+def test_spfresh_api_errors():
+    X = synth.mixture(500, 16, 4, seed=16, clip=False)
+    s = dg.SPFresh.build(X, max_posting_size=32)
+    with pytest.raises(ValueError):
+        s.search([1.0, 2.0], 5, 2)
+    with pytest.raises(RuntimeError):
+        s.insert(np.zeros((2, 8), dtype=np.float32))
+    assert s.stats()["live"] == 500
+    s.close()
