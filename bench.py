@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--variants", default="fp32,bf16_rerank,int8_rerank,pq_rerank")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-rates", default="100000,1000000,0",
+                    help="Poisson arrival rates (req/s) for the serving loop; 0 = all requests at once")
+    ap.add_argument("--serve-requests", type=int, default=200_000)
     return ap.parse_args()
 
 
@@ -349,6 +353,10 @@ def main():
         line["clocks"] = r["clocks"]
         line["gpu_launches"] = args.steps
         line["e2e"] = e2e(args, idx, qidx, head, r["L"], Q, gt, dist, world, dev)
+        if not args.no_serving:
+            line["serving"] = {n: serving(args, idx, qidx, n, results[n]["L"], Q, gt)
+                               for n in dict.fromkeys(["fp32", head]) if n in results}
+            line["p99_ms"] = line["serving"][head]["rates"][-1]["p99_ms"]
         if "fp32" in results:
             line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
     if rank == 0 and head and not args.no_cpu_baseline:
@@ -395,6 +403,42 @@ def e2e(args, idx, qidx, name, L, Q, gt, dist, world, dev):
     return {"value": world * args.nq * args.steps / (ms / 1e3), "unit": "queries/s",
             "h2d_bytes_per_step": int(Q.nbytes), "d2h_bytes_per_step": int(args.nq * (K * 8 + 4)),
             "recall_at_10": round(rec, 4)}
+
+
+def serving(args, idx, qidx, name, L, Q, gt):
+    """Continuous batching: requests arrive one at a time (Poisson) and are
+    admitted into batches as stream slots free up; p50/p99 is measured from
+    each request's scheduled arrival to its result in host memory."""
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import _lib
+
+    trav, rr = VARIANTS[name]
+    target = qidx["pq"] if trav == "codes" else qidx["int8"] if trav == "int8" else idx
+    t = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES,
+         "int8": _lib.TRAVERSE_CODES}[trav]
+    n = args.serve_requests
+    qi = np.arange(n) % len(Q)
+    Qn = Q[qi]
+    out = {"variant": name, "L": L, "max_batch": 2048, "streams": 8, "requests": n, "rates": []}
+    with dg.Server(target, max_batch=2048, streams=8, max_k=K, max_wait_us=0) as srv:
+        srv.run_trace(Qn[:5000], np.zeros(5000), k=K, beam_width=L, rerank_size=L if rr else 0, traversal=t)
+        for rate in [float(x) for x in args.serve_rates.split(",")]:
+            arr = dg.poisson_arrivals(n, rate, seed=3) if rate > 0 else np.zeros(n)
+            b0 = srv.stats()["batches"]
+            res = srv.run_trace(Qn, arr, k=K, beam_width=L, rerank_size=L if rr else 0, traversal=t)
+            lat = res["latency_us"] / 1e3
+            ids = np.full((n, K), 0xFFFFFFFF, np.uint32)
+            for i, r in enumerate(res["ids"]):
+                ids[i, : len(r)] = r
+            hit = [len(set(ids[i].tolist()) & set(gt[qi[i]][:K].tolist())) for i in range(0, n, 7)]
+            row = {"offered_rps": rate or None, "achieved_qps": n / (res["wall_us"] / 1e6),
+                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                   "mean_batch": n / max(1, srv.stats()["batches"] - b0),
+                   "recall_at_10": round(float(np.mean(hit)) / K, 4)}
+            out["rates"].append(row)
+            log(f"[serve] {name} L={L}: {json.dumps(row)}")
+        out["max_in_flight"] = srv.stats()["max_in_flight"]
+    return out
 
 
 # ------------------------------------------------------------ CPU legs

@@ -171,6 +171,62 @@ DG_API DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p, co
 DG_API DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
                            const uint64_t *pool, uint32_t pool_len, uint64_t *out_count);
 
+/* ------------------------------------------------------------- serving loop */
+/* Continuous batching over one DgIndex.  The reference serves a query as a
+ * synchronous call (DiskANN::search_with_dists, src/lib.rs:683-714) and a
+ * batch as a rayon par_iter over such calls (src/lib.rs:709-714); its benches
+ * time sequential request loops (benches/benchmark.rs:183-207).  Here requests
+ * are queued one at a time and a dispatcher thread forms batches of pending
+ * requests with the same k, traversal, rerank size and filter presence (beam
+ * and filter program stay per request), launching each batch on the next free
+ * stream slot.  Requests that arrive while batches run are admitted as soon as
+ * a slot frees, and batches on different slots overlap on the device.  Each
+ * slot's buffers are allocated at creation and charged against
+ * hbm_budget_bytes, so `streams` is the admission limit.  A request returns
+ * exactly what dg_search_batch returns for it alone. */
+typedef struct DgServer DgServer;
+typedef struct {
+  uint32_t max_batch;        /* requests per launch */
+  uint32_t streams;          /* batches in flight at once (one buffer set each) */
+  uint32_t max_k;            /* largest k a request may ask for */
+  uint32_t max_filter_ops;   /* largest filter program of one request */
+  uint32_t max_wait_us;      /* how long a partial batch waits to fill; 0 = launch at once */
+  uint64_t hbm_budget_bytes; /* 0 = no limit; creation fails with DG_ENOMEM beyond it */
+} DgServerConfig;
+typedef struct {
+  uint32_t k;
+  uint32_t beam_width;
+  uint32_t rerank_size;
+  int32_t traversal; /* DgTraversal */
+  const DgFilterOp *filter_ops; /* this request's postfix program (none = no filter) */
+  uint32_t filter_nops;
+  const uint64_t *filter_pool; /* IN values, offsets relative to this pool */
+  uint32_t filter_pool_len;
+} DgRequest;
+
+DG_API DgStatus dg_server_create(DgIndex *idx, const DgServerConfig *cfg, DgServer **out);
+/* Stops the dispatcher and waits for the batches in flight; call it after every
+ * dg_server_wait has returned.  The index must outlive the server. */
+DG_API DgStatus dg_server_destroy(DgServer *s);
+/* Queues one request (query: f32[dim], copied); writes its ticket. */
+DG_API DgStatus dg_server_submit(DgServer *s, const float *query, const DgRequest *req, uint64_t *ticket);
+/* Waits at most timeout_us for a ticket; DG_ETIMEOUT leaves it pending for
+ * another wait.  On success writes k ids / dists (padded past *out_count) and
+ * the time from submission to completion, and releases the ticket. */
+DG_API DgStatus dg_server_wait(DgServer *s, uint64_t ticket, int64_t timeout_us, uint32_t *out_ids,
+                               float *out_dists, uint32_t *out_count, double *latency_us);
+/* Batches launched, requests served, and the most batches ever in flight at once. */
+DG_API DgStatus dg_server_stats(DgServer *s, uint64_t *batches, uint64_t *served, uint32_t *max_in_flight);
+/* Replays an arrival trace: request i (query i, reqs[i]) is submitted by a
+ * native thread at arrival_us[i] after the start.  Results go k-strided per
+ * request into out_ids / out_dists (sum of reqs[i].k entries), counts into
+ * out_counts, latencies into latency_us, and the time from the start until the
+ * last result into *wall_us.  Waits at most timeout_us in total. */
+DG_API DgStatus dg_server_run_trace(DgServer *s, const float *queries, uint32_t n, const DgRequest *reqs,
+                                    const double *arrival_us, int64_t timeout_us, uint32_t *out_ids,
+                                    float *out_dists, uint32_t *out_counts, double *latency_us,
+                                    double *wall_us);
+
 /* ------------------------------------------------------------------ SPFresh */
 /* Posting lists of an SPFresh index (src/spfresh.rs:62-111,250-281): posting
  * slot b has a centroid, a live flag and block_len[b] entries (id, code) out

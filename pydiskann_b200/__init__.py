@@ -24,7 +24,7 @@ from typing import Iterable, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import PAD, check, lib, ptr
+from ._lib import PAD, DgError, check, lib, ptr  # noqa: F401  (DgError is public)
 
 __all__ = [
     "DiskANN", "QuantizedDiskANN", "FilteredDiskANN", "SPFresh", "Filter", "build_graph", "medoid",
@@ -600,3 +600,4 @@ def write_fvecs(path, vectors):
 
 
 from .spfresh import SPFresh  # noqa: E402  (uses the helpers above)
+from .serve import Server, poisson_arrivals  # noqa: E402

@@ -70,6 +70,17 @@ class SpfreshParams(C.Structure):
                 ("probe_ratio", C.c_float), ("flags", C.c_uint32), ("stream", C.c_void_p)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_uint32), ("streams", C.c_uint32), ("max_k", C.c_uint32),
+                ("max_filter_ops", C.c_uint32), ("max_wait_us", C.c_uint32), ("hbm_budget_bytes", C.c_uint64)]
+
+
+class Request(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("beam_width", C.c_uint32), ("rerank_size", C.c_uint32),
+                ("traversal", C.c_int32), ("filter_ops", C.c_void_p), ("filter_nops", C.c_uint32),
+                ("filter_pool", C.c_void_p), ("filter_pool_len", C.c_uint32)]
+
+
 # Every symbol include/dgann.h declares, with its ctypes signature.
 def _signatures():
     vp, u32, u64, i32, f32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float
@@ -86,6 +97,12 @@ def _signatures():
         "dg_search_batch": (st, [vp, vp, vp, u32, vp, vp, vp, vp]),
         "dg_search_batch_static": (st, [vp, vp, vp, u32, vp, vp, vp]),
         "dg_count_matching": (st, [vp, vp, u32, vp, u32, vp]),
+        "dg_server_create": (st, [vp, vp, vp]),
+        "dg_server_destroy": (st, [vp]),
+        "dg_server_submit": (st, [vp, vp, vp, vp]),
+        "dg_server_wait": (st, [vp, u64, C.c_int64, vp, vp, vp, vp]),
+        "dg_server_stats": (st, [vp, vp, vp, vp]),
+        "dg_server_run_trace": (st, [vp, vp, u32, vp, vp, C.c_int64, vp, vp, vp, vp, vp]),
         "dg_spfresh_create": (st, [vp, vp]),
         "dg_spfresh_destroy": (st, [vp]),
         "dg_spfresh_update_blocks": (st, [vp, vp, u32, vp, vp, vp, vp, vp]),

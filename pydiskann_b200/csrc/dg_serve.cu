@@ -1,0 +1,422 @@
+// dg_serve.cu -- continuous-batching request loop over a DgIndex.
+//
+// Requests (one query each, with its own k, beam, rerank, traversal and
+// filter) are queued by dg_server_submit.  A dispatcher thread forms batches
+// of pending requests that share (k, traversal, rerank) and launches each
+// batch on the next free stream slot; a request that arrives while other
+// batches are on the GPU goes into the next batch as soon as a slot is free,
+// and batches on different slots run concurrently on the device.  Every slot
+// owns preallocated pinned host and device buffers, sized at creation and
+// charged against the configured HBM budget, so the number of slots is the
+// admission limit.  A host function enqueued after each batch's result copy
+// completes its requests; dg_server_wait waits for a ticket with a bound.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "dg_index.h"
+
+namespace dg {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServeRequest {
+  uint64_t ticket = 0;
+  std::vector<float> query;
+  uint32_t k = 10, beam = 64, rerank = 0;
+  int32_t traversal = DG_TRAVERSE_F32;
+  std::vector<DgFilterOp> ops;
+  std::vector<uint64_t> pool;
+  Clock::time_point arrival, done_at;
+  bool done = false;
+  DgStatus status = DG_OK;
+  std::string err;  // dg_last_error of the dispatcher thread when status != DG_OK
+  std::vector<uint32_t> ids;
+  std::vector<float> dists;
+  uint32_t count = 0;
+};
+
+struct ServeSlot {
+  cudaStream_t stream = nullptr;
+  float *h_q = nullptr, *d_q = nullptr;
+  uint32_t *h_ids = nullptr, *d_ids = nullptr, *h_cnt = nullptr, *d_cnt = nullptr;
+  float *h_d = nullptr, *d_d = nullptr;
+  uint32_t *h_beam = nullptr;  // pinned: the search stages it with an async copy
+  bool busy = false;
+  std::vector<ServeRequest *> batch;
+  uint32_t k = 0;
+  struct DgServerImpl *owner = nullptr;
+};
+
+}  // namespace dg
+
+struct DgServer {
+  DgIndex *idx = nullptr;
+  DgServerConfig cfg{};
+  std::vector<dg::ServeSlot> slots;
+  std::mutex mu;
+  std::condition_variable cv_submit, cv_done, cv_slot;
+  std::deque<dg::ServeRequest *> pending;
+  std::unordered_map<uint64_t, dg::ServeRequest *> live;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  std::thread dispatcher;
+  std::atomic<uint64_t> batches{0}, served{0};
+  uint32_t in_flight = 0, max_in_flight = 0;  // busy slots (under mu)
+  DgStatus fatal = DG_OK;
+  std::string fatal_msg;
+};
+
+namespace dg {
+
+struct SlotDone {
+  DgServer *s;
+  int slot;
+};
+
+// Runs on the driver's callback thread once the slot's result copies landed;
+// it only touches host memory.
+static void CUDART_CB slot_done(void *arg) {
+  SlotDone *sd = static_cast<SlotDone *>(arg);
+  DgServer *s = sd->s;
+  ServeSlot &sl = s->slots[sd->slot];
+  const auto now = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (size_t i = 0; i < sl.batch.size(); ++i) {
+      ServeRequest *r = sl.batch[i];
+      const uint32_t c = std::min(sl.h_cnt[i], r->k);
+      r->count = c;
+      r->ids.assign(sl.h_ids + i * sl.k, sl.h_ids + i * sl.k + r->k);
+      r->dists.assign(sl.h_d + i * sl.k, sl.h_d + i * sl.k + r->k);
+      r->done_at = now;
+      r->done = true;
+    }
+    s->served += sl.batch.size();
+    sl.batch.clear();
+    sl.busy = false;
+    --s->in_flight;
+  }
+  s->cv_done.notify_all();
+  s->cv_slot.notify_all();
+  delete sd;
+}
+
+static bool same_class(const ServeRequest *a, const ServeRequest *b) {
+  // a filtered search is a different traversal (expanded beam), so requests
+  // with and without a filter never share a batch
+  return a->k == b->k && a->traversal == b->traversal && a->rerank == b->rerank &&
+         a->ops.empty() == b->ops.empty();
+}
+
+static void dispatch_loop(DgServer *s) {
+  const uint32_t dim = s->idx->d;
+  std::vector<uint32_t> offs;
+  std::vector<DgFilterOp> ops;
+  std::vector<uint64_t> pool;
+  cudaSetDevice(s->idx->device);
+  while (true) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_submit.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+    if (s->stop && s->pending.empty()) break;
+    // give a partial batch a short time to fill
+    if (s->pending.size() < s->cfg.max_batch && s->cfg.max_wait_us > 0) {
+      const auto deadline = s->pending.front()->arrival + std::chrono::microseconds(s->cfg.max_wait_us);
+      s->cv_submit.wait_until(lk, deadline, [&] { return s->stop || s->pending.size() >= s->cfg.max_batch; });
+    }
+    // a free slot (admission: every slot holds its own HBM reservation)
+    int slot = -1;
+    s->cv_slot.wait(lk, [&] {
+      for (size_t i = 0; i < s->slots.size(); ++i)
+        if (!s->slots[i].busy) {
+          slot = (int)i;
+          return true;
+        }
+      return s->stop;
+    });
+    if (slot < 0) break;
+    ServeSlot &sl = s->slots[slot];
+    // oldest request fixes the class; take up to max_batch of that class in arrival order
+    ServeRequest *head = s->pending.front();
+    std::vector<ServeRequest *> batch;
+    for (auto it = s->pending.begin(); it != s->pending.end() && batch.size() < s->cfg.max_batch;) {
+      if (same_class(*it, head)) {
+        batch.push_back(*it);
+        it = s->pending.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    sl.busy = true;
+    s->max_in_flight = std::max(s->max_in_flight, ++s->in_flight);
+    sl.batch = batch;
+    sl.k = head->k;
+    lk.unlock();
+
+    const uint32_t nq = (uint32_t)batch.size();
+    offs.assign(1, 0);
+    ops.clear();
+    pool.clear();
+    bool any_filter = false;
+    for (uint32_t i = 0; i < nq; ++i) {
+      ServeRequest *r = batch[i];
+      std::memcpy(sl.h_q + (size_t)i * dim, r->query.data(), dim * sizeof(float));
+      sl.h_beam[i] = r->beam;
+      const uint64_t base = pool.size();
+      for (DgFilterOp o : r->ops) {
+        if (o.op == DG_F_IN) o.a += base;
+        ops.push_back(o);
+      }
+      pool.insert(pool.end(), r->pool.begin(), r->pool.end());
+      any_filter |= !r->ops.empty();
+      offs.push_back((uint32_t)ops.size());
+    }
+    DgStatus st = DG_OK;
+    if (cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)nq * dim * sizeof(float), cudaMemcpyHostToDevice, sl.stream) !=
+        cudaSuccess)
+      st = fail(DG_EDEVICE, "request copy failed");
+    if (st == DG_OK) {
+      DgSearchParams p{};
+      p.k = head->k;
+      p.beam_width = head->beam;
+      p.rerank_size = head->rerank;
+      p.traversal = head->traversal;
+      p.per_query_beam = sl.h_beam;
+      if (any_filter) {
+        p.filter_ops = ops.data();
+        p.filter_offsets = offs.data();
+        p.filter_pool = pool.data();
+        p.filter_pool_len = (uint32_t)pool.size();
+      }
+      p.flags = DG_FLAG_DEVICE_PTRS | DG_FLAG_STREAM;
+      p.stream = sl.stream;
+      st = dg_search_batch(s->idx, &p, sl.d_q, nq, sl.d_ids, sl.d_d, sl.d_cnt, nullptr);
+    }
+    if (st == DG_OK) {
+      const size_t kq = (size_t)nq * head->k;
+      if (cudaMemcpyAsync(sl.h_ids, sl.d_ids, kq * 4, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
+          cudaMemcpyAsync(sl.h_d, sl.d_d, kq * 4, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
+          cudaMemcpyAsync(sl.h_cnt, sl.d_cnt, (size_t)nq * 4, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
+          cudaLaunchHostFunc(sl.stream, slot_done, new SlotDone{s, slot}) != cudaSuccess)
+        st = fail(DG_EDEVICE, "result copy failed");
+    }
+    ++s->batches;
+    if (st != DG_OK) {  // fail the batch's requests, free the slot
+      const std::string why = dg_last_error();
+      std::lock_guard<std::mutex> g(s->mu);
+      for (ServeRequest *r : batch) {
+        r->status = st;
+        r->err = why;
+        r->done = true;
+        r->done_at = Clock::now();
+      }
+      sl.batch.clear();
+      sl.busy = false;
+      --s->in_flight;
+      s->cv_done.notify_all();
+      s->cv_slot.notify_all();
+    }
+  }
+}
+
+static DgStatus check_request(const DgServer *s, const float *query, const DgRequest *rq) {
+  if (!query || !rq) return fail(DG_EINVAL, "null request");
+  if (rq->k == 0 || rq->k > s->cfg.max_k) return fail(DG_EINVAL, "k must be in [1, max_k]");
+  if (rq->beam_width == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
+  if (rq->filter_nops > s->cfg.max_filter_ops) return fail(DG_EINVAL, "filter program above max_filter_ops");
+  if (rq->filter_nops && !rq->filter_ops) return fail(DG_EINVAL, "filter ops missing");
+  if (rq->filter_pool_len && !rq->filter_pool) return fail(DG_EINVAL, "filter pool missing");
+  return DG_OK;
+}
+
+static DgStatus copy_request(const DgServer *s, const float *query, const DgRequest *rq, ServeRequest *r) {
+  const DgStatus st = check_request(s, query, rq);
+  if (st != DG_OK) return st;
+  r->query.assign(query, query + s->idx->d);
+  r->k = rq->k;
+  r->beam = rq->beam_width;
+  r->rerank = rq->rerank_size;
+  r->traversal = rq->traversal;
+  if (rq->filter_nops) {
+    r->ops.assign(rq->filter_ops, rq->filter_ops + rq->filter_nops);
+    if (rq->filter_pool_len) r->pool.assign(rq->filter_pool, rq->filter_pool + rq->filter_pool_len);
+  }
+  return DG_OK;
+}
+
+}  // namespace dg
+
+using namespace dg;
+
+extern "C" {
+
+DgStatus dg_server_destroy(DgServer *s) {
+  if (!s) return DG_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_submit.notify_all();
+  s->cv_slot.notify_all();
+  if (s->dispatcher.joinable()) s->dispatcher.join();
+  cudaSetDevice(s->idx->device);
+  for (ServeSlot &sl : s->slots) {
+    if (sl.stream) cudaStreamSynchronize(sl.stream);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
+    for (void *p : {(void *)sl.h_q, (void *)sl.h_ids, (void *)sl.h_d, (void *)sl.h_cnt, (void *)sl.h_beam})
+      if (p) cudaFreeHost(p);
+    for (void *p : {(void *)sl.d_q, (void *)sl.d_ids, (void *)sl.d_d, (void *)sl.d_cnt})
+      if (p) cudaFree(p);
+  }
+  for (auto &kv : s->live) delete kv.second;  // every submitted request not yet waited for
+  delete s;
+  return DG_OK;
+}
+
+DgStatus dg_server_create(DgIndex *idx, const DgServerConfig *cfg, DgServer **out) {
+  if (!idx || !cfg || !out) return fail(DG_EINVAL, "null argument");
+  *out = nullptr;
+  if (cfg->max_batch == 0 || cfg->streams == 0 || cfg->max_k == 0)
+    return fail(DG_EINVAL, "max_batch, streams and max_k must be >= 1");
+  const size_t slot_bytes = (size_t)cfg->max_batch * (idx->d * 4 + (size_t)cfg->max_k * 8 + 4);
+  if (cfg->hbm_budget_bytes && slot_bytes * cfg->streams > cfg->hbm_budget_bytes)
+    return fail(DG_ENOMEM, "server slots (" + std::to_string(slot_bytes * cfg->streams) +
+                               " bytes) exceed the HBM budget");
+  DG_CUDA(cudaSetDevice(idx->device));
+  DgServer *s = new (std::nothrow) DgServer();
+  if (!s) return fail(DG_ENOMEM, "host allocation failed");
+  s->idx = idx;
+  s->cfg = *cfg;
+  s->slots.resize(cfg->streams);
+  for (ServeSlot &sl : s->slots) {
+    const size_t nq = cfg->max_batch, kq = nq * cfg->max_k;
+    bool ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaMallocHost(&sl.h_q, nq * idx->d * 4) == cudaSuccess && cudaMalloc(&sl.d_q, nq * idx->d * 4) == cudaSuccess;
+    ok = ok && cudaMallocHost(&sl.h_ids, kq * 4) == cudaSuccess && cudaMalloc(&sl.d_ids, kq * 4) == cudaSuccess;
+    ok = ok && cudaMallocHost(&sl.h_d, kq * 4) == cudaSuccess && cudaMalloc(&sl.d_d, kq * 4) == cudaSuccess;
+    ok = ok && cudaMallocHost(&sl.h_cnt, nq * 4) == cudaSuccess && cudaMalloc(&sl.d_cnt, nq * 4) == cudaSuccess;
+    ok = ok && cudaMallocHost(&sl.h_beam, nq * 4) == cudaSuccess;
+    if (!ok) {
+      dg_server_destroy(s);
+      return fail(DG_ENOMEM, "server slot allocation failed");
+    }
+  }
+  s->dispatcher = std::thread(dispatch_loop, s);
+  *out = s;
+  return DG_OK;
+}
+
+DgStatus dg_server_submit(DgServer *s, const float *query, const DgRequest *req, uint64_t *ticket) {
+  if (!s || !ticket) return fail(DG_EINVAL, "null argument");
+  ServeRequest *r = new (std::nothrow) ServeRequest();
+  if (!r) return fail(DG_ENOMEM, "host allocation failed");
+  DgStatus st = copy_request(s, query, req, r);
+  if (st != DG_OK) {
+    delete r;
+    return st;
+  }
+  r->arrival = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) {
+      delete r;
+      return fail(DG_EINVAL, "server is shutting down");
+    }
+    r->ticket = s->next_ticket++;
+    s->live[r->ticket] = r;
+    s->pending.push_back(r);
+    *ticket = r->ticket;
+  }
+  s->cv_submit.notify_one();
+  return DG_OK;
+}
+
+DgStatus dg_server_wait(DgServer *s, uint64_t ticket, int64_t timeout_us, uint32_t *out_ids, float *out_dists,
+                        uint32_t *out_count, double *latency_us) {
+  if (!s) return fail(DG_EINVAL, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->live.find(ticket);
+  if (it == s->live.end()) return fail(DG_EINVAL, "unknown ticket");
+  ServeRequest *r = it->second;
+  const auto deadline = Clock::now() + std::chrono::microseconds(timeout_us < 0 ? 0 : timeout_us);
+  if (!s->cv_done.wait_until(lk, deadline, [&] { return r->done; }))
+    return fail(DG_ETIMEOUT, "request " + std::to_string(ticket) + " not done within the wait bound");
+  s->live.erase(it);
+  lk.unlock();
+  const DgStatus st = r->status;
+  if (st != DG_OK) fail(st, r->err);
+  if (st == DG_OK) {
+    if (out_ids) std::copy(r->ids.begin(), r->ids.end(), out_ids);
+    if (out_dists) std::copy(r->dists.begin(), r->dists.end(), out_dists);
+    if (out_count) *out_count = r->count;
+    if (latency_us)
+      *latency_us = std::chrono::duration<double, std::micro>(r->done_at - r->arrival).count();
+  }
+  delete r;
+  return st;
+}
+
+DgStatus dg_server_stats(DgServer *s, uint64_t *batches, uint64_t *served, uint32_t *max_in_flight) {
+  if (!s) return fail(DG_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (batches) *batches = s->batches.load();
+  if (served) *served = s->served.load();
+  if (max_in_flight) *max_in_flight = s->max_in_flight;
+  return DG_OK;
+}
+
+// Replays an arrival trace from a native thread: request i is submitted at
+// arrival_us[i] (relative to the start) and its latency is written to
+// latency_us[i]; results to out_ids/out_dists (k-strided per request) and
+// out_counts.  Returns once every request completed or timeout_us passed.
+DgStatus dg_server_run_trace(DgServer *s, const float *queries, uint32_t n, const DgRequest *reqs,
+                             const double *arrival_us, int64_t timeout_us, uint32_t *out_ids, float *out_dists,
+                             uint32_t *out_counts, double *latency_us, double *wall_us) {
+  if (!s || !queries || !reqs || !arrival_us || !latency_us) return fail(DG_EINVAL, "null argument");
+  for (uint32_t i = 0; i < n; ++i) {
+    const DgStatus st = check_request(s, queries + (size_t)i * s->idx->d, &reqs[i]);
+    if (st != DG_OK) return fail(st, "request " + std::to_string(i) + ": " + dg_last_error());
+  }
+  std::vector<uint64_t> tickets(n, 0);
+  std::vector<double> lag(n, 0.0);  // submission behind schedule, added to the latency
+  std::atomic<int> submit_err{0};
+  const auto t0 = Clock::now();
+  std::thread producer([&] {
+    for (uint32_t i = 0; i < n; ++i) {
+      const auto at = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::micro>(arrival_us[i]));
+      while (Clock::now() < at) {
+        const auto left = at - Clock::now();
+        if (left > std::chrono::microseconds(50)) std::this_thread::sleep_for(left - std::chrono::microseconds(30));
+      }
+      lag[i] = std::max(0.0, std::chrono::duration<double, std::micro>(Clock::now() - at).count());
+      if (dg_server_submit(s, queries + (size_t)i * s->idx->d, &reqs[i], &tickets[i]) != DG_OK) submit_err = 1;
+    }
+  });
+  producer.join();
+  if (submit_err) return fail(DG_EINVAL, "the server stopped while the trace was submitted");
+  DgStatus st = DG_OK;
+  size_t off = 0;
+  double last_done = 0.0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const int64_t left = timeout_us - (int64_t)std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
+    DgStatus r = dg_server_wait(s, tickets[i], std::max<int64_t>(left, 0), out_ids ? out_ids + off : nullptr,
+                                out_dists ? out_dists + off : nullptr, out_counts ? out_counts + i : nullptr,
+                                latency_us + i);
+    off += reqs[i].k;
+    latency_us[i] = r == DG_OK ? latency_us[i] + lag[i] : -1.0;
+    if (r != DG_OK && st == DG_OK) st = r;
+    if (r == DG_OK) last_done = std::max(last_done, arrival_us[i] + latency_us[i]);
+  }
+  if (wall_us) *wall_us = last_done;
+  return st;
+}
+
+}  // extern "C"
