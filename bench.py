@@ -187,6 +187,17 @@ VARIANTS = {
 }
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time (every rank calls this at the same step)."""
+    if dist is None:
+        return ms
+    import torch
+
+    tt = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def run_variant(idx, qidx, name, Qd, L, out=None, with_stats=False, stream=None):
     """idx: the FP32/BF16 index; qidx: {"pq": QuantizedDiskANN, "int8": ...}."""
     from pydiskann_b200 import _lib
@@ -300,10 +311,7 @@ def main():
             torch.cuda.synchronize()
         total_ms = t_start.elapsed_time(t_end)
         steps_ms = np.array([a.elapsed_time(b) for a, b in ev])
-        if dist is not None:
-            tt = torch.tensor([total_ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total_ms = float(tt.item())
+        total_ms = max_over_ranks(total_ms, dist, dev)
         _, _, _, st = run_variant(idx, qidx, name, Qd, L, with_stats=True)
         stats = st.cpu().numpy().view(np.uint32)
         alg_bytes, work = algorithmic_bytes(name, stats, L)
@@ -395,10 +403,7 @@ def e2e(args, idx, qidx, name, L, Q, gt, dist, world, dev):
     b.record(stream)
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
-    if dist is not None:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, dist, dev)
     rec = recall(outs[0], gt)
     return {"value": world * args.nq * args.steps / (ms / 1e3), "unit": "queries/s",
             "h2d_bytes_per_step": int(Q.nbytes), "d2h_bytes_per_step": int(args.nq * (K * 8 + 4)),
