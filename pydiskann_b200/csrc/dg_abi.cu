@@ -175,6 +175,15 @@ static DgStatus attach_codes_common(DgIndex *idx, int quant, uint32_t code_size)
   return DG_OK;
 }
 
+// Cosine over PQ / RaBitQ codes compares against the decoded code
+// (src/quantized.rs:28-36); its squared norm is per vector, computed once.
+static DgStatus attach_decoded_norms(DgIndex *idx) {
+  if (idx->metric != DG_COSINE) return DG_OK;
+  DgStatus s = dev_alloc(idx, (void **)&idx->dnorm2, idx->n * 4);
+  if (s != DG_OK) return s;
+  return decoded_norms_device(idx, idx->dnorm2, idx->stream);
+}
+
 static DgStatus upload_code_rows(DgIndex *idx, const uint8_t *codes) {
   DG_CUDA(cudaMemcpy2DAsync(idx->codes, idx->code_stride, codes, idx->code_size, idx->code_size,
                             idx->n, cudaMemcpyHostToDevice, idx->stream));
@@ -204,6 +213,7 @@ DgStatus dg_index_attach_pq(DgIndex *idx, uint32_t M, uint32_t K, const float *c
   else s = encode_pq_device(idx->vec, idx->n, idx->d, idx->dpad, M, K, idx->pq_cb, idx->codes,
                             idx->code_stride, idx->stream);
   if (s != DG_OK) return s;
+  if ((s = attach_decoded_norms(idx)) != DG_OK) return s;
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
 }
@@ -257,6 +267,7 @@ DgStatus dg_index_attach_rabitq(DgIndex *idx, uint32_t padded, const float *cent
   else s = encode_rabitq_device(idx->vec, idx->n, idx->d, idx->dpad, padded, idx->rq_centroid,
                                 idx->rq_signs, idx->codes, idx->code_stride, idx->stream);
   if (s != DG_OK) return s;
+  if ((s = attach_decoded_norms(idx)) != DG_OK) return s;
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
 }
@@ -402,6 +413,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   a.rq_padded = idx->rq_padded;
   a.rq_centroid = idx->rq_centroid;
   a.rq_signs = idx->rq_signs;
+  a.dnorm2 = idx->dnorm2;
   a.labels = idx->labels;
   a.nf = idx->nf;
   a.nq = nq;
@@ -455,7 +467,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
   const WarpLayout Ly = warp_layout(trav, lcap, any_filter, hbits, idx->dpad, idx->pq_M, idx->pq_K,
-                                    idx->rq_padded);
+                                    idx->rq_padded, trav == TRAV_RABITQ && met_kind(idx->metric) != MET_L2);
   LaunchInfo info;
   switch (trav) {
     case TRAV_F32: s = launch_search_f32(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
@@ -661,6 +673,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   a.rq_padded = idx->rq_padded;
   a.rq_centroid = idx->rq_centroid;
   a.rq_signs = idx->rq_signs;
+  a.dnorm2 = idx->dnorm2;
   a.labels = idx->labels;
   a.nf = idx->nf;
   a.nq = nq;
@@ -702,7 +715,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
   const WarpLayout Ly = warp_layout(trav, lcap, any_filter, hbits, idx->dpad, idx->pq_M, idx->pq_K,
-                                    idx->rq_padded);
+                                    idx->rq_padded, trav == TRAV_RABITQ && met_kind(idx->metric) != MET_L2);
   LaunchInfo info;
   switch (trav) {
     case TRAV_F32: return launch_search_f32(a, Ly, met, lpr, lcap, any_filter, st, &info);

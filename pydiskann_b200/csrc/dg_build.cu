@@ -111,6 +111,65 @@ __global__ void k_rabitq_encode(const float *v, uint64_t n, uint32_t d, uint32_t
   }
 }
 
+// Squared norm of every decoded PQ code (ProductQuantizer::decode,
+// src/pq.rs:151-160): the |x|^2 term of the cosine metric over codes, summed
+// in coordinate order as angular() does.  One thread per vector.
+__global__ void k_pq_dnorm2(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t M, uint32_t K,
+                            uint32_t ds, const float *cb, float *out) {
+  for (uint64_t row = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; row < n;
+       row += (uint64_t)gridDim.x * blockDim.x) {
+    const uint8_t *code = codes + row * stride;
+    float bb = 0.0f;
+    for (uint32_t m = 0; m < M; ++m) {
+      const float *c = cb + ((size_t)m * K + code[m]) * ds;
+      for (uint32_t j = 0; j < ds; ++j) bb = __fadd_rn(bb, __fmul_rn(c[j], c[j]));
+    }
+    out[row] = bb;
+  }
+}
+
+// Squared norm of every decoded RaBitQ code (src/rabitq.rs:224-238): signs
+// +-1/sqrt(P), three inverse rounds (Hadamard, then sign flip), then
+// c + |v-c| * r over the first d coordinates, summed in coordinate order.
+// One warp per vector.
+__global__ void k_rq_dnorm2(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t d, uint32_t P,
+                            const float *cen, const float *signs, float *out) {
+  extern __shared__ __align__(16) float rbuf[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float *r = rbuf + (size_t)warp * P;
+  const uint64_t gw = blockIdx.x * (uint64_t)(blockDim.x >> 5) + warp;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const float inv = __fdiv_rn(1.0f, __fsqrt_rn((float)P));
+  for (uint64_t row = gw; row < n; row += nw) {
+    const uint8_t *code = codes + row * stride;
+    for (uint32_t i = lane; i < P; i += 32) r[i] = ((code[i >> 3] >> (i & 7)) & 1u) ? inv : -inv;
+    __syncwarp();
+    for (int rd = 2; rd >= 0; --rd) {
+      for (uint32_t h = 1; h < P; h *= 2) {
+        for (uint32_t t = lane; t < P / 2; t += 32) {
+          const uint32_t j = (t / h) * 2 * h + (t % h);
+          const float a = r[j], b = r[j + h];
+          r[j] = __fadd_rn(a, b);
+          r[j + h] = __fsub_rn(a, b);
+        }
+        __syncwarp();
+      }
+      for (uint32_t i = lane; i < P; i += 32) r[i] = __fmul_rn(r[i], signs[rd * P + i]);
+      __syncwarp();
+    }
+    if (lane == 0) {
+      const float norm = __fsqrt_rn(*reinterpret_cast<const float *>(code + P / 8));
+      float bb = 0.0f;
+      for (uint32_t i = 0; i < d; ++i) {
+        const float o = __fadd_rn(cen[i], __fmul_rn(norm, r[i]));
+        bb = __fadd_rn(bb, __fmul_rn(o, o));
+      }
+      out[row] = bb;
+    }
+    __syncwarp();
+  }
+}
+
 __global__ void k_count(const uint64_t *labels, uint64_t n, uint32_t nf, const DgFilterOp *ops,
                         uint32_t nops, const uint64_t *pool, unsigned long long *count) {
   unsigned long long c = 0;
@@ -161,6 +220,22 @@ DgStatus encode_rabitq_device(const float *vec, uint64_t n, uint32_t d, uint32_t
   DG_CUDA(cudaFuncSetAttribute(k_rabitq_encode, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int blocks = (int)std::min<uint64_t>((n + warps - 1) / warps, 148ull * 16);
   k_rabitq_encode<<<blocks, warps * 32, smem, st>>>(vec, n, d, dpad, P, centroid, signs, codes, stride);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+DgStatus decoded_norms_device(const DgIndex *idx, float *out, cudaStream_t st) {
+  if (idx->quant == DG_Q_PQ) {
+    k_pq_dnorm2<<<grid_for(idx->n, 128), 128, 0, st>>>(idx->codes, idx->n, idx->code_stride, idx->pq_M,
+                                                       idx->pq_K, idx->d / idx->pq_M, idx->pq_cb, out);
+  } else {
+    const int warps = 4;
+    const uint32_t P = idx->rq_padded;
+    const size_t smem = (size_t)warps * P * 4;
+    DG_CUDA(cudaFuncSetAttribute(k_rq_dnorm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int blocks = (int)std::min<uint64_t>((idx->n + warps - 1) / warps, 148ull * 16);
+    k_rq_dnorm2<<<blocks, warps * 32, smem, st>>>(idx->codes, idx->n, idx->code_stride, idx->d, P,
+                                                  idx->rq_centroid, idx->rq_signs, out);
+  }
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

@@ -46,6 +46,7 @@ struct SearchArgs {
   uint32_t rq_padded;
   const float *rq_centroid;  // [d]
   const float *rq_signs;     // [3][padded]
+  const float *dnorm2;       // [n] squared norms of the decoded codes (cosine over PQ / RaBitQ)
   // labels / filter
   const uint64_t *labels;
   uint32_t nf;
@@ -77,9 +78,10 @@ struct WarpLayout {
   uint32_t w0, w1, res, cstage, stage, hash, qf, prov, total;
 };
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
+// `decode`: RaBitQ with a cosine / dot metric (rotated query, nibble table).
 __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool filt, uint32_t hbits,
                                                   uint32_t dpad, uint32_t pq_M, uint32_t pq_K,
-                                                  uint32_t rq_padded) {
+                                                  uint32_t rq_padded, bool decode = false) {
   WarpLayout L{};
   uint32_t o = 0;
   L.w0 = o; o += lcap * 8;
@@ -93,6 +95,7 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
   uint32_t p = 0;
   if (trav == TRAV_PQ) p = pq_M * pq_K * 4;
   else if (trav == TRAV_INT8) p = align16(dpad);
+  else if (trav == TRAV_RABITQ && decode) p = 16 + rq_padded * 4 + rq_padded * 16;
   else if (trav == TRAV_RABITQ) p = 4 * (rq_padded / 64) * 8 + 32 + align16(rq_padded * 4);
   else if (trav == TRAV_F16) p = align16(dpad * 4);
   o += align16(p);
@@ -496,6 +499,22 @@ __device__ __forceinline__ float pq_adc(const SearchArgs &a, const float *lut, u
   return d;
 }
 
+// Inner-product table for cosine / dot over PQ codes: the reference decodes
+// the code (centroid concatenation, src/pq.rs:151-160) and evaluates the metric
+// (src/quantized.rs:28-36); q . decode(code) = sum_m ip[m][code_m] with
+// ip[m][c] = q_m . centroid(m, c).
+__device__ __forceinline__ void build_pq_ip_lut(const SearchArgs &a, const float *qs, float *lut, int lane) {
+  const uint32_t total = a.pq_M * a.pq_K;
+  for (uint32_t e = lane; e < total; e += 32) {
+    const uint32_t m = e / a.pq_K;
+    const float *cen = a.pq_cb + (size_t)e * a.pq_ds;
+    const float *qq = qs + m * a.pq_ds;
+    float acc = 0.0f;
+    for (uint32_t j = 0; j < a.pq_ds; ++j) acc = __fadd_rn(acc, __fmul_rn(qq[j], __ldg(cen + j)));
+    lut[e] = acc;
+  }
+}
+
 // int8 query encoding (src/sq.rs:208-220): x*(1/scale) + (-offset/scale),
 // rounded to nearest even and saturated.
 __device__ __forceinline__ uint8_t int8_code(float x, float inv, float beta) {
@@ -612,6 +631,91 @@ __device__ __forceinline__ float rabitq_est(const uint8_t *code, uint32_t P, con
   const float inner = __fadd_rn(__fadd_rn(__fmul_rn(k5[2], (float)S), __fmul_rn(k5[3], (float)C)), k5[4]);
   const float e = __fsub_rn(__fadd_rn(nf.x, k5[0]), __fmul_rn(__fmul_rn(k5[1], nf.y), inner));
   return fmaxf(e, 0.0f);
+}
+
+// ---------------------------------------------- RaBitQ decode (cosine, dot)
+// The reference decodes a RaBitQ code for non-L2 metrics (src/rabitq.rs:224-238,
+// src/quantized.rs:28-36): x = c + |v-c| * unrotate(b / sqrt(P)) truncated to d,
+// b_i = +-1 from the sign bits.  The rotation is orthogonal (each round is a
+// sign flip scaled by 1/sqrt(P) then an unnormalised Hadamard transform), so
+// q . x = q . c + |v-c| * (R q) . b / sqrt(P), with R q the rotated,
+// zero-padded query.  (R q) . b = 2 * sum_{b_i = 1} y_i - sum_i y_i; the masked
+// sum is read from a table of the 16 subset sums of every 4 coordinates.
+// Shared layout at `p`: [qc, Y, 1/sqrt(P), 0] | y[P] | T[P/4][16].
+__device__ inline void rabitq_decode_prepare(const float *q, uint32_t d, uint32_t P, const float *cen,
+                                             const float *signs, uint8_t *p, int lane) {
+  float *hdr = reinterpret_cast<float *>(p);
+  float *y = hdr + 4;
+  float *T = y + P;
+  float qc = 0.0f;
+  for (uint32_t i = lane; i < P; i += 32) {
+    const float v = i < d ? q[i] : 0.0f;
+    y[i] = v;
+    if (i < d) qc = fmaf(v, cen[i], qc);
+  }
+  __syncwarp();
+  for (int rd = 0; rd < 3; ++rd) {
+    for (uint32_t i = lane; i < P; i += 32) y[i] = __fmul_rn(y[i], signs[rd * P + i]);
+    __syncwarp();
+    for (uint32_t h = 1; h < P; h *= 2) {
+      for (uint32_t t = lane; t < P / 2; t += 32) {
+        const uint32_t j = (t / h) * 2 * h + t % h;
+        const float x0 = y[j], x1 = y[j + h];
+        y[j] = __fadd_rn(x0, x1);
+        y[j + h] = __fsub_rn(x0, x1);
+      }
+      __syncwarp();
+    }
+  }
+  float Y = 0.0f;
+  for (uint32_t i = lane; i < P; i += 32) Y += y[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Y += __shfl_xor_sync(kFull, Y, o);
+    qc += __shfl_xor_sync(kFull, qc, o);
+  }
+  for (uint32_t e = lane; e < P * 4; e += 32) {
+    const uint32_t j = e >> 4, nib = e & 15u;
+    float t = 0.0f;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      if ((nib >> b) & 1u) t = __fadd_rn(t, y[4 * j + b]);
+    T[e] = t;
+  }
+  if (lane == 0) {
+    hdr[0] = qc;
+    hdr[1] = Y;
+    hdr[2] = __fdiv_rn(1.0f, __fsqrt_rn((float)P));
+    hdr[3] = 0.0f;
+  }
+  __syncwarp();
+}
+
+// q . decode(code) for one code (one lane).
+__device__ __forceinline__ float rabitq_decode_ip(const uint8_t *code, uint32_t P, const uint8_t *p) {
+  const float *hdr = reinterpret_cast<const float *>(p);
+  const float *T = hdr + 4 + P;
+  float s1 = 0.0f;
+  for (uint32_t c = 0; c < P / 128; ++c) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(code) + c);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int nb = 0; nb < 8; ++nb) s1 += T[((c * 4 + k) * 8 + nb) * 16 + ((w[k] >> (4 * nb)) & 15u)];
+  }
+  if (P % 128) {  // P = 64: one 8-byte word
+    const uint2 v = __ldg(reinterpret_cast<const uint2 *>(code + (P / 128) * 16));
+    const uint32_t w[2] = {v.x, v.y};
+    const uint32_t base = (P / 128) * 32;
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int nb = 0; nb < 8; ++nb) s1 += T[(base + k * 8 + nb) * 16 + ((w[k] >> (4 * nb)) & 15u)];
+  }
+  const float n2 = __ldg(reinterpret_cast<const float *>(code + P / 8));
+  const float ip = (2.0f * s1 - hdr[1]) * hdr[2];
+  return hdr[0] + sqrtf(n2) * ip;
 }
 
 }  // namespace dg

@@ -4,6 +4,22 @@
 
 namespace dg {
 
+// |q|^2 for the cosine metric.  Decoded PQ / RaBitQ codes take it in the
+// sequential order of the oracle's angular(); row traversals reduce across lanes.
+template <int TRAV>
+__device__ __forceinline__ float query_norm2(const float *qs, uint32_t d, int lane) {
+  float qq = 0.0f;
+  if (TRAV == TRAV_PQ || TRAV == TRAV_RABITQ) {
+    if (lane == 0)
+      for (uint32_t i = 0; i < d; ++i) qq = __fadd_rn(qq, __fmul_rn(qs[i], qs[i]));
+    return __shfl_sync(kFull, qq, 0);
+  }
+  for (uint32_t i = lane; i < d; i += 32) qq = fmaf(qs[i], qs[i], qq);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) qq += __shfl_xor_sync(kFull, qq, o);
+  return qq;
+}
+
 struct QueryCtx {
   const DgFilterOp *fops;
   uint32_t fnops;
@@ -42,7 +58,13 @@ __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *ws
   } else if (TRAV == TRAV_PQ) {
     const float *lut = reinterpret_cast<const float *>(wsm + Ly.prov);
     float d = lane < cnt ? pq_adc(a, lut, cand) : 0.0f;
+    if (MET != MET_L2)  // d = q . decode(code)
+      return finish_metric(MET, false, d, (MET == MET_COS && lane < cnt) ? __ldg(a.dnorm2 + cand) : 0.0f, qq);
     return sqrt_l2 ? __fsqrt_rn(d) : d;
+  } else if (MET != MET_L2) {  // RaBitQ, decoded
+    const float ab = lane < cnt ? rabitq_decode_ip(a.codes + (size_t)cand * a.code_stride, a.rq_padded, wsm + Ly.prov)
+                                : 0.0f;
+    return finish_metric(MET, false, ab, (MET == MET_COS && lane < cnt) ? __ldg(a.dnorm2 + cand) : 0.0f, qq);
   } else {  // RaBitQ
     const uint64_t *planes = reinterpret_cast<const uint64_t *>(wsm + Ly.prov);
     const float *k5 = reinterpret_cast<const float *>(wsm + Ly.prov + 4 * (a.rq_padded / 64) * 8);
@@ -61,10 +83,14 @@ __device__ __forceinline__ float exact_distance(const SearchArgs &a, const float
 }
 
 // Per-query quantizer state (QuantizerState::prepare, src/quantized.rs:167-174).
-template <int TRAV>
+template <int TRAV, int MET>
 __device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm, const WarpLayout &Ly,
                                               const float *qs, int lane) {
-  if (TRAV == TRAV_PQ) {
+  if (TRAV == TRAV_PQ && MET != MET_L2) {
+    build_pq_ip_lut(a, qs, reinterpret_cast<float *>(wsm + Ly.prov), lane);
+  } else if (TRAV == TRAV_RABITQ && MET != MET_L2) {
+    rabitq_decode_prepare(qs, a.d, a.rq_padded, a.rq_centroid, a.rq_signs, wsm + Ly.prov, lane);
+  } else if (TRAV == TRAV_PQ) {
     build_pq_lut(a, qs, reinterpret_cast<float *>(wsm + Ly.prov), lane);
   } else if (TRAV == TRAV_INT8) {
     uint8_t *qc8 = wsm + Ly.prov;
@@ -236,12 +262,8 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
   vt.clear(lane);
   __syncwarp();
   float qq = 0.0f;
-  if (MET == MET_COS) {
-    for (uint32_t i = lane; i < a.dpad; i += 32) qq = fmaf(qs[i], qs[i], qq);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) qq += __shfl_xor_sync(kFull, qq, o);
-  }
-  prepare_query<TRAV>(a, wsm, Ly, qs, lane);
+  if (MET == MET_COS) qq = query_norm2<TRAV>(qs, a.d, lane);
+  prepare_query<TRAV, MET>(a, wsm, Ly, qs, lane);
 
   uint64_t w0 = kKeyInvalid, w1 = kKeyInvalid;
   int wsize = 1;
@@ -352,12 +374,8 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
   vt.clear(lane);
   __syncwarp();
   float qq = 0.0f;
-  if (MET == MET_COS) {
-    for (uint32_t i = lane; i < a.dpad; i += 32) qq = fmaf(qs[i], qs[i], qq);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) qq += __shfl_xor_sync(kFull, qq, o);
-  }
-  prepare_query<TRAV>(a, wsm, Ly, qs, lane);
+  if (MET == MET_COS) qq = query_norm2<TRAV>(qs, a.d, lane);
+  prepare_query<TRAV, MET>(a, wsm, Ly, qs, lane);
 
   const uint64_t *labels = a.labels;
   auto allow = [&](uint32_t id) -> bool {

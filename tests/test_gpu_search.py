@@ -233,3 +233,44 @@ def test_edge_cases():
     Z = rng.random((50, 16), dtype=np.float32)
     r = dg.DiskANN.build(Z).search_with_dists(Z[0], 1, 1)
     assert len(r) == 1 and r[0][1] >= 0.0
+
+
+# Cosine / dot over PQ and RaBitQ codes: the reference decodes the code and
+# evaluates the metric (src/quantized.rs:28-36, src/pq.rs:151-160,
+# src/rabitq.rs:224-238).  The kernel takes q . decode(code) from a
+# query-centroid inner-product table (PQ) or in the rotated space (RaBitQ), so
+# the sum is grouped differently from the decoded vector's sequential sum; the
+# |decode(code)|^2 term is bit-identical.  Tolerance: ids agree with the oracle
+# except among near-ties (>= 98 % overlap), distances of common ids within
+# 1e-5 relative + 2e-6 absolute.
+DECODE_CASES = [("pq", "cosine", 96), ("pq", "dot", 64), ("rabitq", "cosine", 96), ("rabitq", "dot", 64),
+                ("rabitq", "cosine", 128)]
+
+
+@pytest.mark.parametrize("quant,metric,d", DECODE_CASES)
+def test_decoded_metrics_within_tolerance(oracle, quant, metric, d):
+    from pydiskann_b200 import synth
+
+    X, Q = synth.cosine(3000, 60, d, seed=6)
+    om = oracle.COSINE if metric == "cosine" else oracle.DOT
+    adj, med = oracle.build_vamana(X, 24, 48, 1.2, seed=3, metric=om)
+    q = dg.QuantizedDiskANN(X, adj, med, metric=metric)
+    o = oracle.OracleIndex(X, adj, med, om)
+    if quant == "pq":
+        cb = dg.pq_train(X, 8, 64, 10, 3000, seed=1)
+        q.attach_pq(cb)
+        o.set_pq(cb, oracle.pq_encode(X, cb))
+    else:
+        cen, signs = dg.rabitq_params(X, seed=3)
+        P = dg.rabitq_padded(d)
+        q.attach_rabitq(cen, signs)
+        o.set_rabitq(P, cen, signs, oracle.rabitq_encode(X, P, cen, signs))
+    for rr in (0, 32):
+        gi, gd, gc = q.search_arrays(Q, 10, 48, rerank_size=rr)
+        oi, od, oc = o.search(Q, 10, 48, rerank=rr, use_codes=True)
+        assert np.array_equal(gc, oc)
+        same = np.mean([len(set(gi[i]) & set(oi[i])) / 10 for i in range(len(Q))])
+        assert same >= 0.98, (quant, metric, rr, same)
+        m = gi == oi
+        assert np.all(np.abs(gd[m] - od[m]) <= 1e-5 * np.abs(od[m]) + 2e-6), (quant, metric, rr)
+    q.close()
