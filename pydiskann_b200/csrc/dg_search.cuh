@@ -75,7 +75,7 @@ constexpr int kStageCap = 256;  // max adjacency degree
 
 // Per-warp shared-memory carve-up (byte offsets), computed on host and device.
 struct WarpLayout {
-  uint32_t w0, w1, res, cstage, stage, hash, qf, prov, total;
+  uint32_t w0, w1, res, cstage, stage, hash, qf, prov, aux, total;
 };
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 // `decode`: RaBitQ with a cosine / dot metric (rotated query, nibble table).
@@ -99,6 +99,8 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
   else if (trav == TRAV_RABITQ) p = 4 * (rq_padded / 64) * 8 + 32 + align16(rq_padded * 4);
   else if (trav == TRAV_F16) p = align16(dpad * 4);
   o += align16(p);
+  L.aux = o;  // 64-key copy of the register-resident working list (beams <= 64)
+  o += lcap == 64 && !filt ? 64 * 8 : 0;
   L.total = align16(o);
   return L;
 }

@@ -161,80 +161,77 @@ __device__ inline void emit_results(const SearchArgs &a, uint32_t q, const uint6
 // Inserts the ns keys of skeys[] into a register-resident sorted list of at
 // most 64 entries (entry i in lane i % 32: w0 for i < 32, w1 above) with
 // capacity cap.  Keys not below a full list's worst entry, keys already listed
-// and repeats within the batch are dropped.
-__device__ __forceinline__ void reg_insert(const uint64_t *skeys, int ns, uint64_t &w0, uint64_t &w1,
-                                           int &wsize, int cap, uint64_t *scat, uint64_t *cst, int lane) {
+// and repeats within the batch are dropped.  Per batch of up to 32 keys the
+// merge has a fixed depth: every key ranks itself within the batch (pairwise
+// for a few keys, a bitonic sort for more) and within the list (binary search
+// over a shared copy), its final slot is list rank + batch rank among the
+// kept keys, and every output slot then gathers either its new key or the
+// list entry that shifts into it.
+__device__ __forceinline__ void reg_insert(const uint64_t *skeys, int ns, uint64_t &w0, uint64_t &w1, int &wsize,
+                                           int cap, uint64_t *scat, uint64_t *lst, uint64_t *cst, int lane) {
+  const uint32_t lt = lanemask_lt(lane);
   for (int b0 = 0; b0 < ns; b0 += 32) {
     const int cnt = min(32, ns - b0);
-    uint64_t kk = lane < cnt ? skeys[b0 + lane] : kKeyInvalid;
+    uint64_t u = lane < cnt ? skeys[b0 + lane] : kKeyInvalid;
     if (wsize >= cap) {
       const uint64_t thr = strip_flag(shfl64(cap - 1 < 32 ? w0 : w1, (cap - 1) & 31));
-      if (!(kk < thr)) kk = kKeyInvalid;
+      if (!(u < thr)) u = kKeyInvalid;
     }
-    const uint32_t vm = __ballot_sync(kFull, kk != kKeyInvalid);
+    const uint32_t vm = __ballot_sync(kFull, u != kKeyInvalid);
     const int s = __popc(vm);
     if (s == 0) continue;
-    // survivors sorted ascending into lanes 0..s-1, repeats flagged dead
-    uint64_t ck;
-    bool alive;
-    if (s > 8) {
-      ck = warp_sort_keys(kk, lane);
-      const uint64_t prev = shfl64(ck, lane > 0 ? lane - 1 : 0);
-      alive = lane < s && !(lane > 0 && prev == ck);
+    // rank within the batch; repeated keys take consecutive ranks, later copies die
+    int rank;
+    bool dead;
+    if (s > 12) {
+      u = warp_sort_keys(u, lane);
+      const uint64_t prev = shfl64(u, lane > 0 ? lane - 1 : 0);
+      rank = lane;
+      dead = lane >= s || (lane > 0 && prev == u);
     } else {
-      if (kk != kKeyInvalid) cst[__popc(vm & lanemask_lt(lane))] = kk;
+      if (u != kKeyInvalid) cst[__popc(vm & lt)] = u;
       __syncwarp();
-      const uint64_t u = lane < s ? cst[lane] : kKeyInvalid;
-      bool al = lane < s;
-      int rank = 0;
-      for (int i = 0; i < s; ++i) {
-        const uint64_t o = shfl64(u, i);
-        if (o < u) ++rank;
-        if (i < lane && o == u) al = false;
-      }
-      __syncwarp();
-      if (al) cst[rank] = u;  // distinct keys: ranks are a permutation of the alive ones
-      const uint32_t am = __ballot_sync(kFull, al);
-      __syncwarp();
-      const int na = __popc(am);
-      ck = lane < na ? cst[lane] : kKeyInvalid;
-      alive = lane < na;
-      __syncwarp();
-    }
-    // rank of every survivor in the list, listed duplicates, and the shift
-    // of every list entry
-    const uint64_t s0 = strip_flag(w0), s1 = strip_flag(w1);
-    int mypos = 0, c0 = 0, c1 = 0;
-    bool myalive = false;
-    const int sn = __popc(__ballot_sync(kFull, lane < 32 && (alive || lane < s)));
-    for (int t = 0; t < sn; ++t) {
-      const uint64_t kt = shfl64(ck, t);
-      const bool at = __shfl_sync(kFull, alive, t);
-      if (!at) continue;  // uniform
-      const uint32_t lt0 = __ballot_sync(kFull, s0 < kt), lt1 = __ballot_sync(kFull, s1 < kt);
-      const bool dup = __any_sync(kFull, s0 == kt || s1 == kt);
-      if (lane == t) {
-        mypos = __popc(lt0) + __popc(lt1);
-        myalive = !dup;
-      }
-      if (!dup) {
-        c0 += kt < s0;
-        c1 += kt < s1;
+      u = lane < s ? cst[lane] : kKeyInvalid;
+      rank = 0;
+      dead = lane >= s;
+      for (int t = 0; t < s; ++t) {
+        const uint64_t o = shfl64(u, t);
+        rank += (o < u) || (o == u && t < lane);
+        dead |= o == u && t < lane;
       }
     }
-    const uint32_t am = __ballot_sync(kFull, myalive);
-    const int nc = __popc(am);
-    if (nc == 0) continue;
-    if (myalive) {
-      const int np = mypos + __popc(am & lanemask_lt(lane));
-      if (np < cap) scat[np] = ck;
-    }
-    if (lane < wsize && lane + c0 < cap) scat[lane + c0] = w0;
-    if (lane + 32 < wsize && lane + 32 + c1 < cap) scat[lane + 32 + c1] = w1;
+    // rank within the list (its stripped keys in shared memory)
+    lst[lane] = strip_flag(w0);
+    lst[lane + 32] = strip_flag(w1);
     __syncwarp();
-    wsize = min(cap, wsize + nc);
-    w0 = lane < wsize ? scat[lane] : kKeyInvalid;
-    w1 = lane + 32 < wsize ? scat[lane + 32] : kKeyInvalid;
+    int p = 0;
+#pragma unroll
+    for (int step = 32; step > 0; step >>= 1)
+      if (p + step <= wsize && lst[p + step - 1] < u) p += step;
+    if (!dead && p < wsize && lst[p] == u) dead = true;  // already listed
+    const uint32_t deadm = __reduce_or_sync(kFull, (lane < s && dead) ? (1u << rank) : 0u);
+    const int na = s - __popc(deadm);
+    if (na == 0) {
+      __syncwarp();
+      continue;
+    }
+    const int pos = p + rank - __popc(deadm & ((1u << (rank & 31)) - 1u));
+    const bool put = !dead && pos < cap;
+    const uint32_t sm0 = __reduce_or_sync(kFull, (put && pos < 32) ? (1u << pos) : 0u);
+    const uint32_t sm1 = __reduce_or_sync(kFull, (put && pos >= 32) ? (1u << (pos & 31)) : 0u);
+    if (put) scat[pos] = u;
+    __syncwarp();
+    // slot l keeps a new key, or the list entry l - (new keys before l)
+    const int i0 = lane - __popc(sm0 & lt);
+    const int i1 = lane + 32 - __popc(sm0) - __popc(sm1 & lt);
+    const uint64_t x0 = shfl64(w0, i0 & 31), x1 = shfl64(w1, i0 & 31);
+    const uint64_t y0 = shfl64(w0, i1 & 31), y1 = shfl64(w1, i1 & 31);
+    const int nsz = min(cap, wsize + na);
+    uint64_t n0 = ((sm0 >> lane) & 1u) ? scat[lane] : (i0 < 32 ? x0 : x1);
+    uint64_t n1 = ((sm1 >> lane) & 1u) ? scat[lane + 32] : (i1 < 32 ? y0 : y1);
+    w0 = lane < nsz ? n0 : kKeyInvalid;
+    w1 = lane + 32 < nsz ? n1 : kKeyInvalid;
+    wsize = nsz;
     __syncwarp();
   }
 }
@@ -247,6 +244,7 @@ template <int TRAV, int MET, int LPR, int LPRF>
 __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *wsm, const WarpLayout &Ly,
                                       int lane) {
   uint64_t *scat = reinterpret_cast<uint64_t *>(wsm + Ly.w0);  // scatter buffer, 64 keys
+  uint64_t *lst = reinterpret_cast<uint64_t *>(wsm + Ly.aux);   // list copy, 64 keys
   uint64_t *skeys = reinterpret_cast<uint64_t *>(wsm + Ly.w1) ; // survivors of one expansion (<= 64)
   uint64_t *cst = reinterpret_cast<uint64_t *>(wsm + Ly.cstage);
   uint32_t *stage = reinterpret_cast<uint32_t *>(wsm + Ly.stage);
@@ -314,7 +312,7 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
     for (int g0 = 0; g0 < ns; g0 += 32) {
       if (nsurv > 32) {  // the 64-key survivor buffer could overflow: insert what it holds
         __syncwarp();
-        reg_insert(skeys, nsurv, w0, w1, wsize, L, scat, cst, lane);
+        reg_insert(skeys, nsurv, w0, w1, wsize, L, scat, lst, cst, lane);
         nsurv = 0;
         thr = wsize >= L ? strip_flag(shfl64(L - 1 < 32 ? w0 : w1, (L - 1) & 31)) : kKeyInvalid;
       }
@@ -328,7 +326,7 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
       nsurv += __popc(m);
     }
     __syncwarp();
-    if (nsurv) reg_insert(skeys, nsurv, w0, w1, wsize, L, scat, cst, lane);
+    if (nsurv) reg_insert(skeys, nsurv, w0, w1, wsize, L, scat, lst, cst, lane);
   }
   // emit through the shared-memory path
   uint64_t *Wm = scat;
