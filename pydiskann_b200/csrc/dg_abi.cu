@@ -123,7 +123,8 @@ DgStatus dg_index_create(const DgIndexDesc *desc, DgIndex **out) {
     return bail(s);
   if ((s = to_device(idx, (void **)&idx->adj, desc->adjacency, idx->n * idx->R * 4)) != DG_OK) return bail(s);
   for (auto &sl : idx->slots) {
-    if (cudaMalloc(&sl.counter, 4) != cudaSuccess) return bail(fail(DG_ENOMEM, "counter allocation"));
+    if (cudaMalloc(&sl.counter, 4 * DgIndex::kPipeChunks) != cudaSuccess)
+      return bail(fail(DG_ENOMEM, "counter allocation"));
     if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess)
       return bail(fail(DG_EDEVICE, "event creation"));
   }
@@ -148,6 +149,13 @@ DgStatus dg_index_destroy(DgIndex *idx) {
   }
   for (void *p : idx->allocations) cudaFree(p);
   if (idx->stream) cudaStreamDestroy(idx->stream);
+  for (cudaStream_t t : {idx->pipe_in, idx->pipe_out, idx->pipe_k[0], idx->pipe_k[1]})
+    if (t) cudaStreamDestroy(t);
+  if (idx->pipe_start) cudaEventDestroy(idx->pipe_start);
+  for (int c = 0; c < DgIndex::kPipeChunks; ++c) {
+    if (idx->pipe_in_ev[c]) cudaEventDestroy(idx->pipe_in_ev[c]);
+    if (idx->pipe_k_ev[c]) cudaEventDestroy(idx->pipe_k_ev[c]);
+  }
   delete idx;
   return DG_OK;
 }
@@ -304,6 +312,42 @@ static int program_depth(const DgFilterOp *ops, uint32_t n, uint64_t pool_len) {
   return mx;
 }
 
+// A slot whose previous call has finished on the device (the lowest such, so a
+// caller that waits for each call keeps reusing the same buffers); when all
+// are in flight, the next one of the ring after its call completes.
+static cudaError_t take_slot(DgIndex *idx, DgIndex::Slot **out) {
+  for (int i = 0; i < DgIndex::kSlots; ++i) {
+    DgIndex::Slot &c = idx->slots[i];
+    if (c.pending) {
+      const cudaError_t e = cudaEventQuery(c.done);
+      if (e == cudaErrorNotReady) continue;
+      if (e != cudaSuccess) return e;
+      c.pending = false;
+    }
+    *out = &c;
+    return cudaSuccess;
+  }
+  DgIndex::Slot &c = idx->slots[idx->next_slot];
+  idx->next_slot = (idx->next_slot + 1) % DgIndex::kSlots;
+  const cudaError_t e = cudaEventSynchronize(c.done);
+  if (e != cudaSuccess) return e;
+  c.pending = false;
+  *out = &c;
+  return cudaSuccess;
+}
+
+static DgStatus pipe_init(DgIndex *idx) {
+  if (idx->pipe_in) return DG_OK;
+  for (cudaStream_t *t : {&idx->pipe_in, &idx->pipe_out, &idx->pipe_k[0], &idx->pipe_k[1]})
+    DG_CUDA(cudaStreamCreateWithFlags(t, cudaStreamNonBlocking));
+  DG_CUDA(cudaEventCreateWithFlags(&idx->pipe_start, cudaEventDisableTiming));
+  for (int c = 0; c < DgIndex::kPipeChunks; ++c) {
+    DG_CUDA(cudaEventCreateWithFlags(&idx->pipe_in_ev[c], cudaEventDisableTiming));
+    DG_CUDA(cudaEventCreateWithFlags(&idx->pipe_k_ev[c], cudaEventDisableTiming));
+  }
+  return DG_OK;
+}
+
 static DgStatus stage_copy(DgIndex::Buf &b, const void *src, size_t bytes, cudaStream_t st) {
   DgStatus s = buf_reserve(b, bytes);
   if (s != DG_OK) return s;
@@ -385,12 +429,9 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   std::lock_guard<std::mutex> lk(idx->mu);
   DG_CUDA(cudaSetDevice(idx->device));
   cudaStream_t st = (p->flags & DG_FLAG_STREAM) || p->stream ? (cudaStream_t)p->stream : idx->stream;
-  DgIndex::Slot &sl = idx->slots[idx->next_slot];
-  idx->next_slot = (idx->next_slot + 1) % DgIndex::kSlots;
-  if (sl.pending) {
-    DG_CUDA(cudaEventSynchronize(sl.done));
-    sl.pending = false;
-  }
+  DgIndex::Slot *slp = nullptr;
+  DG_CUDA(take_slot(idx, &slp));
+  DgIndex::Slot &sl = *slp;
   DgStatus s;
   SearchArgs a{};
   a.n = idx->n;
@@ -438,6 +479,8 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
     a.perL = (const uint32_t *)sl.perl.p;
   }
   const size_t kq = (size_t)nq * p->k;
+  // host calls of many queries: chunks whose copies overlap the other chunks' kernels
+  const uint32_t chunks = devptr || nq < 4096 ? 1u : std::min<uint32_t>(DgIndex::kPipeChunks, nq / 2048);
   if (devptr) {
     a.Q = queries;
     a.out_ids = out_ids;
@@ -445,7 +488,11 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
     a.out_cnt = out_counts;
     a.out_stats = out_stats;
   } else {
-    if ((s = stage_copy(sl.q, queries, (size_t)nq * idx->d * 4, st)) != DG_OK) return s;
+    if (chunks > 1) {
+      if ((s = buf_reserve(sl.q, (size_t)nq * idx->d * 4)) != DG_OK) return s;
+    } else if ((s = stage_copy(sl.q, queries, (size_t)nq * idx->d * 4, st)) != DG_OK) {
+      return s;
+    }
     if ((s = buf_reserve(sl.ids, kq * 4)) != DG_OK) return s;
     if ((s = buf_reserve(sl.dists, kq * 4)) != DG_OK) return s;
     if ((s = buf_reserve(sl.cnt, (size_t)nq * 4)) != DG_OK) return s;
@@ -459,7 +506,6 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
     }
   }
   a.counter = sl.counter;
-  DG_CUDA(cudaMemsetAsync(sl.counter, 0, 4, st));
 
   const int met = met_kind(idx->metric);
   int lpr = 1;
@@ -468,16 +514,62 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
   const WarpLayout Ly = warp_layout(trav, lcap, any_filter, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded, trav == TRAV_RABITQ && met_kind(idx->metric) != MET_L2);
-  LaunchInfo info;
-  switch (trav) {
-    case TRAV_F32: s = launch_search_f32(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
-    case TRAV_BF16: s = launch_search_bf16(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
-    case TRAV_F16: s = launch_search_f16(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
-    case TRAV_INT8: s = launch_search_int8(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
-    case TRAV_PQ: s = launch_search_pq(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
-    default: s = launch_search_rabitq(a, Ly, met, lpr, lcap, any_filter, st, &info); break;
+  auto launch = [&](const SearchArgs &aa, cudaStream_t ss) -> DgStatus {
+    LaunchInfo info;
+    DG_CUDA(cudaMemsetAsync(aa.counter, 0, 4, ss));
+    switch (trav) {
+      case TRAV_F32: return launch_search_f32(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+      case TRAV_BF16: return launch_search_bf16(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+      case TRAV_F16: return launch_search_f16(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+      case TRAV_INT8: return launch_search_int8(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+      case TRAV_PQ: return launch_search_pq(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+      default: return launch_search_rabitq(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+    }
+  };
+  if (chunks > 1) {
+    if ((s = pipe_init(idx)) != DG_OK) return s;
+    DG_CUDA(cudaEventRecord(idx->pipe_start, st));  // after the staged programs / beams on st
+    for (cudaStream_t t : {idx->pipe_in, idx->pipe_out, idx->pipe_k[0], idx->pipe_k[1]})
+      DG_CUDA(cudaStreamWaitEvent(t, idx->pipe_start, 0));
+    const size_t d = idx->d, k = p->k;
+    for (uint32_t c = 0; c < chunks; ++c) {
+      const size_t q0 = (size_t)nq * c / chunks, q1 = (size_t)nq * (c + 1) / chunks;
+      DG_CUDA(cudaMemcpyAsync((float *)sl.q.p + q0 * d, queries + q0 * d, (q1 - q0) * d * 4,
+                              cudaMemcpyHostToDevice, idx->pipe_in));
+      DG_CUDA(cudaEventRecord(idx->pipe_in_ev[c], idx->pipe_in));
+    }
+    for (uint32_t c = 0; c < chunks; ++c) {
+      const size_t q0 = (size_t)nq * c / chunks, q1 = (size_t)nq * (c + 1) / chunks;
+      SearchArgs ac = a;
+      ac.Q = a.Q + q0 * d;
+      ac.nq = (uint32_t)(q1 - q0);
+      ac.out_ids = a.out_ids + q0 * k;
+      ac.out_d = a.out_d + q0 * k;
+      ac.out_cnt = a.out_cnt + q0;
+      if (a.out_stats) ac.out_stats = a.out_stats + 2 * q0;
+      if (a.perL) ac.perL = a.perL + q0;
+      if (a.foffs) ac.foffs = a.foffs + q0;
+      ac.counter = sl.counter + c;
+      cudaStream_t ks = idx->pipe_k[c & 1];
+      DG_CUDA(cudaStreamWaitEvent(ks, idx->pipe_in_ev[c], 0));
+      if ((s = launch(ac, ks)) != DG_OK) return s;
+      DG_CUDA(cudaEventRecord(idx->pipe_k_ev[c], ks));
+      DG_CUDA(cudaStreamWaitEvent(idx->pipe_out, idx->pipe_k_ev[c], 0));
+      DG_CUDA(cudaMemcpyAsync(out_ids + q0 * k, ac.out_ids, (q1 - q0) * k * 4, cudaMemcpyDeviceToHost,
+                              idx->pipe_out));
+      DG_CUDA(cudaMemcpyAsync(out_dists + q0 * k, ac.out_d, (q1 - q0) * k * 4, cudaMemcpyDeviceToHost,
+                              idx->pipe_out));
+      DG_CUDA(cudaMemcpyAsync(out_counts + q0, ac.out_cnt, (q1 - q0) * 4, cudaMemcpyDeviceToHost, idx->pipe_out));
+      if (out_stats)
+        DG_CUDA(cudaMemcpyAsync(out_stats + 2 * q0, ac.out_stats, (q1 - q0) * 8, cudaMemcpyDeviceToHost,
+                                idx->pipe_out));
+    }
+    DG_CUDA(cudaEventRecord(sl.done, idx->pipe_out));
+    DG_CUDA(cudaStreamWaitEvent(st, sl.done, 0));  // later work on the caller's stream follows
+    DG_CUDA(cudaEventSynchronize(sl.done));
+    return DG_OK;
   }
-  if (s != DG_OK) return s;
+  if ((s = launch(a, st)) != DG_OK) return s;
   if (!devptr) {
     DG_CUDA(cudaMemcpyAsync(out_ids, a.out_ids, kq * 4, cudaMemcpyDeviceToHost, st));
     DG_CUDA(cudaMemcpyAsync(out_dists, a.out_d, kq * 4, cudaMemcpyDeviceToHost, st));
@@ -505,12 +597,9 @@ DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
   if (dep < 0 || dep > kFilterStack) return fail(DG_EINVAL, "malformed filter program");
   std::lock_guard<std::mutex> lk(idx->mu);
   DG_CUDA(cudaSetDevice(idx->device));
-  DgIndex::Slot &sl = idx->slots[idx->next_slot];
-  idx->next_slot = (idx->next_slot + 1) % DgIndex::kSlots;
-  if (sl.pending) {
-    DG_CUDA(cudaEventSynchronize(sl.done));
-    sl.pending = false;
-  }
+  DgIndex::Slot *slp = nullptr;
+  DG_CUDA(take_slot(idx, &slp));
+  DgIndex::Slot &sl = *slp;
   DgStatus s;
   if ((s = stage_copy(sl.fops, ops, (size_t)nops * sizeof(DgFilterOp), idx->stream)) != DG_OK) return s;
   if ((s = stage_copy(sl.fpool, pool, (size_t)pool_len * 8, idx->stream)) != DG_OK) return s;

@@ -39,13 +39,20 @@ struct DgIndex {
   };
   struct Slot {
     Buf q, ids, dists, cnt, stats, fops, foffs, fpool, perl;
-    uint32_t *counter = nullptr;  // work counter of the persistent grid
+    uint32_t *counter = nullptr;  // work counters of the persistent grid (one per pipeline chunk)
     cudaEvent_t done = nullptr;
     bool pending = false;
   };
   static constexpr int kSlots = 16;
   Slot slots[kSlots];
   int next_slot = 0;
+  // Host-pointer calls of many queries run as a pipeline of chunks: queries
+  // in on pipe_in, kernels alternating on pipe_k[0..1] (a chunk's kernel
+  // overlaps the previous one's tail), results out on pipe_out.  Created on
+  // first use; calls on one handle are serialised, so one set suffices.
+  static constexpr int kPipeChunks = 4;
+  cudaStream_t pipe_in = nullptr, pipe_out = nullptr, pipe_k[2] = {nullptr, nullptr};
+  cudaEvent_t pipe_start = nullptr, pipe_in_ev[kPipeChunks] = {}, pipe_k_ev[kPipeChunks] = {};
   std::vector<void *> allocations;
 };
 

@@ -274,3 +274,28 @@ def test_decoded_metrics_within_tolerance(oracle, quant, metric, d):
         m = gi == oi
         assert np.all(np.abs(gd[m] - od[m]) <= 1e-5 * np.abs(od[m]) + 2e-6), (quant, metric, rr)
     q.close()
+
+
+def test_host_pipeline_matches_device_call(small_data, small_graph):
+    """Host-pointer calls of >= 4096 queries run as a pipeline of chunks over
+    several streams; results, counts and stats equal the single device-pointer
+    launch, with per-query beams and per-query filter programs."""
+    import torch
+
+    from pydiskann_b200 import synth
+
+    X, _ = small_data
+    adj, med = small_graph
+    g = dg.FilteredDiskANN(X, adj, med, _labels(len(X)))
+    Q = synth.mixture(9000, 128, 32, seed=8, stream=synth.STREAM_QUERY)
+    beams = (16 + np.arange(len(Q)) % 50).astype(np.uint32)
+    fl = [FILTERS[i % len(FILTERS)] if i % 3 == 0 else dg.Filter.none() for i in range(len(Q))]
+    for kw in ({}, {"per_query_beam": beams}, {"per_query_beam": beams, "filters": fl}):
+        hi, hd, hc, hs = g.search_arrays(Q, 10, 40, with_stats=True, **kw)
+        di, dd, dc, ds = g.search_arrays(torch.from_numpy(Q).cuda(), 10, 40, with_stats=True, **kw)
+        torch.cuda.synchronize()
+        assert np.array_equal(hc, dc.cpu().numpy().view(np.uint32))
+        assert np.array_equal(hi, di.cpu().numpy().view(np.uint32))
+        assert np.array_equal(hd, dd.cpu().numpy())
+        assert np.array_equal(hs, ds.cpu().numpy().view(np.uint32))
+    g.close()
