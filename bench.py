@@ -178,6 +178,11 @@ class Clocks:
 
 
 # ------------------------------------------------------------ GPU timing
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+# ncu capture of this bench's own command, keyed by (variant, L, queries, base
+# vectors); profiles/beam_search_int8_1Mx128.md, section 1.
+NCU_TRAFFIC = {("int8_rerank", 40, 10_000, 1_000_000): 1141.5e6 + 47.1e6}
+
 VARIANTS = {
     # name: (traversal, rerank = L?)
     "fp32": ("f32", False),
@@ -356,7 +361,8 @@ def main():
         r = results[head]
         ach = r["alg_bytes_per_launch"] / (r["launch_ms"] / 1e3) / 1e9
         line["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                            "frac": round(ach / hbm, 4), "traffic": None,
+                            "frac": round(ach / hbm, 4),
+                            "traffic": NCU_TRAFFIC.get((head, r["L"], args.nq, args.n)),
                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650"}
         line["clocks"] = r["clocks"]
         line["gpu_launches"] = args.steps
