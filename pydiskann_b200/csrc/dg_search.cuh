@@ -327,12 +327,15 @@ __device__ __forceinline__ float rows_distance(const uint8_t *__restrict__ rows,
   constexpr int RPI = 32 / LPR;
   constexpr int EPC = Chunk<ELEM>::EPC;
   const int g = lane / LPR, r = lane % LPR;
-  float pa[LPR], pb[LPR];
+  // packed two-wide FP32 arithmetic (f32x2 FMA) within a 16-byte chunk; the
+  // pair is folded into the row's running sum once per chunk
+  float sa[LPR], sb[LPR];
   uint32_t ids[LPR];  // DG_PAD marks an empty slot
+  const float2 neg1 = make_float2(-1.0f, -1.0f);
 #pragma unroll
   for (int i = 0; i < LPR; ++i) {
-    pa[i] = 0.0f;
-    pb[i] = 0.0f;
+    sa[i] = 0.0f;
+    sb[i] = 0.0f;
     const int c = i * RPI + g;
     const uint32_t id = __shfl_sync(kFull, cand, c & 31);
     ids[i] = c < cnt ? id : DG_PAD;
@@ -343,30 +346,34 @@ __device__ __forceinline__ float rows_distance(const uint8_t *__restrict__ rows,
 #pragma unroll
     for (int i = 0; i < LPR; ++i)
       if (ids[i] != DG_PAD) v[i] = __ldg(reinterpret_cast<const uint4 *>(rows + (size_t)ids[i] * stride) + chunk);
-    float qv[EPC];
+    float2 q2[EPC / 2];
 #pragma unroll
-    for (int e = 0; e < EPC; ++e) qv[e] = qs[chunk * EPC + e];
+    for (int e = 0; e < EPC / 2; ++e) q2[e] = reinterpret_cast<const float2 *>(qs + chunk * EPC)[e];
 #pragma unroll
     for (int i = 0; i < LPR; ++i) {
       if (ids[i] != DG_PAD) {
         float x[EPC];
         Chunk<ELEM>::unpack(v[i], x);
+        float2 pa = make_float2(0.0f, 0.0f), pb = make_float2(0.0f, 0.0f);
 #pragma unroll
-        for (int e = 0; e < EPC; ++e) {
+        for (int e = 0; e < EPC / 2; ++e) {
+          const float2 x2 = make_float2(x[2 * e], x[2 * e + 1]);
           if (MET == MET_L2) {
-            float df = x[e] - qv[e];
-            pa[i] = fmaf(df, df, pa[i]);
+            const float2 df = __ffma2_rn(q2[e], neg1, x2);  // x - q, one rounding
+            pa = __ffma2_rn(df, df, pa);
           } else {
-            pa[i] = fmaf(x[e], qv[e], pa[i]);
-            if (MET == MET_COS) pb[i] = fmaf(x[e], x[e], pb[i]);
+            pa = __ffma2_rn(x2, q2[e], pa);
+            if (MET == MET_COS) pb = __ffma2_rn(x2, x2, pb);
           }
         }
+        sa[i] += pa.x + pa.y;
+        if (MET == MET_COS) sb[i] += pb.x + pb.y;
       }
     }
   }
-  float a = transpose_reduce<LPR>(pa, lane);
+  float a = transpose_reduce<LPR>(sa, lane);
   float b = 0.0f;
-  if (MET == MET_COS) b = transpose_reduce<LPR>(pb, lane);
+  if (MET == MET_COS) b = transpose_reduce<LPR>(sb, lane);
   // lane l holds candidate (l % LPR) * RPI + l / LPR; route candidate j to lane j
   const int srcl = (lane % RPI) * LPR + lane / RPI;
   a = __shfl_sync(kFull, a, srcl);
