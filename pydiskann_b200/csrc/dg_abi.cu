@@ -240,6 +240,8 @@ DgStatus dg_index_attach_int8(DgIndex *idx, float scale, float offset, const uin
   else s = encode_int8_device(idx->vec, idx->n, idx->d, idx->dpad, scale, offset, idx->codes,
                               idx->code_stride, idx->stream);
   if (s != DG_OK) return s;
+  if ((s = dev_alloc(idx, (void **)&idx->i8_norm, idx->n * 4)) != DG_OK) return s;
+  if ((s = int8_norms_device(idx->codes, idx->n, idx->code_stride, idx->i8_norm, idx->stream)) != DG_OK) return s;
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
 }
@@ -451,6 +453,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   a.pq_cb = idx->pq_cb;
   a.i8_scale = idx->i8_scale;
   a.i8_offset = idx->i8_offset;
+  a.i8_norm = idx->i8_norm;
   a.rq_padded = idx->rq_padded;
   a.rq_centroid = idx->rq_centroid;
   a.rq_signs = idx->rq_signs;
@@ -759,6 +762,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   a.pq_cb = idx->pq_cb;
   a.i8_scale = idx->i8_scale;
   a.i8_offset = idx->i8_offset;
+  a.i8_norm = idx->i8_norm;
   a.rq_padded = idx->rq_padded;
   a.rq_centroid = idx->rq_centroid;
   a.rq_signs = idx->rq_signs;

@@ -30,6 +30,21 @@ __global__ void k_int8(const float *v, uint64_t n, uint32_t d, uint32_t dpad, fl
     out[i] = c < d ? int8_code(v[r * dpad + c], inv, beta) : 0;
   }
 }
+// Sum of squared codes of every int8 row (padding bytes are zero).
+__global__ void k_int8_norm(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 *row = reinterpret_cast<const uint4 *>(codes + r * stride);
+    uint32_t s = 0;
+    for (uint32_t c = 0; c < stride / 16; ++c) {
+      const uint4 v = row[c];
+      s = __dp4a(v.x, v.x, s);
+      s = __dp4a(v.y, v.y, s);
+      s = __dp4a(v.z, v.z, s);
+      s = __dp4a(v.w, v.w, s);
+    }
+    out[r] = s;
+  }
+}
 // ProductQuantizer::encode (src/pq.rs:122-149): argmin with strict '<'.
 __global__ void k_pq_encode(const float *v, uint64_t n, uint32_t dpad, uint32_t M, uint32_t K,
                             uint32_t ds, const float *cb, uint8_t *codes, uint32_t stride) {
@@ -201,6 +216,11 @@ DgStatus encode_int8_device(const float *vec, uint64_t n, uint32_t d, uint32_t d
   const float inv = 1.0f / scale;  // same f32 expressions as Int8Quantizer::encode
   const float beta = -offset / scale;
   k_int8<<<grid_for(n * stride, 256), 256, 0, st>>>(vec, n, d, dpad, inv, beta, codes, stride);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+DgStatus int8_norms_device(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, cudaStream_t st) {
+  k_int8_norm<<<grid_for(n, 256), 256, 0, st>>>(codes, n, stride, out);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

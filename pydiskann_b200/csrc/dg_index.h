@@ -22,6 +22,7 @@ struct DgIndex {
   uint32_t pq_M = 0, pq_K = 0;
   float *pq_cb = nullptr;     // [M][K][d/M]
   float i8_scale = 1.0f, i8_offset = 0.0f;
+  uint32_t *i8_norm = nullptr; // [n] sum of squared int8 codes (tensor-core L2)
   uint32_t rq_padded = 0;
   float *rq_centroid = nullptr, *rq_signs = nullptr;
   float *dnorm2 = nullptr;    // [n] |decode(code)|^2 (cosine over PQ / RaBitQ codes)
@@ -77,6 +78,8 @@ DgStatus encode_bf16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_
 DgStatus encode_rabitq_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint32_t P,
                               const float *centroid, const float *signs, uint8_t *codes,
                               uint32_t stride, cudaStream_t st);
+// Sum of squared codes per vector for int8 codes.
+DgStatus int8_norms_device(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, cudaStream_t st);
 // |decode(code)|^2 per vector for PQ / RaBitQ codes (the cosine metric's |x|^2).
 DgStatus decoded_norms_device(const DgIndex *idx, float *out, cudaStream_t st);
 DgStatus count_matching_device(const uint64_t *labels, uint64_t n, uint32_t nf,

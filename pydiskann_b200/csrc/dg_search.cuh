@@ -43,6 +43,7 @@ struct SearchArgs {
   uint32_t pq_M, pq_K, pq_ds;
   const float *pq_cb;     // [M][K][ds]
   float i8_scale, i8_offset;
+  const uint32_t *i8_norm;  // [n] sum of squared codes (int8 L2 on tensor cores)
   uint32_t rq_padded;
   const float *rq_centroid;  // [d]
   const float *rq_signs;     // [3][padded]
@@ -94,7 +95,7 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
   L.prov = o;
   uint32_t p = 0;
   if (trav == TRAV_PQ) p = pq_M * pq_K * 4;
-  else if (trav == TRAV_INT8) p = align16(dpad);
+  else if (trav == TRAV_INT8) p = align16(dpad) + 16;  // query codes, then |q_code|^2
   else if (trav == TRAV_RABITQ && decode) p = 16 + rq_padded * 4 + rq_padded * 16;
   else if (trav == TRAV_RABITQ) p = 4 * (rq_padded / 64) * 8 + 32 + align16(rq_padded * 4);
   else if (trav == TRAV_F16) p = align16(dpad * 4);
@@ -419,6 +420,73 @@ __device__ __forceinline__ uint32_t int8_l2_group(const uint8_t *__restrict__ co
   uint32_t s = transpose_reduce<LPR>(p, lane);
   const int srcl = (lane % RPI) * LPR + lane / RPI;
   return __shfl_sync(kFull, s, srcl);
+}
+
+// One warp-wide u8 x u8 -> s32 tensor-core step (16 rows x 32 dims x 8 columns).
+__device__ __forceinline__ void mma_u8_16x8x32(int (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// int8 squared distances of up to 32 candidates on the tensor cores, exact:
+// |q - x|^2 = |q|^2 + |x|^2 - 2 q.x in integers.  Candidates form two tiles of
+// 16 rows; lane (g = lane/4, t = lane%4) feeds rows g and g+8 of a tile.  The
+// dims of every 32-wide k step are assigned per lane (any assignment works for
+// a dot product as long as rows and query agree): lane t reads the 16-byte
+// chunks t, t+4, t+8, ... of its rows and of the query, each chunk serving two
+// k steps (bytes 0-7, then 8-15).  Every column of B holds the query, so the
+// t = 0 lane of group g ends with q.x of rows g (c[0]) and g+8 (c[2]).
+__device__ __forceinline__ uint32_t int8_l2_mma(const uint8_t *__restrict__ codes, uint32_t stride,
+                                                const uint8_t *qcode, uint32_t qn,
+                                                const uint32_t *__restrict__ xnorm, uint32_t cand, int cnt,
+                                                int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int nch = (int)(stride >> 4);
+  const int J = (nch + 3) >> 2;
+  const uint32_t id0 = __shfl_sync(kFull, cand, 0);
+  const uint32_t xn = lane < cnt ? __ldg(xnorm + cand) : 0u;  // issued first, used last
+  const bool two = cnt > 16;
+  // rows g, g+8 of tile 0 and (when needed) of tile 1
+  const uint4 *rp[4];
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const int row = g + 8 * h;
+    uint32_t id = __shfl_sync(kFull, cand, row);
+    id = row < cnt ? id : id0;
+    rp[h] = reinterpret_cast<const uint4 *>(codes + (size_t)id * stride);
+  }
+  const uint4 *pq = reinterpret_cast<const uint4 *>(qcode);
+  int c0[4] = {0, 0, 0, 0}, c1[4] = {0, 0, 0, 0};
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  for (int j0 = 0; j0 < J; j0 += 2) {
+    uint4 x[2][4], qv[2];
+    // every load of this step (both tiles) before the first tensor-core op
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int ch = t + 4 * (j0 + u);
+      const bool ok = j0 + u < J && ch < nch;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) x[u][h] = (ok && (h < 2 || two)) ? __ldg(rp[h] + ch) : z;
+      qv[u] = ok ? pq[ch] : z;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      mma_u8_16x8x32(c0, x[u][0].x, x[u][1].x, x[u][0].y, x[u][1].y, qv[u].x, qv[u].y);
+      mma_u8_16x8x32(c0, x[u][0].z, x[u][1].z, x[u][0].w, x[u][1].w, qv[u].z, qv[u].w);
+      if (two) {
+        mma_u8_16x8x32(c1, x[u][2].x, x[u][3].x, x[u][2].y, x[u][3].y, qv[u].x, qv[u].y);
+        mma_u8_16x8x32(c1, x[u][2].z, x[u][3].z, x[u][2].w, x[u][3].w, qv[u].z, qv[u].w);
+      }
+    }
+  }
+  // candidate j = 16T + r sits in lane 4 * (r % 8) of tile T, row half r / 8
+  const int T = lane >> 4, r = lane & 15, src = (r & 7) << 2;
+  const int d00 = __shfl_sync(kFull, c0[0], src), d01 = __shfl_sync(kFull, c0[2], src);
+  const int d10 = __shfl_sync(kFull, c1[0], src), d11 = __shfl_sync(kFull, c1[2], src);
+  const int dot = T == 0 ? (r < 8 ? d00 : d01) : (r < 8 ? d10 : d11);
+  return qn + xn - 2u * (uint32_t)dot;
 }
 
 // int8 codes decoded for non-L2 metrics (src/quantized.rs:28-36): c*scale+offset.

@@ -47,8 +47,8 @@ __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *ws
   } else if (TRAV == TRAV_INT8) {
     if (MET == MET_L2) {
       const uint8_t *qc = wsm + Ly.prov;
-      uint32_t s = int8_l2_group<LPR>(a.codes, a.code_stride, (a.code_stride / 16) / LPR, qc, cand,
-                                      cnt, lane);
+      const uint32_t qn = *reinterpret_cast<const uint32_t *>(qc + align16(a.dpad));
+      const uint32_t s = int8_l2_mma(a.codes, a.code_stride, qc, qn, a.i8_norm, cand, cnt, lane);
       float d = __fmul_rn(__fmul_rn(__uint2float_rn(s), a.i8_scale), a.i8_scale);
       return sqrt_l2 ? __fsqrt_rn(d) : d;
     } else {
@@ -96,7 +96,15 @@ __device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm,
     uint8_t *qc8 = wsm + Ly.prov;
     const float inv = __fdiv_rn(1.0f, a.i8_scale);
     const float beta = __fdiv_rn(-a.i8_offset, a.i8_scale);
-    for (uint32_t i = lane; i < a.dpad; i += 32) qc8[i] = i < a.d ? int8_code(qs[i], inv, beta) : 0;
+    uint32_t qn = 0;
+    for (uint32_t i = lane; i < a.dpad; i += 32) {
+      const uint8_t c = i < a.d ? int8_code(qs[i], inv, beta) : 0;
+      qc8[i] = c;
+      qn += (uint32_t)c * c;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(kFull, qn, o);
+    if (lane == 0) *reinterpret_cast<uint32_t *>(qc8 + align16(a.dpad)) = qn;
   } else if (TRAV == TRAV_F16) {
     float *qh = reinterpret_cast<float *>(wsm + Ly.prov);
     for (uint32_t i = lane; i < a.dpad; i += 32) qh[i] = __half2float(__float2half_rn(qs[i]));
