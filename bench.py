@@ -181,7 +181,7 @@ class Clocks:
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
 # ncu capture of this bench's own command, keyed by (variant, L, queries, base
 # vectors); profiles/beam_search_int8_1Mx128.md, section 1.
-NCU_TRAFFIC = {("int8_rerank", 40, 10_000, 1_000_000): 1141.5e6 + 47.1e6}
+NCU_TRAFFIC = {("int8_rerank", 40, 10_000, 1_000_000): 1204.7e6 + 29.3e6}
 
 VARIANTS = {
     # name: (traversal, rerank = L?)
@@ -370,7 +370,11 @@ def main():
         if not args.no_serving:
             line["serving"] = {n: serving(args, idx, qidx, n, results[n]["L"], Q, gt)
                                for n in dict.fromkeys(["fp32", head]) if n in results}
-            line["p99_ms"] = line["serving"][head]["rates"][-1]["p99_ms"]
+            # headline p99: the highest Poisson load (the saturation run measures queue drain)
+            loaded = [r for r in line["serving"][head]["rates"] if r["offered_rps"]]
+            if loaded:
+                line["p99_ms"] = loaded[-1]["p99_ms"]
+                line["p99_load_rps"] = loaded[-1]["offered_rps"]
         if "fp32" in results:
             line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
     if rank == 0 and head and not args.no_cpu_baseline:
@@ -481,13 +485,15 @@ def cpu_baseline(args, X, Q, adj, med, pq, name, L, threads=None):
     t0 = time.time()
     _oracle_run(o, name, Q[:200], L, threads)
     rate = 200 / max(time.time() - t0, 1e-6)
-    ns = int(min(len(Q), max(200, rate * args.cpu_seconds)))
+    # about cpu_seconds of work: the query set, repeated when one pass is shorter
+    ns = int(min(20 * len(Q), max(200, rate * args.cpu_seconds)))
+    Qs = Q[np.arange(ns) % len(Q)]
     t0 = time.time()
-    _oracle_run(o, name, Q[:ns], L, threads)
+    _oracle_run(o, name, Qs, L, threads)
     dt = time.time() - t0
     return {"value": ns / dt, "unit": "queries/s", "cores": threads, "kind": "port",
-            "sample": f"{ns} of the {len(Q)} queries, variant {name} at L={L}, same graph/codes",
-            "seconds": round(dt, 2)}
+            "sample": f"{ns} queries (the {len(Q)} bench queries, cycled), variant {name} at L={L}, "
+                      f"same graph/codes", "seconds": round(dt, 2)}
 
 
 def reference_arm(args):
