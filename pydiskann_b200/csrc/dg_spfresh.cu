@@ -103,6 +103,15 @@ __device__ __forceinline__ float seq_metric(const float *q, const float *x, uint
   return r > 0.0f ? r : 0.0f;
 }
 
+// The reference's angular / dot from the three sums (RN intrinsics).
+__device__ __forceinline__ float seq_finish(int met, float ab, float aa, float bb) {
+  if (met == MET_DOT) return __fsub_rn(1.0f, ab);
+  if (aa == 0.0f && bb == 0.0f) return 0.0f;
+  if (ab == 0.0f) return 1.0f;
+  const float r = __fsub_rn(1.0f, __fdiv_rn(ab, __fmul_rn(__fsqrt_rn(aa), __fsqrt_rn(bb))));
+  return r > 0.0f ? r : 0.0f;
+}
+
 struct SpfLayout {
   uint32_t p0, p1, r0, r1, cst, qf, prov, total;
 };
@@ -121,7 +130,7 @@ __host__ __device__ inline SpfLayout spf_layout(uint32_t pcap, uint32_t rcap, ui
   if (kind == SPF_PQ) p = pq_M * pq_K * 4;
   else if (kind == SPF_INT8) p = align16(dpad);
   else if (kind == SPF_F16) p = align16(dpad * 4);
-  else if (kind == SPF_RABITQ) p = 4 * (P / 64) * 8 + 32 + align16(P * 4);
+  else if (kind == SPF_RABITQ) p = 4 * (P / 64) * 8 + 32 + align16(P * 4);  // also the decode buffer (P floats)
   o += align16(p);
   L.total = align16(o);
   return L;
@@ -162,7 +171,7 @@ __device__ __forceinline__ float entry_distance(const SpfArgs &a, uint8_t *wsm, 
                                                    row, cnt, lane, qq)
                        : int8_decode_group<2, MET>(a.codes, a.code_stride, ch / 2, qs, a.i8_scale, a.i8_offset, a.d,
                                                    row, cnt, lane, qq);
-  } else {  // PQ (L2 metrics only)
+  } else if (KIND == SPF_PQ && MET == MET_L2) {
     const float *lut = reinterpret_cast<const float *>(wsm + Ly.prov);
     float dd = 0.0f;
     if (lane < cnt) {
@@ -171,6 +180,68 @@ __device__ __forceinline__ float entry_distance(const SpfArgs &a, uint8_t *wsm, 
       for (uint32_t m = 0; m < a.pq_M; ++m) dd = __fadd_rn(dd, lut[m * K + __ldg(crow + m)]);
     }
     return sq ? __fsqrt_rn(dd) : dd;
+  } else if (KIND == SPF_PQ) {
+    // cosine / dot: the metric of the decoded code (centroid concatenation,
+    // src/pq.rs:151-160), summed in coordinate order as the reference's
+    // metric does; one entry per lane
+    float ab = 0.0f, bb = 0.0f;
+    if (lane < cnt) {
+      const uint8_t *crow = a.codes + (size_t)row * a.code_stride;
+      for (uint32_t m = 0; m < a.pq_M; ++m) {
+        const float *cen = a.pq_cb + ((size_t)m * a.pq_K + __ldg(crow + m)) * a.pq_ds;
+        const float *qm = qs + m * a.pq_ds;
+        for (uint32_t j = 0; j < a.pq_ds; ++j) {
+          const float x = __ldg(cen + j);
+          ab = __fadd_rn(ab, __fmul_rn(qm[j], x));
+          bb = __fadd_rn(bb, __fmul_rn(x, x));
+        }
+      }
+    }
+    return seq_finish(MET, ab, qq, bb);
+  } else {
+    // RaBitQ with cosine / dot: decode against the posting centroid
+    // (src/spfresh.rs:344-354, src/rabitq.rs:224-238), one entry at a time
+    // across the warp: signs +-1/sqrt(P), three inverse rounds, c + |v-c| r.
+    const uint32_t P = a.rq_padded;
+    float *r = reinterpret_cast<float *>(wsm + Ly.prov);
+    const float inv = __fdiv_rn(1.0f, __fsqrt_rn((float)P));
+    const uint32_t b = row / a.cap;
+    const float *cen = a.centroids + (size_t)b * a.dpad;
+    float mine = 0.0f;
+    for (int j = 0; j < cnt; ++j) {
+      const uint32_t rj = __shfl_sync(kFull, row, j);
+      const uint8_t *code = a.codes + (size_t)rj * a.code_stride;
+      for (uint32_t i = lane; i < P; i += 32) r[i] = ((__ldg(code + (i >> 3)) >> (i & 7)) & 1u) ? inv : -inv;
+      __syncwarp();
+      for (int rd = 2; rd >= 0; --rd) {
+        for (uint32_t h = 1; h < P; h *= 2) {
+          for (uint32_t t = lane; t < P / 2; t += 32) {
+            const uint32_t x0 = (t / h) * 2 * h + (t % h);
+            const float u = r[x0], v = r[x0 + h];
+            r[x0] = __fadd_rn(u, v);
+            r[x0 + h] = __fsub_rn(u, v);
+          }
+          __syncwarp();
+        }
+        for (uint32_t i = lane; i < P; i += 32) r[i] = __fmul_rn(r[i], a.rq_signs[rd * P + i]);
+        __syncwarp();
+      }
+      const float norm = __fsqrt_rn(__ldg(reinterpret_cast<const float *>(code + P / 8)));
+      float ab = 0.0f, bb = 0.0f;
+      for (uint32_t i = lane; i < a.d; i += 32) {
+        const float o = __fadd_rn(__ldg(cen + i), __fmul_rn(norm, r[i]));
+        ab = fmaf(qs[i], o, ab);
+        bb = fmaf(o, o, bb);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ab += __shfl_xor_sync(kFull, ab, o);
+        bb += __shfl_xor_sync(kFull, bb, o);
+      }
+      if (lane == j) mine = seq_finish(MET, ab, qq, bb);
+      __syncwarp();
+    }
+    return mine;
   }
 }
 
@@ -192,7 +263,12 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
     for (uint32_t i = lane; i < a.dpad; i += 32) qs[i] = i < a.d ? qg[i] : 0.0f;
     __syncwarp();
     float qq = 0.0f;
-    if (MET == MET_COS) {
+    if (MET == MET_COS && (KIND == SPF_PQ || KIND == SPF_RABITQ)) {
+      // |q|^2 in coordinate order, as the reference's angular()
+      if (lane == 0)
+        for (uint32_t i = 0; i < a.d; ++i) qq = __fadd_rn(qq, __fmul_rn(qs[i], qs[i]));
+      qq = __shfl_sync(kFull, qq, 0);
+    } else if (MET == MET_COS) {
       for (uint32_t i = lane; i < a.dpad; i += 32) qq = fmaf(qs[i], qs[i], qq);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) qq += __shfl_xor_sync(kFull, qq, o);
@@ -221,7 +297,7 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
       }
     }
     // ---- per-query code state
-    if (KIND == SPF_PQ) {
+    if (KIND == SPF_PQ && MET == MET_L2) {
       SearchArgs sa{};
       sa.pq_M = a.pq_M;
       sa.pq_K = a.pq_K;
@@ -242,7 +318,7 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
     int rcur = 0, rsize = 0;
     uint32_t *oids32 = nullptr;
     (void)oids32;
-    if (KIND == SPF_RABITQ) {
+    if (KIND == SPF_RABITQ && MET == MET_L2) {
       // ---- 4. search_rabitq: heap of the k smallest exact distances
       const int kk = (int)k;
       uint8_t *pv = wsm + Ly.prov;
@@ -386,7 +462,6 @@ static DgStatus spf_launch(const SpfArgs &a, uint32_t pcap, uint32_t rcap, cudaS
 template <int KIND>
 static DgStatus spf_launch_met(const SpfArgs &a, int met, uint32_t pcap, uint32_t rcap, cudaStream_t st) {
   if (met == MET_L2) return spf_launch<KIND, MET_L2>(a, pcap, rcap, st);
-  if (KIND == SPF_PQ || KIND == SPF_RABITQ) return fail(DG_ENOTSUP, "this code kind supports l2 metrics only");
   if (met == MET_DOT) return spf_launch<KIND, MET_DOT>(a, pcap, rcap, st);
   return spf_launch<KIND, MET_COS>(a, pcap, rcap, st);
 }
@@ -607,9 +682,6 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
   const uint32_t pcap = cap_of(nprobe), rcap = cap_of(want);
   if (!pcap) return fail(DG_ENOTSUP, "n_probe above 1024");
   if (!rcap) return fail(DG_ENOTSUP, "k / rerank_size above 1024");
-  if (s->quant == DG_Q_RABITQ && !rq) return fail(DG_ENOTSUP, "RaBitQ postings support l2 metrics only");
-  if (s->quant == DG_Q_PQ && s->metric != DG_L2 && s->metric != DG_L2SQ)
-    return fail(DG_ENOTSUP, "PQ postings support l2 metrics only");
   const bool devptr = (p->flags & DG_FLAG_DEVICE_PTRS) != 0;
   std::lock_guard<std::mutex> lk(s->mu);
   DG_CUDA(cudaSetDevice(s->device));

@@ -69,6 +69,32 @@ def test_spfresh_scan_matches_oracle(oracle, quant, metric, rerank, ratio):
     s.close()
 
 
+@pytest.mark.parametrize("quant,metric", [("pq", "cosine"), ("pq", "dot"), ("rabitq", "cosine"), ("rabitq", "dot")])
+def test_spfresh_decoded_metrics(oracle, quant, metric):
+    """Cosine / dot over PQ and RaBitQ postings decode the code
+    (src/spfresh.rs:344-354).  PQ decodes in coordinate order as the oracle does
+    (bit-identical); RaBitQ sums the decoded coordinates across lanes, so ids
+    agree except near-ties and distances within 1e-5 relative + 2e-6."""
+    X, Q = synth.cosine(3000, 60, 64, seed=21)
+    s = dg.SPFresh.build(X[:2500], metric=metric, quantizer=quant, rerank_size=0, pq_subspaces=8,
+                         max_posting_size=40, min_posting_size=8, seed=5)
+    s.insert(X[2500:])
+    s.delete(list(range(0, 3000, 13)))
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 6), (7, 40)):
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc), (k, nprobe)
+        if quant == "pq":
+            assert np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
+        else:
+            same = np.mean([len(set(gi[i][:gc[i]]) & set(oi[i][:oc[i]])) / max(1, oc[i]) for i in range(len(Q))])
+            assert same >= 0.98, same
+            m = gi == oi
+            assert np.all(np.abs(gd[m] - od[m]) <= 1e-5 * np.abs(od[m]) + 2e-6)
+    s.close()
+
+
 def test_spfresh_cosine_within_tolerance(oracle):
     X = synth.mixture(3000, 32, 30, seed=14, clip=False)
     s = dg.SPFresh.build(X, metric="cosine", max_posting_size=40, seed=3)
