@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serve-rates", default="100000,1000000,0",
+    ap.add_argument("--serve-rates", default="100000,1000000,2000000,0",
                     help="Poisson arrival rates (req/s) for the serving loop; 0 = all requests at once")
     ap.add_argument("--serve-requests", type=int, default=200_000)
     return ap.parse_args()
@@ -434,8 +434,8 @@ def serving(args, idx, qidx, name, L, Q, gt):
     n = args.serve_requests
     qi = np.arange(n) % len(Q)
     Qn = Q[qi]
-    out = {"variant": name, "L": L, "max_batch": 2048, "streams": 8, "requests": n, "rates": []}
-    with dg.Server(target, max_batch=2048, streams=8, max_k=K, max_wait_us=0) as srv:
+    out = {"variant": name, "L": L, "max_batch": 512, "streams": 16, "requests": n, "rates": []}
+    with dg.Server(target, max_batch=512, streams=16, max_k=K, max_wait_us=0) as srv:
         srv.run_trace(Qn[:5000], np.zeros(5000), k=K, beam_width=L, rerank_size=L if rr else 0, traversal=t)
         for rate in [float(x) for x in args.serve_rates.split(",")]:
             arr = dg.poisson_arrivals(n, rate, seed=3) if rate > 0 else np.zeros(n)

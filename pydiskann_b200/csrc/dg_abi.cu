@@ -39,12 +39,16 @@ DgStatus dev_alloc(DgIndex *idx, void **p, size_t bytes) {
   return DG_OK;
 }
 
+// Grows geometrically (powers of two, at least 64 KiB): a reallocation
+// synchronises the device, so a stream of varying batch sizes must not
+// trigger one per call.
 DgStatus buf_reserve(DgIndex::Buf &b, size_t bytes) {
   if (bytes <= b.cap) return DG_OK;
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.cap = 0;
-  size_t want = std::max<size_t>(bytes, 256);
+  size_t want = 64 * 1024;
+  while (want < bytes) want *= 2;
   DG_CUDA(cudaMalloc(&b.p, want));
   b.cap = want;
   return DG_OK;

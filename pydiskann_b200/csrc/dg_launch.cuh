@@ -15,20 +15,59 @@ struct LaunchInfo {
 
 // Launch geometry: 4 warps per block, as many resident blocks as shared memory
 // allows on every SM, never more warps than queries.
+// Resident blocks per SM of (device, kernel, shared-memory size), and the
+// largest dynamic shared memory already granted to (device, kernel): the
+// attribute and occupancy queries run once, not on every launch (a serving
+// loop launches thousands of small batches per second).
+struct LaunchGeometry {
+  std::mutex mu;
+  std::unordered_map<const void *, int> sms, optin;                  // per device (key: device id)
+  std::unordered_map<uint64_t, int> granted;                           // (device, kernel) -> smem
+  std::unordered_map<uint64_t, std::unordered_map<uint32_t, int>> nb;  // (device, kernel) -> smem -> blocks
+};
+inline LaunchGeometry &launch_geometry() {
+  static LaunchGeometry g;
+  return g;
+}
+
 template <typename K>
 DgStatus launch_persistent(K kernel, const SearchArgs &a, const WarpLayout &Ly, cudaStream_t st,
                            LaunchInfo *info) {
   const uint32_t smem = Ly.total * 4;
   int dev = 0;
   DG_CUDA(cudaGetDevice(&dev));
-  int max_optin = 0, sms = 0;
-  DG_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  if (smem > (uint32_t)max_optin)
-    return fail(DG_ENOTSUP, "search state does not fit in shared memory (beam/quantizer too large)");
-  DG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int nb = 0;
-  DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, 128, smem));
+  LaunchGeometry &G = launch_geometry();
+  const void *kp = reinterpret_cast<const void *>(kernel);
+  const uint64_t key = (reinterpret_cast<uint64_t>(kp) << 8) ^ (uint64_t)dev;
+  const void *dkey = reinterpret_cast<const void *>((uintptr_t)dev + 1);
+  int sms = 0, nb = 0;
+  {
+    std::lock_guard<std::mutex> lk(G.mu);
+    auto s_it = G.sms.find(dkey);
+    if (s_it == G.sms.end()) {
+      int m = 0, o = 0;
+      DG_CUDA(cudaDeviceGetAttribute(&o, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+      DG_CUDA(cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev));
+      G.optin[dkey] = o;
+      s_it = G.sms.emplace(dkey, m).first;
+    }
+    sms = s_it->second;
+    if (smem > (uint32_t)G.optin[dkey])
+      return fail(DG_ENOTSUP, "search state does not fit in shared memory (beam/quantizer too large)");
+    int &gr = G.granted[key];
+    if ((int)smem > gr) {
+      DG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      gr = (int)smem;
+    }
+    auto &per = G.nb[key];
+    auto n_it = per.find(smem);
+    if (n_it == per.end()) {
+      int v = 0;
+      DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, 128, smem));
+      n_it = per.emplace(smem, v).first;
+    }
+    nb = n_it->second;
+  }
   if (nb <= 0) return fail(DG_ENOTSUP, "search kernel cannot be resident on an SM");
   int grid = nb * sms;
   const int need = (int)((a.nq + 3) / 4);

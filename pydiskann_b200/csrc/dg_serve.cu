@@ -47,8 +47,9 @@ struct ServeRequest {
 struct ServeSlot {
   cudaStream_t stream = nullptr;
   float *h_q = nullptr, *d_q = nullptr;
-  uint32_t *h_ids = nullptr, *d_ids = nullptr, *h_cnt = nullptr, *d_cnt = nullptr;
-  float *h_d = nullptr, *d_d = nullptr;
+  // results of a batch of nq requests with k each, in one buffer so that one
+  // copy brings them back: ids u32[nq*k] | dists f32[nq*k] | counts u32[nq]
+  uint8_t *h_out = nullptr, *d_out = nullptr;
   uint32_t *h_beam = nullptr;  // pinned: the search stages it with an async copy
   bool busy = false;
   std::vector<ServeRequest *> batch;
@@ -93,10 +94,14 @@ static void CUDART_CB slot_done(void *arg) {
     std::lock_guard<std::mutex> lk(s->mu);
     for (size_t i = 0; i < sl.batch.size(); ++i) {
       ServeRequest *r = sl.batch[i];
-      const uint32_t c = std::min(sl.h_cnt[i], r->k);
+      const size_t nk = sl.batch.size() * (size_t)sl.k;
+      const uint32_t *ids = reinterpret_cast<const uint32_t *>(sl.h_out);
+      const float *ds = reinterpret_cast<const float *>(sl.h_out + nk * 4);
+      const uint32_t *cnt = reinterpret_cast<const uint32_t *>(sl.h_out + nk * 8);
+      const uint32_t c = std::min(cnt[i], r->k);
       r->count = c;
-      r->ids.assign(sl.h_ids + i * sl.k, sl.h_ids + i * sl.k + r->k);
-      r->dists.assign(sl.h_d + i * sl.k, sl.h_d + i * sl.k + r->k);
+      r->ids.assign(ids + i * sl.k, ids + i * sl.k + r->k);
+      r->dists.assign(ds + i * sl.k, ds + i * sl.k + r->k);
       r->done_at = now;
       r->done = true;
     }
@@ -198,13 +203,15 @@ static void dispatch_loop(DgServer *s) {
       }
       p.flags = DG_FLAG_DEVICE_PTRS | DG_FLAG_STREAM;
       p.stream = sl.stream;
-      st = dg_search_batch(s->idx, &p, sl.d_q, nq, sl.d_ids, sl.d_d, sl.d_cnt, nullptr);
+      const size_t nk = (size_t)nq * head->k;
+      st = dg_search_batch(s->idx, &p, sl.d_q, nq, reinterpret_cast<uint32_t *>(sl.d_out),
+                           reinterpret_cast<float *>(sl.d_out + nk * 4),
+                           reinterpret_cast<uint32_t *>(sl.d_out + nk * 8), nullptr);
     }
     if (st == DG_OK) {
       const size_t kq = (size_t)nq * head->k;
-      if (cudaMemcpyAsync(sl.h_ids, sl.d_ids, kq * 4, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
-          cudaMemcpyAsync(sl.h_d, sl.d_d, kq * 4, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
-          cudaMemcpyAsync(sl.h_cnt, sl.d_cnt, (size_t)nq * 4, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
+      if (cudaMemcpyAsync(sl.h_out, sl.d_out, kq * 8 + (size_t)nq * 4, cudaMemcpyDeviceToHost, sl.stream) !=
+              cudaSuccess ||
           cudaLaunchHostFunc(sl.stream, slot_done, new SlotDone{s, slot}) != cudaSuccess)
         st = fail(DG_EDEVICE, "result copy failed");
     }
@@ -271,9 +278,9 @@ DgStatus dg_server_destroy(DgServer *s) {
   for (ServeSlot &sl : s->slots) {
     if (sl.stream) cudaStreamSynchronize(sl.stream);
     if (sl.stream) cudaStreamDestroy(sl.stream);
-    for (void *p : {(void *)sl.h_q, (void *)sl.h_ids, (void *)sl.h_d, (void *)sl.h_cnt, (void *)sl.h_beam})
+    for (void *p : {(void *)sl.h_q, (void *)sl.h_out, (void *)sl.h_beam})
       if (p) cudaFreeHost(p);
-    for (void *p : {(void *)sl.d_q, (void *)sl.d_ids, (void *)sl.d_d, (void *)sl.d_cnt})
+    for (void *p : {(void *)sl.d_q, (void *)sl.d_out})
       if (p) cudaFree(p);
   }
   for (auto &kv : s->live) delete kv.second;  // every submitted request not yet waited for
@@ -300,9 +307,8 @@ DgStatus dg_server_create(DgIndex *idx, const DgServerConfig *cfg, DgServer **ou
     const size_t nq = cfg->max_batch, kq = nq * cfg->max_k;
     bool ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaMallocHost(&sl.h_q, nq * idx->d * 4) == cudaSuccess && cudaMalloc(&sl.d_q, nq * idx->d * 4) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sl.h_ids, kq * 4) == cudaSuccess && cudaMalloc(&sl.d_ids, kq * 4) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sl.h_d, kq * 4) == cudaSuccess && cudaMalloc(&sl.d_d, kq * 4) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sl.h_cnt, nq * 4) == cudaSuccess && cudaMalloc(&sl.d_cnt, nq * 4) == cudaSuccess;
+    ok = ok && cudaMallocHost(&sl.h_out, kq * 8 + nq * 4) == cudaSuccess &&
+         cudaMalloc(&sl.d_out, kq * 8 + nq * 4) == cudaSuccess;
     ok = ok && cudaMallocHost(&sl.h_beam, nq * 4) == cudaSuccess;
     if (!ok) {
       dg_server_destroy(s);
