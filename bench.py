@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serve-rates", default="100000,1000000,2000000,0",
+    ap.add_argument("--serve-rates", default="100000,1000000,3000000,0",
                     help="Poisson arrival rates (req/s) for the serving loop; 0 = all requests at once")
     ap.add_argument("--serve-requests", type=int, default=200_000)
     return ap.parse_args()

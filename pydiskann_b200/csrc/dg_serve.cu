@@ -19,7 +19,6 @@
 #include <mutex>
 #include <string>
 #include <thread>
-#include <unordered_map>
 #include <vector>
 
 #include "dg_index.h"
@@ -29,7 +28,9 @@ namespace dg {
 using Clock = std::chrono::steady_clock;
 
 struct ServeRequest {
-  uint64_t ticket = 0;
+  uint64_t ticket = 0;  // (generation << 32) | slot
+  uint32_t slot = 0, gen = 1;
+  bool live = false;    // submitted and not yet waited for
   std::vector<float> query;
   uint32_t k = 10, beam = 64, rerank = 0;
   int32_t traversal = DG_TRAVERSE_F32;
@@ -66,17 +67,54 @@ struct DgServer {
   std::mutex mu;
   std::condition_variable cv_submit, cv_done, cv_slot;
   std::deque<dg::ServeRequest *> pending;
-  std::unordered_map<uint64_t, dg::ServeRequest *> live;
-  uint64_t next_ticket = 1;
   bool stop = false;
   std::thread dispatcher;
   std::atomic<uint64_t> batches{0}, served{0};
   uint32_t in_flight = 0, max_in_flight = 0;  // busy slots (under mu)
   DgStatus fatal = DG_OK;
   std::string fatal_msg;
+  // Request records, reused (with their buffers) by later requests so that no
+  // allocation happens per request once the server has warmed up; a ticket
+  // names a record slot and its generation.
+  std::mutex pool_mu;
+  std::vector<dg::ServeRequest *> recs;
+  std::vector<uint32_t> free_slots;
 };
 
 namespace dg {
+
+static ServeRequest *take_request(DgServer *s) {
+  std::lock_guard<std::mutex> lk(s->pool_mu);
+  if (!s->free_slots.empty()) {
+    ServeRequest *r = s->recs[s->free_slots.back()];
+    s->free_slots.pop_back();
+    return r;
+  }
+  ServeRequest *r = new (std::nothrow) ServeRequest();
+  if (!r) return nullptr;
+  r->slot = (uint32_t)s->recs.size();
+  s->recs.push_back(r);
+  return r;
+}
+
+static ServeRequest *record_of(DgServer *s, uint64_t ticket) {
+  const uint32_t slot = (uint32_t)ticket;
+  std::lock_guard<std::mutex> lk(s->pool_mu);
+  return slot < s->recs.size() ? s->recs[slot] : nullptr;
+}
+
+static void give_request(DgServer *s, ServeRequest *r) {
+  r->done = false;
+  r->status = DG_OK;
+  r->err.clear();
+  r->ops.clear();
+  r->pool.clear();
+  r->count = 0;
+  r->live = false;
+  ++r->gen;
+  std::lock_guard<std::mutex> lk(s->pool_mu);
+  s->free_slots.push_back(r->slot);
+}
 
 struct SlotDone {
   DgServer *s;
@@ -90,22 +128,25 @@ static void CUDART_CB slot_done(void *arg) {
   DgServer *s = sd->s;
   ServeSlot &sl = s->slots[sd->slot];
   const auto now = Clock::now();
+  // results into the requests' own buffers (sized at submission) without the
+  // lock: a waiter reads them only after seeing `done`, which is set below
+  const size_t nb = sl.batch.size(), nk = nb * (size_t)sl.k;
+  const uint32_t *ids = reinterpret_cast<const uint32_t *>(sl.h_out);
+  const float *ds = reinterpret_cast<const float *>(sl.h_out + nk * 4);
+  const uint32_t *cnt = reinterpret_cast<const uint32_t *>(sl.h_out + nk * 8);
+  for (size_t i = 0; i < nb; ++i) {
+    ServeRequest *r = sl.batch[i];
+    r->count = std::min(cnt[i], r->k);
+    std::memcpy(r->ids.data(), ids + i * sl.k, r->k * sizeof(uint32_t));
+    std::memcpy(r->dists.data(), ds + i * sl.k, r->k * sizeof(float));
+  }
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    for (size_t i = 0; i < sl.batch.size(); ++i) {
-      ServeRequest *r = sl.batch[i];
-      const size_t nk = sl.batch.size() * (size_t)sl.k;
-      const uint32_t *ids = reinterpret_cast<const uint32_t *>(sl.h_out);
-      const float *ds = reinterpret_cast<const float *>(sl.h_out + nk * 4);
-      const uint32_t *cnt = reinterpret_cast<const uint32_t *>(sl.h_out + nk * 8);
-      const uint32_t c = std::min(cnt[i], r->k);
-      r->count = c;
-      r->ids.assign(ids + i * sl.k, ids + i * sl.k + r->k);
-      r->dists.assign(ds + i * sl.k, ds + i * sl.k + r->k);
+    for (ServeRequest *r : sl.batch) {
       r->done_at = now;
       r->done = true;
     }
-    s->served += sl.batch.size();
+    s->served += nb;
     sl.batch.clear();
     sl.busy = false;
     --s->in_flight;
@@ -125,6 +166,7 @@ static bool same_class(const ServeRequest *a, const ServeRequest *b) {
 static void dispatch_loop(DgServer *s) {
   const uint32_t dim = s->idx->d;
   std::vector<uint32_t> offs;
+  std::vector<ServeRequest *> batch;
   std::vector<DgFilterOp> ops;
   std::vector<uint64_t> pool;
   cudaSetDevice(s->idx->device);
@@ -151,7 +193,7 @@ static void dispatch_loop(DgServer *s) {
     ServeSlot &sl = s->slots[slot];
     // oldest request fixes the class; take up to max_batch of that class in arrival order
     ServeRequest *head = s->pending.front();
-    std::vector<ServeRequest *> batch;
+    batch.clear();
     for (auto it = s->pending.begin(); it != s->pending.end() && batch.size() < s->cfg.max_batch;) {
       if (same_class(*it, head)) {
         batch.push_back(*it);
@@ -249,6 +291,8 @@ static DgStatus copy_request(const DgServer *s, const float *query, const DgRequ
   if (st != DG_OK) return st;
   r->query.assign(query, query + s->idx->d);
   r->k = rq->k;
+  r->ids.resize(rq->k);
+  r->dists.resize(rq->k);
   r->beam = rq->beam_width;
   r->rerank = rq->rerank_size;
   r->traversal = rq->traversal;
@@ -283,7 +327,7 @@ DgStatus dg_server_destroy(DgServer *s) {
     for (void *p : {(void *)sl.d_q, (void *)sl.d_out})
       if (p) cudaFree(p);
   }
-  for (auto &kv : s->live) delete kv.second;  // every submitted request not yet waited for
+  for (ServeRequest *r : s->recs) delete r;
   delete s;
   return DG_OK;
 }
@@ -322,22 +366,22 @@ DgStatus dg_server_create(DgIndex *idx, const DgServerConfig *cfg, DgServer **ou
 
 DgStatus dg_server_submit(DgServer *s, const float *query, const DgRequest *req, uint64_t *ticket) {
   if (!s || !ticket) return fail(DG_EINVAL, "null argument");
-  ServeRequest *r = new (std::nothrow) ServeRequest();
+  ServeRequest *r = take_request(s);
   if (!r) return fail(DG_ENOMEM, "host allocation failed");
   DgStatus st = copy_request(s, query, req, r);
   if (st != DG_OK) {
-    delete r;
+    give_request(s, r);
     return st;
   }
   r->arrival = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) {
-      delete r;
+      delete r;  // not returned to the pool: the server is going away
       return fail(DG_EINVAL, "server is shutting down");
     }
-    r->ticket = s->next_ticket++;
-    s->live[r->ticket] = r;
+    r->ticket = ((uint64_t)r->gen << 32) | r->slot;
+    r->live = true;
     s->pending.push_back(r);
     *ticket = r->ticket;
   }
@@ -348,14 +392,13 @@ DgStatus dg_server_submit(DgServer *s, const float *query, const DgRequest *req,
 DgStatus dg_server_wait(DgServer *s, uint64_t ticket, int64_t timeout_us, uint32_t *out_ids, float *out_dists,
                         uint32_t *out_count, double *latency_us) {
   if (!s) return fail(DG_EINVAL, "null server");
+  ServeRequest *r = record_of(s, ticket);
   std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->live.find(ticket);
-  if (it == s->live.end()) return fail(DG_EINVAL, "unknown ticket");
-  ServeRequest *r = it->second;
+  if (!r || !r->live || r->ticket != ticket) return fail(DG_EINVAL, "unknown ticket");
   const auto deadline = Clock::now() + std::chrono::microseconds(timeout_us < 0 ? 0 : timeout_us);
   if (!s->cv_done.wait_until(lk, deadline, [&] { return r->done; }))
     return fail(DG_ETIMEOUT, "request " + std::to_string(ticket) + " not done within the wait bound");
-  s->live.erase(it);
+  r->live = false;
   lk.unlock();
   const DgStatus st = r->status;
   if (st != DG_OK) fail(st, r->err);
@@ -366,7 +409,7 @@ DgStatus dg_server_wait(DgServer *s, uint64_t ticket, int64_t timeout_us, uint32
     if (latency_us)
       *latency_us = std::chrono::duration<double, std::micro>(r->done_at - r->arrival).count();
   }
-  delete r;
+  give_request(s, r);
   return st;
 }
 
@@ -392,18 +435,53 @@ DgStatus dg_server_run_trace(DgServer *s, const float *queries, uint32_t n, cons
     if (st != DG_OK) return fail(st, "request " + std::to_string(i) + ": " + dg_last_error());
   }
   std::vector<uint64_t> tickets(n, 0);
-  std::vector<double> lag(n, 0.0);  // submission behind schedule, added to the latency
   std::atomic<int> submit_err{0};
   const auto t0 = Clock::now();
+  auto sched = [&](uint32_t i) {
+    return t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::micro>(arrival_us[i]));
+  };
+  // Every request that is due is queued in one critical section; its arrival
+  // is its scheduled time, so latency counts any submission delay.
   std::thread producer([&] {
-    for (uint32_t i = 0; i < n; ++i) {
-      const auto at = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::micro>(arrival_us[i]));
+    std::vector<ServeRequest *> due;
+    uint32_t i = 0;
+    while (i < n) {
+      const auto at = sched(i);
       while (Clock::now() < at) {
         const auto left = at - Clock::now();
         if (left > std::chrono::microseconds(50)) std::this_thread::sleep_for(left - std::chrono::microseconds(30));
       }
-      lag[i] = std::max(0.0, std::chrono::duration<double, std::micro>(Clock::now() - at).count());
-      if (dg_server_submit(s, queries + (size_t)i * s->idx->d, &reqs[i], &tickets[i]) != DG_OK) submit_err = 1;
+      const auto now = Clock::now();
+      const uint32_t i0 = i;
+      due.clear();
+      while (i < n && sched(i) <= now && due.size() < 1024) {
+        ServeRequest *r = take_request(s);
+        if (!r || copy_request(s, queries + (size_t)i * s->idx->d, &reqs[i], r) != DG_OK) {
+          if (r) give_request(s, r);
+          for (ServeRequest *x : due) give_request(s, x);
+          submit_err = 1;
+          return;
+        }
+        r->arrival = sched(i);
+        due.push_back(r);
+        ++i;
+      }
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+          for (ServeRequest *r : due) give_request(s, r);
+          submit_err = 1;
+          return;
+        }
+        for (size_t j = 0; j < due.size(); ++j) {
+          ServeRequest *r = due[j];
+          r->ticket = ((uint64_t)r->gen << 32) | r->slot;
+          r->live = true;
+          s->pending.push_back(r);
+          tickets[i0 + j] = r->ticket;
+        }
+      }
+      s->cv_submit.notify_one();
     }
   });
   producer.join();
@@ -417,7 +495,7 @@ DgStatus dg_server_run_trace(DgServer *s, const float *queries, uint32_t n, cons
                                 out_dists ? out_dists + off : nullptr, out_counts ? out_counts + i : nullptr,
                                 latency_us + i);
     off += reqs[i].k;
-    latency_us[i] = r == DG_OK ? latency_us[i] + lag[i] : -1.0;
+    if (r != DG_OK) latency_us[i] = -1.0;
     if (r != DG_OK && st == DG_OK) st = r;
     if (r == DG_OK) last_done = std::max(last_done, arrival_us[i] + latency_us[i]);
   }
