@@ -299,3 +299,30 @@ def test_host_pipeline_matches_device_call(small_data, small_graph):
         assert np.array_equal(hd, dd.cpu().numpy())
         assert np.array_equal(hs, ds.cpu().numpy().view(np.uint32))
     g.close()
+
+
+@pytest.mark.parametrize("d", [48, 96, 200, 768])
+def test_other_dims_match_oracle(oracle, d):
+    """Dimensions that are not multiples of 128: padded rows (dpad = 32-multiple),
+    ragged 16-byte chunk assignments in the int8 tensor-core tiles (d = 96, 200
+    give 6 and 14 chunks over 4 lanes) and long rows (d = 768).  FP32, BF16 and
+    int8 + rerank, bit-identical on integer data."""
+    from pydiskann_b200 import synth
+
+    X = synth.mixture(2500, d, 24, seed=30 + d)
+    Q = synth.mixture(120, d, 24, seed=30 + d, stream=synth.STREAM_QUERY)
+    if d * 255 * 255 >= 1 << 24:  # keep every FP32 partial sum an exact integer
+        X, Q = np.floor(X / 2), np.floor(Q / 2)
+    adj, med = oracle.build_vamana(X, 24, 48, 1.2, seed=4)
+    o = oracle.OracleIndex(X, adj, med)
+    g = dg.QuantizedDiskANN(X, adj, med)
+    g.enable_bf16()
+    s, off = dg.int8_params(X)
+    g.attach_int8(s, off)
+    assert_same(g.search_arrays(Q, 10, 40, traversal=_lib.TRAVERSE_F32), o.search(Q, 10, 40))
+    # integer data is exact in BF16: the BF16 traversal (+ FP32 rerank) equals FP32
+    assert_same(g.search_arrays(Q, 10, 40, traversal=_lib.TRAVERSE_BF16, rerank_size=40), o.search(Q, 10, 40))
+    o.set_int8(s, off, oracle.int8_encode(X, s, off))
+    for L, rr in ((24, 0), (40, 40)):
+        assert_same(g.search_arrays(Q, 10, L, rerank_size=rr), o.search(Q, 10, L, rerank=rr, use_codes=True))
+    g.close()
