@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--target-recall", type=float, default=0.95)
-    ap.add_argument("--variants", default="fp32,bf16_rerank,int8_rerank,pq_rerank")
+    ap.add_argument("--variants", default="fp32,bf16_rerank,fp8_rerank,int8_rerank,pq_rerank")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
@@ -188,6 +188,7 @@ VARIANTS = {
     "fp32": ("f32", False),
     "bf16_rerank": ("bf16", True),
     "int8_rerank": ("int8", True),
+    "fp8_rerank": ("fp8", True),
     "pq_rerank": ("codes", True),
 }
 
@@ -209,7 +210,7 @@ def run_variant(idx, qidx, name, Qd, L, out=None, with_stats=False, stream=None)
 
     trav, rr = VARIANTS[name]
     t = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES,
-         "int8": _lib.TRAVERSE_CODES}[trav]
+         "int8": _lib.TRAVERSE_CODES, "fp8": _lib.TRAVERSE_FP8}[trav]
     target = qidx["pq"] if trav == "codes" else qidx["int8"] if trav == "int8" else idx
     return target.search_arrays(Qd, K, L, traversal=t, rerank_size=L if rr else 0, out=out,
                                 with_stats=with_stats, stream=stream)
@@ -217,7 +218,8 @@ def run_variant(idx, qidx, name, Qd, L, out=None, with_stats=False, stream=None)
 
 def algorithmic_bytes(name, stats, L, d=128):
     """Bytes the algorithm must read per launch: adjacency rows, distance
-    operands, rerank rows, queries and results (SURVEY 8(d) per-query terms)."""
+    operands, rerank rows, queries and results (per query E·4R + N·bytes per
+    evaluation + L·4d + 4d + 8k)."""
     E = stats[:, 0].astype(np.float64).sum()
     N = stats[:, 1].astype(np.float64).sum()
     nq = stats.shape[0]
@@ -228,6 +230,8 @@ def algorithmic_bytes(name, stats, L, d=128):
         dist, rr = N * 2 * d, nq * L * 4 * d
     elif name == "int8_rerank":
         dist, rr = N * d, nq * L * 4 * d
+    elif name == "fp8_rerank":
+        dist, rr = N * (d + 8), nq * L * 4 * d  # e4m3 row + (scale, norm)
     else:
         dist, rr = N * M, nq * L * 4 * d
     return adj + dist + rr + nq * 4 * d + nq * K * 8, {"expansions_per_query": E / nq, "dist_evals_per_query": N / nq}
@@ -265,10 +269,12 @@ def main():
     t0 = time.time()
     wanted = args.variants.split(",")
     idx, qidx = None, {}
-    if "fp32" in wanted or "bf16_rerank" in wanted:
+    if "fp32" in wanted or "bf16_rerank" in wanted or "fp8_rerank" in wanted:
         idx = dg.DiskANN.from_graph(X, adj, med, device=local)
         if "bf16_rerank" in wanted:
             idx.enable_bf16()
+        if "fp8_rerank" in wanted:
+            idx.enable_fp8()
     if "pq_rerank" in wanted:
         qidx["pq"] = dg.QuantizedDiskANN(X, adj, med, device=local)
         qidx["pq"].attach_pq(cb, codes)
@@ -346,7 +352,8 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": {"fp32": "f32", "bf16_rerank": "bf16+f32", "int8_rerank": "u8+f32"}.get(head, "u8-pq+f32"),
+        "dtype": {"fp32": "f32", "bf16_rerank": "bf16+f32", "int8_rerank": "u8+f32",
+                  "fp8_rerank": "e4m3+f32"}.get(head, "u8-pq+f32"),
         "data": "synthetic (seeded 256-centre Gaussian mixture, 1M x 128, 10k queries)",
         "config": {"workload": f"pq-1Mx128 M={M} R={R} L_build={L_BUILD} alpha={ALPHA} k={K} "
                                f"nq={args.nq} n={args.n}", "variant": head,
@@ -430,7 +437,7 @@ def serving(args, idx, qidx, name, L, Q, gt):
     trav, rr = VARIANTS[name]
     target = qidx["pq"] if trav == "codes" else qidx["int8"] if trav == "int8" else idx
     t = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES,
-         "int8": _lib.TRAVERSE_CODES}[trav]
+         "int8": _lib.TRAVERSE_CODES, "fp8": _lib.TRAVERSE_FP8}[trav]
     n = args.serve_requests
     qi = np.arange(n) % len(Q)
     Qn = Q[qi]

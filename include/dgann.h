@@ -58,7 +58,8 @@ typedef enum { DG_L2SQ = 0, DG_L2 = 1, DG_COSINE = 2, DG_DOT = 3 } DgMetric;
 typedef enum {
   DG_TRAVERSE_F32 = 0,  /* full vectors (DiskANN::distance_to, src/lib.rs:726-733) */
   DG_TRAVERSE_BF16 = 1, /* BF16 copy of the vectors, FP32 accumulate */
-  DG_TRAVERSE_CODES = 2 /* quantized codes (QuantizedDiskANN, src/quantized.rs:13-54) */
+  DG_TRAVERSE_CODES = 2, /* quantized codes (QuantizedDiskANN, src/quantized.rs:13-54) */
+  DG_TRAVERSE_FP8 = 3    /* FP8 e4m3 copy with per-vector scales, FP32 accumulate (dg_index_enable_fp8) */
 } DgTraversal;
 
 typedef enum { DG_Q_NONE = 0, DG_Q_PQ = 1, DG_Q_INT8 = 2, DG_Q_RABITQ = 3, DG_Q_F16 = 4 } DgQuantizer;
@@ -100,6 +101,13 @@ DG_API DgStatus dg_index_destroy(DgIndex *idx);
 
 /* Adds a BF16 copy of the vectors for DG_TRAVERSE_BF16 (FP32 accumulate). */
 DG_API DgStatus dg_index_enable_bf16(DgIndex *idx);
+
+/* Adds an FP8 (e4m3) copy of the vectors for DG_TRAVERSE_FP8: per vector a
+ * scale s = max|x| / 448 and codes e4m3(x / s) (round to nearest even,
+ * saturating), plus |s * e4m3(x / s)|^2.  No counterpart in the reference: a
+ * lower-precision traversal that, like BF16, is meant to be followed by the
+ * exact FP32 rerank (rerank_size). */
+DG_API DgStatus dg_index_enable_fp8(DgIndex *idx);
 
 /* QuantizedDiskANN::from_pq (src/quantized.rs:210-222): codebooks
  * [M][K][dim/M] f32, codes u8[n*M].  Pass codes = NULL to encode on the GPU
@@ -305,6 +313,10 @@ DG_API DgStatus dg_pq_train(const float *X, uint64_t n, uint32_t dim, uint32_t M
 /* ProductQuantizer::encode (src/pq.rs:122-149) on the GPU. */
 DG_API DgStatus dg_pq_encode(const float *X, uint64_t n, uint32_t dim, uint32_t M, uint32_t K,
                       const float *codebooks, int32_t device, uint8_t *out_codes);
+/* The FP8 encoding of dg_index_enable_fp8 on the GPU: codes u8[n*dim] (e4m3)
+ * and scales f32[n].  No counterpart in the reference. */
+DG_API DgStatus dg_fp8_encode(const float *X, uint64_t n, uint32_t dim, int32_t device, uint8_t *out_codes,
+                              float *out_scales);
 /* Exact k nearest neighbours (brute force, FP64 accumulation) on the GPU. */
 DG_API DgStatus dg_exact_knn(const float *X, uint64_t n, uint32_t dim, const float *Q, uint32_t nq,
                       uint32_t k, int32_t metric, int32_t device, uint32_t *out_ids,

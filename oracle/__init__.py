@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _SO = os.path.join(_HERE, "_build", "libdgoracle.so")
 
 L2SQ, L2, COSINE, DOT = 0, 1, 2, 3
-Q_NONE, Q_PQ, Q_INT8, Q_RABITQ, Q_F16 = 0, 1, 2, 3, 4
+Q_NONE, Q_PQ, Q_INT8, Q_RABITQ, Q_F16, Q_FP8 = 0, 1, 2, 3, 4, 5
 PAD = 0xFFFFFFFF
 METRICS = {"l2": L2SQ, "l2sq": L2SQ, "euclidean": L2, "cosine": COSINE, "dot": DOT}
 
@@ -60,7 +60,7 @@ class Index(C.Structure):
         ("pq_M", C.c_uint32), ("pq_K", C.c_uint32), ("pq_codebooks", C.c_void_p),
         ("int8_scale", C.c_float), ("int8_offset", C.c_float), ("rq_padded", C.c_uint32),
         ("rq_centroid", C.c_void_p), ("rq_signs", C.c_void_p), ("labels", C.c_void_p),
-        ("num_fields", C.c_uint32),
+        ("num_fields", C.c_uint32), ("fp8_scale", C.c_void_p),
     ]
 
 
@@ -103,6 +103,9 @@ def _declare(L):
         "dgo_int8_encode": (None, [vp, u64, u32, f32, f32, vp]),
         "dgo_int8_distance": (f32, [vp, vp, u32, f32]),
         "dgo_f16_encode": (None, [vp, u64, u32, vp]),
+        "dgo_fp8_encode": (None, [vp, u64, u32, vp, vp]),
+        "dgo_e4m3_encode": (C.c_uint8, [C.c_float]),
+        "dgo_e4m3_decode": (C.c_float, [C.c_uint8]),
         "dgo_f16_distance": (f32, [vp, vp, u32]),
         "dgo_rabitq_padded": (u32, [u32]),
         "dgo_rabitq_encode": (None, [vp, u64, u32, u32, vp, vp, vp]),
@@ -229,6 +232,13 @@ class OracleIndex:
         self._keep.append(codes)
         self.s.quant, self.s.codes, self.s.code_size = Q_F16, _p(codes), codes.shape[1] * 2
 
+    def set_fp8(self, codes, scales):
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        sc = _f32(scales)
+        self._keep += [codes, sc]
+        self.s.quant, self.s.codes, self.s.code_size = Q_FP8, _p(codes), codes.shape[1]
+        self.s.fp8_scale = _p(sc)
+
     def set_rabitq(self, padded, centroid, signs, codes):
         cen, sg = _f32(centroid), _f32(signs)
         codes = np.ascontiguousarray(codes, dtype=np.uint8)
@@ -312,6 +322,16 @@ def f16_encode(X):
     out = np.empty(X.shape, dtype=np.uint16)
     lib().dgo_f16_encode(_p(X), X.size // X.shape[-1], X.shape[-1], _p(out))
     return out
+
+
+def fp8_encode(X):
+    """(codes u8[n, d] e4m3, scales f32[n]) of the FP8 traversal copy."""
+    X = _f32(X)
+    n, d = X.shape
+    codes = np.empty((n, d), dtype=np.uint8)
+    scales = np.empty(n, dtype=np.float32)
+    lib().dgo_fp8_encode(_p(X), n, d, _p(codes), _p(scales))
+    return codes, scales
 
 
 def rabitq_padded(d):

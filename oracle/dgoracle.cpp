@@ -491,12 +491,53 @@ void rq_decode(const uint8_t *code, uint32_t d, uint32_t P, const float *cen, co
 }
 
 // Per-query prepared state (src/quantized.rs:57-62,167-174).
+// ---------------------------------------------------------------- FP8 e4m3
+// OCP 8-bit floating point, E4M3: bias 7, no infinities, 0x7F / 0xFF are NaN,
+// largest finite 448 (0x7E), subnormals k * 2^-9.  Positive codes 0x00..0x7E
+// are increasing in value, so encoding is a nearest search with ties to the
+// even code; anything at or above 448 saturates to 448.
+static float e4m3_value(uint32_t c) {  // c in 0..0x7E
+  const uint32_t E = c >> 3, f = c & 7u;
+  return E == 0 ? std::ldexp((float)f, -9) : std::ldexp(1.0f + (float)f / 8.0f, (int)E - 7);
+}
+uint8_t e4m3_encode(float x) {
+  if (x != x) return 0x7F;
+  const uint8_t sign = std::signbit(x) ? 0x80 : 0x00;
+  const float a = std::fabs(x);
+  if (a >= 448.0f) return sign | 0x7E;
+  uint32_t lo = 0, hi = 0x7E;  // largest code with value <= a
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) / 2;
+    if (e4m3_value(mid) <= a) lo = mid;
+    else hi = mid - 1;
+  }
+  uint32_t c = lo;
+  if (e4m3_value(c) < a) {
+    const float dl = a - e4m3_value(c), du = e4m3_value(c + 1) - a;
+    if (du < dl || (du == dl && ((c + 1) & 1u) == 0)) c = c + 1;
+  }
+  return sign | (uint8_t)c;
+}
+float e4m3_decode(uint8_t c) {
+  const float v = e4m3_value(c & 0x7Fu);
+  return (c & 0x80u) ? -v : v;
+}
+float fp8_row(const float *x, uint32_t d, uint8_t *code) {  // -> scale
+  float mx = 0.0f;
+  for (uint32_t i = 0; i < d; ++i) mx = std::fmax(mx, std::fabs(x[i]));
+  const float s = mx > 0.0f ? mx / 448.0f : 1.0f;
+  for (uint32_t i = 0; i < d; ++i) code[i] = e4m3_encode(x[i] / s);
+  return s;
+}
+
 struct Prepared {
   std::vector<float> lut;
   std::vector<uint8_t> u8;
   std::vector<uint16_t> h;
   std::vector<uint64_t> planes;
   float k5[5];
+  std::vector<float> fhi, flo;  // FP8: e4m3 values of the scaled query q' and of 16 (q' - hi)
+  float fs = 1.0f, fqq = 0.0f;  // FP8: query scale, |q|^2
 };
 
 void prepare(const DgoIndex &I, const float *q, Prepared &p) {
@@ -515,6 +556,23 @@ void prepare(const DgoIndex &I, const float *q, Prepared &p) {
       p.h.resize(I.d);
       for (uint32_t i = 0; i < I.d; ++i) p.h[i] = f32_to_f16(q[i]);
       break;
+    case DGO_Q_FP8: {
+      float mx = 0.0f, qq = 0.0f;
+      for (uint32_t i = 0; i < I.d; ++i) {
+        mx = std::fmax(mx, std::fabs(q[i]));
+        qq += q[i] * q[i];
+      }
+      p.fs = mx > 0.0f ? mx / 448.0f : 1.0f;
+      p.fqq = qq;
+      p.fhi.resize(I.d);
+      p.flo.resize(I.d);
+      for (uint32_t i = 0; i < I.d; ++i) {
+        const float v = q[i] / p.fs;
+        p.fhi[i] = e4m3_decode(e4m3_encode(v));
+        p.flo[i] = e4m3_decode(e4m3_encode((v - p.fhi[i]) * 16.0f));
+      }
+      break;
+    }
     case DGO_Q_RABITQ:
       p.planes.resize(4 * (I.rq_padded / 64));
       rq_query(q, I.d, I.rq_padded, I.rq_centroid, I.rq_signs, p.planes.data(), p.k5);
@@ -527,6 +585,31 @@ void prepare(const DgoIndex &I, const float *q, Prepared &p) {
 float quantized_distance(const DgoIndex &I, const float *q, uint32_t id, const Prepared &p,
                          std::vector<float> &scratch) {
   const uint8_t *code = I.codes + (uint64_t)id * I.code_size;
+  if (I.quant == DGO_Q_FP8) {
+    // x = s_x e, q = s_q q': q.x = s_x s_q (e.hi + e.lo / 16), contracted as
+    // |q|^2 + |x|^2 - 2 q.x for L2 (FP32 sums in coordinate order)
+    const float sx = I.fp8_scale[id];
+    float ch = 0.0f, cl = 0.0f, xx = 0.0f;
+    for (uint32_t i = 0; i < I.d; ++i) {
+      const float e = e4m3_decode(code[i]);
+      ch += e * p.fhi[i];
+      cl += e * p.flo[i];
+      const float xv = sx * e;
+      xx += xv * xv;
+    }
+    const float dot = sx * p.fs * (ch + cl * 0.0625f);
+    switch (I.metric) {
+      case DGO_L2SQ: return std::fmax(p.fqq + xx - 2.0f * dot, 0.0f);
+      case DGO_L2: return std::sqrt(std::fmax(p.fqq + xx - 2.0f * dot, 0.0f));
+      case DGO_DOT: return 1.0f - dot;
+      default: {
+        if (p.fqq == 0.0f && xx == 0.0f) return 0.0f;
+        if (dot == 0.0f) return 1.0f;
+        const float r = 1.0f - dot / (std::sqrt(p.fqq) * std::sqrt(xx));
+        return r > 0.0f ? r : 0.0f;
+      }
+    }
+  }
   if (I.metric != DGO_L2SQ && I.metric != DGO_L2) {
     scratch.resize(I.d);
     switch (I.quant) {
@@ -861,6 +944,13 @@ void dgo_f16_encode(const float *X, uint64_t n, uint32_t d, uint16_t *codes) {
   for (uint64_t i = 0; i < n * d; ++i) codes[i] = f32_to_f16(X[i]);
 }
 float dgo_f16_distance(const uint16_t *q, const uint16_t *c, uint32_t d) { return f16_dist(q, c, d); }
+uint8_t dgo_e4m3_encode(float x) { return e4m3_encode(x); }
+float dgo_e4m3_decode(uint8_t c) { return e4m3_decode(c); }
+void dgo_fp8_encode(const float *X, uint64_t n, uint32_t d, uint8_t *codes, float *scales) {
+#pragma omp parallel for schedule(static)
+  for (int64_t r = 0; r < (int64_t)n; ++r) scales[r] = fp8_row(X + r * d, d, codes + r * d);
+}
+
 
 uint32_t dgo_rabitq_padded(uint32_t d) {  // src/rabitq.rs:83
   uint32_t p = 1;

@@ -30,7 +30,7 @@ extern "C" {
 #endif
 
 enum { DGO_L2SQ = 0, DGO_L2 = 1, DGO_COSINE = 2, DGO_DOT = 3 };
-enum { DGO_Q_NONE = 0, DGO_Q_PQ = 1, DGO_Q_INT8 = 2, DGO_Q_RABITQ = 3, DGO_Q_F16 = 4 };
+enum { DGO_Q_NONE = 0, DGO_Q_PQ = 1, DGO_Q_INT8 = 2, DGO_Q_RABITQ = 3, DGO_Q_F16 = 4, DGO_Q_FP8 = 5 };
 enum {
   DGO_F_TRUE = 0, DGO_F_EQ = 1, DGO_F_IN = 2, DGO_F_LT = 3, DGO_F_GT = 4,
   DGO_F_RANGE = 5, DGO_F_AND = 6, DGO_F_OR = 7
@@ -64,6 +64,7 @@ typedef struct {
   const float *rq_signs;    /* 3*padded */
   const uint64_t *labels;   /* n*num_fields */
   uint32_t num_fields;
+  const float *fp8_scale;   /* n: per-vector scale of DGO_Q_FP8 codes (e4m3, code_size = d) */
 } DgoIndex;
 
 typedef struct {
@@ -121,6 +122,13 @@ void dgo_int8_encode(const float *X, uint64_t n, uint32_t d, float scale, float 
 float dgo_int8_distance(const uint8_t *q, const uint8_t *c, uint32_t d, float scale);
 void dgo_f16_encode(const float *X, uint64_t n, uint32_t d, uint16_t *codes);
 float dgo_f16_distance(const uint16_t *q, const uint16_t *c, uint32_t d);
+
+/* ---- FP8 e4m3 with per-vector scales (the product's FP8 traversal; no
+ *      counterpart in the reference): s = max|x| / 448, codes e4m3(x / s)
+ *      rounded to nearest even, saturating (OCP 8-bit floating point E4M3) ---- */
+uint8_t dgo_e4m3_encode(float x);
+float dgo_e4m3_decode(uint8_t c);
+void dgo_fp8_encode(const float *X, uint64_t n, uint32_t d, uint8_t *codes, float *scales);
 
 /* ---- RaBitQ (src/rabitq.rs:31-256) ---- */
 uint32_t dgo_rabitq_padded(uint32_t d);

@@ -95,6 +95,16 @@ def pq_encode(vectors, codebooks, device=0) -> np.ndarray:
     return codes
 
 
+def fp8_encode(vectors, device=0):
+    """(codes u8[n, d] e4m3, scales f32[n]) as the FP8 traversal stores them."""
+    X = _f32(vectors)
+    n, d = X.shape
+    codes = np.empty((n, d), dtype=np.uint8)
+    scales = np.empty(n, dtype=np.float32)
+    check(lib().dg_fp8_encode(ptr(X), n, d, device, ptr(codes), ptr(scales)))
+    return codes, scales
+
+
 def exact_knn(vectors, queries, k=10, metric="l2", device=0):
     """Brute-force k nearest neighbours (FP64 accumulation) -> (ids, dists)."""
     X = _f32(vectors)
@@ -287,6 +297,13 @@ class _Index:
         if not self._bf16:
             check(lib().dg_index_enable_bf16(self._h))
             self._bf16 = True
+
+    def enable_fp8(self):
+        """FP8 (e4m3, per-vector scales) copy for ``traversal=TRAVERSE_FP8``; follow
+        it with an FP32 rerank (``rerank_size``).  No counterpart in the reference."""
+        if not getattr(self, "_fp8", False):
+            check(lib().dg_index_enable_fp8(self._h))
+            self._fp8 = True
 
     # -- the batched entry point
     def search_arrays(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32,

@@ -16,7 +16,7 @@ LIB_PATH = os.environ.get("DGANN_LIBRARY", os.path.join(HERE, "libdgann.so"))
 
 DG_OK, DG_EINVAL, DG_ENOMEM, DG_ETIMEOUT, DG_EDEVICE, DG_ENOTSUP = range(6)
 L2SQ, L2, COSINE, DOT = 0, 1, 2, 3
-TRAVERSE_F32, TRAVERSE_BF16, TRAVERSE_CODES = 0, 1, 2
+TRAVERSE_F32, TRAVERSE_BF16, TRAVERSE_CODES, TRAVERSE_FP8 = 0, 1, 2, 3
 Q_NONE, Q_PQ, Q_INT8, Q_RABITQ, Q_F16 = 0, 1, 2, 3, 4
 F_TRUE, F_EQ, F_IN, F_LT, F_GT, F_RANGE, F_AND, F_OR = range(8)
 FLAG_DEVICE_PTRS = 1
@@ -89,6 +89,7 @@ def _signatures():
         "dg_index_create": (st, [vp, vp]),
         "dg_index_destroy": (st, [vp]),
         "dg_index_enable_bf16": (st, [vp]),
+        "dg_index_enable_fp8": (st, [vp]),
         "dg_index_attach_pq": (st, [vp, u32, u32, vp, vp]),
         "dg_index_attach_int8": (st, [vp, f32, f32, vp]),
         "dg_index_attach_f16": (st, [vp]),
@@ -113,6 +114,7 @@ def _signatures():
         "dg_build_vamana": (st, [vp, u64, u32, i32, u32, u32, f32, u64, u32, i32, vp]),
         "dg_pq_train": (st, [vp, u64, u32, u32, u32, u32, u64, u64, i32, vp]),
         "dg_pq_encode": (st, [vp, u64, u32, u32, u32, vp, i32, vp]),
+        "dg_fp8_encode": (st, [vp, u64, u32, i32, vp, vp]),
         "dg_exact_knn": (st, [vp, u64, u32, vp, u32, u32, i32, i32, vp, vp]),
         "dg_last_error": (C.c_char_p, []),
         "dg_version": (i32, []),

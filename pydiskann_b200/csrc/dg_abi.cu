@@ -176,6 +176,20 @@ DgStatus dg_index_enable_bf16(DgIndex *idx) {
   return DG_OK;
 }
 
+DgStatus dg_index_enable_fp8(DgIndex *idx) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  if (idx->fp8) return DG_OK;
+  DgStatus s = dev_alloc(idx, (void **)&idx->fp8, idx->n * idx->dpad);
+  if (s != DG_OK) return s;
+  if ((s = dev_alloc(idx, (void **)&idx->fp8_sn, idx->n * sizeof(float2))) != DG_OK) return s;
+  if ((s = encode_fp8_device(idx->vec, idx->n, idx->d, idx->dpad, idx->fp8, idx->fp8_sn, idx->stream)) != DG_OK)
+    return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
 static DgStatus attach_codes_common(DgIndex *idx, int quant, uint32_t code_size) {
   if (idx->quant != DG_Q_NONE) return fail(DG_EINVAL, "a quantizer is already attached");
   idx->quant = quant;
@@ -377,6 +391,10 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
       if (!idx->bf16) return fail(DG_EINVAL, "BF16 traversal needs dg_index_enable_bf16");
       trav = TRAV_BF16;
       break;
+    case DG_TRAVERSE_FP8:
+      if (!idx->fp8) return fail(DG_EINVAL, "FP8 traversal needs dg_index_enable_fp8");
+      trav = TRAV_FP8;
+      break;
     case DG_TRAVERSE_CODES:
       switch (idx->quant) {
         case DG_Q_PQ: trav = TRAV_PQ; break;
@@ -458,6 +476,8 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   a.i8_scale = idx->i8_scale;
   a.i8_offset = idx->i8_offset;
   a.i8_norm = idx->i8_norm;
+  a.vec_fp8 = idx->fp8;
+  a.fp8_sn = idx->fp8_sn;
   a.rq_padded = idx->rq_padded;
   a.rq_centroid = idx->rq_centroid;
   a.rq_signs = idx->rq_signs;
@@ -530,6 +550,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
       case TRAV_F16: return launch_search_f16(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
       case TRAV_INT8: return launch_search_int8(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
       case TRAV_PQ: return launch_search_pq(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+      case TRAV_FP8: return launch_search_fp8(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
       default: return launch_search_rabitq(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
     }
   };
@@ -678,6 +699,10 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
       if (!idx->bf16) return fail(DG_EINVAL, "BF16 traversal needs dg_index_enable_bf16");
       trav = TRAV_BF16;
       break;
+    case DG_TRAVERSE_FP8:
+      if (!idx->fp8) return fail(DG_EINVAL, "FP8 traversal needs dg_index_enable_fp8");
+      trav = TRAV_FP8;
+      break;
     case DG_TRAVERSE_CODES:
       switch (idx->quant) {
         case DG_Q_PQ: trav = TRAV_PQ; break;
@@ -767,6 +792,8 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   a.i8_scale = idx->i8_scale;
   a.i8_offset = idx->i8_offset;
   a.i8_norm = idx->i8_norm;
+  a.vec_fp8 = idx->fp8;
+  a.fp8_sn = idx->fp8_sn;
   a.rq_padded = idx->rq_padded;
   a.rq_centroid = idx->rq_centroid;
   a.rq_signs = idx->rq_signs;
@@ -820,6 +847,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
     case TRAV_F16: return launch_search_f16(a, Ly, met, lpr, lcap, any_filter, st, &info);
     case TRAV_INT8: return launch_search_int8(a, Ly, met, lpr, lcap, any_filter, st, &info);
     case TRAV_PQ: return launch_search_pq(a, Ly, met, lpr, lcap, any_filter, st, &info);
+    case TRAV_FP8: return launch_search_fp8(a, Ly, met, lpr, lcap, any_filter, st, &info);
     default: return launch_search_rabitq(a, Ly, met, lpr, lcap, any_filter, st, &info);
   }
 }

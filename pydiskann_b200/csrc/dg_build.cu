@@ -30,6 +30,26 @@ __global__ void k_int8(const float *v, uint64_t n, uint32_t d, uint32_t dpad, fl
     out[i] = c < d ? int8_code(v[r * dpad + c], inv, beta) : 0;
   }
 }
+// FP8 rows: per vector s = max|x| / 448 (1 for a zero vector), codes
+// e4m3(x / s) rounded to nearest even with saturation, and |s * e4m3(x / s)|^2
+// summed in coordinate order.  One thread per vector.
+__global__ void k_fp8(const float *v, uint64_t n, uint32_t d, uint32_t dpad, uint8_t *codes, float2 *sn) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+    const float *x = v + r * dpad;
+    float mx = 0.0f;
+    for (uint32_t i = 0; i < d; ++i) mx = fmaxf(mx, fabsf(x[i]));
+    const float s = mx > 0.0f ? __fdiv_rn(mx, 448.0f) : 1.0f;
+    uint8_t *c = codes + r * dpad;
+    float nn = 0.0f;
+    for (uint32_t i = 0; i < dpad; ++i) {
+      const __nv_fp8_storage_t e = i < d ? __nv_cvt_float_to_fp8(__fdiv_rn(x[i], s), __NV_SATFINITE, __NV_E4M3) : 0;
+      c[i] = e;
+      const float xv = __fmul_rn(s, __half2float(__half(__nv_cvt_fp8_to_halfraw(e, __NV_E4M3))));
+      nn = __fadd_rn(nn, __fmul_rn(xv, xv));
+    }
+    sn[r] = make_float2(s, nn);
+  }
+}
 // Sum of squared codes of every int8 row (padding bytes are zero).
 __global__ void k_int8_norm(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
@@ -216,6 +236,12 @@ DgStatus encode_int8_device(const float *vec, uint64_t n, uint32_t d, uint32_t d
   const float inv = 1.0f / scale;  // same f32 expressions as Int8Quantizer::encode
   const float beta = -offset / scale;
   k_int8<<<grid_for(n * stride, 256), 256, 0, st>>>(vec, n, d, dpad, inv, beta, codes, stride);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+DgStatus encode_fp8_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint8_t *codes,
+                           float2 *sn, cudaStream_t st) {
+  k_fp8<<<grid_for(n, 128), 128, 0, st>>>(vec, n, d, dpad, codes, sn);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
@@ -534,6 +560,37 @@ DgStatus dg_medoid(const float *X, uint64_t n, uint32_t dim, int32_t metric, int
   if (s == DG_OK) s = upload_rows_f32(X, n, dim, dpad, v, st);
   if (s == DG_OK) s = medoid_device(v, n, dim, dpad, metric, out_medoid, st);
   if (v) cudaFreeAsync(v, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return s;
+}
+
+DgStatus dg_fp8_encode(const float *X, uint64_t n, uint32_t dim, int32_t device, uint8_t *out_codes,
+                       float *out_scales) {
+  if (!X || !out_codes || !out_scales) return fail(DG_EINVAL, "null argument");
+  if (n == 0 || dim == 0) return DG_OK;
+  DG_CUDA(cudaSetDevice(device));
+  const uint32_t dpad = dpad_of(dim);
+  cudaStream_t st;
+  DG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  float *v = nullptr;
+  uint8_t *codes = nullptr;
+  float2 *sn = nullptr;
+  DgStatus s = DG_OK;
+  if (cudaMallocAsync(&v, n * dpad * 4, st) != cudaSuccess || cudaMallocAsync(&codes, n * dpad, st) != cudaSuccess ||
+      cudaMallocAsync(&sn, n * sizeof(float2), st) != cudaSuccess)
+    s = fail(DG_ENOMEM, "fp8 encode staging");
+  if (s == DG_OK) s = upload_rows_f32(X, n, dim, dpad, v, st);
+  if (s == DG_OK) s = encode_fp8_device(v, n, dim, dpad, codes, sn, st);
+  if (s == DG_OK && cudaMemcpy2DAsync(out_codes, dim, codes, dpad, dim, n, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    s = fail(DG_EDEVICE, "code download");
+  if (s == DG_OK && cudaMemcpy2DAsync(out_scales, 4, sn, sizeof(float2), 4, n, cudaMemcpyDeviceToHost, st) !=
+                        cudaSuccess)
+    s = fail(DG_EDEVICE, "scale download");
+  cudaStreamSynchronize(st);
+  if (v) cudaFreeAsync(v, st);
+  if (codes) cudaFreeAsync(codes, st);
+  if (sn) cudaFreeAsync(sn, st);
   cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
   return s;

@@ -15,6 +15,8 @@ struct DgIndex {
   // HBM layout: every row starts on a 128-byte boundary when dpad*4 >= 128.
   float *vec = nullptr;       // [n][dpad] f32, zero padded
   uint16_t *bf16 = nullptr;   // [n][dpad] bf16 copy (optional)
+  uint8_t *fp8 = nullptr;     // [n][dpad] e4m3 copy (optional)
+  float2 *fp8_sn = nullptr;   // [n] (scale, |decoded|^2) of the e4m3 rows
   uint32_t *adj = nullptr;    // [n][R]
   int32_t quant = DG_Q_NONE;
   uint8_t *codes = nullptr;   // [n][code_stride]
@@ -78,6 +80,9 @@ DgStatus encode_bf16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_
 DgStatus encode_rabitq_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint32_t P,
                               const float *centroid, const float *signs, uint8_t *codes,
                               uint32_t stride, cudaStream_t st);
+// e4m3 rows with per-vector scales (and decoded squared norms) from f32 rows.
+DgStatus encode_fp8_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint8_t *codes,
+                           float2 *sn, cudaStream_t st);
 // Sum of squared codes per vector for int8 codes.
 DgStatus int8_norms_device(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, cudaStream_t st);
 // |decode(code)|^2 per vector for PQ / RaBitQ codes (the cosine metric's |x|^2).

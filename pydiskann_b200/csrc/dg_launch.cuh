@@ -125,5 +125,7 @@ DgStatus launch_search_pq(const SearchArgs &a, const WarpLayout &Ly, int met, in
                           bool filt, cudaStream_t st, LaunchInfo *info);
 DgStatus launch_search_rabitq(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
                               bool filt, cudaStream_t st, LaunchInfo *info);
+DgStatus launch_search_fp8(const SearchArgs &a, const WarpLayout &Ly, int met, int lpr, int lcap,
+                           bool filt, cudaStream_t st, LaunchInfo *info);
 
 }  // namespace dg

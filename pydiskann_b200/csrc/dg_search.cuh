@@ -44,6 +44,8 @@ struct SearchArgs {
   const float *pq_cb;     // [M][K][ds]
   float i8_scale, i8_offset;
   const uint32_t *i8_norm;  // [n] sum of squared codes (int8 L2 on tensor cores)
+  const uint8_t *vec_fp8;   // [n][dpad] e4m3 rows (FP8 traversal)
+  const float2 *fp8_sn;     // [n] (scale, |decoded|^2)
   uint32_t rq_padded;
   const float *rq_centroid;  // [d]
   const float *rq_signs;     // [3][padded]
@@ -69,7 +71,7 @@ struct SearchArgs {
   uint32_t *counter;  // work counter, zero at launch
 };
 
-enum TravKind { TRAV_F32 = 0, TRAV_BF16 = 1, TRAV_PQ = 2, TRAV_INT8 = 3, TRAV_RABITQ = 4, TRAV_F16 = 5 };
+enum TravKind { TRAV_F32 = 0, TRAV_BF16 = 1, TRAV_PQ = 2, TRAV_INT8 = 3, TRAV_RABITQ = 4, TRAV_F16 = 5, TRAV_FP8 = 6 };
 enum MetKind { MET_L2 = 0, MET_DOT = 1, MET_COS = 2 };
 
 constexpr int kStageCap = 256;  // max adjacency degree
@@ -99,6 +101,7 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
   else if (trav == TRAV_RABITQ && decode) p = 16 + rq_padded * 4 + rq_padded * 16;
   else if (trav == TRAV_RABITQ) p = 4 * (rq_padded / 64) * 8 + 32 + align16(rq_padded * 4);
   else if (trav == TRAV_F16) p = align16(dpad * 4);
+  else if (trav == TRAV_FP8) p = 2 * dpad + 16;  // query hi / lo e4m3 codes, then (scale, |q|^2)
   o += align16(p);
   L.aux = o;  // 64-key copy of the register-resident working list (beams <= 64)
   o += lcap == 64 && !filt ? 64 * 8 : 0;
@@ -487,6 +490,67 @@ __device__ __forceinline__ uint32_t int8_l2_mma(const uint8_t *__restrict__ code
   const int d10 = __shfl_sync(kFull, c1[0], src), d11 = __shfl_sync(kFull, c1[2], src);
   const int dot = T == 0 ? (r < 8 ? d00 : d01) : (r < 8 ? d10 : d11);
   return qn + xn - 2u * (uint32_t)dot;
+}
+
+// One warp-wide e4m3 x e4m3 -> f32 tensor-core step (16 rows x 32 dims x 8 columns).
+__device__ __forceinline__ void mma_e4m3_16x8x32(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                                 uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k32.row.col.f32.e4m3.e4m3.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// e.q for up to 32 candidate e4m3 rows e on the tensor cores (FP32
+// accumulate), in the tile and lane layout of int8_l2_mma.  The query enters
+// as two e4m3 columns, hi = e4m3(q') and lo = e4m3(16 (q' - hi)) of the scaled
+// query q', so the result is (e.hi + e.lo / 16) for lane j's candidate.
+// qhl: hi[dpad] then lo[dpad].
+__device__ __forceinline__ float fp8_dot_mma(const uint8_t *__restrict__ rows, uint32_t dpad, const uint8_t *qhl,
+                                             uint32_t cand, int cnt, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int nch = (int)(dpad >> 4);
+  const int J = (nch + 3) >> 2;
+  const uint32_t id0 = __shfl_sync(kFull, cand, 0);
+  const bool two = cnt > 16;
+  const uint4 *rp[4];
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const int row = g + 8 * h;
+    uint32_t id = __shfl_sync(kFull, cand, row);
+    id = row < cnt ? id : id0;
+    rp[h] = reinterpret_cast<const uint4 *>(rows + (size_t)id * dpad);
+  }
+  // column g of B: the hi codes (g = 0), the lo codes (g = 1), zero otherwise
+  const uint4 *pq = reinterpret_cast<const uint4 *>(qhl + (g == 1 ? dpad : 0));
+  float c0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, c1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  for (int j0 = 0; j0 < J; j0 += 2) {
+    uint4 x[2][4], qv[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int ch = t + 4 * (j0 + u);
+      const bool ok = j0 + u < J && ch < nch;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) x[u][h] = (ok && (h < 2 || two)) ? __ldg(rp[h] + ch) : z;
+      qv[u] = (ok && g < 2) ? pq[ch] : z;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      mma_e4m3_16x8x32(c0, x[u][0].x, x[u][1].x, x[u][0].y, x[u][1].y, qv[u].x, qv[u].y);
+      mma_e4m3_16x8x32(c0, x[u][0].z, x[u][1].z, x[u][0].w, x[u][1].w, qv[u].z, qv[u].w);
+      if (two) {
+        mma_e4m3_16x8x32(c1, x[u][2].x, x[u][3].x, x[u][2].y, x[u][3].y, qv[u].x, qv[u].y);
+        mma_e4m3_16x8x32(c1, x[u][2].z, x[u][3].z, x[u][2].w, x[u][3].w, qv[u].z, qv[u].w);
+      }
+    }
+  }
+  // lane 4g: c[0] / c[2] = e.hi of rows g, g+8; c[1] / c[3] = e.lo
+  const int T = lane >> 4, r = lane & 15, src = (r & 7) << 2;
+  const float d00 = __shfl_sync(kFull, fmaf(c0[1], 0.0625f, c0[0]), src);
+  const float d01 = __shfl_sync(kFull, fmaf(c0[3], 0.0625f, c0[2]), src);
+  const float d10 = __shfl_sync(kFull, fmaf(c1[1], 0.0625f, c1[0]), src);
+  const float d11 = __shfl_sync(kFull, fmaf(c1[3], 0.0625f, c1[2]), src);
+  return T == 0 ? (r < 8 ? d00 : d01) : (r < 8 ? d10 : d11);
 }
 
 // int8 codes decoded for non-L2 metrics (src/quantized.rs:28-36): c*scale+offset.

@@ -35,6 +35,14 @@ __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *ws
   if (TRAV == TRAV_F32) {
     return rows_distance<LPR, 0, MET>(reinterpret_cast<const uint8_t *>(a.vec_f32), a.dpad * 4,
                                       (a.dpad / 4) / LPR, qs, cand, cnt, lane, sqrt_l2, qq);
+  } else if (TRAV == TRAV_FP8) {
+    // x = s_x e, q = s_q q': q.x = s_x s_q (e.q'); |q - x|^2 = |q|^2 + |x|^2 - 2 q.x
+    const uint8_t *qhl = wsm + Ly.prov;
+    const float2 qs2 = *reinterpret_cast<const float2 *>(wsm + Ly.prov + 2 * a.dpad);  // (s_q, |q|^2)
+    const float2 sn = lane < cnt ? __ldg(a.fp8_sn + cand) : make_float2(0.0f, 0.0f);
+    const float dot = sn.x * qs2.x * fp8_dot_mma(a.vec_fp8, a.dpad, qhl, cand, cnt, lane);
+    if (MET == MET_L2) return finish_metric(MET, sqrt_l2, fmaxf(qs2.y + sn.y - 2.0f * dot, 0.0f), 0.0f, qq);
+    return finish_metric(MET, false, dot, sn.y, qq);
   } else if (TRAV == TRAV_BF16) {
     return rows_distance<LPR, 1, MET>(reinterpret_cast<const uint8_t *>(a.vec_bf16), a.dpad * 2,
                                       (a.dpad / 8) / LPR, qs, cand, cnt, lane, sqrt_l2, qq);
@@ -105,6 +113,28 @@ __device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm,
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) qn += __shfl_xor_sync(kFull, qn, o);
     if (lane == 0) *reinterpret_cast<uint32_t *>(qc8 + align16(a.dpad)) = qn;
+  } else if (TRAV == TRAV_FP8) {
+    // scaled query q' = q / s_q (s_q = max|q| / 448) as two e4m3 columns
+    uint8_t *hi = wsm + Ly.prov, *lo = hi + a.dpad;
+    float mx = 0.0f, qn = 0.0f;
+    for (uint32_t i = lane; i < a.dpad; i += 32) {
+      mx = fmaxf(mx, fabsf(qs[i]));
+      qn = fmaf(qs[i], qs[i], qn);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+      qn += __shfl_xor_sync(kFull, qn, o);
+    }
+    const float sq = mx > 0.0f ? __fdiv_rn(mx, 448.0f) : 1.0f;
+    for (uint32_t i = lane; i < a.dpad; i += 32) {
+      const float v = __fdiv_rn(qs[i], sq);
+      const __nv_fp8_storage_t h = __nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+      const float hv = __half2float(__half(__nv_cvt_fp8_to_halfraw(h, __NV_E4M3)));
+      hi[i] = h;
+      lo[i] = __nv_cvt_float_to_fp8(__fmul_rn(__fsub_rn(v, hv), 16.0f), __NV_SATFINITE, __NV_E4M3);
+    }
+    if (lane == 0) *reinterpret_cast<float2 *>(wsm + Ly.prov + 2 * a.dpad) = make_float2(sq, qn);
   } else if (TRAV == TRAV_F16) {
     float *qh = reinterpret_cast<float *>(wsm + Ly.prov);
     for (uint32_t i = lane; i < a.dpad; i += 32) qh[i] = __half2float(__float2half_rn(qs[i]));

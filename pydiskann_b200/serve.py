@@ -17,7 +17,8 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib, ptr
 
-_TRAV = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES}
+_TRAV = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES,
+         "fp8": _lib.TRAVERSE_FP8}
 
 # DgRequest as a numpy record (u32 k, beam, rerank; i32 traversal; ops pointer,
 # u32 nops; pool pointer, u32 pool_len), so a trace of 10^5 requests is built

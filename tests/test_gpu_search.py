@@ -326,3 +326,48 @@ def test_other_dims_match_oracle(oracle, d):
     for L, rr in ((24, 0), (40, 40)):
         assert_same(g.search_arrays(Q, 10, L, rerank_size=rr), o.search(Q, 10, L, rerank=rr, use_codes=True))
     g.close()
+
+
+@pytest.mark.parametrize("metric", ["l2", "cosine"])
+def test_fp8_traversal_within_tolerance(oracle, metric):
+    """FP8 traversal (no counterpart in the reference): codes equal the oracle's
+    restatement of e4m3 round-to-nearest-even with saturation bit for bit; the
+    tensor cores accumulate e . q' in their own order, so traversal distances
+    agree within 1e-5 (|q|^2 + |x|^2) and ids except near-ties; after the FP32
+    rerank, distances of common ids are exact."""
+    from pydiskann_b200 import synth
+
+    if metric == "l2":
+        X = synth.mixture(3000, 128, 24, seed=41)
+        Q = synth.mixture(150, 128, 24, seed=41, stream=synth.STREAM_QUERY)
+        om = oracle.L2SQ
+    else:
+        X, Q = synth.cosine(3000, 150, 96, seed=42)
+        om = oracle.COSINE
+    gc, gs = dg.fp8_encode(X)
+    oc, osc = oracle.fp8_encode(X)
+    assert np.array_equal(gc, oc) and np.array_equal(gs, osc)
+    adj, med = oracle.build_vamana(X, 24, 48, 1.2, seed=5, metric=om)
+    g = dg.DiskANN.from_graph(X, adj, med, metric=metric)
+    g.enable_fp8()
+    o = oracle.OracleIndex(X, adj, med, om)
+    o.set_fp8(oc, osc)
+    gi, gd, gn = g.search_arrays(Q, 10, 48, traversal=_lib.TRAVERSE_FP8)
+    oi, od, on = o.search(Q, 10, 48, use_codes=True)
+    assert np.array_equal(gn, on)
+    same = np.mean([len(set(gi[i]) & set(oi[i])) / 10 for i in range(len(Q))])
+    assert same >= 0.97, same
+    qn = (Q.astype(np.float64) ** 2).sum(1)
+    for i in range(len(Q)):
+        for j in range(10):
+            if gi[i, j] == oi[i, j]:
+                xn = float((X[gi[i, j]].astype(np.float64) ** 2).sum())
+                tol = 1e-5 * (qn[i] + xn) if metric == "l2" else 2e-5
+                assert abs(float(gd[i, j]) - float(od[i, j])) <= tol, (i, j, gd[i, j], od[i, j])
+    # with the FP32 rerank of the working set: exact distances, recall near FP32's
+    ri, rd, rn = g.search_arrays(Q, 10, 48, traversal=_lib.TRAVERSE_FP8, rerank_size=48)
+    fi, fd, fn = g.search_arrays(Q, 10, 48, traversal=_lib.TRAVERSE_F32)
+    m = ri == fi
+    assert np.array_equal(rd[m], fd[m])
+    assert np.mean(m) >= 0.9
+    g.close()
