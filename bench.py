@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--serve-rates", default="100000,1000000,3000000,0",
                     help="Poisson arrival rates (req/s) for the serving loop; 0 = all requests at once")
     ap.add_argument("--serve-requests", type=int, default=200_000)
+    ap.add_argument("--no-filtered", action="store_true")
+    ap.add_argument("--filtered-queries", type=int, default=5000)
     return ap.parse_args()
 
 
@@ -384,6 +386,8 @@ def main():
                 line["p99_load_rps"] = loaded[-1]["offered_rps"]
         if "fp32" in results:
             line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
+        if not args.no_filtered:
+            line["filtered"] = filtered(args, X, Q, adj, med, dev, dist)
     if rank == 0 and head and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, X, Q, adj, med, (cb, codes), head, results[head]["L"])
     if rank == 0:
@@ -425,6 +429,83 @@ def e2e(args, idx, qidx, name, L, Q, gt, dist, world, dev):
     return {"value": world * args.nq * args.steps / (ms / 1e3), "unit": "queries/s",
             "h2d_bytes_per_step": int(Q.nbytes), "d2h_bytes_per_step": int(args.nq * (K * 8 + 4)),
             "recall_at_10": round(rec, 4)}
+
+
+def filtered(args, X, Q, adj, med, dev, dist):
+    """Label-filtered search on the same graph (the reference has no
+    filter-aware build): every vector carries 1-3 of 100 labels drawn Zipf(1.0);
+    query i asks Or(Eq(0, l), Eq(1, l), Eq(2, l)) for a uniform label l, so the
+    selectivity spans ~0.5 % to ~35 %.  Ground truth: exact kNN inside each
+    label's subset.  For FP32 and int8 + FP32 rerank: the smallest L reaching
+    recall@10 >= the target, and the device-timed QPS at it."""
+    import torch
+
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import _lib, synth
+
+    t0 = time.time()
+    labels = synth.label_sets(len(X), seed=args.seed)
+    nqf = min(args.filtered_queries, len(Q))
+    Qf = Q[:nqf]
+    ql = np.random.default_rng(args.seed + 7).integers(1, 101, nqf)
+    filt = dg.pack_filters(
+        [dg.Filter.or_([dg.Filter.eq(0, int(l)), dg.Filter.eq(1, int(l)), dg.Filter.eq(2, int(l))]) for l in ql])
+    gt = np.zeros((nqf, K), dtype=np.int64)
+    sel = np.zeros(nqf)
+    for l in np.unique(ql):
+        sub = np.nonzero((labels == np.uint64(l)).any(1))[0]
+        qi = np.nonzero(ql == l)[0]
+        ids, _ = dg.exact_knn(X[sub], Qf[qi], K, device=dev.index)
+        gt[qi] = sub[ids.astype(np.int64)]
+        sel[qi] = len(sub) / len(X)
+    setup_s = time.time() - t0
+    f32 = dg.FilteredDiskANN(X, adj, med, labels, device=dev.index)
+    q8 = dg.QuantizedDiskANN(X, adj, med, device=dev.index)
+    q8.attach_int8(*dg.int8_params(X))
+    q8.attach_labels(labels)
+    Qd = torch.from_numpy(Qf).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {"queries": nqf, "labels": "1-3 of 100 per vector, Zipf(1.0)", "selectivity_min": float(sel.min()),
+           "selectivity_max": float(sel.max()), "setup_s": round(setup_s, 1), "variants": {}}
+    for name, ix, kw in (("fp32", f32, {"traversal": _lib.TRAVERSE_F32}),
+                         ("int8_rerank", q8, {"traversal": _lib.TRAVERSE_CODES})):
+        chosen = None
+        curve = []
+        for L in L_SWEEP:
+            rr = L if name != "fp32" else 0
+            ids, _, _ = ix.search_arrays(Qd, K, L, rerank_size=rr, filters=filt, **kw)
+            torch.cuda.synchronize()
+            rec = recall(ids.cpu().numpy().view(np.uint32), gt)
+            curve.append((L, round(rec, 4)))
+            if rec >= args.target_recall:
+                chosen = (L, rec)
+                break
+        if chosen is None:
+            out["variants"][name] = {"recall_curve": curve}
+            continue
+        L, rec = chosen
+        rr = L if name != "fp32" else 0
+        res = ix.search_arrays(Qd, K, L, rerank_size=rr, filters=filt, **kw)
+        for _ in range(args.warmup):
+            ix.search_arrays(Qd, K, L, rerank_size=rr, filters=filt, out=res, **kw)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            ix.search_arrays(Qd, K, L, rerank_size=rr, filters=filt, out=res, **kw)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b), dist, dev)
+        _, _, _, st = ix.search_arrays(Qd, K, L, rerank_size=rr, filters=filt, with_stats=True, **kw)
+        stats = st.cpu().numpy().view(np.uint32)
+        out["variants"][name] = {"L": L, "recall_at_10": round(rec, 4), "qps": nqf * args.steps / (ms / 1e3),
+                                 "ms_per_step": ms / args.steps, "recall_curve": curve,
+                                 "expansions_per_query": float(stats[:, 0].mean()),
+                                 "dist_evals_per_query": float(stats[:, 1].mean())}
+        log(f"[filtered] {name}: {json.dumps(out['variants'][name])}")
+    f32.close()
+    q8.close()
+    return out
 
 
 def serving(args, idx, qidx, name, L, Q, gt):

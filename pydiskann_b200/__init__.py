@@ -221,6 +221,19 @@ class Filter:
         return f"Filter.{self._kind}{self._args!r}"
 
 
+class PackedFilters:
+    """Per-query filter programs compiled once, for repeated batched searches
+    (``search_arrays(..., filters=pack_filters(list_of_filters))``)."""
+
+    def __init__(self, filters):
+        self.n = len(filters)
+        self.arr, self.offs, self.pool, self.plen = _pack_programs([f.program() for f in filters])
+
+
+def pack_filters(filters):
+    return PackedFilters(list(filters))
+
+
 def _pack_programs(progs):
     """[(ops, pool)] per query -> (FilterOp array, offsets u32[nq+1], pool u64)."""
     all_ops, offs, pool = [], [0], []
@@ -348,7 +361,12 @@ class _Index:
             if stream is not None:
                 p.flags = _lib.FLAG_STREAM
                 p.stream = stream
-        if filters is not None:
+        if isinstance(filters, PackedFilters):
+            if filters.n != nq:
+                raise ValueError("one filter per query expected")
+            p.filter_ops, p.filter_offsets = C.cast(filters.arr, C.c_void_p), ptr(filters.offs)
+            p.filter_pool, p.filter_pool_len = ptr(filters.pool), filters.plen
+        elif filters is not None:
             if isinstance(filters, Filter):
                 if not filters.is_none():
                     arr, offs, pool, plen = _pack_programs([filters.program()])

@@ -371,3 +371,14 @@ def test_fp8_traversal_within_tolerance(oracle, metric):
     assert np.array_equal(rd[m], fd[m])
     assert np.mean(m) >= 0.9
     g.close()
+
+
+def test_packed_filters_equal_per_call_programs(small_data, small_graph):
+    X, Q = small_data
+    adj, med = small_graph
+    g = dg.FilteredDiskANN(X, adj, med, _labels(len(X)))
+    fl = [FILTERS[i % len(FILTERS)] if i % 4 else dg.Filter.none() for i in range(len(Q))]
+    a = g.search_arrays(Q, 10, 40, filters=fl)
+    b = g.search_arrays(Q, 10, 40, filters=dg.pack_filters(fl))
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    g.close()
