@@ -63,6 +63,8 @@ def parse():
                     help="Poisson arrival rates (req/s) for the serving loop; 0 = all requests at once")
     ap.add_argument("--serve-requests", type=int, default=200_000)
     ap.add_argument("--no-filtered", action="store_true")
+    ap.add_argument("--no-spfresh", action="store_true")
+    ap.add_argument("--spfresh-n", type=int, default=2_000_000)
     ap.add_argument("--filtered-queries", type=int, default=5000)
     return ap.parse_args()
 
@@ -388,6 +390,8 @@ def main():
             line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
         if not args.no_filtered:
             line["filtered"] = filtered(args, X, Q, adj, med, dev, dist)
+        if not args.no_spfresh:
+            line["spfresh"] = spfresh_scan(args, dev, dist)
     if rank == 0 and head and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, X, Q, adj, med, (cb, codes), head, results[head]["L"])
     if rank == 0:
@@ -505,6 +509,50 @@ def filtered(args, X, Q, adj, med, dev, dist):
         log(f"[filtered] {name}: {json.dumps(out['variants'][name])}")
     f32.close()
     q8.close()
+    return out
+
+
+def spfresh_scan(args, dev, dist):
+    """SPFresh posting scans: Zipf(1.1)-weighted 1024-centre mixture, 96
+    dims, max posting 250 (n / 125 postings), 10k queries, k = 10.  Postings
+    are bulk-loaded (exact nearest-centroid assignment + 2-means splits); the
+    smallest n_probe reaching the recall target is timed on the device."""
+    import torch
+
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import synth
+
+    t0 = time.time()
+    Xs, Qs = synth.spfresh(args.spfresh_n, 10_000, seed=args.seed)
+    gt, _ = dg.exact_knn(Xs, Qs, K, device=dev.index)
+    t1 = time.time()
+    s = dg.SPFresh.bulk_load(Xs, max_posting_size=250, seed=args.seed, device=dev.index)
+    load_s = time.time() - t1
+    st = s.stats()
+    out = {"n": len(Xs), "dim": Xs.shape[1], "queries": len(Qs), "postings": st["postings"],
+           "max_posting": st["max_posting"], "bulk_load_s": round(load_s, 1), "setup_s": round(time.time() - t0, 1)}
+    Qd = torch.from_numpy(Qs).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    curve = []
+    for nprobe in (16, 64, 256, 1024):
+        ids, _, _ = s.search_arrays(Qd, K, nprobe)
+        for _ in range(args.warmup):
+            s.search_arrays(Qd, K, nprobe)
+        torch.cuda.synchronize()
+        rec = recall(ids.cpu().numpy().astype(np.int64), gt.astype(np.int64))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            s.search_arrays(Qd, K, nprobe)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b), dist, dev) / args.steps
+        curve.append({"nprobe": nprobe, "recall_at_10": round(rec, 4), "qps": len(Qs) / (ms / 1e3), "ms_per_step": ms})
+        if rec >= args.target_recall:
+            break
+    out["curve"] = curve
+    log(f"[spfresh] {json.dumps(out)}")
+    s.close()
     return out
 
 

@@ -45,6 +45,35 @@ def _dist_rows(metric, v, C_):
     return np.maximum(r, 0.0)
 
 
+def _dist_matrix(metric, V, C_):
+    """metric_eval(v, c) for every row v of V and row c of C_ (float64), as an
+    [len(V), len(C_)] matrix (squared L2 as |v|^2 + |c|^2 - 2 v.c), in blocks."""
+    V = np.asarray(V, dtype=np.float64)
+    Cm = np.asarray(C_, dtype=np.float64)
+    out = np.empty((len(V), len(Cm)), dtype=np.float64)
+    if len(V) == 0 or len(Cm) == 0:
+        return out
+    cc = (Cm * Cm).sum(1)[None, :]
+    step = max(1, (1 << 24) // max(1, len(Cm)))
+    for s in range(0, len(V), step):
+        blk = V[s:s + step]
+        if metric in (_lib.L2SQ, _lib.L2):
+            d = np.maximum((blk * blk).sum(1)[:, None] + cc - 2.0 * (blk @ Cm.T), 0.0)
+            out[s:s + step] = np.sqrt(d) if metric == _lib.L2 else d
+            continue
+        ab = blk @ Cm.T
+        if metric == _lib.DOT:
+            out[s:s + step] = 1.0 - ab
+            continue
+        aa = (blk * blk).sum(1)[:, None]
+        bb = (Cm * Cm).sum(1)[None, :]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r = 1.0 - ab / (np.sqrt(aa) * np.sqrt(bb))
+        r = np.where((aa == 0) & (bb == 0), 0.0, np.where(ab == 0, 1.0, r))
+        out[s:s + step] = np.maximum(r, 0.0)
+    return out
+
+
 def _fht(v):
     """Unnormalised fast Walsh-Hadamard transform along the last axis (src/rabitq.rs:31-43)."""
     v = v.copy()
@@ -204,6 +233,58 @@ class SPFresh:
         s._sync()
         return s
 
+    @staticmethod
+    def bulk_load(vectors, metric="l2", quantizer=None, qparams=None, rerank_size=0, max_posting_size=128,
+                  min_posting_size=16, reassign_neighbors=16, probe_ratio=float("inf"), seed=0, device=0):
+        """Postings from a nearest-centroid assignment instead of one insert per
+        vector: n / (max_posting / 2) centroids sampled from the vectors (as
+        SPFresh::build seeds them, src/spfresh.rs:801-807), every vector assigned
+        to its nearest centroid on the GPU (exact), and postings above
+        max_posting_size split by the same 2-means as an insert-time split
+        (without relocating neighbours).  The result satisfies the index's
+        invariants, so inserts, deletes and searches continue as after build();
+        it is for large loads, where per-vector insertion is host-bound."""
+        import pydiskann_b200 as dg
+
+        X = np.ascontiguousarray(vectors, dtype=np.float32)
+        if X.ndim != 2 or len(X) == 0:
+            raise RuntimeError("Index error: No vectors provided")
+        if device is None:
+            raise ValueError("bulk_load assigns on the GPU; give a device")
+        qp = dict(qparams or {})
+        if quantizer == "int8" and not qp:
+            qp["scale"], qp["offset"] = dg.int8_params(X)
+        s = SPFresh(X.shape[1], metric, quantizer, qp, rerank_size, max_posting_size, min_posting_size,
+                    reassign_neighbors, probe_ratio, device)
+        n = len(X)
+        k = max(1, n // max(max_posting_size // 2, 1))
+        rng = np.random.default_rng([seed, 0x5EED])
+        C = X[rng.choice(n, size=min(k, n), replace=False)]
+        assign, _ = dg.exact_knn(C, X, 1, metric=metric, device=device)
+        assign = assign[:, 0].astype(np.int64)
+        order = np.argsort(assign, kind="stable")
+        bounds = np.searchsorted(assign[order], np.arange(len(C) + 1))
+        queue = [(C[c], order[bounds[c]:bounds[c + 1]]) for c in range(len(C)) if bounds[c + 1] > bounds[c]]
+        finals = []
+        while queue:
+            c, mem = queue.pop()
+            if len(mem) > max_posting_size:
+                c1, c2, side = kmeans2(X[mem], s.metric)
+                queue.append((c1, mem[~side]))
+                queue.append((c2, mem[side]))
+            else:
+                finals.append((np.asarray(c, dtype=np.float32), mem))
+        s.cent = np.stack([c for c, _ in finals]).astype(np.float32)
+        s.live_b = np.ones(len(finals), dtype=bool)
+        s.ids = [mem.astype(np.uint64) for _, mem in finals]
+        s.codes = [s.codec.encode(X[mem], s.cent[b] if s.codec.residual else None) for b, (_, mem) in enumerate(finals)]
+        s._dirty = set(range(len(finals)))
+        s.raw = X.copy()
+        s.next_id = n
+        s.live = n
+        s._sync()
+        return s
+
     # ------------------------------------------------------------ host state
     def _len(self, b):
         return len(self.ids[b])
@@ -289,12 +370,10 @@ class SPFresh:
             chunk = X[c0:c0 + CHUNK]
             self.created = []
             live = np.nonzero(self.live_b)[0]
-            targets = []
             if len(live):
-                Cm = self.cent[live].astype(np.float64)
-                for v in chunk:
-                    d = _dist_rows(self.metric, v, Cm).astype(np.float32)
-                    targets.append(int(live[np.lexsort((live, d))[0]]))
+                # nearest live posting per vector; f32 distances, lowest slot on ties
+                D = _dist_matrix(self.metric, chunk, self.cent[live]).astype(np.float32)
+                targets = [int(t) for t in live[np.argmin(D, axis=1)]]
             else:
                 targets = [None] * len(chunk)
             for j, v in enumerate(chunk):
@@ -304,11 +383,12 @@ class SPFresh:
                 if best is None:
                     nn = self._nearest(v, 1)
                     best = nn[0] if nn else None
-                for c in list(self.created):
-                    if self._is_live(c):
-                        dc = self._dist(v, c)
-                        if best is None or dc < best[1]:
-                            best = (c, dc)
+                cr = [c for c in self.created if self._is_live(c)]
+                if cr:  # postings split off earlier in this chunk
+                    dc = _dist_rows(self.metric, v, self.cent[cr])
+                    for c, dd in zip(cr, dc):
+                        if best is None or dd < best[1]:
+                            best = (c, float(dd))
                 b = best[0] if best is not None else self._new_posting(v.copy())
                 self._push(b, id_, self._encode(v, b))
                 if self._len(b) >= self.max_posting:
@@ -322,15 +402,14 @@ class SPFresh:
         ids, _ = self._live_entries(p)
         cands = [t for t in cands if t != p and self._is_live(t)]
         moves = []
-        if not cands:
+        if not cands or len(ids) == 0:
             return moves
-        for id_ in ids:
-            v = self.raw[int(id_)]
-            dp = self._dist(v, p)
-            d = _dist_rows(self.metric, v, self.cent[cands])
-            i = int(np.argmin(d))
-            if d[i] < dp:
-                moves.append((int(id_), cands[i]))
+        V = self.raw[ids.astype(np.int64)]
+        D = _dist_matrix(self.metric, V, self.cent[[p] + cands])
+        best = np.argmin(D[:, 1:], axis=1)
+        better = D[np.arange(len(ids)), 1 + best] < D[:, 0]
+        for j in np.nonzero(better)[0]:
+            moves.append((int(ids[j]), cands[int(best[j])]))
         return moves
 
     def _drain(self, queue):

@@ -136,3 +136,22 @@ def test_spfresh_api_errors():
         s.insert(np.zeros((2, 8), dtype=np.float32))
     assert s.stats()["live"] == 500
     s.close()
+
+
+def test_bulk_load_scans_match_oracle(oracle):
+    """bulk_load builds postings from an exact nearest-centroid assignment; the
+    scans over them equal the oracle's, and updates continue afterwards."""
+    X = synth.mixture(6000, 32, 40, seed=31, clip=False)
+    s = dg.SPFresh.bulk_load(X, max_posting_size=40, seed=3)
+    st = s.stats()
+    assert st["live"] == 6000 and st["max_posting"] <= 40
+    assert sorted(np.concatenate([s.ids[b] for b in range(len(s.live_b)) if s.live_b[b]]).tolist()) == list(range(6000))
+    s.insert(synth.mixture(300, 32, 40, seed=32, clip=False))
+    s.delete(list(range(0, 6300, 17)))
+    Q = synth.mixture(100, 32, 40, seed=31, stream=synth.STREAM_QUERY, clip=False)
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 8), (10, 64)):
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od)
+    s.close()
