@@ -47,7 +47,7 @@ struct DgSpfresh {
   cudaStream_t stream = nullptr;
   std::mutex mu;
   std::vector<void *> allocs;
-  DgIndex::Buf q, oids, od, ocnt;
+  DgIndex::Buf q, oids, od, ocnt, route;  // route: query x posting routing distances of one chunk
 };
 
 namespace dg {
@@ -75,6 +75,7 @@ struct SpfArgs {
   float *out_d;
   uint32_t *out_cnt;
   uint32_t *counter;
+  const float *route;  // [nq][nblocks] routing distances (null: computed in the scan kernel)
 };
 
 enum SpfKind { SPF_RAW = 0, SPF_PQ = 1, SPF_INT8 = 2, SPF_F16 = 3, SPF_RABITQ = 4 };
@@ -101,6 +102,97 @@ __device__ __forceinline__ float seq_metric(const float *q, const float *x, uint
   if (ab == 0.0f) return 1.0f;
   const float r = __fsub_rn(1.0f, __fdiv_rn(ab, __fmul_rn(__fsqrt_rn(aa), __fsqrt_rn(bb))));
   return r > 0.0f ? r : 0.0f;
+}
+
+// ---------------------------------------------------------------- routing
+// Query x posting-centroid distances, each pair summed in coordinate order
+// with the rounding of seq_metric (so routing is unchanged), as a tiled
+// kernel: a block covers 64 queries x 64 centroids, staged 32 dimensions at a
+// time in shared memory (row-major, rows padded to 33 floats: coalesced,
+// conflict-free staging and at most 2-way conflicts in the reads); each thread
+// owns a 4 x 4 tile of pairs.  Zero padding beyond d adds +0 and leaves every
+// sum unchanged.
+constexpr int kRT = 64, kRD = 32, kRS = kRD + 1;
+__global__ void __launch_bounds__(256) k_route(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
+                                               const float *__restrict__ C, uint32_t nb, uint32_t d, uint32_t dpad,
+                                               int metric, float *__restrict__ D) {
+  __shared__ float qt[kRT * kRS];
+  __shared__ float ct[kRT * kRS];
+  __shared__ float qn[kRT], cn[kRT];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const uint32_t q0 = blockIdx.y * kRT, c0 = blockIdx.x * kRT;
+  const bool l2 = metric == DG_L2SQ || metric == DG_L2;
+  if (metric == DG_COSINE && threadIdx.x < 2 * kRT) {  // |q|^2, |c|^2 in coordinate order
+    const int r = threadIdx.x & (kRT - 1);
+    const bool isq = threadIdx.x < kRT;
+    const uint32_t row = (isq ? q0 : c0) + r;
+    float s2 = 0.0f;
+    if (row < (isq ? nq : nb)) {
+      const float *x = isq ? Q + (size_t)row * qstride : C + (size_t)row * dpad;
+      for (uint32_t i = 0; i < d; ++i) s2 = __fadd_rn(s2, __fmul_rn(x[i], x[i]));
+    }
+    (isq ? qn : cn)[r] = s2;
+  }
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  for (uint32_t k0 = 0; k0 < dpad; k0 += kRD) {
+    for (int e = threadIdx.x; e < kRT * kRD; e += 256) {
+      const int r = e / kRD, k = e % kRD;
+      const uint32_t kk = k0 + k;
+      qt[r * kRS + k] = (q0 + r < nq && kk < d) ? Q[(size_t)(q0 + r) * qstride + kk] : 0.0f;
+      ct[r * kRS + k] = (c0 + r < nb && kk < dpad) ? C[(size_t)(c0 + r) * dpad + kk] : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kRD; ++k) {
+      float av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        av[i] = qt[(ty * 4 + i) * kRS + k];
+        bv[i] = ct[(tx * 4 + i) * kRS + k];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (l2) {
+            const float t = __fsub_rn(av[i], bv[j]);
+            acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(t, t));
+          } else {
+            acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(av[i], bv[j]));
+          }
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t q = q0 + ty * 4 + i;
+    if (q >= nq) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t c = c0 + tx * 4 + j;
+      if (c >= nb) continue;
+      const float a = acc[i][j];
+      float v;
+      if (metric == DG_L2SQ) v = a;
+      else if (metric == DG_L2) v = __fsqrt_rn(a);
+      else if (metric == DG_DOT) v = __fsub_rn(1.0f, a);
+      else {
+        const float aa = qn[ty * 4 + i], bb = cn[tx * 4 + j];
+        if (aa == 0.0f && bb == 0.0f) v = 0.0f;
+        else if (a == 0.0f) v = 1.0f;
+        else {
+          const float r = __fsub_rn(1.0f, __fdiv_rn(a, __fmul_rn(__fsqrt_rn(aa), __fsqrt_rn(bb))));
+          v = r > 0.0f ? r : 0.0f;
+        }
+      }
+      D[(size_t)q * nb + c] = v;
+    }
+  }
 }
 
 // The reference's angular / dot from the three sums (RN intrinsics).
@@ -279,7 +371,10 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
     for (uint32_t b0 = 0; b0 < a.nblocks; b0 += 32) {
       const uint32_t b = b0 + lane;
       uint64_t key = kKeyInvalid;
-      if (b < a.nblocks && a.live[b]) key = make_key(seq_metric(qs, a.centroids + (size_t)b * a.dpad, a.d, a.metric), b);
+      if (b < a.nblocks && a.live[b])
+        key = make_key(a.route ? __ldg(a.route + (size_t)q * a.nblocks + b)
+                               : seq_metric(qs, a.centroids + (size_t)b * a.dpad, a.d, a.metric),
+                       b);
       insert_batch(key, P, pcur, psize, nprobe, cst, lane);
     }
     // ---- 2. probe_ratio cut
@@ -486,7 +581,7 @@ DgStatus dg_spfresh_destroy(DgSpfresh *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (void *p : s->allocs) cudaFree(p);
-  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt})
+  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route})
     if (b->p) cudaFree(b->p);
   if (s->counter) cudaFree(s->counter);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -732,16 +827,40 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
     a.out_d = (float *)s->od.p;
     a.out_cnt = (uint32_t *)s->ocnt.p;
   }
-  DG_CUDA(cudaMemsetAsync(s->counter, 0, 4, st));
   const int met = s->metric == DG_DOT ? MET_DOT : s->metric == DG_COSINE ? MET_COS : MET_L2;
-  switch (s->quant) {
-    case DG_Q_NONE: r = spf_launch_met<SPF_RAW>(a, met, pcap, rcap, st); break;
-    case DG_Q_PQ: r = spf_launch_met<SPF_PQ>(a, met, pcap, rcap, st); break;
-    case DG_Q_INT8: r = spf_launch_met<SPF_INT8>(a, met, pcap, rcap, st); break;
-    case DG_Q_F16: r = spf_launch_met<SPF_F16>(a, met, pcap, rcap, st); break;
-    default: r = spf_launch_met<SPF_RABITQ>(a, met, pcap, rcap, st); break;
+  auto scan = [&](const SpfArgs &aa) -> DgStatus {
+    DG_CUDA(cudaMemsetAsync(s->counter, 0, 4, st));
+    switch (s->quant) {
+      case DG_Q_NONE: return spf_launch_met<SPF_RAW>(aa, met, pcap, rcap, st);
+      case DG_Q_PQ: return spf_launch_met<SPF_PQ>(aa, met, pcap, rcap, st);
+      case DG_Q_INT8: return spf_launch_met<SPF_INT8>(aa, met, pcap, rcap, st);
+      case DG_Q_F16: return spf_launch_met<SPF_F16>(aa, met, pcap, rcap, st);
+      default: return spf_launch_met<SPF_RABITQ>(aa, met, pcap, rcap, st);
+    }
+  };
+  if (s->nblocks >= 512) {
+    // many postings: route all queries of a chunk in one tiled kernel (the
+    // matrix of a chunk stays below 1 GiB), then scan the chunk
+    const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nq, (1ull << 28) / s->nblocks));
+    if ((r = buf_reserve(s->route, (size_t)chunk * s->nblocks * 4)) != DG_OK) return r;
+    for (uint32_t q0 = 0; q0 < nq; q0 += chunk) {
+      const uint32_t qn = std::min(chunk, nq - q0);
+      SpfArgs ac = a;
+      ac.Q = a.Q + (size_t)q0 * s->d;
+      ac.nq = qn;
+      ac.out_ids = a.out_ids + (size_t)q0 * p->k;
+      ac.out_d = a.out_d + (size_t)q0 * p->k;
+      ac.out_cnt = a.out_cnt + q0;
+      ac.route = (const float *)s->route.p;
+      dim3 grid((s->nblocks + kRT - 1) / kRT, (qn + kRT - 1) / kRT);
+      k_route<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, s->nblocks, s->d, s->dpad, s->metric,
+                                    (float *)s->route.p);
+      DG_CUDA(cudaGetLastError());
+      if ((r = scan(ac)) != DG_OK) return r;
+    }
+  } else if ((r = scan(a)) != DG_OK) {
+    return r;
   }
-  if (r != DG_OK) return r;
   if (!devptr) {
     DG_CUDA(cudaMemcpyAsync(out_ids, a.out_ids, kq * 8, cudaMemcpyDeviceToHost, st));
     DG_CUDA(cudaMemcpyAsync(out_dists, a.out_d, kq * 4, cudaMemcpyDeviceToHost, st));

@@ -155,3 +155,30 @@ def test_bulk_load_scans_match_oracle(oracle):
         oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
         assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od)
     s.close()
+
+
+@pytest.mark.parametrize("metric", ["l2", "euclidean", "cosine"])
+def test_many_postings_routing_kernel_matches_oracle(oracle, metric):
+    """With >= 512 postings the routing distances come from a separate tiled
+    kernel (each pair summed in coordinate order, as the oracle); ids, counts
+    and distances stay bit-identical (cosine within 1e-5)."""
+    if metric == "cosine":
+        X, Q = synth.cosine(30000, 200, 48, seed=33)
+    else:
+        X = synth.mixture(30000, 48, 64, seed=33, clip=False)
+        Q = synth.mixture(200, 48, 64, seed=33, stream=synth.STREAM_QUERY, clip=False)
+    s = dg.SPFresh.bulk_load(X, metric=metric, max_posting_size=32, seed=6)
+    assert s.stats()["postings"] >= 512
+    s.delete(list(range(0, 30000, 23)))
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 4), (10, 40), (5, 300)):
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc), (k, nprobe)
+        if metric == "cosine":
+            assert np.mean(gi == oi) >= 0.98
+            m = gi == oi
+            assert np.allclose(gd[m], od[m], rtol=1e-5, atol=1e-6)
+        else:
+            assert np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
+    s.close()
