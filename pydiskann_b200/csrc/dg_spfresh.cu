@@ -3,7 +3,8 @@
 //
 // One warp per query, persistent grid with a work counter:
 //   1. routing: the distance from the query to every live posting centroid,
-//      each summed sequentially by one lane in the order the oracle sums it,
+//      each summed sequentially in the order the oracle sums it (by one lane
+//      in this kernel for few postings, by the tiled k_route for >= 512),
 //      kept as the nprobe smallest (distance, posting) keys (nearest,
 //      src/spfresh.rs:358-378; brute force at every posting count);
 //   2. the probe_ratio cut (:683-687);
@@ -368,14 +369,30 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
     // ---- 1. routing
     const int nprobe = (int)max(a.nprobe, 1u);
     int pcur = 0, psize = 0;
-    for (uint32_t b0 = 0; b0 < a.nblocks; b0 += 32) {
-      const uint32_t b = b0 + lane;
-      uint64_t key = kKeyInvalid;
-      if (b < a.nblocks && a.live[b])
-        key = make_key(a.route ? __ldg(a.route + (size_t)q * a.nblocks + b)
-                               : seq_metric(qs, a.centroids + (size_t)b * a.dpad, a.d, a.metric),
-                       b);
-      insert_batch(key, P, pcur, psize, nprobe, cst, lane);
+    if (a.route) {
+      // precomputed distances: the loads of 8 batches go out before their
+      // (in-order) insertions
+      const float *rq = a.route + (size_t)q * a.nblocks;
+      for (uint32_t b0 = 0; b0 < a.nblocks; b0 += 32 * 8) {
+        uint64_t keys[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const uint32_t b = b0 + 32u * u + lane;
+          const bool ok = b < a.nblocks && __ldg(a.live + b);
+          const float dv = b < a.nblocks ? __ldg(rq + b) : 0.0f;
+          keys[u] = ok ? make_key(dv, b) : kKeyInvalid;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) insert_batch(keys[u], P, pcur, psize, nprobe, cst, lane);
+      }
+    } else {
+      for (uint32_t b0 = 0; b0 < a.nblocks; b0 += 32) {
+        const uint32_t b = b0 + lane;
+        uint64_t key = kKeyInvalid;
+        if (b < a.nblocks && a.live[b])
+          key = make_key(seq_metric(qs, a.centroids + (size_t)b * a.dpad, a.d, a.metric), b);
+        insert_batch(key, P, pcur, psize, nprobe, cst, lane);
+      }
     }
     // ---- 2. probe_ratio cut
     int np = psize;
