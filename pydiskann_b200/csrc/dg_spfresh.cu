@@ -49,6 +49,7 @@ struct DgSpfresh {
   std::mutex mu;
   std::vector<void *> allocs;
   DgIndex::Buf q, oids, od, ocnt, route;  // route: query x posting routing distances of one chunk
+  DgIndex::Buf live_idx;                   // [0]: number of live postings, then their slot indices
 };
 
 namespace dg {
@@ -76,7 +77,8 @@ struct SpfArgs {
   float *out_d;
   uint32_t *out_cnt;
   uint32_t *counter;
-  const float *route;  // [nq][nblocks] routing distances (null: computed in the scan kernel)
+  const float *route;        // [nq][nblocks] routing distances (null: computed in the scan kernel)
+  const uint32_t *route_idx; // [1 + live] count, then the live slots the columns of `route` belong to
 };
 
 enum SpfKind { SPF_RAW = 0, SPF_PQ = 1, SPF_INT8 = 2, SPF_F16 = 3, SPF_RABITQ = 4 };
@@ -106,7 +108,14 @@ __device__ __forceinline__ float seq_metric(const float *q, const float *x, uint
 }
 
 // ---------------------------------------------------------------- routing
-// Query x posting-centroid distances, each pair summed in coordinate order
+// The live posting slots, compacted (in any order: routing keeps the nprobe
+// smallest unique (distance, slot) keys, which does not depend on the order).
+__global__ void k_live_idx(const uint8_t *live, uint32_t nb, uint32_t *out) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+    if (live[b]) out[1 + atomicAdd(out, 1u)] = b;
+}
+
+// Query x live-posting-centroid distances, each pair summed in coordinate order
 // with the rounding of seq_metric (so routing is unchanged), as a tiled
 // kernel: a block covers 64 queries x 64 centroids, staged 32 dimensions at a
 // time in shared memory (row-major, rows padded to 33 floats: coalesced,
@@ -114,14 +123,20 @@ __device__ __forceinline__ float seq_metric(const float *q, const float *x, uint
 // owns a 4 x 4 tile of pairs.  Zero padding beyond d adds +0 and leaves every
 // sum unchanged.
 constexpr int kRT = 64, kRD = 32, kRS = kRD + 1;
+// Columns follow cidx[1 ..] (cidx[0] live postings; blocks past it exit),
+// rows of D are ldd floats apart.
 __global__ void __launch_bounds__(256) k_route(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
-                                               const float *__restrict__ C, uint32_t nb, uint32_t d, uint32_t dpad,
-                                               int metric, float *__restrict__ D) {
+                                               const float *__restrict__ C, const uint32_t *__restrict__ cidx,
+                                               uint32_t d, uint32_t dpad, int metric, float *__restrict__ D,
+                                               uint32_t ldd) {
   __shared__ float qt[kRT * kRS];
   __shared__ float ct[kRT * kRS];
   __shared__ float qn[kRT], cn[kRT];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const uint32_t q0 = blockIdx.y * kRT, c0 = blockIdx.x * kRT;
+  const uint32_t nb = __ldg(cidx);
+  if (c0 >= nb) return;  // the whole block: fewer live postings than slots
+  const uint32_t *col = cidx + 1;
   const bool l2 = metric == DG_L2SQ || metric == DG_L2;
   if (metric == DG_COSINE && threadIdx.x < 2 * kRT) {  // |q|^2, |c|^2 in coordinate order
     const int r = threadIdx.x & (kRT - 1);
@@ -129,7 +144,7 @@ __global__ void __launch_bounds__(256) k_route(const float *__restrict__ Q, uint
     const uint32_t row = (isq ? q0 : c0) + r;
     float s2 = 0.0f;
     if (row < (isq ? nq : nb)) {
-      const float *x = isq ? Q + (size_t)row * qstride : C + (size_t)row * dpad;
+      const float *x = isq ? Q + (size_t)row * qstride : C + (size_t)col[row] * dpad;
       for (uint32_t i = 0; i < d; ++i) s2 = __fadd_rn(s2, __fmul_rn(x[i], x[i]));
     }
     (isq ? qn : cn)[r] = s2;
@@ -144,7 +159,7 @@ __global__ void __launch_bounds__(256) k_route(const float *__restrict__ Q, uint
       const int r = e / kRD, k = e % kRD;
       const uint32_t kk = k0 + k;
       qt[r * kRS + k] = (q0 + r < nq && kk < d) ? Q[(size_t)(q0 + r) * qstride + kk] : 0.0f;
-      ct[r * kRS + k] = (c0 + r < nb && kk < dpad) ? C[(size_t)(c0 + r) * dpad + kk] : 0.0f;
+      ct[r * kRS + k] = (c0 + r < nb && kk < dpad) ? C[(size_t)col[c0 + r] * dpad + kk] : 0.0f;
     }
     __syncthreads();
 #pragma unroll 4
@@ -191,7 +206,7 @@ __global__ void __launch_bounds__(256) k_route(const float *__restrict__ Q, uint
           v = r > 0.0f ? r : 0.0f;
         }
       }
-      D[(size_t)q * nb + c] = v;
+      D[(size_t)q * ldd + c] = v;
     }
   }
 }
@@ -373,14 +388,14 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
       // precomputed distances: the loads of 8 batches go out before their
       // (in-order) insertions
       const float *rq = a.route + (size_t)q * a.nblocks;
-      for (uint32_t b0 = 0; b0 < a.nblocks; b0 += 32 * 8) {
+      const uint32_t nl = __ldg(a.route_idx);
+      const uint32_t *col = a.route_idx + 1;
+      for (uint32_t j0 = 0; j0 < nl; j0 += 32 * 8) {
         uint64_t keys[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          const uint32_t b = b0 + 32u * u + lane;
-          const bool ok = b < a.nblocks && __ldg(a.live + b);
-          const float dv = b < a.nblocks ? __ldg(rq + b) : 0.0f;
-          keys[u] = ok ? make_key(dv, b) : kKeyInvalid;
+          const uint32_t j = j0 + 32u * u + lane;
+          keys[u] = j < nl ? make_key(__ldg(rq + j), __ldg(col + j)) : kKeyInvalid;
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) insert_batch(keys[u], P, pcur, psize, nprobe, cst, lane);
@@ -598,7 +613,7 @@ DgStatus dg_spfresh_destroy(DgSpfresh *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (void *p : s->allocs) cudaFree(p);
-  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route})
+  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx})
     if (b->p) cudaFree(b->p);
   if (s->counter) cudaFree(s->counter);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -860,6 +875,11 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
     // matrix of a chunk stays below 1 GiB), then scan the chunk
     const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nq, (1ull << 28) / s->nblocks));
     if ((r = buf_reserve(s->route, (size_t)chunk * s->nblocks * 4)) != DG_OK) return r;
+    if ((r = buf_reserve(s->live_idx, ((size_t)s->nblocks + 1) * 4)) != DG_OK) return r;
+    uint32_t *lidx = (uint32_t *)s->live_idx.p;
+    DG_CUDA(cudaMemsetAsync(lidx, 0, 4, st));
+    k_live_idx<<<(s->nblocks + 255) / 256, 256, 0, st>>>(s->live, s->nblocks, lidx);
+    DG_CUDA(cudaGetLastError());
     for (uint32_t q0 = 0; q0 < nq; q0 += chunk) {
       const uint32_t qn = std::min(chunk, nq - q0);
       SpfArgs ac = a;
@@ -869,9 +889,10 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
       ac.out_d = a.out_d + (size_t)q0 * p->k;
       ac.out_cnt = a.out_cnt + q0;
       ac.route = (const float *)s->route.p;
+      ac.route_idx = lidx;
       dim3 grid((s->nblocks + kRT - 1) / kRT, (qn + kRT - 1) / kRT);
-      k_route<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, s->nblocks, s->d, s->dpad, s->metric,
-                                    (float *)s->route.p);
+      k_route<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric,
+                                    (float *)s->route.p, s->nblocks);
       DG_CUDA(cudaGetLastError());
       if ((r = scan(ac)) != DG_OK) return r;
     }
