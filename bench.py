@@ -390,8 +390,10 @@ def main():
             line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
         if not args.no_filtered:
             line["filtered"] = filtered(args, X, Q, adj, med, dev, dist)
-        if not args.no_spfresh:
-            line["spfresh"] = spfresh_scan(args, dev, dist)
+        if not args.no_spfresh and rank == 0:
+            # one replica is enough for this secondary measurement (it stages
+            # several GB of posting blocks on the host)
+            line["spfresh"] = spfresh_scan(args, dev, None)
     if rank == 0 and head and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, X, Q, adj, med, (cb, codes), head, results[head]["L"])
     if rank == 0:

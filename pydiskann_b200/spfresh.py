@@ -565,7 +565,10 @@ class SPFresh:
         if self._h is not None:
             lib().dg_spfresh_destroy(self._h)
             self._h = None
-        nb = max(2 * len(self.live_b), 16)
+        # room for new postings without re-creating the mirror: x2 for small
+        # indexes, +25 % for large ones (host staging is slots x cap x code bytes)
+        n_slots = len(self.live_b)
+        nb = max(2 * n_slots if n_slots < 4096 else n_slots + n_slots // 4, 16)
         id_cap = max(2 * self.next_id, 1024)
         cent, live, lens, ids, codes = self.host_arrays(nb)
         raw = np.ascontiguousarray(self.raw[: self.next_id])
