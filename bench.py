@@ -454,8 +454,8 @@ def filtered(args, X, Q, adj, med, dev, dist):
     nqf = min(args.filtered_queries, len(Q))
     Qf = Q[:nqf]
     ql = np.random.default_rng(args.seed + 7).integers(1, 101, nqf)
-    filt = dg.pack_filters(
-        [dg.Filter.or_([dg.Filter.eq(0, int(l)), dg.Filter.eq(1, int(l)), dg.Filter.eq(2, int(l))]) for l in ql])
+    flist = [dg.Filter.or_([dg.Filter.eq(0, int(l)), dg.Filter.eq(1, int(l)), dg.Filter.eq(2, int(l))]) for l in ql]
+    filt = dg.pack_filters(flist)
     gt = np.zeros((nqf, K), dtype=np.int64)
     sel = np.zeros(nqf)
     for l in np.unique(ql):
@@ -466,6 +466,7 @@ def filtered(args, X, Q, adj, med, dev, dist):
         sel[qi] = len(sub) / len(X)
     setup_s = time.time() - t0
     f32 = dg.FilteredDiskANN(X, adj, med, labels, device=dev.index)
+    f32.enable_bf16()
     q8 = dg.QuantizedDiskANN(X, adj, med, device=dev.index)
     q8.attach_int8(*dg.int8_params(X))
     q8.attach_labels(labels)
@@ -473,8 +474,10 @@ def filtered(args, X, Q, adj, med, dev, dist):
     stream = torch.cuda.current_stream(dev)
     out = {"queries": nqf, "labels": "1-3 of 100 per vector, Zipf(1.0)", "selectivity_min": float(sel.min()),
            "selectivity_max": float(sel.max()), "setup_s": round(setup_s, 1), "variants": {}}
-    for name, ix, kw in (("fp32", f32, {"traversal": _lib.TRAVERSE_F32}),
-                         ("int8_rerank", q8, {"traversal": _lib.TRAVERSE_CODES})):
+    variants = (("fp32", f32, {"traversal": _lib.TRAVERSE_F32}),
+                ("bf16_rerank", f32, {"traversal": _lib.TRAVERSE_BF16}),
+                ("int8_rerank", q8, {"traversal": _lib.TRAVERSE_CODES}))
+    for name, ix, kw in variants:
         chosen = None
         curve = []
         for L in L_SWEEP:
@@ -509,6 +512,27 @@ def filtered(args, X, Q, adj, med, dev, dist):
                                  "expansions_per_query": float(stats[:, 0].mean()),
                                  "dist_evals_per_query": float(stats[:, 1].mean())}
         log(f"[filtered] {name}: {json.dumps(out['variants'][name])}")
+    # filtered serving: Poisson arrivals, each request with its own label filter
+    n_srv, rate = 50_000, 200_000.0
+    qi = np.arange(n_srv) % nqf
+    out["serving"] = {"requests": n_srv, "offered_rps": rate, "variants": {}}
+    for name, ix, kw in variants:
+        v = out["variants"].get(name, {})
+        if "L" not in v or name == "int8_rerank":
+            continue
+        L = v["L"]
+        with dg.Server(ix, max_batch=512, streams=16, max_k=K) as srv:
+            srv.run_trace(Qf[:2000], np.zeros(2000), k=K, beam_width=L, rerank_size=L if name != "fp32" else 0,
+                          traversal=kw["traversal"], filters=flist[:2000])
+            res = srv.run_trace(Qf[qi], dg.poisson_arrivals(n_srv, rate, seed=5), k=K, beam_width=L,
+                                rerank_size=L if name != "fp32" else 0, traversal=kw["traversal"],
+                                filters=[flist[i] for i in qi])
+        lat = res["latency_us"] / 1e3
+        hits = [len(set(res["ids"][i].tolist()) & set(gt[qi[i]].tolist())) for i in range(0, n_srv, 5)]
+        out["serving"]["variants"][name] = {
+            "L": L, "achieved_qps": n_srv / (res["wall_us"] / 1e6), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "recall_at_10": round(float(np.mean(hits)) / K, 4)}
+        log(f"[filtered serve] {name}: {json.dumps(out['serving']['variants'][name])}")
     f32.close()
     q8.close()
     return out
