@@ -119,6 +119,9 @@ DG_API DgStatus dg_index_attach_pq(DgIndex *idx, uint32_t M, uint32_t K, const f
 DG_API DgStatus dg_index_attach_int8(DgIndex *idx, float scale, float offset, const uint8_t *codes);
 /* QuantizedDiskANN::from_f16 (src/quantized.rs:225-236). */
 DG_API DgStatus dg_index_attach_f16(DgIndex *idx);
+/* The same with the codes given: u16[n*dim] f16 bit patterns, as a QANN
+ * sidecar stores them (src/quantized.rs:490-509); NULL encodes on the GPU. */
+DG_API DgStatus dg_index_attach_f16_codes(DgIndex *idx, const uint8_t *codes);
 /* QuantizedDiskANN::from_rabitq (src/quantized.rs:239-249): padded dim,
  * centroid f32[dim], signs f32[3*padded] (src/rabitq.rs:78-107); codes of
  * padded/8+8 bytes or NULL to encode on the GPU (src/rabitq.rs:218-256). */
@@ -126,6 +129,11 @@ DG_API DgStatus dg_index_attach_rabitq(DgIndex *idx, uint32_t padded, const floa
                                 const float *signs, const uint8_t *codes);
 /* FilteredDiskANN labels (src/filtered.rs:140-160): u64[n*num_fields]. */
 DG_API DgStatus dg_index_attach_labels(DgIndex *idx, uint32_t num_fields, const uint64_t *labels);
+/* The attached quantizer's codes, n rows of code_size bytes in the layout the
+ * QANN sidecar stores (QuantizedDiskANN::quantized_to_bytes, src/quantized.rs:
+ * 490-509); out = NULL only reports code_size.  Lets a caller persist an index
+ * whose codes were encoded on the GPU. */
+DG_API DgStatus dg_index_get_codes(DgIndex *idx, uint8_t *out, uint64_t out_len, uint32_t *code_size);
 
 typedef struct {
   uint32_t k;

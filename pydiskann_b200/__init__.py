@@ -9,8 +9,11 @@ binding (pydiskann 0.5.5, python/src/lib.rs):
     RuntimeError, out-of-range ids IndexError.
 Every search runs in libdgann.so (hand-written sm_100a kernels); there is no
 CPU path.  Index construction (Vamana graph, PQ codebooks, codes) also runs
-on the GPU.  ``path`` arguments are accepted for signature compatibility;
-on-disk persistence is not part of this package.
+on the GPU.  Indexes persist in the reference's own file formats
+(pydiskann_b200/formats.py): ``build(path=...)`` writes the DANN core file
+(and, for FilteredDiskANN, ``{path}.idx`` / ``{path}.labels``), ``open`` /
+``from_bytes`` load files and buffers the reference wrote, ``to_bytes`` and
+``save_quantized`` write what the reference loads.
 
 Batched array entry points (``search_arrays``) take numpy arrays or CUDA
 tensors and return arrays, for callers that keep queries and results in HBM.
@@ -19,11 +22,13 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import warnings
 from typing import Iterable, Sequence
 
 import numpy as np
 
 from . import _lib
+from . import formats as _fmt
 from ._lib import PAD, DgError, check, lib, ptr  # noqa: F401  (DgError is public)
 
 __all__ = [
@@ -39,6 +44,15 @@ def _metric(m: str) -> int:
         return _METRICS[m]
     except KeyError:
         raise ValueError(f"unknown metric: {m}") from None
+
+
+def _check_recorded_metric(meta, metric):
+    """open_index_with / from_bytes (src/lib.rs:558-564, 583-589): the caller's metric
+    is used; a different recorded distance only warns."""
+    want = _fmt.DISTANCE_NAMES[metric]
+    if meta.distance_name != want:
+        warnings.warn(f"index recorded distance `{meta.distance_name}` but you opened with `{want}`",
+                      RuntimeWarning, stacklevel=3)
 
 
 def _f32(x, dim=None) -> np.ndarray:
@@ -306,6 +320,10 @@ class _Index:
             raise IndexError(id)
         return self._X[id].tolist()
 
+    def to_bytes(self) -> bytes:
+        """DiskANN::to_bytes (src/lib.rs:630-632): the DANN core file's bytes."""
+        return _fmt.core_bytes(self._X, self.adjacency, self.medoid_id, self._metric_name)
+
     def enable_bf16(self):
         if not self._bf16:
             check(lib().dg_index_enable_bf16(self._h))
@@ -410,11 +428,29 @@ class DiskANN(_Index):
         if X.ndim != 2 or X.shape[0] == 0:
             raise RuntimeError("Index error: No vectors provided")
         adj, med = build_graph(X, max_degree, build_beam_width, alpha, metric, seed, None, device)
+        if path is not None:  # build_index_with_params writes the core file (src/lib.rs:355-505)
+            _fmt.write_core(path, X, adj, med, metric)
         return DiskANN(X, adj, med, metric, device)
 
     @staticmethod
     def from_graph(vectors, adjacency, medoid_id, metric="l2", device=0, hbm_budget_bytes=0):
         return DiskANN(vectors, adjacency, medoid_id, metric, device, hbm_budget_bytes)
+
+    @staticmethod
+    def open(path, metric="l2", device=0, hbm_budget_bytes=0):
+        """DiskANN::open_index_with (src/lib.rs:507-577): a DANN core file."""
+        _metric(metric)
+        m, X, A = _fmt.read_core(path)
+        _check_recorded_metric(m, metric)
+        return DiskANN(X, A, m.medoid_id, metric, device, hbm_budget_bytes)
+
+    @staticmethod
+    def from_bytes(data, metric="l2", device=0, hbm_budget_bytes=0):
+        """DiskANN::from_bytes (src/lib.rs:580-601): a core file's bytes."""
+        _metric(metric)
+        m, X, A = _fmt.parse_core(data)
+        _check_recorded_metric(m, metric)
+        return DiskANN(X, A, m.medoid_id, metric, device, hbm_budget_bytes)
 
     def search_with_dists(self, query, k=10, beam_width=128):
         ids, ds, cnt = self.search_arrays(_f32(query).reshape(1, -1), k, beam_width)
@@ -446,6 +482,8 @@ class QuantizedDiskANN(_Index):
         if X.ndim != 2 or X.shape[0] == 0:
             raise RuntimeError("Index error: No vectors provided")
         adj, med = build_graph(X, max_degree, build_beam_width, alpha, metric, seed, None, device)
+        if path is not None:  # build_* writes the base core file (src/quantized.rs:584-634)
+            _fmt.write_core(path, X, adj, med, metric)
         q = QuantizedDiskANN(X, adj, med, metric, device, rerank_size)
         if quantizer == "f16":
             q.attach_f16()
@@ -472,8 +510,14 @@ class QuantizedDiskANN(_Index):
         check(lib().dg_index_attach_int8(self._h, float(scale), float(offset), ptr(c)))
         self._quant = ("int8", (scale, offset))
 
-    def attach_f16(self):
-        check(lib().dg_index_attach_f16(self._h))
+    def attach_f16(self, codes=None):
+        """codes: u16[n, dim] f16 bit patterns (a QANN sidecar's); None encodes on the GPU."""
+        c = None
+        if codes is not None:
+            c = np.ascontiguousarray(codes).view(np.uint8).reshape(self.num_vectors, -1)
+            if c.shape[1] != 2 * self.dim:
+                raise ValueError(f"F16 codes must be {2 * self.dim} bytes per vector")
+        check(lib().dg_index_attach_f16_codes(self._h, ptr(c)))
         self._quant = ("f16", None)
 
     def attach_rabitq(self, centroid, signs, codes=None):
@@ -482,6 +526,77 @@ class QuantizedDiskANN(_Index):
         c = None if codes is None else np.ascontiguousarray(codes, dtype=np.uint8)
         check(lib().dg_index_attach_rabitq(self._h, padded, ptr(cen), ptr(sg), ptr(c)))
         self._quant = ("rabitq", (cen, sg))
+
+    # -- persistence: the QANN sidecar (src/quantized.rs:420-575)
+    @staticmethod
+    def open(base_path, quantized_path, metric="l2", rerank_size=0, device=0, hbm_budget_bytes=0):
+        """QuantizedDiskANN::open (src/quantized.rs:444-454): a core file and its sidecar."""
+        _metric(metric)
+        m, X, A = _fmt.read_core(base_path)
+        _check_recorded_metric(m, metric)
+        state, codes = _fmt.read_sidecar(quantized_path, m.num_vectors)
+        q = QuantizedDiskANN(X, A, m.medoid_id, metric, device, rerank_size, hbm_budget_bytes)
+        q.attach_state(state, codes)
+        return q
+
+    @staticmethod
+    def from_bytes(data, metric="l2", rerank_size=0, device=0, hbm_budget_bytes=0):
+        """QuantizedDiskANN::from_bytes (src/quantized.rs:468-488): [base_len][core][sidecar]."""
+        _metric(metric)
+        base, rest = _fmt.split_prefixed(data)
+        m, X, A = _fmt.parse_core(base)
+        _check_recorded_metric(m, metric)
+        state, codes = _fmt.parse_sidecar(rest, m.num_vectors)
+        q = QuantizedDiskANN(X, A, m.medoid_id, metric, device, rerank_size, hbm_budget_bytes)
+        q.attach_state(state, codes)
+        return q
+
+    def attach_state(self, state, codes=None):
+        """Attaches a formats.QuantizerState (the sidecar's quantizer) and its codes."""
+        if state.dim != self.dim:
+            raise RuntimeError(f"Index error: quantizer dim {state.dim} != index dim {self.dim}")
+        if state.kind == "pq":
+            cb = state.codebooks.reshape(state.num_subspaces, state.num_centroids, state.subspace_dim)
+            self.attach_pq(cb, codes)
+        elif state.kind == "int8":
+            self.attach_int8(state.scale, state.offset, codes)
+        elif state.kind == "f16":
+            self.attach_f16(codes)
+        else:
+            if state.padded != rabitq_padded(self.dim):
+                raise RuntimeError(f"Index error: RaBitQ padded {state.padded} != {rabitq_padded(self.dim)}")
+            self.attach_rabitq(state.centroid, state.signs, codes)
+
+    def quantizer_state(self):
+        """The attached quantizer as the sidecar's QuantizerState."""
+        if self._quant is None:
+            raise RuntimeError("Index error: no quantizer attached")
+        kind, p = self._quant
+        if kind == "pq":
+            M, K, ds = p.shape
+            return _fmt.QuantizerState("pq", self.dim, M, K, ds, codebooks=p.reshape(-1))
+        if kind == "int8":
+            return _fmt.QuantizerState("int8", self.dim, scale=p[0], offset=p[1])
+        if kind == "f16":
+            return _fmt.QuantizerState("f16", self.dim)
+        cen, sg = p
+        return _fmt.QuantizerState("rabitq", self.dim, padded=sg.size // 3, centroid=cen, signs=sg)
+
+    def codes(self) -> np.ndarray:
+        """The codes in HBM, u8[n, code_size] as the sidecar stores them."""
+        cs = C.c_uint32()
+        check(lib().dg_index_get_codes(self._h, None, 0, C.byref(cs)))
+        out = np.empty((self.num_vectors, cs.value), np.uint8)
+        check(lib().dg_index_get_codes(self._h, ptr(out), out.size, None))
+        return out
+
+    def save_quantized(self, path):
+        """QuantizedDiskANN::save_quantized (src/quantized.rs:435-441)."""
+        _fmt.write_sidecar(path, self.quantizer_state(), self.codes())
+
+    def to_bytes(self) -> bytes:
+        """QuantizedDiskANN::to_bytes (src/quantized.rs:456-466)."""
+        return _fmt.join_prefixed(super().to_bytes(), _fmt.sidecar_bytes(self.quantizer_state(), self.codes()))
 
     def search_arrays(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_CODES,
                       rerank_size=None, **kw):
@@ -542,7 +657,38 @@ class FilteredDiskANN(_Index):
             raise RuntimeError(f"Index error: vectors.len() ({X.shape[0]}) != labels.len() ({len(lab)})")
         adj, med = build_graph(X, max_degree, build_beam_width, alpha, metric, seed, None, device)
         arr = np.asarray(lab, dtype=np.uint64).reshape(X.shape[0], nf)
+        if path is not None:  # {path}.idx and {path}.labels (src/filtered.rs:202-208)
+            _fmt.write_core(f"{path}.idx", X, adj, med, metric)
+            _fmt.write_labels(f"{path}.labels", arr)
         return FilteredDiskANN(X, adj, med, arr, metric, device)
+
+    @staticmethod
+    def open(path, metric="l2", device=0, hbm_budget_bytes=0):
+        """FilteredDiskANN::open (src/filtered.rs:219-241): `{path}.idx` and `{path}.labels`."""
+        _metric(metric)
+        m, X, A = _fmt.read_core(f"{path}.idx")
+        _check_recorded_metric(m, metric)
+        return FilteredDiskANN._with_labels(m, X, A, _fmt.read_labels(f"{path}.labels"), metric, device,
+                                            hbm_budget_bytes)
+
+    @staticmethod
+    def from_bytes(data, metric="l2", device=0, hbm_budget_bytes=0):
+        """FilteredDiskANN::from_bytes (src/filtered.rs:256-285): [index_len][core][labels]."""
+        _metric(metric)
+        base, rest = _fmt.split_prefixed(data, "index data")
+        m, X, A = _fmt.parse_core(base)
+        _check_recorded_metric(m, metric)
+        return FilteredDiskANN._with_labels(m, X, A, _fmt.parse_labels(rest), metric, device, hbm_budget_bytes)
+
+    @staticmethod
+    def _with_labels(m, X, A, lab, metric, device, hbm_budget_bytes):
+        if lab.shape[0] != m.num_vectors:
+            raise RuntimeError(f"Index error: Labels count ({lab.shape[0]}) != index vectors ({m.num_vectors})")
+        return FilteredDiskANN(X, A, m.medoid_id, lab, metric, device, hbm_budget_bytes)
+
+    def to_bytes(self) -> bytes:
+        """FilteredDiskANN::to_bytes (src/filtered.rs:245-254)."""
+        return _fmt.join_prefixed(super().to_bytes(), _fmt.labels_bytes(self._labels))
 
     @property
     def num_fields(self) -> int:

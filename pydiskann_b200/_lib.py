@@ -93,8 +93,10 @@ def _signatures():
         "dg_index_attach_pq": (st, [vp, u32, u32, vp, vp]),
         "dg_index_attach_int8": (st, [vp, f32, f32, vp]),
         "dg_index_attach_f16": (st, [vp]),
+        "dg_index_attach_f16_codes": (st, [vp, vp]),
         "dg_index_attach_rabitq": (st, [vp, u32, vp, vp, vp]),
         "dg_index_attach_labels": (st, [vp, u32, vp]),
+        "dg_index_get_codes": (st, [vp, vp, u64, vp]),
         "dg_search_batch": (st, [vp, vp, vp, u32, vp, vp, vp, vp]),
         "dg_search_batch_static": (st, [vp, vp, vp, u32, vp, vp, vp]),
         "dg_count_matching": (st, [vp, vp, u32, vp, u32, vp]),

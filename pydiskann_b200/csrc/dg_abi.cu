@@ -264,15 +264,18 @@ DgStatus dg_index_attach_int8(DgIndex *idx, float scale, float offset, const uin
   return DG_OK;
 }
 
-DgStatus dg_index_attach_f16(DgIndex *idx) {
+DgStatus dg_index_attach_f16(DgIndex *idx) { return dg_index_attach_f16_codes(idx, nullptr); }
+
+DgStatus dg_index_attach_f16_codes(DgIndex *idx, const uint8_t *codes) {
   if (!idx) return fail(DG_EINVAL, "null index");
   std::lock_guard<std::mutex> lk(idx->mu);
   DG_CUDA(cudaSetDevice(idx->device));
   DgStatus s = attach_codes_common(idx, DG_Q_F16, idx->dpad * 2);
   if (s != DG_OK) return s;
   idx->code_size = idx->d * 2;
-  if ((s = encode_f16_device(idx->vec, idx->n, idx->dpad, (uint16_t *)idx->codes, idx->stream)) != DG_OK)
-    return s;
+  if (codes) s = upload_code_rows(idx, codes);
+  else s = encode_f16_device(idx->vec, idx->n, idx->dpad, (uint16_t *)idx->codes, idx->stream);
+  if (s != DG_OK) return s;
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
 }
@@ -309,6 +312,20 @@ DgStatus dg_index_attach_labels(DgIndex *idx, uint32_t num_fields, const uint64_
   DgStatus s = to_device(idx, (void **)&idx->labels, labels ? (const void *)labels : (const void *)"",
                          std::max<size_t>(idx->n * num_fields * 8, 8));
   if (s != DG_OK) return s;
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+DgStatus dg_index_get_codes(DgIndex *idx, uint8_t *out, uint64_t out_len, uint32_t *code_size) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  if (idx->quant == DG_Q_NONE) return fail(DG_EINVAL, "no quantizer is attached");
+  if (code_size) *code_size = idx->code_size;
+  if (!out) return DG_OK;
+  if (out_len < idx->n * (uint64_t)idx->code_size) return fail(DG_EINVAL, "output buffer smaller than n * code_size");
+  DG_CUDA(cudaSetDevice(idx->device));
+  DG_CUDA(cudaMemcpy2DAsync(out, idx->code_size, idx->codes, idx->code_stride, idx->code_size, idx->n,
+                            cudaMemcpyDeviceToHost, idx->stream));
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
 }

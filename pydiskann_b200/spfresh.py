@@ -198,6 +198,8 @@ class SPFresh:
         self._dev_ids = 0
         self._raw_synced = 0
         self._del_synced = set()
+        self.centroid_beam = 64  # SPFreshConfig::centroid_beam, kept for the saved config
+        self.path = None
 
     # ------------------------------------------------------------ building
     @staticmethod
@@ -221,8 +223,8 @@ class SPFresh:
         elif quantizer == "pq":
             qp["codebooks"] = dg.pq_train(X, pq_subspaces, 256, 20, 50_000, seed, device)
         elif quantizer == "rabitq":
-            _, signs = dg.rabitq_params(X, seed)
-            qp["padded"], qp["signs"] = dg.rabitq_padded(X.shape[1]), signs
+            cen, signs = dg.rabitq_params(X, seed)
+            qp["padded"], qp["signs"], qp["centroid"] = dg.rabitq_padded(X.shape[1]), signs, cen
         s = SPFresh(X.shape[1], metric, quantizer, qp, rerank_size, max_posting_size, min_posting_size,
                     reassign_neighbors, probe_ratio, device)
         k = max(1, len(X) // max(max_posting_size // 2, 1))
@@ -231,6 +233,8 @@ class SPFresh:
             s._new_posting(X[i].copy())
         s._insert(X)
         s._sync()
+        if path is not None:  # SPFresh::build saves at `path` (src/spfresh.rs:785-817)
+            s.save(path)
         return s
 
     @staticmethod
@@ -519,6 +523,83 @@ class SPFresh:
         return {"live": self.live, "deleted": len(self.deleted), "postings": int(self.live_b.sum()),
                 "max_posting": max(sizes) if sizes else 0}
 
+    # ------------------------------------------------------------ persistence
+    @staticmethod
+    def open(path, metric="l2", device=0):
+        """SPFresh::open (src/spfresh.rs:819-850) of the files SPFresh::save wrote:
+        `{path}.spf` (metadata), `.postings` (blocks), `.vectors` (raw rows) and
+        `.centroids` (the centroid graph; checked, not used -- routing here is exact)."""
+        from . import formats as F
+
+        if metric not in _METRICS:
+            raise ValueError(f"unknown metric: {metric}")
+        meta = F.parse_spf(_read(f"{path}.spf"))
+        F.check_incremental_header(_read(f"{path}.centroids"))
+        kind, qp = _codec_params(meta.quantizer)
+        cfg, d, nb = meta.cfg, meta.dim, len(meta.block_cid)
+        s = SPFresh(d, metric, kind, qp, cfg.rerank_size, max(cfg.max_posting_size, 2), cfg.min_posting_size,
+                    cfg.reassign_neighbors, cfg.probe_ratio, device)
+        s.centroid_beam = cfg.centroid_beam
+        block = F.spf_block_bytes(cfg, meta.quantizer, d)
+        posts = F.parse_postings(_read(f"{path}.postings"), nb, block, s.codec.size)
+        live = meta.block_cid != np.uint64(F.SPF_FREE)
+        s.cent = np.zeros((nb, d), dtype=np.float32)
+        for b in np.nonzero(live)[0]:
+            s.cent[b] = meta.block_centroid[b]
+        s.live_b = live
+        s.ids = [ids if live[b] else ids[:0] for b, (ids, _) in enumerate(posts)]
+        s.codes = [codes if live[b] else codes[:0] for b, (_, codes) in enumerate(posts)]
+        s.free = [int(b) for b in np.nonzero(~live)[0]]
+        n = meta.next_id
+        for b, ids in enumerate(s.ids):
+            if len(ids) and int(ids.max()) >= n:
+                raise RuntimeError(f"Index error: block {b} holds id {int(ids.max())} >= next_id {n}")
+        if meta.deleted.size and int(meta.deleted.max()) >= n:
+            raise RuntimeError(f"Index error: deleted id {int(meta.deleted.max())} >= next_id {n}")
+        raw = np.frombuffer(_read(f"{path}.vectors"), dtype="<f4")
+        if raw.size < n * d:
+            raise RuntimeError(f"Index error: vectors file holds {raw.size // max(d, 1)} rows, next_id {n}")
+        s.raw = raw[: n * d].reshape(n, d).astype(np.float32)
+        s.next_id, s.deleted, s.live = n, {int(i) for i in meta.deleted}, int(meta.live)
+        s.path = path
+        s._dirty = set(range(nb))
+        s._sync()
+        return s
+
+    def save(self, path=None):
+        """SPFresh::save (src/spfresh.rs:852-859): the four files SPFresh::open reads.
+
+        Live postings get consecutive centroid ids in a delta-only
+        IncrementalDiskANN (the layout the reference's centroid graph has
+        before any merge), whose graph is a Vamana graph over the centroids
+        built on the GPU (IncrementalConfig's delta parameters: degree 32,
+        beam 64, alpha 1.2, src/incremental.rs:31-43)."""
+        from . import formats as F
+
+        path = path or self.path
+        if path is None:
+            raise RuntimeError("Index error: no path to save to")
+        q = _quantizer_state(self)
+        cfg = F.SPFreshConfig(self.max_posting, self.min_posting, self.probe_ratio, self.rerank_size,
+                              self.reassign_neighbors, self.centroid_beam)
+        nb = len(self.live_b)
+        live_blocks = np.nonzero(self.live_b)[0]
+        cid = np.full(nb, F.SPF_FREE, dtype=np.uint64)
+        cid[live_blocks] = np.uint64(F.DELTA_ID_OFFSET) + np.arange(len(live_blocks), dtype=np.uint64)
+        cents = [self.cent[b].astype(np.float32) if self.live_b[b] else np.zeros(0, np.float32) for b in range(nb)]
+        meta = F.SPFreshMeta(self.dim, cfg, q, cid, cents, self.next_id,
+                             np.array(sorted(self.deleted), dtype=np.uint64), self.live)
+        block = F.spf_block_bytes(cfg, q, self.dim)
+        F._write(f"{path}.postings", F.postings_bytes(list(zip(self.ids, self.codes)), block, self.codec.size))
+        rows = np.zeros((max(self.next_id, 1024), self.dim), dtype="<f4")
+        rows[: self.next_id] = self.raw[: self.next_id]
+        F._write(f"{path}.vectors", rows.tobytes())
+        C_ = np.ascontiguousarray(self.cent[live_blocks], dtype=np.float32)
+        graph, ep = _centroid_graph(C_, self.metric_name, self.device)
+        F._write(f"{path}.centroids", F.incremental_bytes(C_.reshape(-1, self.dim), graph, ep, 32))
+        F._write(f"{path}.spf", F.spf_bytes(meta))
+        self.path = path
+
     # ------------------------------------------------------------ device side
     def host_arrays(self, nblocks=None):
         """Posting slots as the flat arrays of DgSpfreshDesc."""
@@ -653,3 +734,68 @@ class SPFresh:
         ids, ds, cnt = self.search_arrays(queries, k, n_probe)
         return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
 
+
+
+def _read(path):
+    try:
+        with open(path, "rb") as f:
+            return f.read()
+    except OSError as e:
+        raise RuntimeError(f"I/O error: {e}") from None
+
+
+def _codec_params(q):
+    """(codec kind, params) of a saved QuantizerState (None = raw f32 rows)."""
+    if q is None:
+        return None, {}
+    if q.kind == "pq":
+        return "pq", {"codebooks": q.codebooks.reshape(q.num_subspaces, q.num_centroids, q.subspace_dim)}
+    if q.kind == "int8":
+        return "int8", {"scale": q.scale, "offset": q.offset}
+    if q.kind == "rabitq":
+        return "rabitq", {"padded": q.padded, "signs": q.signs, "centroid": q.centroid}
+    return "f16", {}
+
+
+def _quantizer_state(s):
+    from . import formats as F
+
+    k, p = s.codec.kind, s.codec.p
+    if k is None:
+        return None
+    if k == "pq":
+        cb = np.asarray(p["codebooks"], dtype=np.float32)
+        M, K, ds = cb.shape
+        return F.QuantizerState("pq", s.dim, M, K, ds, codebooks=cb.reshape(-1))
+    if k == "int8":
+        return F.QuantizerState("int8", s.dim, scale=float(p["scale"]), offset=float(p["offset"]))
+    if k == "rabitq":
+        cen = p.get("centroid")
+        if cen is None:  # RaBitQ::train's centroid: the mean row (src/rabitq.rs:78-90)
+            cen = (s.raw[: s.next_id].astype(np.float64).sum(0) / max(s.next_id, 1)).astype(np.float32)
+        return F.QuantizerState("rabitq", s.dim, padded=int(p["padded"]), centroid=np.asarray(cen, np.float32),
+                                signs=np.asarray(p["signs"], dtype=np.float32))
+    return F.QuantizerState("f16", s.dim)
+
+
+def _centroid_graph(C_, metric, device):
+    """Adjacency lists (local indexes) and entry point over the live centroids."""
+    n = len(C_)
+    if n == 0:
+        return [], None
+    if n == 1:
+        return [[]], 0
+    if device is not None:
+        import pydiskann_b200 as dg
+
+        adj, med = dg.build_graph(C_, max_degree=min(32, n - 1), build_beam_width=64, alpha=1.2,
+                                  metric=metric, device=device)
+        return [row[row != _lib.PAD].tolist() for row in np.asarray(adj)], int(med)
+    # host-only instance: exact nearest-centroid lists
+    graph = []
+    for c0 in range(0, n, 1024):
+        D = _dist_matrix(_METRICS[metric], C_[c0:c0 + 1024], C_)
+        for i in range(len(D)):
+            D[i, c0 + i] = np.inf
+        graph += np.argsort(D, axis=1, kind="stable")[:, : min(32, n - 1)].tolist()
+    return graph, 0
