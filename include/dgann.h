@@ -129,6 +129,38 @@ DG_API DgStatus dg_index_attach_rabitq(DgIndex *idx, uint32_t padded, const floa
                                 const float *signs, const uint8_t *codes);
 /* FilteredDiskANN labels (src/filtered.rs:140-160): u64[n*num_fields]. */
 DG_API DgStatus dg_index_attach_labels(DgIndex *idx, uint32_t num_fields, const uint64_t *labels);
+/* Base + delta (incremental) search, IncrementalDiskANN (src/incremental.rs):
+ * the index holds the unified view's rows -- base rows, then delta rows, then
+ * spare capacity (unreachable until rows are written) -- with adjacency rows of
+ * max_degree slots (UnifiedView, :349-471).
+ *
+ * Entry points: ids[0] (the base medoid) and optionally ids[1] (base count +
+ * the delta layer's entry point), seeded as UnifiedView::entry_points
+ * (:383-392). */
+DG_API DgStatus dg_index_set_entry_points(DgIndex *idx, const uint32_t *ids, uint32_t n);
+/* Marks (deleted = 1) or clears unified ids in the tombstone bitmap; results
+ * skip marked ids (is_live, :463-470) and, while tombstone_count > 0, searches
+ * use tombstone_config (:505-516): expanded beam max(2L, k + min(count, L)),
+ * 2x iterations, early-termination factor 1.5.  tombstone_count is the size
+ * of the caller's tombstone set (which may hold ids the index does not have). */
+DG_API DgStatus dg_index_set_tombstones(DgIndex *idx, const uint32_t *ids, uint64_t n, int32_t deleted,
+                                        uint64_t tombstone_count);
+/* Overwrites rows [first, first + count): f32 vectors (dim each; BF16 / FP8
+ * copies are re-encoded), adjacency (max_degree each) and labels (num_fields
+ * each); a NULL pointer leaves that part unchanged.  Vectors of an index with
+ * quantized codes cannot be replaced (DG_ENOTSUP). */
+DG_API DgStatus dg_index_update_rows(DgIndex *idx, uint64_t first, uint64_t count, const float *vectors,
+                                     const uint32_t *adjacency, const uint64_t *labels);
+/* DeltaLayer::add_vectors (src/incremental.rs:114-166) on the host: inserts
+ * rows [n_old, n_old + n_new) of `vectors` ([n][dim] f32) into the delta graph
+ * `adjacency` ([n][max_degree] u32, DG_PAD padded, lists in the reference's
+ * order), each by greedy search from the entry point (beam max(2R, 16)),
+ * alpha-pruning (robust_prune, alpha 1.2, src/lib.rs:977-1034) and back-edges
+ * (pruned when a list is full); *entry_point (-1 = none) becomes the medoid
+ * of all rows (compute_medoid, :168-193) when more than one row exists. */
+DG_API DgStatus dg_delta_insert(const float *vectors, uint32_t dim, int32_t metric, uint32_t max_degree,
+                                uint32_t *adjacency, uint64_t n_old, uint64_t n_new, int64_t *entry_point);
+
 /* The attached quantizer's codes, n rows of code_size bytes in the layout the
  * QANN sidecar stores (QuantizedDiskANN::quantized_to_bytes, src/quantized.rs:
  * 490-509); out = NULL only reports code_size.  Lets a caller persist an index

@@ -95,6 +95,7 @@ def _declare(L):
         "dgo_build_vamana": (C.c_int, [vp, u64, u32, i32, u32, u32, f32, u64, u32, vp, i32]),
         "dgo_beam_search_table": (C.c_int, [vp, u32, vp, vp, vp, u32, u32, u32, i32, u32, u32, f32, vp, vp, vp]),
         "dgo_search_batch": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, vp, i32]),
+        "dgo_incremental_search_batch": (C.c_int, [vp, vp, vp, u32, vp, u64, vp, u32, vp, vp, vp, i32]),
         "dgo_filter_matches": (C.c_int, [vp, u32, vp, vp, u32]),
         "dgo_pq_encode": (None, [vp, u64, u32, u32, u32, vp, vp, i32]),
         "dgo_pq_lut": (None, [vp, u32, u32, u32, vp, vp]),
@@ -272,6 +273,28 @@ class OracleIndex:
                                _p(cnt), _p(st), threads)
         if with_stats:
             return ids, ds, cnt, st
+        return ids, ds, cnt
+
+    def incremental_search(self, Q, k, L, seeds, dead=None, ntomb=0, filter_ops=None, filter_pool=(),
+                           threads=0):
+        """IncrementalDiskANN search over this unified view (base rows, then delta
+        rows): `seeds` entry points, `dead` a bool per row, `ntomb` the tombstone count."""
+        Q = _f32(Q).reshape(-1, self.s.d)
+        nq = Q.shape[0]
+        p = SearchParams()
+        p.k, p.beam_width = k, L
+        keep = []
+        if filter_ops:
+            arr, n, pool = filter_program(filter_ops, filter_pool)
+            keep += [arr, pool]
+            p.filter, p.filter_nops, p.filter_pool = C.cast(arr, C.c_void_p), n, _p(pool)
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        dd = None if dead is None else np.ascontiguousarray(dead, dtype=np.uint8)
+        ids = np.zeros((nq, k), dtype=np.uint32)
+        ds = np.zeros((nq, k), dtype=np.float32)
+        cnt = np.zeros(nq, dtype=np.uint32)
+        lib().dgo_incremental_search_batch(C.byref(self.s), C.byref(p), _p(sd), len(sd), _p(dd), int(ntomb),
+                                           _p(Q), nq, _p(ids), _p(ds), _p(cnt), threads)
         return ids, ds, cnt
 
 

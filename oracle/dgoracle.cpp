@@ -887,6 +887,47 @@ int dgo_search_batch(const DgoIndex *idx, const DgoSearchParams *p, const float 
   return 0;
 }
 
+int dgo_incremental_search_batch(const DgoIndex *idx, const DgoSearchParams *p, const uint32_t *seeds,
+                                 uint32_t nseeds, const uint8_t *dead, uint64_t ntomb, const float *Q,
+                                 uint32_t nq, uint32_t *out_ids, float *out_d, uint32_t *out_cnt,
+                                 int32_t nthreads) {
+  const DgoIndex &I = *idx;
+  const uint32_t k = p->k, L = p->beam_width;
+  const bool labeled = p->filter_nops > 0;
+  BeamCfg cfg;
+  if (labeled) {  // search_filtered_with_dists (src/incremental.rs:1048-1062)
+    cfg.filtered = true;
+    cfg.expanded = std::max(L * 4, k * 10);
+    cfg.max_iter = (uint64_t)cfg.expanded * 2;
+    cfg.early = 1.5f;
+  } else if (ntomb > 0) {  // tombstone_config (src/incremental.rs:505-516)
+    cfg.filtered = true;
+    cfg.expanded = std::max<uint64_t>((uint64_t)L * 2, k + std::min<uint64_t>(ntomb, L));
+    cfg.max_iter = (uint64_t)cfg.expanded * 2;
+    cfg.early = 1.5f;
+  }
+  const int nt = nthreads_of(nthreads);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+  for (int64_t qi = 0; qi < (int64_t)nq; ++qi) {
+    const float *q = Q + (uint64_t)qi * I.d;
+    // UnifiedView::is_live (:463-470), and the label filter when one is given
+    auto allow = [&](uint32_t id) -> bool {
+      if (id >= I.n || (dead && dead[id])) return false;
+      return !labeled || filter_eval(p->filter, p->filter_nops, p->filter_pool,
+                                     I.labels + (uint64_t)id * I.num_fields, I.num_fields);
+    };
+    auto dist = [&](uint32_t id) { return metric_eval(I.metric, q, I.vectors + (uint64_t)id * I.d, I.d); };
+    std::vector<Cand> out;
+    if (nseeds) beam_search(seeds, nseeds, L, k, dist, AdjNbrs{I.adjacency, I.R}, allow, cfg, out, nullptr);
+    for (uint32_t j = 0; j < k; ++j) {
+      out_ids[qi * k + j] = j < out.size() ? out[j].id : DGO_PAD;
+      out_d[qi * k + j] = j < out.size() ? out[j].d : kInf;
+    }
+    out_cnt[qi] = (uint32_t)std::min<size_t>(out.size(), k);
+  }
+  return 0;
+}
+
 int dgo_filter_matches(const DgoFilterOp *prog, uint32_t nops, const uint64_t *pool,
                        const uint64_t *labels, uint32_t num_fields) {
   return filter_eval(prog, nops, pool, labels, num_fields) ? 1 : 0;

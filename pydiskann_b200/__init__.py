@@ -32,7 +32,8 @@ from . import formats as _fmt
 from ._lib import PAD, DgError, check, lib, ptr  # noqa: F401  (DgError is public)
 
 __all__ = [
-    "DiskANN", "QuantizedDiskANN", "FilteredDiskANN", "SPFresh", "Filter", "build_graph", "medoid",
+    "DiskANN", "QuantizedDiskANN", "FilteredDiskANN", "IncrementalDiskANN", "SPFresh", "Filter", "build_graph",
+    "medoid",
     "pq_train", "pq_encode", "exact_knn", "read_fvecs", "write_fvecs", "read_ivecs",
 ]
 
@@ -781,4 +782,5 @@ def write_fvecs(path, vectors):
 
 
 from .spfresh import SPFresh  # noqa: E402  (uses the helpers above)
+from .incremental import IncrementalDiskANN  # noqa: E402
 from .serve import Server, poisson_arrivals  # noqa: E402

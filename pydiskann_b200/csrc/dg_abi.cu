@@ -316,6 +316,75 @@ DgStatus dg_index_attach_labels(DgIndex *idx, uint32_t num_fields, const uint64_
   return DG_OK;
 }
 
+DgStatus dg_index_set_entry_points(DgIndex *idx, const uint32_t *ids, uint32_t n) {
+  if (!idx || !ids) return fail(DG_EINVAL, "null argument");
+  if (n < 1 || n > 2) return fail(DG_EINVAL, "one or two entry points");
+  for (uint32_t i = 0; i < n; ++i)
+    if (ids[i] >= idx->n) return fail(DG_EINVAL, "entry point " + std::to_string(ids[i]) + " out of range");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  idx->medoid = ids[0];
+  idx->seed2 = n == 2 ? ids[1] : DG_PAD;
+  return DG_OK;
+}
+
+DgStatus dg_index_set_tombstones(DgIndex *idx, const uint32_t *ids, uint64_t n, int32_t deleted,
+                                 uint64_t tombstone_count) {
+  if (!idx || (!ids && n)) return fail(DG_EINVAL, "null argument");
+  for (uint64_t i = 0; i < n; ++i)
+    if (ids[i] >= idx->n) return fail(DG_EINVAL, "tombstone id " + std::to_string(ids[i]) + " out of range");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  const size_t words = (idx->n + 31) / 32;
+  if (!idx->tomb) {
+    DgStatus s = dev_alloc(idx, (void **)&idx->tomb, words * 4);
+    if (s != DG_OK) return s;
+    idx->tomb_host.assign(words, 0u);
+  }
+  for (uint64_t i = 0; i < n; ++i) {
+    const uint32_t bit = 1u << (ids[i] & 31);
+    if (deleted) idx->tomb_host[ids[i] >> 5] |= bit;
+    else idx->tomb_host[ids[i] >> 5] &= ~bit;
+  }
+  idx->ntomb = tombstone_count;
+  DG_CUDA(cudaMemcpyAsync(idx->tomb, idx->tomb_host.data(), words * 4, cudaMemcpyHostToDevice, idx->stream));
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
+DgStatus dg_index_update_rows(DgIndex *idx, uint64_t first, uint64_t count, const float *vectors,
+                              const uint32_t *adjacency, const uint64_t *labels) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  if (first > idx->n || count > idx->n - first) return fail(DG_EINVAL, "rows out of range");
+  if (vectors && idx->quant != DG_Q_NONE)
+    return fail(DG_ENOTSUP, "rows of an index with quantized codes cannot be replaced");
+  if (labels && !idx->labels) return fail(DG_EINVAL, "the index has no labels");
+  if (adjacency)
+    for (uint64_t i = 0; i < count * idx->R; ++i)
+      if (adjacency[i] != DG_PAD && adjacency[i] >= idx->n)
+        return fail(DG_EINVAL, "neighbour id " + std::to_string(adjacency[i]) + " out of range");
+  if (!count) return DG_OK;
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  DgStatus s;
+  if (vectors) {
+    float *rows = idx->vec + first * idx->dpad;
+    if ((s = upload_rows_f32(vectors, count, idx->d, idx->dpad, rows, idx->stream)) != DG_OK) return s;
+    if (idx->bf16 && (s = encode_bf16_device(rows, count, idx->dpad, idx->bf16 + first * idx->dpad, idx->stream)) != DG_OK)
+      return s;
+    if (idx->fp8 && (s = encode_fp8_device(rows, count, idx->d, idx->dpad, idx->fp8 + first * idx->dpad,
+                                           idx->fp8_sn + first, idx->stream)) != DG_OK)
+      return s;
+  }
+  if (adjacency)
+    DG_CUDA(cudaMemcpyAsync(idx->adj + first * idx->R, adjacency, count * idx->R * 4, cudaMemcpyHostToDevice,
+                            idx->stream));
+  if (labels)
+    DG_CUDA(cudaMemcpyAsync(idx->labels + first * idx->nf, labels, count * idx->nf * 8, cudaMemcpyHostToDevice,
+                            idx->stream));
+  DG_CUDA(cudaStreamSynchronize(idx->stream));
+  return DG_OK;
+}
+
 DgStatus dg_index_get_codes(DgIndex *idx, uint8_t *out, uint64_t out_len, uint32_t *code_size) {
   if (!idx) return fail(DG_EINVAL, "null index");
   std::lock_guard<std::mutex> lk(idx->mu);
@@ -328,6 +397,29 @@ DgStatus dg_index_get_codes(DgIndex *idx, uint8_t *out, uint64_t out_len, uint32
                             cudaMemcpyDeviceToHost, idx->stream));
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
+}
+
+// Working-set entries a search needs (the kernel sizes w from the same rules)
+// and whether it runs the filtered kernel: label filters (src/filtered.rs:35-56)
+// or the tombstones of a base + delta index (tombstone_config,
+// src/incremental.rs:505-516).  A second entry point keeps w at two or more.
+static uint64_t working_need(const DgIndex *idx, uint32_t maxL, uint32_t k, uint32_t search_k, bool any_filter,
+                             bool *filt) {
+  const bool tombed = idx->tomb && idx->ntomb > 0;
+  uint64_t need = maxL;
+  if (any_filter) need = std::max<uint64_t>({(uint64_t)maxL * 4, (uint64_t)k * 10, search_k});
+  else if (tombed)
+    need = std::max<uint64_t>({(uint64_t)maxL * 2, search_k + std::min<uint64_t>(idx->ntomb, maxL), search_k});
+  if (idx->seed2 != DG_PAD) need = std::max<uint64_t>(need, 2);
+  *filt = any_filter || tombed;
+  return need;
+}
+
+static void index_state(const DgIndex *idx, SearchArgs &a) {
+  a.seed2 = idx->seed2;
+  const bool tombed = idx->tomb && idx->ntomb > 0;
+  a.tomb = tombed ? idx->tomb : nullptr;
+  a.ntomb = tombed ? (uint32_t)std::min<uint64_t>(idx->ntomb, 0xffffffffu) : 0;
 }
 
 // Stack depth a postfix program needs; -1 if it is malformed.
@@ -454,11 +546,11 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   if (any_filter && !idx->labels) return fail(DG_EINVAL, "filtered search needs attached labels");
   const bool reranked = trav != TRAV_F32 && p->rerank_size > 0;
   const uint32_t search_k = reranked ? std::max(p->rerank_size, p->k) : p->k;
-  uint64_t need = maxL;
-  if (any_filter) need = std::max<uint64_t>({(uint64_t)maxL * 4, (uint64_t)p->k * 10, search_k});
+  bool filt = false;
+  const uint64_t need = working_need(idx, maxL, p->k, search_k, any_filter, &filt);
   int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
   if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
-  if (reranked && !any_filter && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
+  if (reranked && !filt && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
   // visited table: 2^hbits words of two 16-bit tags (about 3 tags per
   // visited node at these beams); DG_HBITS overrides for tuning
   uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
@@ -480,6 +572,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   a.dpad = idx->dpad;
   a.R = idx->R;
   a.medoid = idx->medoid;
+  index_state(idx, a);
   a.metric = idx->metric;
   a.vec_f32 = idx->vec;
   a.vec_bf16 = idx->bf16;
@@ -556,19 +649,19 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   if (trav == TRAV_F32) lpr = 8;
   else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
-  const WarpLayout Ly = warp_layout(trav, lcap, any_filter, hbits, idx->dpad, idx->pq_M, idx->pq_K,
+  const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded, trav == TRAV_RABITQ && met_kind(idx->metric) != MET_L2);
   auto launch = [&](const SearchArgs &aa, cudaStream_t ss) -> DgStatus {
     LaunchInfo info;
     DG_CUDA(cudaMemsetAsync(aa.counter, 0, 4, ss));
     switch (trav) {
-      case TRAV_F32: return launch_search_f32(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
-      case TRAV_BF16: return launch_search_bf16(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
-      case TRAV_F16: return launch_search_f16(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
-      case TRAV_INT8: return launch_search_int8(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
-      case TRAV_PQ: return launch_search_pq(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
-      case TRAV_FP8: return launch_search_fp8(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
-      default: return launch_search_rabitq(aa, Ly, met, lpr, lcap, any_filter, ss, &info);
+      case TRAV_F32: return launch_search_f32(aa, Ly, met, lpr, lcap, filt, ss, &info);
+      case TRAV_BF16: return launch_search_bf16(aa, Ly, met, lpr, lcap, filt, ss, &info);
+      case TRAV_F16: return launch_search_f16(aa, Ly, met, lpr, lcap, filt, ss, &info);
+      case TRAV_INT8: return launch_search_int8(aa, Ly, met, lpr, lcap, filt, ss, &info);
+      case TRAV_PQ: return launch_search_pq(aa, Ly, met, lpr, lcap, filt, ss, &info);
+      case TRAV_FP8: return launch_search_fp8(aa, Ly, met, lpr, lcap, filt, ss, &info);
+      default: return launch_search_rabitq(aa, Ly, met, lpr, lcap, filt, ss, &info);
     }
   };
   if (chunks > 1) {
@@ -762,11 +855,11 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   if (any_filter && !idx->labels) return fail(DG_EINVAL, "filtered search needs attached labels");
   const bool reranked = trav != TRAV_F32 && p->rerank_size > 0;
   const uint32_t search_k = reranked ? std::max(p->rerank_size, p->k) : p->k;
-  uint64_t need = maxL;
-  if (any_filter) need = std::max<uint64_t>({(uint64_t)maxL * 4, (uint64_t)p->k * 10, search_k});
+  bool filt = false;
+  const uint64_t need = working_need(idx, maxL, p->k, search_k, any_filter, &filt);
   const int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
   if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
-  if (reranked && !any_filter && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
+  if (reranked && !filt && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
   uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
   uint32_t hB = 1;
   while (hB < 32 && (1ull << hB) < idx->n) ++hB;
@@ -796,6 +889,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   a.dpad = idx->dpad;
   a.R = idx->R;
   a.medoid = idx->medoid;
+  index_state(idx, a);
   a.metric = idx->metric;
   a.vec_f32 = idx->vec;
   a.vec_bf16 = idx->bf16;
@@ -855,16 +949,16 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   if (trav == TRAV_F32) lpr = 8;
   else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
-  const WarpLayout Ly = warp_layout(trav, lcap, any_filter, hbits, idx->dpad, idx->pq_M, idx->pq_K,
+  const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded, trav == TRAV_RABITQ && met_kind(idx->metric) != MET_L2);
   LaunchInfo info;
   switch (trav) {
-    case TRAV_F32: return launch_search_f32(a, Ly, met, lpr, lcap, any_filter, st, &info);
-    case TRAV_BF16: return launch_search_bf16(a, Ly, met, lpr, lcap, any_filter, st, &info);
-    case TRAV_F16: return launch_search_f16(a, Ly, met, lpr, lcap, any_filter, st, &info);
-    case TRAV_INT8: return launch_search_int8(a, Ly, met, lpr, lcap, any_filter, st, &info);
-    case TRAV_PQ: return launch_search_pq(a, Ly, met, lpr, lcap, any_filter, st, &info);
-    case TRAV_FP8: return launch_search_fp8(a, Ly, met, lpr, lcap, any_filter, st, &info);
-    default: return launch_search_rabitq(a, Ly, met, lpr, lcap, any_filter, st, &info);
+    case TRAV_F32: return launch_search_f32(a, Ly, met, lpr, lcap, filt, st, &info);
+    case TRAV_BF16: return launch_search_bf16(a, Ly, met, lpr, lcap, filt, st, &info);
+    case TRAV_F16: return launch_search_f16(a, Ly, met, lpr, lcap, filt, st, &info);
+    case TRAV_INT8: return launch_search_int8(a, Ly, met, lpr, lcap, filt, st, &info);
+    case TRAV_PQ: return launch_search_pq(a, Ly, met, lpr, lcap, filt, st, &info);
+    case TRAV_FP8: return launch_search_fp8(a, Ly, met, lpr, lcap, filt, st, &info);
+    default: return launch_search_rabitq(a, Ly, met, lpr, lcap, filt, st, &info);
   }
 }

@@ -30,6 +30,11 @@ struct DgIndex {
   float *dnorm2 = nullptr;    // [n] |decode(code)|^2 (cosine over PQ / RaBitQ codes)
   uint64_t *labels = nullptr; // [n][nf]
   uint32_t nf = 0;
+  // base + delta (incremental) search state
+  uint32_t seed2 = DG_PAD;             // second entry point, DG_PAD = none
+  uint32_t *tomb = nullptr;            // [ceil(n/32)] deleted-id bitmap (device)
+  std::vector<uint32_t> tomb_host;     // its host copy
+  uint64_t ntomb = 0;                  // tombstone count the search config uses
   cudaStream_t stream = nullptr;
   uint64_t hbm_budget = 0, hbm_used = 0;
   std::mutex mu;

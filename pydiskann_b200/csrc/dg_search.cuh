@@ -50,6 +50,10 @@ struct SearchArgs {
   const float *rq_centroid;  // [d]
   const float *rq_signs;     // [3][padded]
   const float *dnorm2;       // [n] squared norms of the decoded codes (cosine over PQ / RaBitQ)
+  // base + delta (incremental) search: a second entry point and deleted ids
+  uint32_t seed2;            // DG_PAD = one seed (the medoid)
+  const uint32_t *tomb;      // [ceil(n/32)] deleted-id bitmap, null = no tombstones
+  uint32_t ntomb;            // tombstone count the search config uses (> 0 when tomb is set)
   // labels / filter
   const uint64_t *labels;
   uint32_t nf;

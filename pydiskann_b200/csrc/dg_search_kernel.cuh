@@ -288,7 +288,9 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
   uint32_t *stage = reinterpret_cast<uint32_t *>(wsm + Ly.stage);
   const Visited vt{reinterpret_cast<uint32_t *>(wsm + Ly.hash), a.hbits, a.hB};
   float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
-  const int L = (int)(a.perL ? a.perL[q] : a.L);
+  const bool two = a.seed2 != DG_PAD && a.seed2 != a.medoid;
+  // both seeds enter w unconditionally (src/lib.rs:218-229), so w holds at least two
+  const int L = max((int)(a.perL ? a.perL[q] : a.L), two ? 2 : 1);
   const uint32_t k = a.k;
   const bool use_rerank = TRAV != TRAV_F32 && a.rerank > 0;
   const uint32_t search_k = use_rerank ? max(a.rerank, k) : k;
@@ -312,6 +314,20 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
       w0 = make_key(d, cand);
       vt.test_and_set(cand);
     }
+    __syncwarp();
+  }
+  if (two) {  // the delta layer's entry point (UnifiedView::entry_points, src/incremental.rs:383-392)
+    const uint32_t cand = a.seed2;
+    float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, 1, lane, qq);
+    d = __shfl_sync(kFull, d, 0);
+    const uint64_t key = make_key(d, cand), first = shfl64(w0, 0);
+    if (lane == 0) {
+      vt.test_and_set(cand);
+      w0 = key < first ? key : first;
+    }
+    if (lane == 1) w0 = key < first ? first : key;
+    wsize = 2;
+    n_dist = 2;
     __syncwarp();
   }
   while (true) {
@@ -397,12 +413,19 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     qc.fops = a.fops + a.foffs[q];
     qc.fnops = a.foffs[q + 1] - a.foffs[q];
   }
-  const bool filtered = FILT && qc.fnops > 0;
+  const bool labeled = FILT && qc.fnops > 0;
+  const bool tombed = FILT && a.tomb != nullptr;
+  const bool filtered = labeled || tombed;
   uint32_t working = L, max_iter = 0xffffffffu;
-  if (filtered) {  // src/filtered.rs:35-56
+  if (labeled) {  // src/filtered.rs:35-56, src/incremental.rs:1048-1062
     working = max(L * 4, k * 10);
     max_iter = working * 2;
+  } else if (tombed) {  // tombstone_config (src/incremental.rs:505-516)
+    working = max(L * 2, search_k + min(a.ntomb, L));
+    max_iter = working * 2;
   }
+  const bool two = a.seed2 != DG_PAD && a.seed2 != a.medoid;
+  if (two) working = max(working, 2u);  // both seeds enter w (src/lib.rs:218-229)
 
   // ---- query into shared memory (zero padded), norms, visited table
   const float *qg = a.Q + (size_t)q * a.d;
@@ -414,13 +437,26 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
   prepare_query<TRAV, MET>(a, wsm, Ly, qs, lane);
 
   const uint64_t *labels = a.labels;
+  // a result must be live (UnifiedView::is_live, src/incremental.rs:463-470) and match
   auto allow = [&](uint32_t id) -> bool {
-    return filter_eval(qc.fops, qc.fnops, a.fpool, labels + (size_t)id * a.nf, a.nf);
+    if (a.tomb && ((__ldg(a.tomb + (id >> 5)) >> (id & 31)) & 1u)) return false;
+    return !labeled || filter_eval(qc.fops, qc.fnops, a.fpool, labels + (size_t)id * a.nf, a.nf);
   };
 
   // ---- seed: the medoid (DiskANN::search_with_dists seeds [medoid])
   int cur = 0, wsize = 0, rsize = 0;
   uint32_t n_exp = 0, n_dist = 0;
+  // merges this lane's match key (kKeyInvalid = none) into the result list
+  auto add_results = [&](uint64_t mk) {
+    const int nm = prepare_batch(mk, RES, rsize, (int)search_k, cst, lane);
+    if (nm > 0) {
+      // merge in place through the non-current w buffer as scratch
+      uint64_t *tmp = W[cur ^ 1];
+      rsize = merge_keys(RES, rsize, tmp, (int)search_k, cst, nm, lane);
+      for (int i = lane; i < rsize; i += 32) RES[i] = tmp[i];
+      __syncwarp();
+    }
+  };
   {
     const uint32_t cand = a.medoid;
     float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, 1, lane, qq);
@@ -434,6 +470,17 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     if (filtered) rsize = __shfl_sync(kFull, (lane == 0 && allow(cand)) ? 1 : 0, 0);
     n_dist = 1;
     __syncwarp();
+  }
+  if (two) {  // the delta layer's entry point (UnifiedView::entry_points, src/incremental.rs:383-392)
+    const uint32_t cand = a.seed2;
+    float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, 1, lane, qq);
+    d = __shfl_sync(kFull, d, 0);
+    const uint64_t key = lane == 0 ? make_key(d, cand) : kKeyInvalid;
+    if (lane == 0) vt.test_and_set(cand);
+    __syncwarp();
+    insert_batch(key, W, cur, wsize, (int)working, cst, lane);
+    if (filtered) add_results((lane == 0 && allow(cand)) ? key : kKeyInvalid);
+    n_dist = 2;
   }
 
   while (true) {
@@ -487,18 +534,8 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
       bool match = false;
       if (filtered && lane < cnt) match = allow(cand);
       insert_batch(key, W, cur, wsize, (int)working, cst, lane);
-      if (filtered) {
-        // result list: every visited match, kept as the search_k smallest
-        uint64_t mk = (lane < cnt && match) ? make_key(d, cand) : kKeyInvalid;
-        const int nm = prepare_batch(mk, RES, rsize, (int)search_k, cst, lane);
-        if (nm > 0) {
-          // merge in place through the non-current w buffer as scratch
-          uint64_t *tmp = W[cur ^ 1];
-          rsize = merge_keys(RES, rsize, tmp, (int)search_k, cst, nm, lane);
-          for (int i = lane; i < rsize; i += 32) RES[i] = tmp[i];
-          __syncwarp();
-        }
-      }
+      // result list: every visited match, kept as the search_k smallest
+      if (filtered) add_results((lane < cnt && match) ? make_key(d, cand) : kKeyInvalid);
     }
   }
 

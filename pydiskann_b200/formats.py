@@ -602,20 +602,92 @@ def postings_bytes(blocks, block: int, code_size: int) -> bytes:
     return out.tobytes()
 
 
-def incremental_bytes(vectors, graph, entry_point, max_degree, tombstones=()) -> bytes:
-    """IncrementalDiskANN::to_bytes (src/incremental.rs:1234-1327) of an index
-    with no base layer, labels or quantizer: the delta rows, their adjacency
-    lists (local indexes), entry point (-1 = none), max degree, tombstones."""
+def incremental_bytes(vectors, graph, entry_point, max_degree, tombstones=(), base=None, labels=None,
+                      dim=None) -> bytes:
+    """IncrementalDiskANN::to_bytes (src/incremental.rs:1234-1327) without a
+    quantizer section: the base core bytes (or none), the delta rows, their
+    adjacency lists (local indexes), entry point (-1 = none), max degree,
+    tombstones, and labels as (num_fields, base_labels, delta_labels) or None."""
     V = np.ascontiguousarray(vectors, dtype="<f4")
-    parts = [struct.pack("<IIBQQ", INCR_MAGIC, INCR_FORMAT_VERSION, 0, V.shape[1], V.shape[0]), V.tobytes(),
-             struct.pack("<Q", len(graph))]
+    d = V.shape[1] if V.ndim == 2 and V.shape[1] else int(dim or 0)
+    V = V.reshape(-1, d) if d else V.reshape(0, 0)
+    parts = [struct.pack("<II", INCR_MAGIC, INCR_FORMAT_VERSION)]
+    parts += [b"\x00"] if base is None else [b"\x01", struct.pack("<Q", len(base)), bytes(base)]
+    parts += [struct.pack("<QQ", d, V.shape[0]), V.tobytes(), struct.pack("<Q", len(graph))]
     for nb in graph:
         a = np.asarray(nb, dtype="<u4")
         parts += [struct.pack("<I", a.size), a.tobytes()]
     ts = np.asarray(list(tombstones), dtype="<u8")
-    parts += [struct.pack("<qQQ", -1 if entry_point is None else int(entry_point), max_degree, ts.size), ts.tobytes(),
-              b"\x00\x00"]
+    parts += [struct.pack("<qQQ", -1 if entry_point is None else int(entry_point), max_degree, ts.size), ts.tobytes()]
+    if labels is None:
+        parts.append(b"\x00")
+    else:
+        nf, bl, dl = labels
+        bl = np.ascontiguousarray(bl, dtype="<u8").reshape(-1, nf) if nf else np.zeros((len(bl), 0), "<u8")
+        dl = np.ascontiguousarray(dl, dtype="<u8").reshape(-1, nf) if nf else np.zeros((len(dl), 0), "<u8")
+        parts += [b"\x01", struct.pack("<QQ", nf, len(bl)), bl.tobytes(), struct.pack("<Q", len(dl)), dl.tobytes()]
+    parts.append(b"\x00")  # no quantizer
     return b"".join(parts)
+
+
+def parse_incremental(buf) -> dict:
+    """IncrementalDiskANN::from_bytes_v1 (src/incremental.rs:1451-1611): base
+    bytes (or None), dim, delta vectors f32[n, dim], adjacency lists, entry
+    point, max degree, tombstones, labels as (num_fields, base, delta) or None.
+    The older layout without the magic and a quantizer section are refused."""
+    b = memoryview(buf).cast("B")
+    r = _Reader(b)
+
+    def trunc(fn):
+        try:
+            return fn()
+        except RuntimeError:
+            raise _index_error("Incremental buffer truncated") from None
+
+    if len(b) < 4:
+        raise _index_error("Incremental buffer too small")
+    if struct.unpack_from("<I", b, 0)[0] != INCR_MAGIC:
+        raise _index_error("incremental buffers without the INCR magic (the older layout) are not supported")
+    r.u32()
+    ver = trunc(r.u32)
+    if ver != INCR_FORMAT_VERSION:
+        raise _index_error(f"Unsupported incremental format version: {ver}")
+    base = None
+    if trunc(r.u8) == 1:
+        n = trunc(r.u64)
+        s = trunc(lambda: r._take(n))
+        base = b[s:s + n]
+    dim = trunc(r.u64)
+    nd = trunc(r.u64)
+    s = trunc(lambda: r._take(nd * dim * 4))
+    V = np.frombuffer(b, dtype="<f4", count=nd * dim, offset=s).reshape(nd, dim).astype(np.float32)
+    ng = trunc(r.u64)
+    graph = []
+    for _ in range(ng):
+        deg = trunc(r.u32)
+        s = trunc(lambda: r._take(deg * 4))
+        graph.append(np.frombuffer(b, dtype="<u4", count=deg, offset=s).astype(np.uint32).tolist())
+    ep = struct.unpack("<q", bytes(b[trunc(lambda: r._take(8)):][:8]))[0]
+    max_degree = trunc(r.u64)
+    nt = trunc(r.u64)
+    s = trunc(lambda: r._take(nt * 8))
+    tomb = np.frombuffer(b, dtype="<u8", count=nt, offset=s).astype(np.uint64).tolist()
+    labels = None
+    if trunc(r.u8) == 1:
+        nf = trunc(r.u64)
+        nbl = trunc(r.u64)
+        s = trunc(lambda: r._take(nbl * nf * 8))
+        bl = np.frombuffer(b, dtype="<u8", count=nbl * nf, offset=s).reshape(nbl, nf).astype(np.uint64)
+        ndl = trunc(r.u64)
+        s = trunc(lambda: r._take(ndl * nf * 8))
+        dl = np.frombuffer(b, dtype="<u8", count=ndl * nf, offset=s).reshape(ndl, nf).astype(np.uint64)
+        labels = (nf, bl, dl)
+    if trunc(r.u8) == 1:
+        raise _index_error("incremental indexes with a quantizer section are not supported")
+    if len(graph) != nd:
+        raise _index_error(f"{len(graph)} adjacency lists for {nd} delta vectors")
+    return {"base": base, "dim": dim, "vectors": V, "graph": graph, "entry_point": None if ep < 0 else ep,
+            "max_degree": max_degree, "tombstones": tomb, "labels": labels}
 
 
 def check_incremental_header(buf):
