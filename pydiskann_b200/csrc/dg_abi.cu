@@ -402,7 +402,7 @@ DgStatus dg_index_get_codes(DgIndex *idx, uint8_t *out, uint64_t out_len, uint32
 // Working-set entries a search needs (the kernel sizes w from the same rules)
 // and whether it runs the filtered kernel: label filters (src/filtered.rs:35-56)
 // or the tombstones of a base + delta index (tombstone_config,
-// src/incremental.rs:505-516).  A second entry point keeps w at two or more.
+// src/incremental.rs:505-516).
 static uint64_t working_need(const DgIndex *idx, uint32_t maxL, uint32_t k, uint32_t search_k, bool any_filter,
                              bool *filt) {
   const bool tombed = idx->tomb && idx->ntomb > 0;
@@ -410,7 +410,9 @@ static uint64_t working_need(const DgIndex *idx, uint32_t maxL, uint32_t k, uint
   if (any_filter) need = std::max<uint64_t>({(uint64_t)maxL * 4, (uint64_t)k * 10, search_k});
   else if (tombed)
     need = std::max<uint64_t>({(uint64_t)maxL * 2, search_k + std::min<uint64_t>(idx->ntomb, maxL), search_k});
-  if (idx->seed2 != DG_PAD) need = std::max<uint64_t>(need, 2);
+  // two entry points run in the general kernel (the 64-entry register-list
+  // kernel seeds the medoid only), which a capacity above 64 selects
+  if (idx->seed2 != DG_PAD) need = std::max<uint64_t>(need, 65);
   *filt = any_filter || tombed;
   return need;
 }

@@ -288,9 +288,7 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
   uint32_t *stage = reinterpret_cast<uint32_t *>(wsm + Ly.stage);
   const Visited vt{reinterpret_cast<uint32_t *>(wsm + Ly.hash), a.hbits, a.hB};
   float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
-  const bool two = a.seed2 != DG_PAD && a.seed2 != a.medoid;
-  // both seeds enter w unconditionally (src/lib.rs:218-229), so w holds at least two
-  const int L = max((int)(a.perL ? a.perL[q] : a.L), two ? 2 : 1);
+  const int L = (int)(a.perL ? a.perL[q] : a.L);
   const uint32_t k = a.k;
   const bool use_rerank = TRAV != TRAV_F32 && a.rerank > 0;
   const uint32_t search_k = use_rerank ? max(a.rerank, k) : k;
@@ -314,20 +312,6 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
       w0 = make_key(d, cand);
       vt.test_and_set(cand);
     }
-    __syncwarp();
-  }
-  if (two) {  // the delta layer's entry point (UnifiedView::entry_points, src/incremental.rs:383-392)
-    const uint32_t cand = a.seed2;
-    float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, 1, lane, qq);
-    d = __shfl_sync(kFull, d, 0);
-    const uint64_t key = make_key(d, cand), first = shfl64(w0, 0);
-    if (lane == 0) {
-      vt.test_and_set(cand);
-      w0 = key < first ? key : first;
-    }
-    if (lane == 1) w0 = key < first ? first : key;
-    wsize = 2;
-    n_dist = 2;
     __syncwarp();
   }
   while (true) {
@@ -457,33 +441,35 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
       __syncwarp();
     }
   };
-  {
-    const uint32_t cand = a.medoid;
-    float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, 1, lane, qq);
-    d = __shfl_sync(kFull, d, 0);
-    if (lane == 0) {
-      W[0][0] = make_key(d, cand);
-      vt.test_and_set(cand);
-      if (filtered && allow(cand)) RES[0] = make_key(d, cand);
+  // ---- seeds: the medoid, and the delta layer's entry point of a base +
+  // delta index (UnifiedView::entry_points, src/incremental.rs:383-392).  They
+  // are the first staged batch the loop merges (src/lib.rs:218-233).
+  int ns = two ? 2 : 1;
+  if (lane == 0) {
+    stage[0] = a.medoid;
+    vt.test_and_set(a.medoid);
+    if (two) {
+      stage[1] = a.seed2;
+      vt.test_and_set(a.seed2);
     }
-    wsize = 1;
-    if (filtered) rsize = __shfl_sync(kFull, (lane == 0 && allow(cand)) ? 1 : 0, 0);
-    n_dist = 1;
-    __syncwarp();
   }
-  if (two) {  // the delta layer's entry point (UnifiedView::entry_points, src/incremental.rs:383-392)
-    const uint32_t cand = a.seed2;
-    float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, 1, lane, qq);
-    d = __shfl_sync(kFull, d, 0);
-    const uint64_t key = lane == 0 ? make_key(d, cand) : kKeyInvalid;
-    if (lane == 0) vt.test_and_set(cand);
-    __syncwarp();
-    insert_batch(key, W, cur, wsize, (int)working, cst, lane);
-    if (filtered) add_results((lane == 0 && allow(cand)) ? key : kKeyInvalid);
-    n_dist = 2;
-  }
+  __syncwarp();
 
   while (true) {
+    n_dist += ns;
+    // ---- distances and merge, 32 candidates at a time
+    for (int g0 = 0; g0 < ns; g0 += 32) {
+      const int cnt = min(32, ns - g0);
+      const uint32_t cand = lane < cnt ? stage[g0 + lane] : DG_PAD;
+      const float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, cnt, lane, qq);
+      uint64_t key = lane < cnt ? make_key(d, cand) : kKeyInvalid;
+      bool match = false;
+      if (filtered && lane < cnt) match = allow(cand);
+      insert_batch(key, W, cur, wsize, (int)working, cst, lane);
+      // result list: every visited match, kept as the search_k smallest
+      if (filtered) add_results((lane < cnt && match) ? make_key(d, cand) : kKeyInvalid);
+    }
+
     // first unexpanded entry of w (the frontier minimum)
     int idx = -1;
     for (int base = 0; base < wsize; base += 32) {
@@ -512,7 +498,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     // ---- stage unvisited neighbours
     const uint32_t node = key_id(best);
     const uint32_t *row = a.adj + (size_t)node * a.R;
-    int ns = 0;
+    ns = 0;
     for (uint32_t j0 = 0; j0 < a.R; j0 += 32) {
       const uint32_t j = j0 + lane;
       const uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
@@ -523,20 +509,6 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
       ns += __popc(m);
     }
     __syncwarp();
-    n_dist += ns;
-
-    // ---- distances and merge, 32 candidates at a time
-    for (int g0 = 0; g0 < ns; g0 += 32) {
-      const int cnt = min(32, ns - g0);
-      const uint32_t cand = lane < cnt ? stage[g0 + lane] : DG_PAD;
-      const float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, cnt, lane, qq);
-      uint64_t key = lane < cnt ? make_key(d, cand) : kKeyInvalid;
-      bool match = false;
-      if (filtered && lane < cnt) match = allow(cand);
-      insert_batch(key, W, cur, wsize, (int)working, cst, lane);
-      // result list: every visited match, kept as the search_k smallest
-      if (filtered) add_results((lane < cnt && match) ? make_key(d, cand) : kKeyInvalid);
-    }
   }
 
   // ---- emit
