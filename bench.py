@@ -208,16 +208,35 @@ def max_over_ranks(ms, dist, device):
     return float(tt.item())
 
 
-def run_variant(idx, qidx, name, Qd, L, out=None, with_stats=False, stream=None):
-    """idx: the FP32/BF16 index; qidx: {"pq": QuantizedDiskANN, "int8": ...}."""
+def run_variant(idx, qidx, name, Qd, L, out=None, with_stats=False, stream=None, rerank=True):
+    """idx: the FP32/BF16 index; qidx: {"pq": QuantizedDiskANN, "int8": ...}.
+    rerank=False returns the traversal's own distances (no FP32 rerank)."""
     from pydiskann_b200 import _lib
 
     trav, rr = VARIANTS[name]
     t = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES,
          "int8": _lib.TRAVERSE_CODES, "fp8": _lib.TRAVERSE_FP8}[trav]
     target = qidx["pq"] if trav == "codes" else qidx["int8"] if trav == "int8" else idx
-    return target.search_arrays(Qd, K, L, traversal=t, rerank_size=L if rr else 0, out=out,
+    return target.search_arrays(Qd, K, L, traversal=t, rerank_size=L if rr and rerank else 0, out=out,
                                 with_stats=with_stats, stream=stream)
+
+
+def distance_error(X, Q, ids, ds, metric_sq=True):
+    """Relative error of returned distances against FP64 squared L2 of the same
+    (query, id) pairs: {"max", "mean"} over every returned neighbour."""
+    ids = np.asarray(ids)
+    ds = np.asarray(ds, dtype=np.float64)
+    ok = ids != 0xFFFFFFFF
+    errs = []
+    for q0 in range(0, len(Q), 1000):
+        sl = slice(q0, q0 + 1000)
+        I = np.where(ok[sl], ids[sl], 0).astype(np.int64)
+        diff = X[I].astype(np.float64) - Q[sl, None, :].astype(np.float64)
+        exact = (diff * diff).sum(-1)
+        e = np.abs(ds[sl] - exact) / np.maximum(exact, 1e-30)
+        errs.append(e[ok[sl]])
+    e = np.concatenate(errs) if errs else np.zeros(0)
+    return {"max": float(e.max()) if e.size else 0.0, "mean": float(e.mean()) if e.size else 0.0}
 
 
 def algorithmic_bytes(name, stats, L, d=128):
@@ -327,14 +346,20 @@ def main():
         total_ms = t_start.elapsed_time(t_end)
         steps_ms = np.array([a.elapsed_time(b) for a, b in ev])
         total_ms = max_over_ranks(total_ms, dist, dev)
-        _, _, _, st = run_variant(idx, qidx, name, Qd, L, with_stats=True)
+        ri, rd, _, st = run_variant(idx, qidx, name, Qd, L, with_stats=True)
         stats = st.cpu().numpy().view(np.uint32)
         alg_bytes, work = algorithmic_bytes(name, stats, L)
+        # accuracy against the FP64 oracle: returned distances, the traversal's
+        # own distances (rerank off) and the recall shortfall
+        ti, td, _ = run_variant(idx, qidx, name, Qd, L, rerank=False)
+        acc = {"dist_rel_err": distance_error(X, Q, ri.cpu().numpy().view(np.uint32), rd.cpu().numpy()),
+               "traversal_dist_rel_err": distance_error(X, Q, ti.cpu().numpy().view(np.uint32), td.cpu().numpy()),
+               "recall_delta_vs_fp64": round(1.0 - rec, 4)}
         results[name] = {
             "L": L, "recall_at_10": round(rec, 4), "qps": world * args.nq * args.steps / (total_ms / 1e3),
             "ms_per_step": total_ms / args.steps, "p50_ms": float(np.percentile(steps_ms, 50)),
             "p99_ms": float(np.percentile(steps_ms, 99)), "launch_ms": float(steps_ms.mean()),
-            "alg_bytes_per_launch": alg_bytes, **work, "clocks": ck.summary(),
+            "alg_bytes_per_launch": alg_bytes, **work, **acc, "clocks": ck.summary(),
         }
         log(f"[time] {name}: {json.dumps(results[name])}")
 

@@ -301,6 +301,37 @@ def test_host_pipeline_matches_device_call(small_data, small_graph):
     g.close()
 
 
+def test_pinned_host_buffers(small_data, small_graph):
+    """Pinned host buffers (torch pin_memory, as a serving host keeps them)
+    give the results of pageable buffers and of the device call, for a single
+    launch and for the chunk pipeline, with per-query beams and filters."""
+    import torch
+
+    from pydiskann_b200 import synth
+
+    X, _ = small_data
+    adj, med = small_graph
+    g = dg.FilteredDiskANN(X, adj, med, _labels(len(X)))
+    for nq in (300, 9000):
+        Q = synth.mixture(nq, 128, 32, seed=9, stream=synth.STREAM_QUERY)
+        beams = (16 + np.arange(nq) % 50).astype(np.uint32)
+        fl = [FILTERS[i % len(FILTERS)] if i % 4 == 0 else dg.Filter.none() for i in range(nq)]
+        Qp = torch.from_numpy(Q).pin_memory().numpy()
+        for kw in ({}, {"per_query_beam": beams, "filters": fl}):
+            out = (torch.zeros((nq, 10), dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                   torch.zeros((nq, 10), dtype=torch.float32).pin_memory().numpy(),
+                   torch.zeros((nq,), dtype=torch.int32).pin_memory().numpy().view(np.uint32))
+            zi, zd, zc = g.search_arrays(Qp, 10, 40, out=out, **kw)
+            assert zi is out[0]
+            hi, hd, hc = g.search_arrays(Q, 10, 40, **kw)
+            di, dd, dc = g.search_arrays(torch.from_numpy(Q).cuda(), 10, 40, **kw)
+            torch.cuda.synchronize()
+            assert np.array_equal(zc, hc) and np.array_equal(zi, hi) and np.array_equal(zd, hd)
+            assert np.array_equal(zc, dc.cpu().numpy().view(np.uint32))
+            assert np.array_equal(zi, di.cpu().numpy().view(np.uint32))
+    g.close()
+
+
 @pytest.mark.parametrize("d", [48, 96, 200, 768])
 def test_other_dims_match_oracle(oracle, d):
     """Dimensions that are not multiples of 128: padded rows (dpad = 32-multiple),
