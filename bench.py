@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--no-spfresh", action="store_true")
     ap.add_argument("--spfresh-n", type=int, default=2_000_000)
     ap.add_argument("--filtered-queries", type=int, default=5000)
+    ap.add_argument("--cosine", action="store_true",
+                    help="also run the quantized cosine workload (1M x 768, 20k queries, uneven beams)")
+    ap.add_argument("--cosine-n", type=int, default=1_000_000)
+    ap.add_argument("--cosine-nq", type=int, default=20_000)
     return ap.parse_args()
 
 
@@ -415,6 +419,8 @@ def main():
             line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
         if not args.no_filtered:
             line["filtered"] = filtered(args, X, Q, adj, med, dev, dist)
+        if args.cosine and rank == 0:
+            line["quantized_cosine"] = quantized_cosine(args, dev)
         if not args.no_spfresh and rank == 0:
             # one replica is enough for this secondary measurement (it stages
             # several GB of posting blocks on the host)
@@ -560,6 +566,102 @@ def filtered(args, X, Q, adj, med, dev, dist):
         log(f"[filtered serve] {name}: {json.dumps(out['serving']['variants'][name])}")
     f32.close()
     q8.close()
+    return out
+
+
+def cosine_distance_error(X, Q, ids, ds):
+    """Relative error of returned cosine distances against FP64 1 - cos of the
+    same (query, id) pairs."""
+    ids = np.asarray(ids)
+    ok = ids != 0xFFFFFFFF
+    errs = []
+    qn = np.linalg.norm(Q.astype(np.float64), axis=1)
+    for q0 in range(0, len(Q), 1000):
+        sl = slice(q0, q0 + 1000)
+        I = np.where(ok[sl], ids[sl], 0).astype(np.int64)
+        V = X[I].astype(np.float64)
+        dot = np.einsum("qkd,qd->qk", V, Q[sl].astype(np.float64))
+        exact = 1.0 - dot / (np.linalg.norm(V, axis=2) * qn[sl, None])
+        e = np.abs(np.asarray(ds[sl], np.float64) - exact) / np.maximum(np.abs(exact), 1e-12)
+        errs.append(e[ok[sl]])
+    e = np.concatenate(errs)
+    return {"max": float(e.max()), "mean": float(e.mean())}
+
+
+def quantized_cosine(args, dev):
+    """The quantized cosine workload: 1M x 768 embeddings with an anisotropic
+    power-law spectrum (exponent -0.5), unit norm, BF16 values; 20k queries
+    whose beams are drawn uniformly from {32..256} and run in one launch; k =
+    10 and an FP32 rerank of the top 4k = 40 candidates.  Vamana R = 64, L_build
+    = 128 (cosine).  FP32 (exact) traversal beside BF16, FP8, int8 (global
+    min/max) and RaBitQ codes; recall against FP64 exact kNN and the relative
+    error of the returned and of the traversal distances against FP64."""
+    import torch
+
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import _lib, synth
+
+    t0 = time.time()
+    X, Q = synth.cosine(args.cosine_n, args.cosine_nq, 768, args.seed)
+    setup = {"data_s": round(time.time() - t0, 1)}
+    key = f"cos_n{args.cosine_n}_q{args.cosine_nq}_s{args.seed}"
+    d = os.path.join(CACHE, key)
+    fa, fm, fg = (os.path.join(d, f + ".npy") for f in ("adj", "meta", "gt"))
+    if all(os.path.exists(f) for f in (fa, fm, fg)):
+        adj, med, gt = np.load(fa), int(np.load(fm)[0]), np.load(fg)
+    else:
+        t0 = time.time()
+        adj, med = dg.build_graph(X, 64, 128, 1.2, metric="cosine", seed=args.seed, device=dev.index or 0)
+        setup["graph_build_s"] = round(time.time() - t0, 1)
+        t0 = time.time()
+        gt, _ = dg.exact_knn(X, Q, K, metric="cosine", device=dev.index or 0)
+        setup["ground_truth_s"] = round(time.time() - t0, 1)
+        os.makedirs(d, exist_ok=True)
+        for f, v in ((fa, adj), (fm, np.array([med])), (fg, gt)):
+            np.save(f, v)
+    log(f"[cosine] setup {setup}")
+    beams = np.random.default_rng([args.seed, 77]).integers(32, 257, size=len(Q)).astype(np.uint32)
+    base = dg.DiskANN.from_graph(X, adj, med, metric="cosine", device=dev.index or 0)
+    base.enable_bf16()
+    base.enable_fp8()
+    q8 = dg.QuantizedDiskANN(X, adj, med, metric="cosine", device=dev.index or 0)
+    q8.attach_int8(*dg.int8_params(X))
+    rq = dg.QuantizedDiskANN(X, adj, med, metric="cosine", device=dev.index or 0)
+    cen, signs = dg.rabitq_params(X, args.seed)
+    rq.attach_rabitq(cen, signs)
+    Qd = torch.from_numpy(Q).to(dev)
+    variants = (("fp32", base, _lib.TRAVERSE_F32, 0), ("bf16_rerank", base, _lib.TRAVERSE_BF16, 4 * K),
+                ("fp8_rerank", base, _lib.TRAVERSE_FP8, 4 * K), ("int8_rerank", q8, _lib.TRAVERSE_CODES, 4 * K),
+                ("rabitq_rerank", rq, _lib.TRAVERSE_CODES, 4 * K))
+    out = {"n": len(X), "dim": 768, "queries": len(Q), "beams": "uniform 32..256 per query",
+           "rerank": 4 * K, "setup": setup, "variants": {}}
+    stream = torch.cuda.current_stream(dev)
+    for name, ix, trav, rr in variants:
+        run = lambda rerank=rr, o=None: ix.search_arrays(Qd, K, 256, traversal=trav, rerank_size=rerank,
+                                                         per_query_beam=beams, out=o)
+        res = run()
+        for _ in range(max(args.warmup, 1)):
+            run(o=res)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for a, b in ev:
+            a.record(stream)
+            run(o=res)
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = np.array([a.elapsed_time(b) for a, b in ev])
+        ids = res[0].cpu().numpy().view(np.uint32)
+        rec = recall(ids, gt)
+        ti, td, _ = run(rerank=0)
+        out["variants"][name] = {
+            "recall_at_10": round(rec, 4), "recall_delta_vs_fp64": round(1.0 - rec, 4),
+            "qps": len(Q) / (ms.mean() / 1e3), "ms_per_step": float(ms.mean()), "p99_ms": float(np.percentile(ms, 99)),
+            "dist_rel_err": cosine_distance_error(X, Q, ids, res[1].cpu().numpy()),
+            "traversal_dist_rel_err": cosine_distance_error(X, Q, ti.cpu().numpy().view(np.uint32), td.cpu().numpy()),
+        }
+        log(f"[cosine] {name}: {json.dumps(out['variants'][name])}")
+    for ix in (base, q8, rq):
+        ix.close()
     return out
 
 
