@@ -259,7 +259,11 @@ DgStatus dg_index_attach_int8(DgIndex *idx, float scale, float offset, const uin
                               idx->code_stride, idx->stream);
   if (s != DG_OK) return s;
   if ((s = dev_alloc(idx, (void **)&idx->i8_norm, idx->n * 4)) != DG_OK) return s;
-  if ((s = int8_norms_device(idx->codes, idx->n, idx->code_stride, idx->i8_norm, idx->stream)) != DG_OK) return s;
+  const bool decoded = idx->metric == DG_COSINE || idx->metric == DG_DOT;
+  if (decoded && (s = dev_alloc(idx, (void **)&idx->i8_sum, idx->n * 4)) != DG_OK) return s;
+  if ((s = int8_norms_device(idx->codes, idx->n, idx->code_stride, idx->i8_norm, idx->i8_sum, idx->stream)) !=
+      DG_OK)
+    return s;
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
 }
@@ -588,6 +592,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   a.i8_scale = idx->i8_scale;
   a.i8_offset = idx->i8_offset;
   a.i8_norm = idx->i8_norm;
+  a.i8_sum = idx->i8_sum;
   a.vec_fp8 = idx->fp8;
   a.fp8_sn = idx->fp8_sn;
   a.rq_padded = idx->rq_padded;
@@ -652,7 +657,8 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
   const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
-                                    idx->rq_padded, trav == TRAV_RABITQ && met_kind(idx->metric) != MET_L2);
+                                    idx->rq_padded,
+                                    (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2);
   auto launch = [&](const SearchArgs &aa, cudaStream_t ss) -> DgStatus {
     LaunchInfo info;
     DG_CUDA(cudaMemsetAsync(aa.counter, 0, 4, ss));
@@ -905,6 +911,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   a.i8_scale = idx->i8_scale;
   a.i8_offset = idx->i8_offset;
   a.i8_norm = idx->i8_norm;
+  a.i8_sum = idx->i8_sum;
   a.vec_fp8 = idx->fp8;
   a.fp8_sn = idx->fp8_sn;
   a.rq_padded = idx->rq_padded;
@@ -952,7 +959,8 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   else if (trav == TRAV_BF16 || trav == TRAV_F16) lpr = lanes_per_row(idx->dpad / 8);
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
   const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
-                                    idx->rq_padded, trav == TRAV_RABITQ && met_kind(idx->metric) != MET_L2);
+                                    idx->rq_padded,
+                                    (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2);
   LaunchInfo info;
   switch (trav) {
     case TRAV_F32: return launch_search_f32(a, Ly, met, lpr, lcap, filt, st, &info);

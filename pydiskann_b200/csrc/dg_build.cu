@@ -51,18 +51,23 @@ __global__ void k_fp8(const float *v, uint64_t n, uint32_t d, uint32_t dpad, uin
   }
 }
 // Sum of squared codes of every int8 row (padding bytes are zero).
-__global__ void k_int8_norm(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out) {
+__global__ void k_int8_norm(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, uint32_t *sums) {
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
     const uint4 *row = reinterpret_cast<const uint4 *>(codes + r * stride);
-    uint32_t s = 0;
+    uint32_t s = 0, t = 0;
     for (uint32_t c = 0; c < stride / 16; ++c) {
       const uint4 v = row[c];
       s = __dp4a(v.x, v.x, s);
       s = __dp4a(v.y, v.y, s);
       s = __dp4a(v.z, v.z, s);
       s = __dp4a(v.w, v.w, s);
+      t = __dp4a(v.x, 0x01010101u, t);
+      t = __dp4a(v.y, 0x01010101u, t);
+      t = __dp4a(v.z, 0x01010101u, t);
+      t = __dp4a(v.w, 0x01010101u, t);
     }
     out[r] = s;
+    if (sums) sums[r] = t;
   }
 }
 // ProductQuantizer::encode (src/pq.rs:122-149): argmin with strict '<'.
@@ -245,8 +250,9 @@ DgStatus encode_fp8_device(const float *vec, uint64_t n, uint32_t d, uint32_t dp
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }
-DgStatus int8_norms_device(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, cudaStream_t st) {
-  k_int8_norm<<<grid_for(n, 256), 256, 0, st>>>(codes, n, stride, out);
+DgStatus int8_norms_device(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, uint32_t *sums,
+                           cudaStream_t st) {
+  k_int8_norm<<<grid_for(n, 256), 256, 0, st>>>(codes, n, stride, out, sums);
   DG_CUDA(cudaGetLastError());
   return DG_OK;
 }

@@ -25,6 +25,7 @@ struct DgIndex {
   float *pq_cb = nullptr;     // [M][K][d/M]
   float i8_scale = 1.0f, i8_offset = 0.0f;
   uint32_t *i8_norm = nullptr; // [n] sum of squared int8 codes (tensor-core L2)
+  uint32_t *i8_sum = nullptr;  // [n] sum of int8 codes (tensor-core cosine / dot)
   uint32_t rq_padded = 0;
   float *rq_centroid = nullptr, *rq_signs = nullptr;
   float *dnorm2 = nullptr;    // [n] |decode(code)|^2 (cosine over PQ / RaBitQ codes)
@@ -89,7 +90,9 @@ DgStatus encode_rabitq_device(const float *vec, uint64_t n, uint32_t d, uint32_t
 DgStatus encode_fp8_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint8_t *codes,
                            float2 *sn, cudaStream_t st);
 // Sum of squared codes per vector for int8 codes.
-DgStatus int8_norms_device(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, cudaStream_t st);
+// Per-row sum of squared codes (out) and, when sums is not null, sum of codes.
+DgStatus int8_norms_device(const uint8_t *codes, uint64_t n, uint32_t stride, uint32_t *out, uint32_t *sums,
+                           cudaStream_t st);
 // |decode(code)|^2 per vector for PQ / RaBitQ codes (the cosine metric's |x|^2).
 DgStatus decoded_norms_device(const DgIndex *idx, float *out, cudaStream_t st);
 DgStatus count_matching_device(const uint64_t *labels, uint64_t n, uint32_t nf,

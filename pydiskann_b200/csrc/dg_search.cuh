@@ -44,6 +44,7 @@ struct SearchArgs {
   const float *pq_cb;     // [M][K][ds]
   float i8_scale, i8_offset;
   const uint32_t *i8_norm;  // [n] sum of squared codes (int8 L2 on tensor cores)
+  const uint32_t *i8_sum;   // [n] sum of codes (int8 cosine / dot on tensor cores)
   const uint8_t *vec_fp8;   // [n][dpad] e4m3 rows (FP8 traversal)
   const float2 *fp8_sn;     // [n] (scale, |decoded|^2)
   uint32_t rq_padded;
@@ -85,7 +86,8 @@ struct WarpLayout {
   uint32_t w0, w1, res, cstage, stage, hash, qf, prov, aux, total;
 };
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
-// `decode`: RaBitQ with a cosine / dot metric (rotated query, nibble table).
+// `decode`: RaBitQ or int8 with a cosine / dot metric (RaBitQ: rotated query
+// and nibble table; int8: four signed digit columns of the query).
 __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool filt, uint32_t hbits,
                                                   uint32_t dpad, uint32_t pq_M, uint32_t pq_K,
                                                   uint32_t rq_padded, bool decode = false) {
@@ -101,6 +103,7 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
   L.prov = o;
   uint32_t p = 0;
   if (trav == TRAV_PQ) p = pq_M * pq_K * 4;
+  else if (trav == TRAV_INT8 && decode) p = 4 * align16(dpad) + 16;  // query digits, then (scale, sum q)
   else if (trav == TRAV_INT8) p = align16(dpad) + 16;  // query codes, then |q_code|^2
   else if (trav == TRAV_RABITQ && decode) p = 16 + rq_padded * 4 + rq_padded * 16;
   else if (trav == TRAV_RABITQ) p = 4 * (rq_padded / 64) * 8 + 32 + align16(rq_padded * 4);
@@ -494,6 +497,80 @@ __device__ __forceinline__ uint32_t int8_l2_mma(const uint8_t *__restrict__ code
   const int d10 = __shfl_sync(kFull, c1[0], src), d11 = __shfl_sync(kFull, c1[2], src);
   const int dot = T == 0 ? (r < 8 ? d00 : d01) : (r < 8 ? d10 : d11);
   return qn + xn - 2u * (uint32_t)dot;
+}
+
+__device__ __forceinline__ void mma_u8s8_16x8x32(int (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                                 uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k32.row.col.s32.u8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// sum_i t_i c_i for up to 32 candidate int8 code rows c, where the query enters
+// as t_i = D0 2^24 + D1 2^16 + D2 2^8 + D3 with signed 8-bit digits D0..D3 held
+// as four columns of the tensor-core B operand (digit j: column j; qdig: four
+// arrays of dpad digits, align16(dpad) apart).  Every column product is an
+// exact integer; the result is exact in double.  Tile and lane layout of
+// int8_l2_mma.
+__device__ __forceinline__ double int8_dot_mma(const uint8_t *__restrict__ codes, uint32_t stride,
+                                               const uint8_t *qdig, uint32_t dstride, uint32_t cand, int cnt,
+                                               int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int nch = (int)(stride >> 4);
+  const int J = (nch + 3) >> 2;
+  const uint32_t id0 = __shfl_sync(kFull, cand, 0);
+  const bool two = cnt > 16;
+  const uint4 *rp[4];
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const int row = g + 8 * h;
+    uint32_t id = __shfl_sync(kFull, cand, row);
+    id = row < cnt ? id : id0;
+    rp[h] = reinterpret_cast<const uint4 *>(codes + (size_t)id * stride);
+  }
+  // B column g holds digit g (columns 4..7 stay zero)
+  const uint4 *pq = reinterpret_cast<const uint4 *>(qdig + (size_t)(g & 3) * dstride);
+  const bool col = g < 4;
+  int c0[4] = {0, 0, 0, 0}, c1[4] = {0, 0, 0, 0};
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  for (int j0 = 0; j0 < J; j0 += 2) {
+    uint4 x[2][4], qv[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int ch = t + 4 * (j0 + u);
+      const bool ok = j0 + u < J && ch < nch;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) x[u][h] = (ok && (h < 2 || two)) ? __ldg(rp[h] + ch) : z;
+      qv[u] = ok && col ? pq[ch] : z;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      mma_u8s8_16x8x32(c0, x[u][0].x, x[u][1].x, x[u][0].y, x[u][1].y, qv[u].x, qv[u].y);
+      mma_u8s8_16x8x32(c0, x[u][0].z, x[u][1].z, x[u][0].w, x[u][1].w, qv[u].z, qv[u].w);
+      if (two) {
+        mma_u8s8_16x8x32(c1, x[u][2].x, x[u][3].x, x[u][2].y, x[u][3].y, qv[u].x, qv[u].y);
+        mma_u8s8_16x8x32(c1, x[u][2].z, x[u][3].z, x[u][2].w, x[u][3].w, qv[u].z, qv[u].w);
+      }
+    }
+  }
+  // candidate j = 16T + r: row r % 8 (+8 when r >= 8) of tile T; columns 0, 1
+  // sit in lane 4 (r % 8), columns 2, 3 in lane 4 (r % 8) + 1
+  const int T = lane >> 4, r = lane & 15, s0 = (r & 7) << 2, hi = r >= 8 ? 2 : 0;
+  int v[2][4];
+#pragma unroll
+  for (int tt = 0; tt < 2; ++tt) {
+    const int(&c)[4] = tt == 0 ? c0 : c1;
+    const int e0 = __shfl_sync(kFull, c[0], s0), e1 = __shfl_sync(kFull, c[1], s0);
+    const int e2 = __shfl_sync(kFull, c[2], s0), e3 = __shfl_sync(kFull, c[3], s0);
+    const int f0 = __shfl_sync(kFull, c[0], s0 + 1), f1 = __shfl_sync(kFull, c[1], s0 + 1);
+    const int f2 = __shfl_sync(kFull, c[2], s0 + 1), f3 = __shfl_sync(kFull, c[3], s0 + 1);
+    v[tt][0] = hi ? e2 : e0;
+    v[tt][1] = hi ? e3 : e1;
+    v[tt][2] = hi ? f2 : f0;
+    v[tt][3] = hi ? f3 : f1;
+  }
+  const int *S = T == 0 ? v[0] : v[1];
+  return (double)S[0] * 16777216.0 + (double)S[1] * 65536.0 + (double)S[2] * 256.0 + (double)S[3];
 }
 
 // One warp-wide e4m3 x e4m3 -> f32 tensor-core step (16 rows x 32 dims x 8 columns).

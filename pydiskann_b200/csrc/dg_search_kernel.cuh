@@ -60,8 +60,20 @@ __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *ws
       float d = __fmul_rn(__fmul_rn(__uint2float_rn(s), a.i8_scale), a.i8_scale);
       return sqrt_l2 ? __fsqrt_rn(d) : d;
     } else {
-      return int8_decode_group<LPR, MET>(a.codes, a.code_stride, (a.code_stride / 16) / LPR, qs,
-                                         a.i8_scale, a.i8_offset, a.d, cand, cnt, lane, qq);
+      // decoded v = s c + o (src/quantized.rs:28-36, src/sq.rs decode): q.v = s (q.c) + o sum(q),
+      // |v|^2 = s^2 sum(c^2) + 2 s o sum(c) + d o^2, with q.c on the tensor cores
+      const uint8_t *qd = wsm + Ly.prov;
+      const uint32_t ds = align16(a.dpad);
+      const double2 qp = *reinterpret_cast<const double2 *>(qd + 4 * ds);  // (q scale, sum q)
+      const uint32_t c2 = lane < cnt ? __ldg(a.i8_norm + cand) : 0u;
+      const uint32_t c1 = lane < cnt ? __ldg(a.i8_sum + cand) : 0u;
+      const double qc = int8_dot_mma(a.codes, a.code_stride, qd, ds, cand, cnt, lane) * qp.x;
+      const double sc = a.i8_scale, of = a.i8_offset;
+      const float dot = (float)(sc * qc + of * qp.y);
+      const float vv = MET == MET_COS ? (float)(sc * sc * (double)c2 + 2.0 * sc * of * (double)c1 +
+                                                (double)a.d * of * of)
+                                      : 0.0f;
+      return finish_metric(MET, false, dot, vv, qq);
     }
   } else if (TRAV == TRAV_PQ) {
     const float *lut = reinterpret_cast<const float *>(wsm + Ly.prov);
@@ -100,6 +112,39 @@ __device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm,
     rabitq_decode_prepare(qs, a.d, a.rq_padded, a.rq_centroid, a.rq_signs, wsm + Ly.prov, lane);
   } else if (TRAV == TRAV_PQ) {
     build_pq_lut(a, qs, reinterpret_cast<float *>(wsm + Ly.prov), lane);
+  } else if (TRAV == TRAV_INT8 && MET != MET_L2) {
+    // q_i ~ M t_i / F, t_i = round(q_i F / M) with F = 127 * 2^24 (M = max |q_i|),
+    // split into four signed 8-bit digits t = D0 2^24 + D1 2^16 + D2 2^8 + D3
+    uint8_t *dig = wsm + Ly.prov;
+    const uint32_t ds = align16(a.dpad);
+    float mx = 0.0f;
+    double sq = 0.0;
+    for (uint32_t i = lane; i < a.dpad; i += 32) {
+      mx = fmaxf(mx, fabsf(qs[i]));
+      sq += (double)qs[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+      sq += __shfl_xor_sync(kFull, sq, o);
+    }
+    const double F = 2130706432.0;  // 127 * 2^24: |t| <= F keeps D0 within [-127, 127]
+    const double inv = mx > 0.0f ? F / (double)mx : 0.0;
+    for (uint32_t i = lane; i < a.dpad; i += 32) {
+      long long t = i < a.d ? __double2ll_rn((double)qs[i] * inv) : 0;
+      int8_t dd[4];
+#pragma unroll
+      for (int j = 3; j > 0; --j) {
+        const int dj = (int)((t + 128) & 255) - 128;
+        dd[j] = (int8_t)dj;
+        t = (t - dj) >> 8;
+      }
+      dd[0] = (int8_t)t;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dig[j * ds + i] = (uint8_t)dd[j];
+    }
+    if (lane == 0)
+      *reinterpret_cast<double2 *>(dig + 4 * ds) = make_double2(mx > 0.0f ? (double)mx / F : 0.0, sq);
   } else if (TRAV == TRAV_INT8) {
     uint8_t *qc8 = wsm + Ly.prov;
     const float inv = __fdiv_rn(1.0f, a.i8_scale);

@@ -235,16 +235,18 @@ def test_edge_cases():
     assert len(r) == 1 and r[0][1] >= 0.0
 
 
-# Cosine / dot over PQ and RaBitQ codes: the reference decodes the code and
-# evaluates the metric (src/quantized.rs:28-36, src/pq.rs:151-160,
-# src/rabitq.rs:224-238).  The kernel takes q . decode(code) from a
-# query-centroid inner-product table (PQ) or in the rotated space (RaBitQ), so
-# the sum is grouped differently from the decoded vector's sequential sum; the
-# |decode(code)|^2 term is bit-identical.  Tolerance: ids agree with the oracle
-# except among near-ties (>= 98 % overlap), distances of common ids within
-# 1e-5 relative + 2e-6 absolute.
+# Cosine / dot over PQ, RaBitQ and int8 codes: the reference decodes the code
+# and evaluates the metric (src/quantized.rs:28-36, src/pq.rs:151-160,
+# src/rabitq.rs:224-238, src/sq.rs:222-225).  The kernel takes
+# q . decode(code) from a query-centroid inner-product table (PQ), in the
+# rotated space (RaBitQ), or as s (q . c) + o sum(q) with q . c on the tensor
+# cores (int8, the query as four 8-bit digit columns), so the sum is grouped
+# differently from the decoded vector's sequential sum.  Tolerance: ids agree
+# with the oracle except among near-ties (>= 98 % overlap), distances of common
+# ids within 1e-5 relative + 2e-6 absolute.
 DECODE_CASES = [("pq", "cosine", 96), ("pq", "dot", 64), ("rabitq", "cosine", 96), ("rabitq", "dot", 64),
-                ("rabitq", "cosine", 128)]
+                ("rabitq", "cosine", 128), ("int8", "cosine", 96), ("int8", "dot", 64), ("int8", "cosine", 768),
+                ("int8", "dot", 200)]
 
 
 @pytest.mark.parametrize("quant,metric,d", DECODE_CASES)
@@ -260,6 +262,10 @@ def test_decoded_metrics_within_tolerance(oracle, quant, metric, d):
         cb = dg.pq_train(X, 8, 64, 10, 3000, seed=1)
         q.attach_pq(cb)
         o.set_pq(cb, oracle.pq_encode(X, cb))
+    elif quant == "int8":
+        s, off = dg.int8_params(X)
+        q.attach_int8(s, off)
+        o.set_int8(s, off, oracle.int8_encode(X, s, off))
     else:
         cen, signs = dg.rabitq_params(X, seed=3)
         P = dg.rabitq_padded(d)
