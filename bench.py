@@ -225,6 +225,17 @@ def run_variant(idx, qidx, name, Qd, L, out=None, with_stats=False, stream=None,
                                 with_stats=with_stats, stream=stream)
 
 
+def autotune_variant(idx, qidx, name, Qd, L):
+    """dg_index_autotune on the variant's own search (same queries, k, L)."""
+    from pydiskann_b200 import _lib
+
+    trav, rr = VARIANTS[name]
+    t = {"f32": _lib.TRAVERSE_F32, "bf16": _lib.TRAVERSE_BF16, "codes": _lib.TRAVERSE_CODES,
+         "int8": _lib.TRAVERSE_CODES, "fp8": _lib.TRAVERSE_FP8}[trav]
+    target = qidx["pq"] if trav == "codes" else qidx["int8"] if trav == "int8" else idx
+    return target.autotune(Qd, K, L, traversal=t, rerank_size=L if rr else 0, reps=3)
+
+
 def distance_error(X, Q, ids, ds, metric_sq=True):
     """Relative error of returned distances against FP64 squared L2 of the same
     (query, id) pairs: {"max", "mean"} over every returned neighbour."""
@@ -326,9 +337,13 @@ def main():
                 break
         log(f"[sweep] {name}: {chosen.get(name)} curve {curves[name]}")
 
-    # ---- timing per variant (device-resident queries and results)
+    # ---- timing per variant (device-resident queries and results), after the
+    # autotuner picked the visited-table size for this exact search
     results = {}
+    tuned = {}
     for name, (L, rec) in chosen.items():
+        tuned[name] = autotune_variant(idx, qidx, name, Qd, L)
+        log(f"[autotune] {name}: {tuned[name]}")
         out = run_variant(idx, qidx, name, Qd, L)
         for _ in range(args.warmup):
             run_variant(idx, qidx, name, Qd, L, out=out)
@@ -363,7 +378,8 @@ def main():
             "L": L, "recall_at_10": round(rec, 4), "qps": world * args.nq * args.steps / (total_ms / 1e3),
             "ms_per_step": total_ms / args.steps, "p50_ms": float(np.percentile(steps_ms, 50)),
             "p99_ms": float(np.percentile(steps_ms, 99)), "launch_ms": float(steps_ms.mean()),
-            "alg_bytes_per_launch": alg_bytes, **work, **acc, "clocks": ck.summary(),
+            "alg_bytes_per_launch": alg_bytes, **work, **acc, "visited_table_bits": tuned[name]["hbits"],
+            "clocks": ck.summary(),
         }
         log(f"[time] {name}: {json.dumps(results[name])}")
 
@@ -639,6 +655,8 @@ def quantized_cosine(args, dev):
     for name, ix, trav, rr in variants:
         run = lambda rerank=rr, o=None: ix.search_arrays(Qd, K, 256, traversal=trav, rerank_size=rerank,
                                                          per_query_beam=beams, out=o)
+        tune = ix.autotune(Qd, K, 256, traversal=trav, rerank_size=rr, per_query_beam=beams, reps=1)
+        log(f"[cosine] autotune {name}: {tune}")
         res = run()
         for _ in range(max(args.warmup, 1)):
             run(o=res)
@@ -658,6 +676,7 @@ def quantized_cosine(args, dev):
             "qps": len(Q) / (ms.mean() / 1e3), "ms_per_step": float(ms.mean()), "p99_ms": float(np.percentile(ms, 99)),
             "dist_rel_err": cosine_distance_error(X, Q, ids, res[1].cpu().numpy()),
             "traversal_dist_rel_err": cosine_distance_error(X, Q, ti.cpu().numpy().view(np.uint32), td.cpu().numpy()),
+            "visited_table_bits": tune["hbits"],
         }
         log(f"[cosine] {name}: {json.dumps(out['variants'][name])}")
     for ix in (base, q8, rq):

@@ -196,6 +196,17 @@ DG_API DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const flo
                          uint32_t *out_ids, float *out_dists, uint32_t *out_counts,
                          uint32_t *out_stats);
 
+/* Launch-schedule autotuner (no counterpart in the reference): times this
+ * exact search -- the caller's parameters and queries (host or device per
+ * p->flags) -- with each per-query visited-table size from 2^8 to 2^13 words
+ * (the table's shared memory sets how many queries an SM holds; a smaller
+ * table recomputes the distances of ids it forgets, never changes results)
+ * and keeps the fastest for later searches of the same traversal, working-set
+ * capacity and filtering.  ms_per_call[6] (may be NULL) receives the mean time
+ * per call of each size, -1 where the size did not fit in shared memory. */
+DG_API DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const float *queries, uint32_t nq,
+                                  uint32_t reps, uint32_t *best_hbits, float *ms_per_call);
+
 /* dg_search_batch for callers that cannot have device memory allocated for
  * them (hosts whose device memory belongs to a separate pool manager,
  * latency-critical threads that must not pay cudaMalloc's implicit device

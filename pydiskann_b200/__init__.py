@@ -338,15 +338,9 @@ class _Index:
             self._fp8 = True
 
     # -- the batched entry point
-    def search_arrays(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32,
-                      rerank_size=0, filters=None, per_query_beam=None, out=None, stream=None,
-                      with_stats=False):
-        """Batched search over numpy arrays (host) or CUDA tensors (device).
-
-        Returns (ids u32[nq,k], dists f32[nq,k], counts u32[nq]) of the same
-        kind as `queries`; rows are padded with PAD / +inf past counts.
-        `filters` is one Filter for all queries or a list of one per query.
-        """
+    def _params(self, queries, k, beam_width, traversal, rerank_size, filters, per_query_beam, out, stream,
+                with_stats):
+        """DgSearchParams and buffers of one batched call (see search_arrays)."""
         dev = hasattr(queries, "data_ptr") and getattr(queries, "is_cuda", False)
         p = _lib.SearchParams()
         p.k, p.beam_width, p.rerank_size, p.traversal = k, beam_width, rerank_size, traversal
@@ -403,11 +397,38 @@ class _Index:
             pl = np.ascontiguousarray(per_query_beam, dtype=np.uint32)
             keep.append(pl)
             p.per_query_beam = ptr(pl)
+        return p, Q, nq, out, stats, keep
+
+    def search_arrays(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32,
+                      rerank_size=0, filters=None, per_query_beam=None, out=None, stream=None,
+                      with_stats=False):
+        """Batched search over numpy arrays (host) or CUDA tensors (device).
+
+        Returns (ids u32[nq,k], dists f32[nq,k], counts u32[nq]) of the same
+        kind as `queries`; rows are padded with PAD / +inf past counts.
+        `filters` is one Filter for all queries or a list of one per query.
+        """
+        p, Q, nq, out, stats, keep = self._params(queries, k, beam_width, traversal, rerank_size, filters,
+                                                  per_query_beam, out, stream, with_stats)
         check(lib().dg_search_batch(self._h, C.byref(p), ptr(Q), nq, ptr(out[0]), ptr(out[1]),
                                     ptr(out[2]), ptr(stats)))
+        del keep
         if with_stats:
             return out[0], out[1], out[2], stats
         return out
+
+    def autotune(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32, rerank_size=0, filters=None,
+                 per_query_beam=None, reps=3):
+        """Times this search (same arguments as search_arrays) with each
+        visited-table size and keeps the fastest for later searches of the same
+        kind (dg_index_autotune).  Returns {"hbits": chosen, "ms": {bits: ms per call}}."""
+        p, Q, nq, _, _, keep = self._params(queries, k, beam_width, traversal, rerank_size, filters,
+                                            per_query_beam, None, None, False)
+        best = C.c_uint32()
+        ms = (C.c_float * 6)()
+        check(lib().dg_index_autotune(self._h, C.byref(p), ptr(Q), nq, reps, C.byref(best), ms))
+        del keep
+        return {"hbits": best.value, "ms": {8 + i: round(ms[i], 4) for i in range(6) if ms[i] >= 0}}
 
     # -- reference-shaped helpers
     def _rows(self, ids, dists, cnt):
@@ -603,6 +624,10 @@ class QuantizedDiskANN(_Index):
                       rerank_size=None, **kw):
         rr = self.rerank_size if rerank_size is None else rerank_size
         return super().search_arrays(queries, k, beam_width, traversal, rr, **kw)
+
+    def autotune(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_CODES, rerank_size=None, **kw):
+        rr = self.rerank_size if rerank_size is None else rerank_size
+        return super().autotune(queries, k, beam_width, traversal, rr, **kw)
 
     def search_with_dists(self, query, k=10, beam_width=128):
         ids, ds, cnt = self.search_arrays(_f32(query).reshape(1, -1), k, beam_width)

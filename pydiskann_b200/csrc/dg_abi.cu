@@ -421,6 +421,29 @@ static uint64_t working_need(const DgIndex *idx, uint32_t maxL, uint32_t k, uint
   return need;
 }
 
+// visited-table sizes dg_index_autotune tries (log2 words per query)
+static constexpr uint32_t kTuneMinBits = 8, kTuneMaxBits = 13;
+
+static uint32_t tune_key(int trav, int lcap, bool filt) {
+  return ((uint32_t)trav << 20) | ((uint32_t)lcap << 1) | (filt ? 1u : 0u);
+}
+
+static uint32_t visited_bits(DgIndex *idx, int trav, int lcap, bool filt, uint32_t maxL) {
+  uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
+  {
+    std::lock_guard<std::mutex> lk(idx->mu);
+    if (idx->hbits_force > 0) {
+      hbits = (uint32_t)idx->hbits_force;
+      idx->last_key = tune_key(trav, lcap, filt);
+    } else {
+      auto it = idx->tuned_hbits.find(tune_key(trav, lcap, filt));
+      if (it != idx->tuned_hbits.end()) hbits = it->second;
+    }
+  }
+  if (const char *e = std::getenv("DG_HBITS")) hbits = (uint32_t)std::max(6, std::min(14, atoi(e)));
+  return hbits;
+}
+
 static void index_state(const DgIndex *idx, SearchArgs &a) {
   a.seed2 = idx->seed2;
   const bool tombed = idx->tomb && idx->ntomb > 0;
@@ -558,9 +581,9 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
   if (reranked && !filt && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
   // visited table: 2^hbits words of two 16-bit tags (about 3 tags per
-  // visited node at these beams); DG_HBITS overrides for tuning
-  uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
-  if (const char *e = std::getenv("DG_HBITS")) hbits = (uint32_t)std::max(6, std::min(14, atoi(e)));
+  // visited node at these beams), or the size dg_index_autotune measured
+  // fastest for this kind of search; DG_HBITS overrides both
+  const uint32_t hbits = visited_bits(idx, trav, lcap, filt, maxL);
   uint32_t hB = 1;
   while (hB < 32 && (1ull << hB) < idx->n) ++hB;
   hB = std::max(hB, hbits);
@@ -731,6 +754,84 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   return DG_OK;
 }
 
+DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const float *queries, uint32_t nq,
+                           uint32_t reps, uint32_t *best_hbits, float *ms_per_call) {
+  if (!idx || !p || !queries || nq == 0) return fail(DG_EINVAL, "null argument or no queries");
+  reps = std::max(reps, 1u);
+  DG_CUDA(cudaSetDevice(idx->device));
+  struct Scratch {
+    void *p[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~Scratch() {
+      if (st) cudaStreamSynchronize(st);
+      for (void *q : p)
+        if (q) cudaFree(q);
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+      if (st) cudaStreamDestroy(st);
+    }
+  } sc;
+  const size_t kq = (size_t)nq * std::max(p->k, 1u);
+  const float *dq = queries;
+  if (!(p->flags & DG_FLAG_DEVICE_PTRS)) {
+    DG_CUDA(cudaMalloc(&sc.p[0], (size_t)nq * idx->d * 4));
+    DG_CUDA(cudaMemcpy(sc.p[0], queries, (size_t)nq * idx->d * 4, cudaMemcpyHostToDevice));
+    dq = (const float *)sc.p[0];
+  }
+  DG_CUDA(cudaMalloc(&sc.p[1], kq * 4));
+  DG_CUDA(cudaMalloc(&sc.p[2], kq * 4));
+  DG_CUDA(cudaMalloc(&sc.p[3], (size_t)nq * 4));
+  DG_CUDA(cudaStreamCreateWithFlags(&sc.st, cudaStreamNonBlocking));
+  DG_CUDA(cudaEventCreate(&sc.e[0]));
+  DG_CUDA(cudaEventCreate(&sc.e[1]));
+  DgSearchParams pp = *p;
+  pp.flags = p->flags | DG_FLAG_DEVICE_PTRS | DG_FLAG_STREAM;
+  pp.stream = sc.st;
+  float best_ms = 0.0f;
+  uint32_t best = 0, key = 0;
+  DgStatus result = DG_OK;
+  for (uint32_t hb = kTuneMinBits; hb <= kTuneMaxBits; ++hb) {
+    if (ms_per_call) ms_per_call[hb - kTuneMinBits] = -1.0f;
+    {
+      std::lock_guard<std::mutex> lk(idx->mu);
+      idx->hbits_force = (int)hb;
+    }
+    auto run = [&]() {
+      return dg_search_batch(idx, &pp, dq, nq, (uint32_t *)sc.p[1], (float *)sc.p[2], (uint32_t *)sc.p[3],
+                             nullptr);
+    };
+    DgStatus s = run();  // warm-up; a table that does not fit in shared memory is skipped
+    if (s == DG_OK) {
+      cudaEventRecord(sc.e[0], sc.st);
+      for (uint32_t r = 0; r < reps && s == DG_OK; ++r) s = run();
+      cudaEventRecord(sc.e[1], sc.st);
+    }
+    if (s == DG_OK && cudaEventSynchronize(sc.e[1]) == cudaSuccess) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, sc.e[0], sc.e[1]);
+      ms /= (float)reps;
+      if (ms_per_call) ms_per_call[hb - kTuneMinBits] = ms;
+      if (!best || ms < best_ms) {
+        best = hb;
+        best_ms = ms;
+        std::lock_guard<std::mutex> lk(idx->mu);
+        key = idx->last_key;
+      }
+    } else if (s != DG_ENOTSUP) {
+      result = s;
+      break;
+    }
+  }
+  std::lock_guard<std::mutex> lk(idx->mu);
+  idx->hbits_force = 0;
+  if (result != DG_OK) return result;
+  if (!best) return fail(DG_ENOTSUP, "no visited-table size fits this search");
+  idx->tuned_hbits[key] = best;
+  if (best_hbits) *best_hbits = best;
+  return DG_OK;
+}
+
 DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t nops,
                            const uint64_t *pool, uint32_t pool_len, uint64_t *out_count) {
   if (!idx || !out_count) return fail(DG_EINVAL, "null argument");
@@ -868,7 +969,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   const int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
   if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
   if (reranked && !filt && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
-  uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
+  const uint32_t hbits = visited_bits(idx, trav, lcap, filt, maxL);
   uint32_t hB = 1;
   while (hB < 32 && (1ull << hB) < idx->n) ++hB;
   hB = std::max(hB, hbits);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -36,6 +37,11 @@ struct DgIndex {
   uint32_t *tomb = nullptr;            // [ceil(n/32)] deleted-id bitmap (device)
   std::vector<uint32_t> tomb_host;     // its host copy
   uint64_t ntomb = 0;                  // tombstone count the search config uses
+  // visited-table size (log2 words per query) chosen by dg_index_autotune per
+  // (traversal, working-set capacity, filtered); hbits_force > 0 pins it while tuning
+  std::map<uint32_t, uint32_t> tuned_hbits;
+  int hbits_force = 0;
+  uint32_t last_key = 0;  // key of the last search run with hbits_force set
   cudaStream_t stream = nullptr;
   uint64_t hbm_budget = 0, hbm_used = 0;
   std::mutex mu;

@@ -338,6 +338,37 @@ def test_pinned_host_buffers(small_data, small_graph):
     g.close()
 
 
+def test_autotune_keeps_results(oracle, small_data, small_graph):
+    """dg_index_autotune tries every visited-table size, keeps the fastest, and
+    searches afterwards return exactly what the oracle returns (a smaller table
+    only recomputes distances of forgotten ids)."""
+    X, Q = small_data
+    adj, med = small_graph
+    lab = _labels(len(X))
+    s, off = dg.int8_params(X)
+    q = dg.QuantizedDiskANN(X, adj, med)
+    q.attach_int8(s, off)
+    q.attach_labels(lab)
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_int8(s, off, oracle.int8_encode(X, s, off))
+    o.set_labels(lab)
+    f = FILTERS[3]
+    ops, pool = f.program()
+    for kw, okw in (({}, {}), ({"filters": f}, {"filter_ops": ops, "filter_pool": pool})):
+        t = q.autotune(Q, 10, 48, rerank_size=24, reps=2, **kw)
+        assert 8 <= t["hbits"] <= 13 and t["hbits"] in t["ms"] and len(t["ms"]) >= 3
+        assert_same(q.search_arrays(Q, 10, 48, rerank_size=24, **kw),
+                    o.search(Q, 10, 48, rerank=24, use_codes=True, **okw))
+    for hb in (8, 13):  # the extremes, forced: identical results
+        import os
+        os.environ["DG_HBITS"] = str(hb)
+        try:
+            assert_same(q.search_arrays(Q, 10, 48, rerank_size=24), o.search(Q, 10, 48, rerank=24, use_codes=True))
+        finally:
+            del os.environ["DG_HBITS"]
+    q.close()
+
+
 @pytest.mark.parametrize("d", [48, 96, 200, 768])
 def test_other_dims_match_oracle(oracle, d):
     """Dimensions that are not multiples of 128: padded rows (dpad = 32-multiple),
