@@ -541,6 +541,8 @@ def filtered(args, X, Q, adj, med, dev, dist):
             continue
         L, rec = chosen
         rr = L if name != "fp32" else 0
+        tune = ix.autotune(Qd, K, L, rerank_size=rr, filters=filt, reps=2, **kw)
+        log(f"[filtered] autotune {name}: {tune}")
         res = ix.search_arrays(Qd, K, L, rerank_size=rr, filters=filt, **kw)
         for _ in range(args.warmup):
             ix.search_arrays(Qd, K, L, rerank_size=rr, filters=filt, out=res, **kw)
@@ -557,7 +559,8 @@ def filtered(args, X, Q, adj, med, dev, dist):
         out["variants"][name] = {"L": L, "recall_at_10": round(rec, 4), "qps": nqf * args.steps / (ms / 1e3),
                                  "ms_per_step": ms / args.steps, "recall_curve": curve,
                                  "expansions_per_query": float(stats[:, 0].mean()),
-                                 "dist_evals_per_query": float(stats[:, 1].mean())}
+                                 "dist_evals_per_query": float(stats[:, 1].mean()),
+                                 "visited_table_bits": tune["hbits"]}
         log(f"[filtered] {name}: {json.dumps(out['variants'][name])}")
     # filtered serving: Poisson arrivals, each request with its own label filter
     n_srv, rate = 50_000, 200_000.0
