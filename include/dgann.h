@@ -145,10 +145,16 @@ DG_API DgStatus dg_index_set_entry_points(DgIndex *idx, const uint32_t *ids, uin
  * of the caller's tombstone set (which may hold ids the index does not have). */
 DG_API DgStatus dg_index_set_tombstones(DgIndex *idx, const uint32_t *ids, uint64_t n, int32_t deleted,
                                         uint64_t tombstone_count);
+/* Rows at or past `limit` carry no codes: code traversals score them with the
+ * exact FP32 distance, as IncrementalDiskANN::search_with_dists scores delta
+ * rows of a quantized base (src/incremental.rs:944-968).  limit = 0 or n:
+ * every row is coded (the default). */
+DG_API DgStatus dg_index_set_code_limit(DgIndex *idx, uint64_t limit);
 /* Overwrites rows [first, first + count): f32 vectors (dim each; BF16 / FP8
  * copies are re-encoded), adjacency (max_degree each) and labels (num_fields
- * each); a NULL pointer leaves that part unchanged.  Vectors of an index with
- * quantized codes cannot be replaced (DG_ENOTSUP). */
+ * each); a NULL pointer leaves that part unchanged.  Vectors of rows that
+ * carry quantized codes cannot be replaced (DG_ENOTSUP); rows past the code
+ * limit can. */
 DG_API DgStatus dg_index_update_rows(DgIndex *idx, uint64_t first, uint64_t count, const float *vectors,
                                      const uint32_t *adjacency, const uint64_t *labels);
 /* DeltaLayer::add_vectors (src/incremental.rs:114-166) on the host: inserts

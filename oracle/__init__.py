@@ -95,7 +95,7 @@ def _declare(L):
         "dgo_build_vamana": (C.c_int, [vp, u64, u32, i32, u32, u32, f32, u64, u32, vp, i32]),
         "dgo_beam_search_table": (C.c_int, [vp, u32, vp, vp, vp, u32, u32, u32, i32, u32, u32, f32, vp, vp, vp]),
         "dgo_search_batch": (C.c_int, [vp, vp, vp, u32, vp, vp, vp, vp, vp, i32]),
-        "dgo_incremental_search_batch": (C.c_int, [vp, vp, vp, u32, vp, u64, vp, u32, vp, vp, vp, i32]),
+        "dgo_incremental_search_batch": (C.c_int, [vp, vp, vp, u32, vp, u64, u64, vp, u32, vp, vp, vp, i32]),
         "dgo_filter_matches": (C.c_int, [vp, u32, vp, vp, u32]),
         "dgo_pq_encode": (None, [vp, u64, u32, u32, u32, vp, vp, i32]),
         "dgo_pq_lut": (None, [vp, u32, u32, u32, vp, vp]),
@@ -276,13 +276,14 @@ class OracleIndex:
         return ids, ds, cnt
 
     def incremental_search(self, Q, k, L, seeds, dead=None, ntomb=0, filter_ops=None, filter_pool=(),
-                           threads=0):
+                           threads=0, use_codes=False, rerank=0, code_limit=None):
         """IncrementalDiskANN search over this unified view (base rows, then delta
-        rows): `seeds` entry points, `dead` a bool per row, `ntomb` the tombstone count."""
+        rows): `seeds` entry points, `dead` a bool per row, `ntomb` the tombstone
+        count; with use_codes, rows below code_limit are scored by their codes."""
         Q = _f32(Q).reshape(-1, self.s.d)
         nq = Q.shape[0]
         p = SearchParams()
-        p.k, p.beam_width = k, L
+        p.k, p.beam_width, p.use_codes, p.rerank_size = k, L, int(use_codes), rerank
         keep = []
         if filter_ops:
             arr, n, pool = filter_program(filter_ops, filter_pool)
@@ -293,8 +294,9 @@ class OracleIndex:
         ids = np.zeros((nq, k), dtype=np.uint32)
         ds = np.zeros((nq, k), dtype=np.float32)
         cnt = np.zeros(nq, dtype=np.uint32)
+        cl = self.s.n if code_limit is None else code_limit
         lib().dgo_incremental_search_batch(C.byref(self.s), C.byref(p), _p(sd), len(sd), _p(dd), int(ntomb),
-                                           _p(Q), nq, _p(ids), _p(ds), _p(cnt), threads)
+                                           int(cl), _p(Q), nq, _p(ids), _p(ds), _p(cnt), threads)
         return ids, ds, cnt
 
 

@@ -888,12 +888,15 @@ int dgo_search_batch(const DgoIndex *idx, const DgoSearchParams *p, const float 
 }
 
 int dgo_incremental_search_batch(const DgoIndex *idx, const DgoSearchParams *p, const uint32_t *seeds,
-                                 uint32_t nseeds, const uint8_t *dead, uint64_t ntomb, const float *Q,
-                                 uint32_t nq, uint32_t *out_ids, float *out_d, uint32_t *out_cnt,
+                                 uint32_t nseeds, const uint8_t *dead, uint64_t ntomb, uint64_t code_limit,
+                                 const float *Q, uint32_t nq, uint32_t *out_ids, float *out_d, uint32_t *out_cnt,
                                  int32_t nthreads) {
   const DgoIndex &I = *idx;
   const uint32_t k = p->k, L = p->beam_width;
   const bool labeled = p->filter_nops > 0;
+  // a label filter searches exact distances (search_filtered_with_dists ignores the quantizer)
+  const bool codes = p->use_codes && !labeled;
+  const uint32_t search_k = codes && p->rerank_size > 0 ? std::max(p->rerank_size, k) : k;
   BeamCfg cfg;
   if (labeled) {  // search_filtered_with_dists (src/incremental.rs:1048-1062)
     cfg.filtered = true;
@@ -902,7 +905,7 @@ int dgo_incremental_search_batch(const DgoIndex *idx, const DgoSearchParams *p, 
     cfg.early = 1.5f;
   } else if (ntomb > 0) {  // tombstone_config (src/incremental.rs:505-516)
     cfg.filtered = true;
-    cfg.expanded = std::max<uint64_t>((uint64_t)L * 2, k + std::min<uint64_t>(ntomb, L));
+    cfg.expanded = std::max<uint64_t>((uint64_t)L * 2, search_k + std::min<uint64_t>(ntomb, L));
     cfg.max_iter = (uint64_t)cfg.expanded * 2;
     cfg.early = 1.5f;
   }
@@ -916,9 +919,24 @@ int dgo_incremental_search_batch(const DgoIndex *idx, const DgoSearchParams *p, 
       return !labeled || filter_eval(p->filter, p->filter_nops, p->filter_pool,
                                      I.labels + (uint64_t)id * I.num_fields, I.num_fields);
     };
-    auto dist = [&](uint32_t id) { return metric_eval(I.metric, q, I.vectors + (uint64_t)id * I.d, I.d); };
+    auto exact = [&](uint32_t id) { return metric_eval(I.metric, q, I.vectors + (uint64_t)id * I.d, I.d); };
     std::vector<Cand> out;
-    if (nseeds) beam_search(seeds, nseeds, L, k, dist, AdjNbrs{I.adjacency, I.R}, allow, cfg, out, nullptr);
+    if (codes) {
+      Prepared prep;
+      prepare(I, q, prep);
+      std::vector<float> scratch;
+      auto dist = [&](uint32_t id) {
+        return id < code_limit ? quantized_distance(I, q, id, prep, scratch) : exact(id);
+      };
+      if (nseeds) beam_search(seeds, nseeds, L, search_k, dist, AdjNbrs{I.adjacency, I.R}, allow, cfg, out, nullptr);
+      if (p->rerank_size > 0) {  // :972-981: exact distances, sorted, truncated to k
+        for (auto &c : out) c.d = exact(c.id);
+        std::stable_sort(out.begin(), out.end(), [](const Cand &a, const Cand &b) { return a.d < b.d; });
+        if (out.size() > k) out.resize(k);
+      }
+    } else if (nseeds) {
+      beam_search(seeds, nseeds, L, k, exact, AdjNbrs{I.adjacency, I.R}, allow, cfg, out, nullptr);
+    }
     for (uint32_t j = 0; j < k; ++j) {
       out_ids[qi * k + j] = j < out.size() ? out[j].id : DGO_PAD;
       out_d[qi * k + j] = j < out.size() ? out[j].d : kInf;

@@ -104,10 +104,12 @@ int dgo_beam_search_table(const uint32_t *adj, uint32_t R, const float *node_dis
 /* IncrementalDiskANN::search_with_dists / search_filtered_with_dists
  * (src/incremental.rs:934-1070) over the unified view held in idx (base rows,
  * then delta rows): nseeds entry points, dead[id] != 0 for tombstoned rows,
- * ntomb = size of the tombstone set (selects tombstone_config, :505-516). */
+ * ntomb = size of the tombstone set (selects tombstone_config, :505-516).
+ * With p->use_codes (and no label filter), rows below code_limit are scored
+ * by their codes and the rest exactly, then p->rerank_size reranks (:944-990). */
 int dgo_incremental_search_batch(const DgoIndex *idx, const DgoSearchParams *p, const uint32_t *seeds,
-                                 uint32_t nseeds, const uint8_t *dead, uint64_t ntomb, const float *Q,
-                                 uint32_t nq, uint32_t *out_ids, float *out_d, uint32_t *out_cnt,
+                                 uint32_t nseeds, const uint8_t *dead, uint64_t ntomb, uint64_t code_limit,
+                                 const float *Q, uint32_t nq, uint32_t *out_ids, float *out_d, uint32_t *out_cnt,
                                  int32_t nthreads);
 int dgo_search_batch(const DgoIndex *idx, const DgoSearchParams *p, const float *Q, uint32_t nq,
                      const uint32_t *per_query_L, uint32_t *out_ids, float *out_d,

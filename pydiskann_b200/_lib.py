@@ -99,6 +99,7 @@ def _signatures():
         "dg_index_get_codes": (st, [vp, vp, u64, vp]),
         "dg_index_autotune": (st, [vp, vp, vp, u32, u32, vp, vp]),
         "dg_index_set_entry_points": (st, [vp, vp, u32]),
+        "dg_index_set_code_limit": (st, [vp, u64]),
         "dg_index_set_tombstones": (st, [vp, vp, u64, i32, u64]),
         "dg_index_update_rows": (st, [vp, u64, u64, vp, vp, vp]),
         "dg_delta_insert": (st, [vp, u32, i32, u32, vp, u64, u64, vp]),

@@ -355,12 +355,21 @@ DgStatus dg_index_set_tombstones(DgIndex *idx, const uint32_t *ids, uint64_t n, 
   return DG_OK;
 }
 
+DgStatus dg_index_set_code_limit(DgIndex *idx, uint64_t limit) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  if (limit > idx->n) return fail(DG_EINVAL, "code limit above the number of rows");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  idx->code_limit = limit;
+  return DG_OK;
+}
+
 DgStatus dg_index_update_rows(DgIndex *idx, uint64_t first, uint64_t count, const float *vectors,
                               const uint32_t *adjacency, const uint64_t *labels) {
   if (!idx) return fail(DG_EINVAL, "null index");
   if (first > idx->n || count > idx->n - first) return fail(DG_EINVAL, "rows out of range");
-  if (vectors && idx->quant != DG_Q_NONE)
-    return fail(DG_ENOTSUP, "rows of an index with quantized codes cannot be replaced");
+  const uint64_t coded = idx->code_limit && idx->code_limit < idx->n ? idx->code_limit : idx->n;
+  if (vectors && idx->quant != DG_Q_NONE && first < coded)
+    return fail(DG_ENOTSUP, "rows with quantized codes cannot be replaced (set a code limit below them)");
   if (labels && !idx->labels) return fail(DG_EINVAL, "the index has no labels");
   if (adjacency)
     for (uint64_t i = 0; i < count * idx->R; ++i)
@@ -449,6 +458,7 @@ static void index_state(const DgIndex *idx, SearchArgs &a) {
   const bool tombed = idx->tomb && idx->ntomb > 0;
   a.tomb = tombed ? idx->tomb : nullptr;
   a.ntomb = tombed ? (uint32_t)std::min<uint64_t>(idx->ntomb, 0xffffffffu) : 0;
+  a.code_limit = idx->code_limit && idx->code_limit < idx->n ? idx->code_limit : idx->n;
 }
 
 // Stack depth a postfix program needs; -1 if it is malformed.

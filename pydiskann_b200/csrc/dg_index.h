@@ -37,6 +37,7 @@ struct DgIndex {
   uint32_t *tomb = nullptr;            // [ceil(n/32)] deleted-id bitmap (device)
   std::vector<uint32_t> tomb_host;     // its host copy
   uint64_t ntomb = 0;                  // tombstone count the search config uses
+  uint64_t code_limit = 0;             // rows >= code_limit have no codes (0 = every row has)
   // visited-table size (log2 words per query) chosen by dg_index_autotune per
   // (traversal, working-set capacity, filtered); hbits_force > 0 pins it while tuning
   std::map<uint32_t, uint32_t> tuned_hbits;

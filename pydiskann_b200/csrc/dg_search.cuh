@@ -55,6 +55,7 @@ struct SearchArgs {
   uint32_t seed2;            // DG_PAD = one seed (the medoid)
   const uint32_t *tomb;      // [ceil(n/32)] deleted-id bitmap, null = no tombstones
   uint32_t ntomb;            // tombstone count the search config uses (> 0 when tomb is set)
+  uint64_t code_limit;       // code traversals score rows >= code_limit exactly (delta rows); n = none
   // labels / filter
   const uint64_t *labels;
   uint32_t nf;

@@ -102,6 +102,28 @@ __device__ __forceinline__ float exact_distance(const SearchArgs &a, const float
                                      (a.dpad / 4) / LPRF, qs, cand, cnt, lane, a.metric == DG_L2, qq);
 }
 
+// Exact FP32 distance of one row by one lane (few registers): code traversals
+// of a base + delta index use it for delta rows, which carry no codes
+// (IncrementalDiskANN::search_with_dists scores them with distance_to,
+// src/incremental.rs:955-968).  Padding columns are zero in the row and query.
+template <int MET>
+__device__ __forceinline__ float exact_row_distance(const SearchArgs &a, const float *qs, uint32_t id, float qq) {
+  const float4 *row = reinterpret_cast<const float4 *>(a.vec_f32 + (size_t)id * a.dpad);
+  const float4 *q4 = reinterpret_cast<const float4 *>(qs);
+  float acc = 0.0f, bb = 0.0f;
+  for (uint32_t c = 0; c < a.dpad / 4; ++c) {
+    const float4 v = __ldg(row + c), q = q4[c];
+    if (MET == MET_L2) {
+      const float t0 = q.x - v.x, t1 = q.y - v.y, t2 = q.z - v.z, t3 = q.w - v.w;
+      acc = fmaf(t0, t0, fmaf(t1, t1, fmaf(t2, t2, fmaf(t3, t3, acc))));
+    } else {
+      acc = fmaf(q.x, v.x, fmaf(q.y, v.y, fmaf(q.z, v.z, fmaf(q.w, v.w, acc))));
+      if (MET == MET_COS) bb = fmaf(v.x, v.x, fmaf(v.y, v.y, fmaf(v.z, v.z, fmaf(v.w, v.w, bb))));
+    }
+  }
+  return finish_metric(MET, a.metric == DG_L2, acc, bb, qq);
+}
+
 // Per-query quantizer state (QuantizerState::prepare, src/quantized.rs:167-174).
 template <int TRAV, int MET>
 __device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm, const WarpLayout &Ly,
@@ -506,7 +528,9 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     for (int g0 = 0; g0 < ns; g0 += 32) {
       const int cnt = min(32, ns - g0);
       const uint32_t cand = lane < cnt ? stage[g0 + lane] : DG_PAD;
-      const float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, cnt, lane, qq);
+      float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, cnt, lane, qq);
+      if (TRAV != TRAV_F32 && a.code_limit < a.n && lane < cnt && cand >= a.code_limit)
+        d = exact_row_distance<MET>(a, qs, cand, qq);
       uint64_t key = lane < cnt ? make_key(d, cand) : kKeyInvalid;
       bool match = false;
       if (filtered && lane < cnt) match = allow(cand);

@@ -603,11 +603,12 @@ def postings_bytes(blocks, block: int, code_size: int) -> bytes:
 
 
 def incremental_bytes(vectors, graph, entry_point, max_degree, tombstones=(), base=None, labels=None,
-                      dim=None) -> bytes:
-    """IncrementalDiskANN::to_bytes (src/incremental.rs:1234-1327) without a
-    quantizer section: the base core bytes (or none), the delta rows, their
-    adjacency lists (local indexes), entry point (-1 = none), max degree,
-    tombstones, and labels as (num_fields, base_labels, delta_labels) or None."""
+                      dim=None, quantizer=None) -> bytes:
+    """IncrementalDiskANN::to_bytes (src/incremental.rs:1234-1327): the base core
+    bytes (or none), the delta rows, their adjacency lists (local indexes),
+    entry point (-1 = none), max degree, tombstones, labels as (num_fields,
+    base_labels, delta_labels) or None, and the quantizer as (code_size,
+    rerank_size, QuantizerState, base codes) or None."""
     V = np.ascontiguousarray(vectors, dtype="<f4")
     d = V.shape[1] if V.ndim == 2 and V.shape[1] else int(dim or 0)
     V = V.reshape(-1, d) if d else V.reshape(0, 0)
@@ -626,15 +627,22 @@ def incremental_bytes(vectors, graph, entry_point, max_degree, tombstones=(), ba
         bl = np.ascontiguousarray(bl, dtype="<u8").reshape(-1, nf) if nf else np.zeros((len(bl), 0), "<u8")
         dl = np.ascontiguousarray(dl, dtype="<u8").reshape(-1, nf) if nf else np.zeros((len(dl), 0), "<u8")
         parts += [b"\x01", struct.pack("<QQ", nf, len(bl)), bl.tobytes(), struct.pack("<Q", len(dl)), dl.tobytes()]
-    parts.append(b"\x00")  # no quantizer
+    if quantizer is None:
+        parts.append(b"\x00")
+    else:
+        cs, rr, st, codes = quantizer
+        q = quantizer_state_bytes(st)
+        c = np.ascontiguousarray(codes, dtype=np.uint8).reshape(-1)
+        parts += [b"\x01", struct.pack("<QQQ", cs, rr, len(q)), q, struct.pack("<Q", c.size), c.tobytes()]
     return b"".join(parts)
 
 
 def parse_incremental(buf) -> dict:
     """IncrementalDiskANN::from_bytes_v1 (src/incremental.rs:1451-1611): base
     bytes (or None), dim, delta vectors f32[n, dim], adjacency lists, entry
-    point, max degree, tombstones, labels as (num_fields, base, delta) or None.
-    The older layout without the magic and a quantizer section are refused."""
+    point, max degree, tombstones, labels as (num_fields, base, delta) or None,
+    quantizer as (code_size, rerank_size, QuantizerState, codes u8[]) or None.
+    The older layout without the magic is refused."""
     b = memoryview(buf).cast("B")
     r = _Reader(b)
 
@@ -682,12 +690,21 @@ def parse_incremental(buf) -> dict:
         s = trunc(lambda: r._take(ndl * nf * 8))
         dl = np.frombuffer(b, dtype="<u8", count=ndl * nf, offset=s).reshape(ndl, nf).astype(np.uint64)
         labels = (nf, bl, dl)
+    quant = None
     if trunc(r.u8) == 1:
-        raise _index_error("incremental indexes with a quantizer section are not supported")
+        cs, rr, ql = trunc(r.u64), trunc(r.u64), trunc(r.u64)
+        s = trunc(lambda: r._take(ql))
+        st = _read_state(_Reader(b, s, s + ql))
+        _check_state(st)
+        if st.code_size != cs:
+            raise _index_error(f"code_size {cs} != {st.kind} code size {st.code_size}")
+        nc = trunc(r.u64)
+        s = trunc(lambda: r._take(nc))
+        quant = (cs, rr, st, np.frombuffer(b, dtype=np.uint8, count=nc, offset=s).copy())
     if len(graph) != nd:
         raise _index_error(f"{len(graph)} adjacency lists for {nd} delta vectors")
     return {"base": base, "dim": dim, "vectors": V, "graph": graph, "entry_point": None if ep < 0 else ep,
-            "max_degree": max_degree, "tombstones": tomb, "labels": labels}
+            "max_degree": max_degree, "tombstones": tomb, "labels": labels, "quantizer": quant}
 
 
 def check_incremental_header(buf):

@@ -30,7 +30,8 @@ class IncrementalDiskANN:
     """IncrementalDiskANN<D> with the binding's methods (python/src/lib.rs:126-205)."""
 
     def __init__(self, vectors, adjacency, medoid_id, metric="l2", labels=None, delta_threshold=10_000,
-                 tombstone_ratio=0.1, delta_max_degree=32, device=0):
+                 tombstone_ratio=0.1, delta_max_degree=32, device=0, quantizer=None, qparams=None, rerank_size=0,
+                 base_codes=None):
         if metric not in _METRICS:
             raise ValueError(f"unknown metric: {metric}")
         X = np.ascontiguousarray(vectors, dtype=np.float32)
@@ -52,6 +53,12 @@ class IncrementalDiskANN:
             raise RuntimeError(f"Index error: vectors.len() ({len(X)}) != labels.len() ({len(self._bL)})")
         self._dL = np.zeros((0, self._nf), np.uint64)
         self.tombstones: set[int] = set()
+        # quantized base (build_quantized_*, src/incremental.rs:674-827): base rows
+        # are scored by their codes, delta rows exactly; rerank_size reranks
+        if quantizer not in (None, "f16", "int8", "pq", "rabitq"):
+            raise ValueError(f"unknown quantizer: {quantizer}")
+        self.quantizer, self._qp, self.rerank_size = quantizer, dict(qparams or {}), rerank_size
+        self._base_codes = None if base_codes is None else np.ascontiguousarray(base_codes, dtype=np.uint8)
         self._ix = None
         self._cap = 0
         self._mirror(1024)
@@ -66,8 +73,8 @@ class IncrementalDiskANN:
         file at `path` when one is given."""
         import pydiskann_b200 as dg
 
-        if quantizer is not None:
-            raise ValueError("quantized incremental indexes are not supported; build without a quantizer")
+        if quantizer not in (None, "f16", "int8", "pq", "rabitq"):
+            raise ValueError(f"unknown quantizer: {quantizer}")
         X = np.ascontiguousarray(vectors, dtype=np.float32)
         if X.ndim != 2 or X.shape[0] == 0:
             raise RuntimeError("Index error: No vectors provided")
@@ -76,7 +83,15 @@ class IncrementalDiskANN:
         adj, med = dg.build_graph(X, max_degree, build_beam_width, alpha, metric, seed, None, device)
         if path is not None:
             _fmt.write_core(path, X, adj, med, metric)
-        return IncrementalDiskANN(X, adj, med, metric, labels, delta_threshold, tombstone_ratio, device=device)
+        qp = {}
+        if quantizer == "int8":  # trained on the build vectors, as build_quantized_int8
+            qp["scale"], qp["offset"] = dg.int8_params(X)
+        elif quantizer == "pq":
+            qp["codebooks"] = dg.pq_train(X, pq_subspaces, 256, 20, 50_000, seed, device)
+        elif quantizer == "rabitq":
+            qp["centroid"], qp["signs"] = dg.rabitq_params(X, seed)
+        return IncrementalDiskANN(X, adj, med, metric, labels, delta_threshold, tombstone_ratio, device=device,
+                                  quantizer=quantizer, qparams=qp, rerank_size=rerank_size)
 
     @staticmethod
     def open(path, metric="l2", device=0):
@@ -120,7 +135,11 @@ class IncrementalDiskANN:
             A[nb: nb + self._dn] = self._delta_rows(0, self._dn)[1]
         import pydiskann_b200 as dg
 
-        self._ix = dg._Index(X, A, self._bmed, self.metric_name, self.device)
+        if self.quantizer is None:
+            self._ix = dg._Index(X, A, self._bmed, self.metric_name, self.device)
+        else:
+            self._ix = dg.QuantizedDiskANN(X, A, self._bmed, self.metric_name, self.device, self.rerank_size)
+            self._attach_codes(n)
         self._h = self._ix._h
         if self._nf:
             Lb = np.zeros((n, self._nf), np.uint64)
@@ -131,6 +150,24 @@ class IncrementalDiskANN:
             self._ix.enable_bf16()
         self._publish_seeds()
         self._publish_tombstones(list(self.tombstones))
+
+    def _attach_codes(self, n):
+        """Codes of the base rows (given, or encoded on the GPU); rows past the
+        base carry none (dg_index_set_code_limit)."""
+        codes = None
+        if self._base_codes is not None:
+            codes = np.zeros((n, self._base_codes.shape[1]), np.uint8)
+            codes[: self.base_count] = self._base_codes
+        q, p = self.quantizer, self._qp
+        if q == "int8":
+            self._ix.attach_int8(p["scale"], p["offset"], codes)
+        elif q == "f16":
+            self._ix.attach_f16(None if codes is None else codes.view(np.uint16))
+        elif q == "pq":
+            self._ix.attach_pq(p["codebooks"], codes)
+        else:
+            self._ix.attach_rabitq(p["centroid"], p["signs"], codes)
+        check(lib().dg_index_set_code_limit(self._ix._h, self.base_count))
 
     def _publish_seeds(self):
         """UnifiedView::entry_points (src/incremental.rs:383-392)."""
@@ -239,15 +276,18 @@ class IncrementalDiskANN:
         g[delta] = np.uint64(DELTA_ID_OFFSET) + (ids[delta].astype(np.uint64) - np.uint64(nb))
         return g
 
-    def search_arrays(self, queries, k=10, beam_width=128, filters=None, traversal=_lib.TRAVERSE_F32,
-                      rerank_size=0):
+    def search_arrays(self, queries, k=10, beam_width=128, filters=None, traversal=None, rerank_size=None):
         """Batched search: (ids u64[nq, k], dists f32[nq, k], counts u32[nq]).
         A filter only applies to an index with labels, as in
         search_filtered_with_dists (src/incremental.rs:1020-1030)."""
         Q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, self.dim)
         if filters is not None and not self._nf:
             filters = None
-        ids, ds, cnt = self._ix.search_arrays(Q, k, beam_width, traversal, rerank_size, filters=filters)
+        if traversal is None:  # the quantizer's codes unless a label filter is given (:1020-1070)
+            traversal = _lib.TRAVERSE_CODES if self.quantizer and filters is None else _lib.TRAVERSE_F32
+        if rerank_size is None:
+            rerank_size = self.rerank_size if traversal == _lib.TRAVERSE_CODES else 0
+        ids, ds, cnt = _Index_search(self._ix, Q, k, beam_width, traversal, rerank_size, filters)
         return self._to_global(ids, cnt), ds, cnt
 
     def enable_bf16(self):
@@ -309,6 +349,7 @@ class IncrementalDiskANN:
         if new_path is not None:
             _fmt.write_core(new_path, X, adj, med, self.metric_name)
         self._bX, self._bA, self._bmed, self._bL = X, adj, int(med), L
+        self._base_codes = None  # re-encoded with the same quantizer (:1180-1190)
         self._dX = np.zeros((0, self.dim), np.float32)
         self._dA = np.zeros((0, self._dR), np.uint32)
         self._dL = np.zeros((0, self._nf), np.uint64)
@@ -330,13 +371,31 @@ class IncrementalDiskANN:
         if self._nf:
             labels = (self._nf, self._bL, self._dL[: self._dn])
         base = _fmt.core_bytes(self._bX, self._bA, self._bmed, self.metric_name)
+        quant = None
+        if self.quantizer:
+            st = self._state()
+            quant = (st.code_size, self.rerank_size, st, self._ix.codes()[: self.base_count])
         return _fmt.incremental_bytes(self._dX[: self._dn], graph, None if self._ep < 0 else self._ep, self._dR,
-                                      sorted(self.tombstones), base=base, labels=labels, dim=self.dim)
+                                      sorted(self.tombstones), base=base, labels=labels, dim=self.dim,
+                                      quantizer=quant)
+
+    def _state(self):
+        """The quantizer as the serialized QuantizerState."""
+        q, p = self.quantizer, self._qp
+        if q == "int8":
+            return _fmt.QuantizerState("int8", self.dim, scale=float(p["scale"]), offset=float(p["offset"]))
+        if q == "f16":
+            return _fmt.QuantizerState("f16", self.dim)
+        if q == "pq":
+            cb = np.asarray(p["codebooks"], np.float32)
+            return _fmt.QuantizerState("pq", self.dim, *cb.shape, codebooks=cb.reshape(-1))
+        sg = np.asarray(p["signs"], np.float32)
+        return _fmt.QuantizerState("rabitq", self.dim, padded=sg.size // 3,
+                                   centroid=np.asarray(p["centroid"], np.float32), signs=sg)
 
     @staticmethod
     def from_bytes(data, metric="l2", device=0):
-        """IncrementalDiskANN::from_bytes (src/incremental.rs:1332-1611), INCR v2
-        without a quantizer section."""
+        """IncrementalDiskANN::from_bytes (src/incremental.rs:1332-1611), INCR v2."""
         if metric not in _METRICS:
             raise ValueError(f"unknown metric: {metric}")
         p = _fmt.parse_incremental(data)
@@ -344,7 +403,19 @@ class IncrementalDiskANN:
             raise RuntimeError("Index error: an incremental index without a base layer is not supported")
         m, X, A = _fmt.parse_core(p["base"])
         lab = p["labels"]
-        ix = IncrementalDiskANN(X, A, m.medoid_id, metric, None if lab is None else lab[1], device=device)
+        qz = p["quantizer"]
+        kw = {}
+        if qz is not None:
+            code_size, rerank, st, codes = qz
+            if st.dim != m.dim or codes.size != m.num_vectors * code_size:
+                raise RuntimeError("Index error: quantizer section does not match the base index")
+            qp = {"int8": lambda: {"scale": st.scale, "offset": st.offset}, "f16": lambda: {},
+                  "pq": lambda: {"codebooks": st.codebooks.reshape(st.num_subspaces, st.num_centroids,
+                                                                   st.subspace_dim)},
+                  "rabitq": lambda: {"centroid": st.centroid, "signs": st.signs}}[st.kind]()
+            kw = {"quantizer": st.kind, "qparams": qp, "rerank_size": int(rerank),
+                  "base_codes": codes.reshape(m.num_vectors, code_size)}
+        ix = IncrementalDiskANN(X, A, m.medoid_id, metric, None if lab is None else lab[1], device=device, **kw)
         ix._dR = max(int(p["max_degree"]), max((len(g) for g in p["graph"]), default=0), 1)
         dn = len(p["vectors"])
         ix._dX = np.array(p["vectors"], dtype=np.float32).reshape(dn, ix.dim)
@@ -361,3 +432,11 @@ class IncrementalDiskANN:
         ix.tombstones = set(int(t) for t in p["tombstones"])
         ix._mirror(max(1024, dn))
         return ix
+
+
+def _Index_search(ix, Q, k, L, traversal, rerank_size, filters):
+    """The mirror's batched search with the base class's argument order (a
+    QuantizedDiskANN mirror defaults its traversal and rerank otherwise)."""
+    import pydiskann_b200 as dg
+
+    return dg._Index.search_arrays(ix, Q, k, L, traversal, rerank_size, filters=filters)

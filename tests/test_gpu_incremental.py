@@ -145,3 +145,53 @@ def test_growth_compaction_and_bytes(inc, small_data, oracle):
     assert st["base_vectors"] == live and st["delta_vectors"] == 0 and st["tombstones"] == 0
     got = ix.search(X[3100], 1, 64)
     assert len(got) == 1 and got[0] < DELTA_ID_OFFSET
+
+
+@pytest.mark.parametrize("quantizer", ["int8", "pq", "rabitq", "f16"])
+def test_quantized_base(small_data, oracle, quantizer):
+    """build_quantized_* (src/incremental.rs:674-827): base rows are scored by
+    their codes, delta rows exactly, then the FP32 rerank; the oracle runs the
+    same search over the same codes with tombstones in play."""
+    import oracle as o
+
+    X, Q = small_data
+    base = X[:2500]
+    badj, bmed = o.build_vamana(base, R=24, L_build=48, alpha=1.2, seed=5)
+    qp = {}
+    if quantizer == "int8":
+        qp["scale"], qp["offset"] = dg.int8_params(base)
+    elif quantizer == "pq":
+        qp["codebooks"] = dg.pq_train(base, 16, 256, 8, 2500, seed=2)
+    elif quantizer == "rabitq":
+        qp["centroid"], qp["signs"] = dg.rabitq_params(base, seed=2)
+    ix = dg.IncrementalDiskANN(base, badj, bmed, quantizer=quantizer, qparams=qp, rerank_size=24)
+    ix.add_vectors(X[2500:3100])
+    ix.delete_vectors(list(range(0, 2500, 17)) + [DELTA_ID_OFFSET + 5])
+    X_u, A, seeds, dead = _unified(ix)
+    ov = oracle.OracleIndex(X_u, A, seeds[0])
+    codes = np.zeros((len(X_u), ix._ix.codes().shape[1]), np.uint8)
+    codes[: ix.base_count] = ix._ix.codes()[: ix.base_count]
+    if quantizer == "int8":
+        ov.set_int8(qp["scale"], qp["offset"], codes)
+    elif quantizer == "pq":
+        ov.set_pq(qp["codebooks"], codes)
+    elif quantizer == "rabitq":
+        ov.set_rabitq(dg.rabitq_padded(X.shape[1]), qp["centroid"], qp["signs"], codes)
+    else:
+        ov.set_f16(codes.view(np.uint16))
+    for rr in (0, 24):
+        oi, od, oc = ov.incremental_search(Q, 10, 48, seeds, dead, len(ix.tombstones), use_codes=True, rerank=rr,
+                                           code_limit=ix.base_count)
+        gi, gd, gc = ix.search_arrays(Q, 10, 48, rerank_size=rr)
+        nb = ix.base_count
+        want = oi.astype(np.uint64)
+        dl = (oi != PAD) & (oi >= nb)
+        want[dl] = np.uint64(DELTA_ID_OFFSET) + (oi[dl].astype(np.uint64) - np.uint64(nb))
+        assert np.array_equal(gc, oc)
+        assert np.array_equal(gi, np.where(oi == PAD, np.uint64(PAD), want)), quantizer
+        assert np.array_equal(gd, od), quantizer
+    back = dg.IncrementalDiskANN.from_bytes(ix.to_bytes())
+    for x, y in zip(ix.search_arrays(Q, 10, 48), back.search_arrays(Q, 10, 48)):
+        assert np.array_equal(x, y)
+    back.close()
+    ix.close()

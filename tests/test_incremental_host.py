@@ -77,7 +77,18 @@ def test_incremental_bytes_with_base_labels_tombstones():
     assert np.array_equal(p["labels"][1], BL) and np.array_equal(p["labels"][2], DL)
     with pytest.raises(RuntimeError, match="truncated"):
         F.parse_incremental(raw[:-20])
-    with pytest.raises(RuntimeError, match="quantizer"):
-        F.parse_incremental(raw[:-1] + b"\x01")
+    with pytest.raises(RuntimeError, match="truncated"):
+        F.parse_incremental(raw[:-1] + b"\x01")  # a quantizer flag with no section
+    # quantizer section (src/incremental.rs:1308-1324): code size, rerank size,
+    # bincode QuantizerState, base codes
+    st = F.QuantizerState("int8", 2, scale=0.5, offset=-1.0)
+    codes = np.array([[1, 2], [3, 4]], np.uint8)
+    rq = F.incremental_bytes(V, [[1], [0]], 0, 32, [], base=core, quantizer=(2, 7, st, codes))
+    qbody = struct.pack("<IQff", 2, 2, 0.5, -1.0)
+    assert rq.endswith(b"\x00" + b"\x01" + struct.pack("<QQQ", 2, 7, len(qbody)) + qbody + struct.pack("<Q", 4)
+                       + codes.tobytes())
+    pq = F.parse_incremental(rq)
+    cs, rr, st2, c2 = pq["quantizer"]
+    assert (cs, rr, st2.kind, st2.scale, st2.offset) == (2, 7, "int8", 0.5, -1.0) and np.array_equal(c2, codes.ravel())
     with pytest.raises(RuntimeError, match="Unsupported incremental format version: 1"):
         F.parse_incremental(struct.pack("<II", 0x494E4352, 1) + raw[8:])
