@@ -50,6 +50,9 @@ struct DgSpfresh {
   std::vector<void *> allocs;
   DgIndex::Buf q, oids, od, ocnt, route;  // route: query x posting routing distances of one chunk
   DgIndex::Buf live_idx;                   // [0]: number of live postings, then their slot indices
+  // posting-major scan of one chunk: probes per query, (query, posting) pairs
+  // grouped by posting, work items, per-pair candidate lists
+  DgIndex::Buf probe, probe_cnt, pcount, pstart, pfill, istart, pair_q, pos_of, items, pair_keys, pair_cnt, misc;
 };
 
 namespace dg {
@@ -79,6 +82,8 @@ struct SpfArgs {
   uint32_t *counter;
   const float *route;        // [nq][nblocks] routing distances (null: computed in the scan kernel)
   const uint32_t *route_idx; // [1 + live] count, then the live slots the columns of `route` belong to
+  uint32_t *probe_out;       // non-null: write each query's probed slots ([nq][nprobe]) and stop
+  uint32_t *probe_cnt;       // [nq] number of probed slots
 };
 
 enum SpfKind { SPF_RAW = 0, SPF_PQ = 1, SPF_INT8 = 2, SPF_F16 = 3, SPF_RABITQ = 4 };
@@ -423,6 +428,12 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
         np = first_out;
       }
     }
+    if (a.probe_out) {  // posting-major scan: hand over the probed postings
+      for (int i = lane; i < np; i += 32) a.probe_out[(size_t)q * a.nprobe + i] = key_id(P[pcur][i]);
+      if (lane == 0) a.probe_cnt[q] = (uint32_t)np;
+      __syncwarp();
+      continue;
+    }
     // ---- per-query code state
     if (KIND == SPF_PQ && MET == MET_L2) {
       SearchArgs sa{};
@@ -586,6 +597,394 @@ static DgStatus spf_launch(const SpfArgs &a, uint32_t pcap, uint32_t rcap, cudaS
   return DG_OK;
 }
 
+// ------------------------------------------------ posting-major scan (raw f32, L2)
+// A batch probes each posting from many queries (10k queries x 64 probes over
+// 24k postings: ~27 each).  Instead of every query reading its postings, the
+// (query, posting) pairs are grouped by posting and one CTA loads a posting's
+// entries into shared memory once and scores every query that probes it,
+// keeping each pair's k best; a per-query merge then forms the result.  The
+// result is the k smallest (distance, id) keys over the live entries of the
+// probed postings, as the query-major scan (src/spfresh.rs:702-727); each
+// distance is a sequential FP32 sum in coordinate order (the oracle's).
+constexpr int kPmQ = 32;   // queries per work item
+constexpr int kPmT = 64;   // entries per shared-memory tile
+constexpr int kPmK = 64;   // largest k of the posting-major scan
+
+// Radix pass of k_pm_select: among this warp's keys matching (prefix, mask),
+// counts `width` bits at `shift`, then finds the bucket holding the need-th
+// key.  Returns that bucket; need becomes its rank inside the bucket.
+template <typename KeyOf>
+__device__ __forceinline__ uint32_t pm_radix_pass(uint32_t *hist, uint32_t nl, KeyOf key_of, uint32_t prefix,
+                                                  uint32_t mask, int shift, int width, uint32_t &need, int lane) {
+  const uint32_t nb = 1u << width;
+  for (uint32_t i = lane; i < nb; i += 32) hist[i] = 0u;
+  __syncwarp();
+  for (uint32_t j = lane; j < nl; j += 32) {
+    bool ok;
+    const uint32_t v = key_of(j, ok);
+    if (ok && (v & mask) == prefix) atomicAdd(hist + ((v >> shift) & (nb - 1)), 1u);
+  }
+  __syncwarp();
+  // each lane sums nb / 32 consecutive buckets; a warp scan of the sums
+  const uint32_t per = nb / 32;
+  uint32_t sum = 0;
+  for (uint32_t i = 0; i < per; ++i) sum += hist[lane * per + i];
+  uint32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const uint32_t excl = incl - sum;
+  const uint32_t owner = __ffs(__ballot_sync(kFull, incl >= need)) - 1;
+  uint32_t bucket = 0, below = 0;
+  if (lane == (int)owner) {
+    uint32_t c = excl;
+    for (uint32_t i = 0; i < per; ++i) {
+      const uint32_t h = hist[lane * per + i];
+      if (c + h >= need) {
+        bucket = lane * per + i;
+        below = c;
+        break;
+      }
+      c += h;
+    }
+  }
+  bucket = __shfl_sync(kFull, bucket, owner);
+  below = __shfl_sync(kFull, below, owner);
+  need -= below;
+  __syncwarp();
+  return bucket;
+}
+
+// The posting-major scan's probes: per query (one warp) the exact set of the
+// nprobe smallest (distance, slot) keys of its routing row -- the set the
+// query-major kernel's sorted selection holds (src/spfresh.rs:358-378) -- by
+// radix select over the distance bits (three passes; distances are >= 0 under
+// L2, so their bits order as the values) and, for keys equal to the cut-off
+// distance, over the slot numbers (two passes), then the probe_ratio cut
+// (:690-700).  Unordered output.
+__global__ void __launch_bounds__(128) k_pm_select(const float *route, const uint32_t *route_idx, uint32_t nq,
+                                                   uint32_t nblocks, uint32_t nprobe, float probe_ratio,
+                                                   uint32_t *probe_out, uint32_t *probe_cnt) {
+  __shared__ uint32_t hist_all[4][2048];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t *hist = hist_all[warp];
+  const uint32_t nl = __ldg(route_idx);
+  const uint32_t *col = route_idx + 1;
+  for (uint32_t q = blockIdx.x * 4 + warp; q < nq; q += gridDim.x * 4) {
+    const float *rq = route + (size_t)q * nblocks;
+    const uint32_t take = min(nprobe, nl);
+    // the nearest distance, for the probe_ratio cut
+    float d0 = __int_as_float(0x7f800000);
+    for (uint32_t j = lane; j < nl; j += 32) d0 = fminf(d0, __ldg(rq + j));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d0 = fminf(d0, __shfl_xor_sync(kFull, d0, o));
+    uint32_t tbits = 0xffffffffu, tslot = 0xffffffffu;  // cut-off key (all keys when take == nl)
+    if (take > 0 && take < nl) {
+      uint32_t need = take, prefix = 0, mask = 0;
+      auto dist_bits = [&](uint32_t j, bool &ok) {
+        ok = true;
+        return __float_as_uint(__ldg(rq + j));
+      };
+      const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+      for (int ps = 0; ps < 3; ++ps) {
+        const uint32_t b = pm_radix_pass(hist, nl, dist_bits, prefix, mask, shifts[ps], widths[ps], need, lane);
+        prefix |= b << shifts[ps];
+        mask |= ((1u << widths[ps]) - 1u) << shifts[ps];
+      }
+      tbits = prefix;  // `need` keys at exactly this distance are taken, the smallest slots first
+      auto tie_slot = [&](uint32_t j, bool &ok) {
+        ok = __float_as_uint(__ldg(rq + j)) == tbits;
+        return __ldg(col + j);
+      };
+      uint32_t sp = 0, sm = 0;
+      const int ts[2] = {11, 0}, tw[2] = {11, 11};
+      for (int ps = 0; ps < 2; ++ps) {
+        const uint32_t b = pm_radix_pass(hist, nl, tie_slot, sp, sm, ts[ps], tw[ps], need, lane);
+        sp |= b << ts[ps];
+        sm |= ((1u << tw[ps]) - 1u) << ts[ps];
+      }
+      tslot = sp;
+    }
+    const bool cut = isfinite(probe_ratio) && d0 >= 0.0f;
+    const float lim = cut ? __fmul_rn(d0, fmaxf(probe_ratio, 1.0f)) : __int_as_float(0x7f800000);
+    uint32_t n_out = 0;
+    for (uint32_t j0 = 0; j0 < nl; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      bool sel = false;
+      uint32_t slot = 0;
+      if (j < nl) {
+        const float dv = __ldg(rq + j);
+        const uint32_t bits = __float_as_uint(dv);
+        slot = __ldg(col + j);
+        sel = (bits < tbits || (bits == tbits && slot <= tslot)) && !(dv > lim);
+      }
+      const uint32_t m = __ballot_sync(kFull, sel);
+      if (sel) probe_out[(size_t)q * nprobe + n_out + __popc(m & lanemask_lt(lane))] = slot;
+      n_out += __popc(m);
+    }
+    if (lane == 0) probe_cnt[q] = n_out;
+    __syncwarp();
+  }
+}
+
+__global__ void k_pm_count(const uint32_t *probe, const uint32_t *cnt, uint32_t nq, uint32_t nprobe,
+                           uint32_t *pcount) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < (uint64_t)nq * nprobe;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t q = (uint32_t)(t / nprobe), i = (uint32_t)(t % nprobe);
+    if (i < cnt[q]) atomicAdd(pcount + probe[t], 1u);
+  }
+}
+
+// Exclusive scans of pcount (pair starts) and of ceil(pcount / kPmQ) (item
+// starts) over nb postings; out[nb] of each receives the total.  One block.
+__global__ void __launch_bounds__(1024) k_pm_scan(const uint32_t *pcount, uint32_t nb, uint32_t *pstart,
+                                                  uint32_t *istart) {
+  __shared__ uint32_t sp[1024], si[1024];
+  const uint32_t t = threadIdx.x, per = (nb + 1023) / 1024;
+  const uint32_t b0 = min(nb, t * per), b1 = min(nb, b0 + per);
+  uint32_t a = 0, c = 0;
+  for (uint32_t b = b0; b < b1; ++b) {
+    a += pcount[b];
+    c += (pcount[b] + kPmQ - 1) / kPmQ;
+  }
+  sp[t] = a;
+  si[t] = c;
+  __syncthreads();
+  for (uint32_t o = 1; o < 1024; o <<= 1) {
+    const uint32_t va = t >= o ? sp[t - o] : 0u, vc = t >= o ? si[t - o] : 0u;
+    __syncthreads();
+    sp[t] += va;
+    si[t] += vc;
+    __syncthreads();
+  }
+  a = sp[t] - a;  // exclusive prefix of this thread's range
+  c = si[t] - c;
+  for (uint32_t b = b0; b < b1; ++b) {
+    pstart[b] = a;
+    istart[b] = c;
+    a += pcount[b];
+    c += (pcount[b] + kPmQ - 1) / kPmQ;
+  }
+  if (t == 1023) {
+    pstart[nb] = sp[1023];
+    istart[nb] = si[1023];
+  }
+}
+
+__global__ void k_pm_scatter(const uint32_t *probe, const uint32_t *cnt, uint32_t nq, uint32_t nprobe,
+                             const uint32_t *pstart, uint32_t *pfill, uint32_t *pair_q, uint32_t *pos_of) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < (uint64_t)nq * nprobe;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t q = (uint32_t)(t / nprobe), i = (uint32_t)(t % nprobe);
+    if (i >= cnt[q]) continue;
+    const uint32_t b = probe[t];
+    const uint32_t pos = pstart[b] + atomicAdd(pfill + b, 1u);
+    pair_q[pos] = q;
+    pos_of[t] = pos;
+  }
+}
+
+// items: (posting, first pair, pair count <= kPmQ)
+__global__ void k_pm_items(const uint32_t *pcount, const uint32_t *pstart, const uint32_t *istart, uint32_t nb,
+                           uint4 *items) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const uint32_t c = pcount[b];
+    for (uint32_t j = 0; j * kPmQ < c; ++j)
+      items[istart[b] + j] = make_uint4(b, pstart[b] + j * kPmQ, min((uint32_t)kPmQ, c - j * kPmQ), 0u);
+  }
+}
+
+// One CTA (8 warps) per work item at a time: the item's queries and a tile of
+// the posting's entries in shared memory; warp w scores queries w, w+8, ...
+// against two entries per lane and keeps each query's k best.
+__global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4 *items, const uint32_t *n_items,
+                                                          uint32_t *item_counter, const uint32_t *pair_q,
+                                                          uint64_t *pair_keys, uint32_t *pair_cnt, uint32_t k) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t dq = a.dpad, dt = a.d + 1;  // query rows padded; tile rows d + 1 (conflict-free columns)
+  float *qsm = reinterpret_cast<float *>(smem);                              // [kPmQ][dpad]
+  float *tile = qsm + kPmQ * dq;                                             // [kPmT][d + 1]
+  uint32_t *tid = reinterpret_cast<uint32_t *>(tile + kPmT * dt);            // [kPmT] ids
+  uint64_t *lists = reinterpret_cast<uint64_t *>(tid + kPmT + (kPmT & 1));   // [kPmQ][2][kPmK]
+  uint64_t *cst = lists + (size_t)kPmQ * 2 * kPmK;                           // [8][32]
+  __shared__ uint32_t s_item;
+  const uint32_t total = *n_items;
+  const bool sq = a.metric == DG_L2;
+  while (true) {
+    if (threadIdx.x == 0) s_item = atomicAdd(item_counter, 1u);
+    __syncthreads();
+    const uint32_t it = s_item;
+    __syncthreads();
+    if (it >= total) break;
+    const uint4 item = items[it];
+    const uint32_t b = item.x, p0 = item.y, m = item.z;
+    for (uint32_t t = threadIdx.x; t < m * dq; t += blockDim.x) {
+      const uint32_t j = t / dq, i = t % dq;
+      qsm[t] = i < a.d ? __ldg(a.Q + (size_t)pair_q[p0 + j] * a.d + i) : 0.0f;
+    }
+    // this warp's queries: j = warp + 8 u (u < 4)
+    int cur[4] = {0, 0, 0, 0}, size[4] = {0, 0, 0, 0};
+    const uint32_t n_e = a.len[b];
+    for (uint32_t e0 = 0; e0 < n_e; e0 += kPmT) {
+      const uint32_t ne = min((uint32_t)kPmT, n_e - e0);
+      __syncthreads();  // the previous tile is consumed (and the queries are in place)
+      for (uint32_t t = threadIdx.x; t < ne * a.d; t += blockDim.x) {
+        const uint32_t r = t / a.d, i = t % a.d;
+        tile[r * dt + i] = __ldg(reinterpret_cast<const float *>(a.codes + (size_t)(b * a.cap + e0 + r) * a.code_stride) + i);
+      }
+      for (uint32_t r = threadIdx.x; r < kPmT; r += blockDim.x) {
+        uint32_t id = DG_PAD;
+        if (r < ne) {
+          id = __ldg(a.ids + b * a.cap + e0 + r);
+          if (is_deleted(a.deleted, id)) id = DG_PAD;
+        }
+        tid[r] = id;
+      }
+      __syncthreads();
+      float acc[4][2];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = 0.0f;
+      const float *e0p = tile + (size_t)lane * dt, *e1p = tile + (size_t)(lane + 32) * dt;
+#pragma unroll 8
+      for (uint32_t i = 0; i < a.d; ++i) {
+        const float x0 = e0p[i], x1 = e1p[i];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const uint32_t j = warp + 8 * u;
+          if (j < m) {
+            const float qv = qsm[j * dq + i];
+            const float t0 = __fsub_rn(qv, x0), t1 = __fsub_rn(qv, x1);
+            acc[u][0] = __fadd_rn(acc[u][0], __fmul_rn(t0, t0));
+            acc[u][1] = __fadd_rn(acc[u][1], __fmul_rn(t1, t1));
+          }
+        }
+      }
+      const uint32_t id0 = tid[lane], id1 = tid[lane + 32];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t j = warp + 8 * u;
+        if (j >= m) continue;  // warp-uniform
+        uint64_t *const bufs[2] = {lists + (size_t)j * 2 * kPmK, lists + (size_t)j * 2 * kPmK + kPmK};
+        const float d0 = sq ? __fsqrt_rn(acc[u][0]) : acc[u][0], d1 = sq ? __fsqrt_rn(acc[u][1]) : acc[u][1];
+        insert_batch(id0 != DG_PAD ? make_key(d0, id0) : kKeyInvalid, bufs, cur[u], size[u], (int)k,
+                     cst + warp * 32, lane);
+        insert_batch(id1 != DG_PAD ? make_key(d1, id1) : kKeyInvalid, bufs, cur[u], size[u], (int)k,
+                     cst + warp * 32, lane);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t j = warp + 8 * u;
+      if (j >= m) continue;
+      const uint64_t *lst = lists + (size_t)j * 2 * kPmK + (size_t)cur[u] * kPmK;
+      for (int i = lane; i < size[u]; i += 32) pair_keys[(size_t)(p0 + j) * k + i] = lst[i];
+      if (lane == 0) pair_cnt[p0 + j] = (uint32_t)size[u];
+    }
+  }
+}
+
+// Per query: the k best keys over its probed postings' pair lists.
+__global__ void __launch_bounds__(128) k_pm_merge(const uint32_t *probe_cnt, const uint32_t *pos_of, uint32_t nq,
+                                                  uint32_t nprobe, const uint64_t *pair_keys,
+                                                  const uint32_t *pair_cnt, uint32_t k, uint64_t *out_ids,
+                                                  float *out_d, uint32_t *out_cnt) {
+  __shared__ __align__(16) uint64_t lists[4][2][kPmK];
+  __shared__ __align__(16) uint64_t cst[4][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t *const bufs[2] = {lists[warp][0], lists[warp][1]};
+  for (uint32_t q = blockIdx.x * 4 + warp; q < nq; q += gridDim.x * 4) {
+    int cur = 0, size = 0;
+    const uint32_t np = probe_cnt[q];
+    for (uint32_t i = 0; i < np; ++i) {
+      const uint32_t pos = pos_of[(size_t)q * nprobe + i];
+      const uint32_t c = pair_cnt[pos];
+      for (uint32_t j0 = 0; j0 < c; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        insert_batch(j < c ? pair_keys[(size_t)pos * k + j] : kKeyInvalid, bufs, cur, size, (int)k, cst[warp], lane);
+      }
+    }
+    const int count = min(size, (int)k);
+    for (int i = lane; i < (int)k; i += 32) {
+      out_ids[(size_t)q * k + i] = i < count ? (uint64_t)key_id(bufs[cur][i]) : DG_PAD64;
+      out_d[(size_t)q * k + i] = i < count ? key_dist(bufs[cur][i]) : __int_as_float(0x7f800000);
+    }
+    if (lane == 0) out_cnt[q] = (uint32_t)count;
+    __syncwarp();
+  }
+}
+
+static size_t pm_smem(uint32_t d, uint32_t dpad) {
+  return ((size_t)kPmQ * dpad + (size_t)kPmT * (d + 1)) * 4 + (kPmT + (kPmT & 1)) * 4 + (size_t)kPmQ * 2 * kPmK * 8 +
+         8 * 32 * 8;
+}
+
+// Posting-major scan of one chunk whose routing matrix is in ac.route: probes
+// (the query-major kernel stops after selecting them), pairs grouped by
+// posting, the scan, the per-query merge.
+static DgStatus pm_scan_chunk(DgSpfresh *s, const SpfArgs &ac, uint32_t nprobe, uint32_t k, uint32_t pcap,
+                              uint32_t rcap, cudaStream_t st) {
+  DgStatus r;
+  const uint32_t qn = ac.nq, nb = s->nblocks;
+  const size_t npairs = (size_t)qn * nprobe;
+  const size_t nitems = npairs / kPmQ + nb + 1;
+  if ((r = buf_reserve(s->probe, npairs * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->probe_cnt, (size_t)qn * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->pcount, ((size_t)nb + 1) * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->pstart, ((size_t)nb + 1) * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->pfill, ((size_t)nb + 1) * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->istart, ((size_t)nb + 1) * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->pair_q, npairs * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->pos_of, npairs * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->items, nitems * 16)) != DG_OK) return r;
+  if ((r = buf_reserve(s->pair_keys, npairs * k * 8)) != DG_OK) return r;
+  if ((r = buf_reserve(s->pair_cnt, npairs * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->misc, 16)) != DG_OK) return r;
+  uint32_t *probe = (uint32_t *)s->probe.p, *pcnt = (uint32_t *)s->probe_cnt.p;
+  uint32_t *pcount = (uint32_t *)s->pcount.p, *pstart = (uint32_t *)s->pstart.p, *pfill = (uint32_t *)s->pfill.p;
+  uint32_t *istart = (uint32_t *)s->istart.p, *counter = (uint32_t *)s->misc.p;
+  if (nprobe > 64) {
+    // wide probes: radix select (a sorted list of nprobe keys costs more)
+    k_pm_select<<<(unsigned)std::min<uint32_t>((qn + 3) / 4, 148 * 16), 128, 0, st>>>(
+        ac.route, ac.route_idx, qn, nb, nprobe, ac.probe_ratio, probe, pcnt);
+    DG_CUDA(cudaGetLastError());
+  } else {
+    // the query-major kernel's selection, stopped before its scan
+    SpfArgs ap = ac;
+    ap.probe_out = probe;
+    ap.probe_cnt = pcnt;
+    DG_CUDA(cudaMemsetAsync(ap.counter, 0, 4, st));
+    if ((r = spf_launch<SPF_RAW, MET_L2>(ap, pcap, rcap, st)) != DG_OK) return r;
+  }
+  DG_CUDA(cudaMemsetAsync(pcount, 0, ((size_t)nb + 1) * 4, st));
+  DG_CUDA(cudaMemsetAsync(pfill, 0, ((size_t)nb + 1) * 4, st));
+  DG_CUDA(cudaMemsetAsync(counter, 0, 4, st));
+  const unsigned gp = (unsigned)std::min<size_t>((npairs + 255) / 256, 148 * 16);
+  k_pm_count<<<gp, 256, 0, st>>>(probe, pcnt, qn, nprobe, pcount);
+  k_pm_scan<<<1, 1024, 0, st>>>(pcount, nb, pstart, istart);
+  k_pm_scatter<<<gp, 256, 0, st>>>(probe, pcnt, qn, nprobe, pstart, pfill, (uint32_t *)s->pair_q.p,
+                                   (uint32_t *)s->pos_of.p);
+  k_pm_items<<<(nb + 255) / 256, 256, 0, st>>>(pcount, pstart, istart, nb, (uint4 *)s->items.p);
+  DG_CUDA(cudaGetLastError());
+  const size_t smem = pm_smem(s->d, s->dpad);
+  DG_CUDA(cudaFuncSetAttribute(k_pm_scan_postings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0, sms = 0;
+  DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pm_scan_postings, 256, smem));
+  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+  if (per_sm < 1) return fail(DG_ENOTSUP, "posting-major scan does not fit on an SM");
+  k_pm_scan_postings<<<per_sm * sms, 256, smem, st>>>(ac, (const uint4 *)s->items.p, istart + nb, counter,
+                                                      (const uint32_t *)s->pair_q.p, (uint64_t *)s->pair_keys.p,
+                                                      (uint32_t *)s->pair_cnt.p, k);
+  k_pm_merge<<<(unsigned)std::min<uint32_t>((qn + 3) / 4, 148 * 16), 128, 0, st>>>(
+      pcnt, (const uint32_t *)s->pos_of.p, qn, nprobe, (const uint64_t *)s->pair_keys.p,
+      (const uint32_t *)s->pair_cnt.p, k, ac.out_ids, ac.out_d, ac.out_cnt);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
 template <int KIND>
 static DgStatus spf_launch_met(const SpfArgs &a, int met, uint32_t pcap, uint32_t rcap, cudaStream_t st) {
   if (met == MET_L2) return spf_launch<KIND, MET_L2>(a, pcap, rcap, st);
@@ -613,7 +1012,9 @@ DgStatus dg_spfresh_destroy(DgSpfresh *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (void *p : s->allocs) cudaFree(p);
-  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx})
+  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx, &s->probe, &s->probe_cnt,
+                          &s->pcount, &s->pstart, &s->pfill, &s->istart, &s->pair_q, &s->pos_of, &s->items,
+                          &s->pair_keys, &s->pair_cnt, &s->misc})
     if (b->p) cudaFree(b->p);
   if (s->counter) cudaFree(s->counter);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -870,6 +1271,13 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
       default: return spf_launch_met<SPF_RABITQ>(aa, met, pcap, rcap, st);
     }
   };
+  // raw f32 postings under L2 in batches that probe each posting from about 16
+  // queries or more: the posting-major scan (each probed posting read once per
+  // chunk instead of once per probing query); sparser batches stay query-major
+  const bool posting_major = s->nblocks >= 512 && s->quant == DG_Q_NONE &&
+                             (s->metric == DG_L2 || s->metric == DG_L2SQ) && p->k <= (uint32_t)kPmK && nq >= 256 &&
+                             (uint64_t)nq * nprobe >= 16ull * s->nblocks && s->nblocks < (1u << 22) &&
+                             pm_smem(s->d, s->dpad) <= 200 * 1024;
   if (s->nblocks >= 512) {
     // many postings: route all queries of a chunk in one tiled kernel (the
     // matrix of a chunk stays below 1 GiB), then scan the chunk
@@ -894,7 +1302,11 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
       k_route<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric,
                                     (float *)s->route.p, s->nblocks);
       DG_CUDA(cudaGetLastError());
-      if ((r = scan(ac)) != DG_OK) return r;
+      if (posting_major) {
+        if ((r = pm_scan_chunk(s, ac, nprobe, p->k, pcap, rcap, st)) != DG_OK) return r;
+      } else if ((r = scan(ac)) != DG_OK) {
+        return r;
+      }
     }
   } else if ((r = scan(a)) != DG_OK) {
     return r;

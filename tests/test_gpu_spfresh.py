@@ -182,3 +182,32 @@ def test_many_postings_routing_kernel_matches_oracle(oracle, metric):
         else:
             assert np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
     s.close()
+
+
+@pytest.mark.parametrize("metric", ["l2", "euclidean"])
+def test_posting_major_scan_matches_oracle(oracle, metric):
+    """Batches of >= 256 queries over >= 512 raw postings under L2 run the
+    posting-major scan (pairs grouped by posting, one shared-memory load of a
+    posting for all its queries, per-query merge; probes above 64 chosen by a
+    radix select).  Results equal the oracle's and the query-major scan's (a
+    batch of fewer than 256 queries), with tombstones, a probe_ratio cut and k
+    up to 64."""
+    X = synth.mixture(30000, 48, 64, seed=35, clip=False)
+    Q = synth.mixture(700, 48, 64, seed=35, stream=synth.STREAM_QUERY, clip=False)
+    s = dg.SPFresh.bulk_load(X, metric=metric, max_posting_size=32, seed=7)
+    assert s.stats()["postings"] >= 512
+    s.delete(list(range(0, 30000, 19)))
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 4), (10, 64), (64, 40), (1, 300)):
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
+        qi, qd, qc = s.search_arrays(Q[:200], k, nprobe)  # query-major
+        assert np.array_equal(qi, gi[:200]) and np.array_equal(qd, gd[:200]) and np.array_equal(qc, gc[:200])
+    s.probe_ratio = 1.5
+    view, keep = oracle_view(oracle, s)
+    for nprobe in (64, 200):  # probes chosen by the sorted selection / the radix select
+        gi, gd, gc = s.search_arrays(Q, 10, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, 10, nprobe)
+        assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od), nprobe
+    s.close()
