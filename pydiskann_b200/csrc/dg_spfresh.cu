@@ -605,7 +605,8 @@ static DgStatus spf_launch(const SpfArgs &a, uint32_t pcap, uint32_t rcap, cudaS
 // keeping each pair's k best; a per-query merge then forms the result.  The
 // result is the k smallest (distance, id) keys over the live entries of the
 // probed postings, as the query-major scan (src/spfresh.rs:702-727); each
-// distance is a sequential FP32 sum in coordinate order (the oracle's).
+// distance is |q|^2 + |x|^2 - 2 q.x with FP32 FMA sums (exact on
+// integer-valued data, within FP32 rounding otherwise).
 constexpr int kPmQ = 32;   // queries per work item
 constexpr int kPmT = 64;   // entries per shared-memory tile
 constexpr int kPmK = 64;   // largest k of the posting-major scan
@@ -805,11 +806,15 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
                                                           uint64_t *pair_keys, uint32_t *pair_cnt, uint32_t k) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t dq = a.dpad, dt = a.d + 1;  // query rows padded; tile rows d + 1 (conflict-free columns)
+  // query rows dpad floats; tile rows d + 4 floats: 16-byte rows whose float4
+  // columns fall in distinct banks within each quarter warp
+  const uint32_t dq = a.dpad, dt = a.d + 4, d4 = a.d / 4;
   float *qsm = reinterpret_cast<float *>(smem);                              // [kPmQ][dpad]
-  float *tile = qsm + kPmQ * dq;                                             // [kPmT][d + 1]
+  float *tile = qsm + kPmQ * dq;                                             // [kPmT][d + 4]
   uint32_t *tid = reinterpret_cast<uint32_t *>(tile + kPmT * dt);            // [kPmT] ids
-  uint64_t *lists = reinterpret_cast<uint64_t *>(tid + kPmT + (kPmT & 1));   // [kPmQ][2][kPmK]
+  float *xn = reinterpret_cast<float *>(tid + kPmT);                         // [kPmT] |x|^2
+  float *qn = xn + kPmT;                                                     // [kPmQ] |q|^2
+  uint64_t *lists = reinterpret_cast<uint64_t *>(qn + kPmQ);                 // [kPmQ][2][kPmK]
   uint64_t *cst = lists + (size_t)kPmQ * 2 * kPmK;                           // [8][32]
   __shared__ uint32_t s_item;
   const uint32_t total = *n_items;
@@ -826,15 +831,22 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
       const uint32_t j = t / dq, i = t % dq;
       qsm[t] = i < a.d ? __ldg(a.Q + (size_t)pair_q[p0 + j] * a.d + i) : 0.0f;
     }
+    __syncthreads();
+    if (threadIdx.x < m) {
+      float s2 = 0.0f;
+      for (uint32_t i = 0; i < a.d; ++i) s2 = fmaf(qsm[threadIdx.x * dq + i], qsm[threadIdx.x * dq + i], s2);
+      qn[threadIdx.x] = s2;
+    }
     // this warp's queries: j = warp + 8 u (u < 4)
     int cur[4] = {0, 0, 0, 0}, size[4] = {0, 0, 0, 0};
     const uint32_t n_e = a.len[b];
     for (uint32_t e0 = 0; e0 < n_e; e0 += kPmT) {
       const uint32_t ne = min((uint32_t)kPmT, n_e - e0);
       __syncthreads();  // the previous tile is consumed (and the queries are in place)
-      for (uint32_t t = threadIdx.x; t < ne * a.d; t += blockDim.x) {
-        const uint32_t r = t / a.d, i = t % a.d;
-        tile[r * dt + i] = __ldg(reinterpret_cast<const float *>(a.codes + (size_t)(b * a.cap + e0 + r) * a.code_stride) + i);
+      for (uint32_t t = threadIdx.x; t < ne * d4; t += blockDim.x) {
+        const uint32_t r = t / d4, c = t % d4;
+        reinterpret_cast<float4 *>(tile + r * dt)[c] =
+            __ldg(reinterpret_cast<const float4 *>(a.codes + (size_t)(b * a.cap + e0 + r) * a.code_stride) + c);
       }
       for (uint32_t r = threadIdx.x; r < kPmT; r += blockDim.x) {
         uint32_t id = DG_PAD;
@@ -845,21 +857,28 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         tid[r] = id;
       }
       __syncthreads();
+      if (threadIdx.x < ne) {
+        const float *row = tile + threadIdx.x * dt;
+        float s2 = 0.0f;
+        for (uint32_t i = 0; i < a.d; ++i) s2 = fmaf(row[i], row[i], s2);
+        xn[threadIdx.x] = s2;
+      }
+      __syncthreads();
       float acc[4][2];
 #pragma unroll
       for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = 0.0f;
-      const float *e0p = tile + (size_t)lane * dt, *e1p = tile + (size_t)(lane + 32) * dt;
-#pragma unroll 8
-      for (uint32_t i = 0; i < a.d; ++i) {
-        const float x0 = e0p[i], x1 = e1p[i];
+      const float4 *e0p = reinterpret_cast<const float4 *>(tile + (size_t)lane * dt);
+      const float4 *e1p = reinterpret_cast<const float4 *>(tile + (size_t)(lane + 32) * dt);
+#pragma unroll 2
+      for (uint32_t c = 0; c < d4; ++c) {
+        const float4 x0 = e0p[c], x1 = e1p[c];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const uint32_t j = warp + 8 * u;
           if (j < m) {
-            const float qv = qsm[j * dq + i];
-            const float t0 = __fsub_rn(qv, x0), t1 = __fsub_rn(qv, x1);
-            acc[u][0] = __fadd_rn(acc[u][0], __fmul_rn(t0, t0));
-            acc[u][1] = __fadd_rn(acc[u][1], __fmul_rn(t1, t1));
+            const float4 qv = reinterpret_cast<const float4 *>(qsm + j * dq)[c];
+            acc[u][0] = fmaf(qv.w, x0.w, fmaf(qv.z, x0.z, fmaf(qv.y, x0.y, fmaf(qv.x, x0.x, acc[u][0]))));
+            acc[u][1] = fmaf(qv.w, x1.w, fmaf(qv.z, x1.z, fmaf(qv.y, x1.y, fmaf(qv.x, x1.x, acc[u][1]))));
           }
         }
       }
@@ -869,7 +888,11 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         const uint32_t j = warp + 8 * u;
         if (j >= m) continue;  // warp-uniform
         uint64_t *const bufs[2] = {lists + (size_t)j * 2 * kPmK, lists + (size_t)j * 2 * kPmK + kPmK};
-        const float d0 = sq ? __fsqrt_rn(acc[u][0]) : acc[u][0], d1 = sq ? __fsqrt_rn(acc[u][1]) : acc[u][1];
+        // |q - x|^2 = |q|^2 + |x|^2 - 2 q.x (exact on integer-valued data)
+        const float qq = qn[j];
+        const float s0 = fmaxf(__fsub_rn(__fadd_rn(qq, xn[lane]), __fmul_rn(2.0f, acc[u][0])), 0.0f);
+        const float s1 = fmaxf(__fsub_rn(__fadd_rn(qq, xn[lane + 32]), __fmul_rn(2.0f, acc[u][1])), 0.0f);
+        const float d0 = sq ? __fsqrt_rn(s0) : s0, d1 = sq ? __fsqrt_rn(s1) : s1;
         insert_batch(id0 != DG_PAD ? make_key(d0, id0) : kKeyInvalid, bufs, cur[u], size[u], (int)k,
                      cst + warp * 32, lane);
         insert_batch(id1 != DG_PAD ? make_key(d1, id1) : kKeyInvalid, bufs, cur[u], size[u], (int)k,
@@ -918,7 +941,7 @@ __global__ void __launch_bounds__(128) k_pm_merge(const uint32_t *probe_cnt, con
 }
 
 static size_t pm_smem(uint32_t d, uint32_t dpad) {
-  return ((size_t)kPmQ * dpad + (size_t)kPmT * (d + 1)) * 4 + (kPmT + (kPmT & 1)) * 4 + (size_t)kPmQ * 2 * kPmK * 8 +
+  return ((size_t)kPmQ * dpad + (size_t)kPmT * (d + 4)) * 4 + (2 * kPmT + kPmQ) * 4 + (size_t)kPmQ * 2 * kPmK * 8 +
          8 * 32 * 8;
 }
 
@@ -1276,7 +1299,7 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
   // chunk instead of once per probing query); sparser batches stay query-major
   const bool posting_major = s->nblocks >= 512 && s->quant == DG_Q_NONE &&
                              (s->metric == DG_L2 || s->metric == DG_L2SQ) && p->k <= (uint32_t)kPmK && nq >= 256 &&
-                             (uint64_t)nq * nprobe >= 16ull * s->nblocks && s->nblocks < (1u << 22) &&
+                             (uint64_t)nq * nprobe >= 16ull * s->nblocks && s->nblocks < (1u << 22) && s->d % 4 == 0 &&
                              pm_smem(s->d, s->dpad) <= 200 * 1024;
   if (s->nblocks >= 512) {
     // many postings: route all queries of a chunk in one tiled kernel (the
