@@ -287,7 +287,7 @@ class IncrementalDiskANN:
             traversal = _lib.TRAVERSE_CODES if self.quantizer and filters is None else _lib.TRAVERSE_F32
         if rerank_size is None:
             rerank_size = self.rerank_size if traversal == _lib.TRAVERSE_CODES else 0
-        ids, ds, cnt = _Index_search(self._ix, Q, k, beam_width, traversal, rerank_size, filters)
+        ids, ds, cnt = _mirror_search(self._ix, Q, k, beam_width, traversal, rerank_size, filters)
         return self._to_global(ids, cnt), ds, cnt
 
     def enable_bf16(self):
@@ -434,7 +434,7 @@ class IncrementalDiskANN:
         return ix
 
 
-def _Index_search(ix, Q, k, L, traversal, rerank_size, filters):
+def _mirror_search(ix, Q, k, L, traversal, rerank_size, filters):
     """The mirror's batched search with the base class's argument order (a
     QuantizedDiskANN mirror defaults its traversal and rerank otherwise)."""
     import pydiskann_b200 as dg
