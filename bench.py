@@ -27,7 +27,6 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -236,7 +235,7 @@ def autotune_variant(idx, qidx, name, Qd, L):
     return target.autotune(Qd, K, L, traversal=t, rerank_size=L if rr else 0, reps=3)
 
 
-def distance_error(X, Q, ids, ds, metric_sq=True):
+def distance_error(X, Q, ids, ds):
     """Relative error of returned distances against FP64 squared L2 of the same
     (query, id) pairs: {"max", "mean"} over every returned neighbour."""
     ids = np.asarray(ids)
