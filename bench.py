@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--cosine", action="store_true",
                     help="also run the quantized cosine workload (1M x 768, 20k queries, uneven beams)")
     ap.add_argument("--cosine-n", type=int, default=1_000_000)
+    ap.add_argument("--filtered-serving", action="store_true",
+                    help="also run the filtered serving workload (1M x 256, labels, R=48, Poisson 5k-200k req/s)")
+    ap.add_argument("--fs-n", type=int, default=1_000_000)
     ap.add_argument("--cosine-nq", type=int, default=20_000)
     return ap.parse_args()
 
@@ -436,6 +439,8 @@ def main():
             line["filtered"] = filtered(args, X, Q, adj, med, dev, dist)
         if args.cosine and rank == 0:
             line["quantized_cosine"] = quantized_cosine(args, dev)
+        if args.filtered_serving and rank == 0:
+            line["filtered_serving"] = filtered_serving(args, dev)
         if not args.no_spfresh and rank == 0:
             # one replica is enough for this secondary measurement (it stages
             # several GB of posting blocks on the host)
@@ -584,6 +589,64 @@ def filtered(args, X, Q, adj, med, dev, dist):
         log(f"[filtered serve] {name}: {json.dumps(out['serving']['variants'][name])}")
     f32.close()
     q8.close()
+    return out
+
+
+def filtered_serving(args, dev):
+    """The filtered serving workload: 1M x 256 Gaussian mixture (512 centres),
+    each vector with 1-3 of 100 labels drawn Zipf(1.0); a Vamana graph with
+    R = 48 (the reference has no filter-aware build); queries ask Or(Eq(0, l),
+    Eq(1, l), Eq(2, l)) for a uniform label l (selectivity ~0.5 % to ~35 %).
+    Requests with their own filters arrive as Poisson streams at 5k-200k req/s
+    through the serving loop, for k in {10, 100} and L in {64, 200}, FP32 and
+    BF16 + FP32 rerank; p50 / p99 latency, achieved QPS and recall@10 against
+    exact kNN inside each label's subset."""
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import _lib, synth
+
+    t0 = time.time()
+    nq = 5000
+    X, Q, labels = synth.filtered(args.fs_n, nq, 256, args.seed)
+    adj, med = dg.build_graph(X, 48, 128, 1.2, seed=args.seed, device=dev.index or 0)
+    setup = {"data_and_graph_s": round(time.time() - t0, 1)}
+    ql = np.random.default_rng(args.seed + 11).integers(1, 101, nq)
+    flist = [dg.Filter.or_([dg.Filter.eq(0, int(l)), dg.Filter.eq(1, int(l)), dg.Filter.eq(2, int(l))]) for l in ql]
+    t0 = time.time()
+    gt = np.zeros((nq, K), dtype=np.int64)
+    for l in np.unique(ql):
+        sub = np.nonzero((labels == np.uint64(l)).any(1))[0]
+        qi = np.nonzero(ql == l)[0]
+        ids, _ = dg.exact_knn(X[sub], Q[qi], K, device=dev.index or 0)
+        gt[qi] = sub[ids.astype(np.int64)]
+    setup["ground_truth_s"] = round(time.time() - t0, 1)
+    log(f"[filtered serving] setup {setup}")
+    ix = dg.FilteredDiskANN(X, adj, med, labels, device=dev.index or 0)
+    ix.enable_bf16()
+    out = {"n": len(X), "dim": 256, "R": 48, "queries": nq, "setup": setup, "runs": []}
+    rates = (5_000, 20_000, 50_000, 100_000, 200_000)
+    for name, trav in (("fp32", _lib.TRAVERSE_F32), ("bf16_rerank", _lib.TRAVERSE_BF16)):
+        for k in (10, 100):
+            for L in (64, 200):
+                rr = L if name != "fp32" else 0
+                tune = ix.autotune(Q[:2000], k, L, traversal=trav, rerank_size=rr, filters=flist[:2000], reps=1)
+                with dg.Server(ix, max_batch=512, streams=16, max_k=100) as srv:
+                    srv.run_trace(Q[:1000], np.zeros(1000), k=k, beam_width=L, rerank_size=rr, traversal=trav,
+                                  filters=flist[:1000])
+                    for rate in rates:
+                        n = int(max(2000, rate * 1.0))
+                        qi = np.arange(n) % nq
+                        res = srv.run_trace(Q[qi], dg.poisson_arrivals(n, rate, seed=rate), k=k, beam_width=L,
+                                            rerank_size=rr, traversal=trav, filters=[flist[i] for i in qi])
+                        lat = res["latency_us"] / 1e3
+                        hits = [len(set(res["ids"][i][:K].tolist()) & set(gt[qi[i]].tolist()))
+                                for i in range(0, n, max(1, n // 2000))]
+                        r = {"variant": name, "k": k, "L": L, "offered_rps": rate,
+                             "achieved_qps": round(n / (res["wall_us"] / 1e6)), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                             "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                             "recall_at_10": round(float(np.mean(hits)) / K, 4), "visited_table_bits": tune["hbits"]}
+                        out["runs"].append(r)
+                        log(f"[filtered serving] {json.dumps(r)}")
+    ix.close()
     return out
 
 
