@@ -142,7 +142,12 @@ DG_API DgStatus dg_index_set_entry_points(DgIndex *idx, const uint32_t *ids, uin
  * skip marked ids (is_live, :463-470) and, while tombstone_count > 0, searches
  * use tombstone_config (:505-516): expanded beam max(2L, k + min(count, L)),
  * 2x iterations, early-termination factor 1.5.  tombstone_count is the size
- * of the caller's tombstone set (which may hold ids the index does not have). */
+ * of the caller's tombstone set (which may hold ids the index does not have).
+ * This call and dg_index_update_rows rewrite device state only after every
+ * dg_search_batch already issued (on any stream) has finished, as the
+ * reference's searches hold a read lock for their whole run; the GPU orders
+ * them and the host does not wait.  dg_search_batch_static calls are the
+ * caller's to order. */
 DG_API DgStatus dg_index_set_tombstones(DgIndex *idx, const uint32_t *ids, uint64_t n, int32_t deleted,
                                         uint64_t tombstone_count);
 /* Rows at or past `limit` carry no codes: code traversals score them with the
@@ -337,7 +342,10 @@ DG_API DgStatus dg_spfresh_create(const DgSpfreshDesc *desc, DgSpfresh **out);
 DG_API DgStatus dg_spfresh_destroy(DgSpfresh *s);
 /* Replaces whole posting slots after host-side insert / split / merge
  * (Inner::rewrite / push, src/spfresh.rs:294-320): centroids f32[n*dim],
- * live u8[n], lens u32[n], ids u64[n*block_cap], codes [n*block_cap][code_size]. */
+ * live u8[n], lens u32[n], ids u64[n*block_cap], codes [n*block_cap][code_size].
+ * This call, dg_spfresh_put_raw and dg_spfresh_set_deleted run after every
+ * search already issued on the handle has finished on the GPU (the reference
+ * takes its RwLock for writing, src/spfresh.rs:862-871). */
 DG_API DgStatus dg_spfresh_update_blocks(DgSpfresh *s, const uint32_t *blocks, uint32_t n,
                                          const float *centroids, const uint8_t *live,
                                          const uint32_t *lens, const uint64_t *entry_ids,
@@ -347,7 +355,9 @@ DG_API DgStatus dg_spfresh_put_raw(DgSpfresh *s, uint64_t first_id, const float 
 /* SPFresh::delete tombstones (src/spfresh.rs:863-871); deleted = 0 clears. */
 DG_API DgStatus dg_spfresh_set_deleted(DgSpfresh *s, const uint64_t *ids, uint64_t n, int32_t deleted);
 /* SPFresh::search_with_dists / search_batch (src/spfresh.rs:671-770,886-908):
- * out_ids u64[nq*k] (DG_PAD64 padded), out_dists f32[nq*k], out_counts u32[nq]. */
+ * out_ids u64[nq*k] (DG_PAD64 padded), out_dists f32[nq*k], out_counts u32[nq].
+ * Searches of one handle share its scratch: each waits on the GPU for the
+ * previous one, whatever stream either runs on. */
 DG_API DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const float *queries,
                                         uint32_t nq, uint64_t *out_ids, float *out_dists,
                                         uint32_t *out_counts);

@@ -6,6 +6,7 @@ libdgann.so raises, and there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import os
 
 import numpy as np
@@ -168,3 +169,18 @@ def ptr(a):
     if hasattr(a, "data_ptr"):
         return C.c_void_p(a.data_ptr())
     raise TypeError(type(a))
+
+
+def locked(fn):
+    """Run a method under its object's `_lock` (a threading.RLock).  Updates and
+    searches of one index from several threads then see whole updates, as the
+    reference's RwLock-guarded state gives (src/incremental.rs:521-534,
+    src/spfresh.rs:778); a search never meets a device mirror that an insert
+    is replacing."""
+
+    @functools.wraps(fn)
+    def run(self, *args, **kwargs):
+        with self._lock:
+            return fn(self, *args, **kwargs)
+
+    return run

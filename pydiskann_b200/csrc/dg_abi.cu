@@ -331,6 +331,19 @@ DgStatus dg_index_set_entry_points(DgIndex *idx, const uint32_t *ids, uint32_t n
   return DG_OK;
 }
 
+// Orders idx->stream after every search already issued, on any stream (the
+// reference's searches hold a read lock for their whole run, so an update
+// never lands under one): rows, adjacency, labels and tombstones are rewritten
+// only once those searches are done.  The caller holds idx->mu.
+static cudaError_t after_searches(DgIndex *idx) {
+  for (auto &sl : idx->slots) {
+    if (!sl.pending) continue;
+    const cudaError_t e = cudaStreamWaitEvent(idx->stream, sl.done, 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 DgStatus dg_index_set_tombstones(DgIndex *idx, const uint32_t *ids, uint64_t n, int32_t deleted,
                                  uint64_t tombstone_count) {
   if (!idx || (!ids && n)) return fail(DG_EINVAL, "null argument");
@@ -350,6 +363,7 @@ DgStatus dg_index_set_tombstones(DgIndex *idx, const uint32_t *ids, uint64_t n, 
     else idx->tomb_host[ids[i] >> 5] &= ~bit;
   }
   idx->ntomb = tombstone_count;
+  DG_CUDA(after_searches(idx));
   DG_CUDA(cudaMemcpyAsync(idx->tomb, idx->tomb_host.data(), words * 4, cudaMemcpyHostToDevice, idx->stream));
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
@@ -378,6 +392,7 @@ DgStatus dg_index_update_rows(DgIndex *idx, uint64_t first, uint64_t count, cons
   if (!count) return DG_OK;
   std::lock_guard<std::mutex> lk(idx->mu);
   DG_CUDA(cudaSetDevice(idx->device));
+  DG_CUDA(after_searches(idx));
   DgStatus s;
   if (vectors) {
     float *rows = idx->vec + first * idx->dpad;

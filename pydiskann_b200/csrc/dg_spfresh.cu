@@ -46,6 +46,11 @@ struct DgSpfresh {
   float *rq_signs = nullptr;
   uint32_t *counter = nullptr;
   cudaStream_t stream = nullptr;
+  // recorded after each search on its stream: the next search (which reuses
+  // the same scratch) and every update wait for it on the GPU, so a search
+  // issued on a caller's stream never has its scratch or postings rewritten
+  // under it
+  cudaEvent_t searched = nullptr;
   std::mutex mu;
   std::vector<void *> allocs;
   DgIndex::Buf q, oids, od, ocnt, route;  // route: query x posting routing distances of one chunk
@@ -1034,6 +1039,10 @@ DgStatus dg_spfresh_destroy(DgSpfresh *s) {
   if (!s) return DG_OK;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->searched) {
+    cudaEventSynchronize(s->searched);
+    cudaEventDestroy(s->searched);
+  }
   for (void *p : s->allocs) cudaFree(p);
   for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx, &s->probe, &s->probe_cnt,
                           &s->pcount, &s->pstart, &s->pfill, &s->istart, &s->pair_q, &s->pos_of, &s->items,
@@ -1106,6 +1115,8 @@ DgStatus dg_spfresh_create(const DgSpfreshDesc *desc, DgSpfresh **out) {
   s->rq_padded = desc->rq_padded;
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(DG_EDEVICE, "stream creation failed"));
+  if (cudaEventCreateWithFlags(&s->searched, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(DG_EDEVICE, "event creation failed"));
   DgStatus st;
   const size_t nb = s->nblocks, slots = nb * s->cap;
   if ((st = spf_alloc(s, (void **)&s->centroids, nb * dpad * 4)) != DG_OK) return bail(st);
@@ -1166,6 +1177,7 @@ DgStatus dg_spfresh_update_blocks(DgSpfresh *s, const uint32_t *blocks, uint32_t
   std::lock_guard<std::mutex> lk(s->mu);
   DG_CUDA(cudaSetDevice(s->device));
   cudaStream_t ss = s->stream;
+  DG_CUDA(cudaStreamWaitEvent(ss, s->searched, 0));
   std::vector<uint32_t> ids32(s->cap);
   for (uint32_t u = 0; u < nupd; ++u) {
     const uint32_t b = blocks[u];
@@ -1195,6 +1207,7 @@ DgStatus dg_spfresh_put_raw(DgSpfresh *s, uint64_t first_id, const float *vector
   if (first_id + n > s->id_cap) return fail(DG_EINVAL, "raw rows beyond id_capacity");
   std::lock_guard<std::mutex> lk(s->mu);
   DG_CUDA(cudaSetDevice(s->device));
+  DG_CUDA(cudaStreamWaitEvent(s->stream, s->searched, 0));
   DgStatus st = upload_rows_f32(vectors, n, s->d, s->dpad, s->raw + first_id * s->dpad, s->stream);
   if (st != DG_OK) return st;
   DG_CUDA(cudaStreamSynchronize(s->stream));
@@ -1205,6 +1218,7 @@ DgStatus dg_spfresh_set_deleted(DgSpfresh *s, const uint64_t *ids, uint64_t n, i
   if (!s || (n && !ids)) return fail(DG_EINVAL, "null argument");
   std::lock_guard<std::mutex> lk(s->mu);
   DG_CUDA(cudaSetDevice(s->device));
+  DG_CUDA(cudaStreamWaitEvent(s->stream, s->searched, 0));
   const size_t words = (s->id_cap + 31) / 32 + 1;
   std::vector<uint32_t> bm(words);
   DG_CUDA(cudaMemcpyAsync(bm.data(), s->deleted, words * 4, cudaMemcpyDeviceToHost, s->stream));
@@ -1237,6 +1251,7 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
   std::lock_guard<std::mutex> lk(s->mu);
   DG_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = (p->flags & DG_FLAG_STREAM) || p->stream ? (cudaStream_t)p->stream : s->stream;
+  DG_CUDA(cudaStreamWaitEvent(st, s->searched, 0));  // the previous search's scratch is free again
   SpfArgs a{};
   a.d = s->d;
   a.dpad = s->dpad;
@@ -1338,8 +1353,9 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
     DG_CUDA(cudaMemcpyAsync(out_ids, a.out_ids, kq * 8, cudaMemcpyDeviceToHost, st));
     DG_CUDA(cudaMemcpyAsync(out_dists, a.out_d, kq * 4, cudaMemcpyDeviceToHost, st));
     DG_CUDA(cudaMemcpyAsync(out_counts, a.out_cnt, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
-    DG_CUDA(cudaStreamSynchronize(st));
   }
+  DG_CUDA(cudaEventRecord(s->searched, st));
+  if (!devptr) DG_CUDA(cudaStreamSynchronize(st));
   return DG_OK;
 }
 

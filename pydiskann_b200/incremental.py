@@ -14,13 +14,14 @@ entry point.  Ids are the reference's: base ids as they are, delta ids
 from __future__ import annotations
 
 import ctypes as C
+import threading
 import warnings
 
 import numpy as np
 
 from . import _lib
 from . import formats as _fmt
-from ._lib import PAD, check, lib, ptr
+from ._lib import PAD, check, lib, locked, ptr
 
 DELTA_ID_OFFSET = 1 << 48
 _METRICS = {"l2": _lib.L2SQ, "cosine": _lib.COSINE, "dot": _lib.DOT, "euclidean": _lib.L2}
@@ -61,6 +62,7 @@ class IncrementalDiskANN:
         self._base_codes = None if base_codes is None else np.ascontiguousarray(base_codes, dtype=np.uint8)
         self._ix = None
         self._cap = 0
+        self._lock = threading.RLock()
         self._mirror(1024)
 
     # ------------------------------------------------------------ building
@@ -187,6 +189,7 @@ class IncrementalDiskANN:
         arr = np.asarray(rows if rows else [0], np.uint32)
         check(lib().dg_index_set_tombstones(self._h, ptr(arr), len(rows), deleted, len(self.tombstones)))
 
+    @locked
     def close(self):
         if getattr(self, "_ix", None) is not None:
             self._ix.close()
@@ -225,6 +228,7 @@ class IncrementalDiskANN:
                 raise RuntimeError(f"Index error: Label {i} has {len(l)} fields, expected {self._nf}")
         return self._add(X, np.asarray(lab, dtype=np.uint64).reshape(len(X), self._nf))
 
+    @locked
     def _add(self, X, labels):
         n_old, n_new = self._dn, len(X)
         need = n_old + n_new
@@ -259,12 +263,14 @@ class IncrementalDiskANN:
                 self._publish_tombstones(born)
         return [DELTA_ID_OFFSET + j for j in range(n_old, need)]
 
+    @locked
     def delete_vectors(self, ids):
         """delete_vectors (src/incremental.rs:908-915): tombstones."""
         new = [int(i) for i in ids if int(i) not in self.tombstones]
         self.tombstones.update(new)
         self._publish_tombstones(new)
 
+    @locked
     def is_deleted(self, id):  # noqa: A002
         return int(id) in self.tombstones
 
@@ -276,6 +282,7 @@ class IncrementalDiskANN:
         g[delta] = np.uint64(DELTA_ID_OFFSET) + (ids[delta].astype(np.uint64) - np.uint64(nb))
         return g
 
+    @locked
     def search_arrays(self, queries, k=10, beam_width=128, filters=None, traversal=None, rerank_size=None):
         """Batched search: (ids u64[nq, k], dists f32[nq, k], counts u32[nq]).
         A filter only applies to an index with labels, as in
@@ -290,6 +297,7 @@ class IncrementalDiskANN:
         ids, ds, cnt = _mirror_search(self._ix, Q, k, beam_width, traversal, rerank_size, filters)
         return self._to_global(ids, cnt), ds, cnt
 
+    @locked
     def enable_bf16(self):
         """BF16 copy of the unified rows for ``traversal=TRAVERSE_BF16`` (kept in
         step with inserts); no counterpart in the reference."""
@@ -315,6 +323,7 @@ class IncrementalDiskANN:
         return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
 
     # ------------------------------------------------------------ state
+    @locked
     def get_vector(self, id):  # noqa: A002
         """get_vector (src/incremental.rs:1083-1098)."""
         id = int(id)  # noqa: A001
@@ -323,6 +332,7 @@ class IncrementalDiskANN:
             return self._dX[j].tolist() if j < self._dn else None
         return self._bX[id].tolist() if id < self.base_count else None
 
+    @locked
     def should_compact(self):
         """should_compact (src/incremental.rs:1100-1122)."""
         if self._dn >= self.delta_threshold:
@@ -330,6 +340,7 @@ class IncrementalDiskANN:
         total = self.base_count + self._dn
         return total > 0 and np.float32(len(self.tombstones)) / np.float32(total) >= np.float32(self.tombstone_ratio)
 
+    @locked
     def compact(self, new_path=None, max_degree=None, build_beam_width=128, alpha=1.2, seed=0):
         """compact (src/incremental.rs:1124-1205): the live base and delta rows, in
         id order, become a new base (Vamana graph built on the GPU); the delta
@@ -357,6 +368,7 @@ class IncrementalDiskANN:
         self.tombstones = set()
         self._mirror(1024)
 
+    @locked
     def stats(self):
         """stats (src/incremental.rs:1613-1626)."""
         nb = self.base_count
@@ -364,6 +376,7 @@ class IncrementalDiskANN:
                 "total_live": max(nb + self._dn - len(self.tombstones), 0), "dim": self.dim}
 
     # ------------------------------------------------------------ persistence
+    @locked
     def to_bytes(self) -> bytes:
         """IncrementalDiskANN::to_bytes (src/incremental.rs:1234-1327)."""
         graph = [row[row != PAD].tolist() for row in self._dA[: self._dn]]

@@ -18,11 +18,12 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import threading
 
 import numpy as np
 
 from . import _lib
-from ._lib import check, lib, ptr
+from ._lib import check, lib, locked, ptr
 
 _METRICS = {"l2": _lib.L2SQ, "cosine": _lib.COSINE, "dot": _lib.DOT, "euclidean": _lib.L2}
 CHUNK = 4096
@@ -200,6 +201,7 @@ class SPFresh:
         self._del_synced = set()
         self.centroid_beam = 64  # SPFreshConfig::centroid_beam, kept for the saved config
         self.path = None
+        self._lock = threading.RLock()
 
     # ------------------------------------------------------------ building
     @staticmethod
@@ -350,6 +352,7 @@ class SPFresh:
         return float(_dist_rows(self.metric, v, self.cent[b:b + 1])[0])
 
     # --------------------------------------------------------------- updates
+    @locked
     def insert(self, vectors):
         """Inner::insert (src/spfresh.rs:416-476); returns the new ids."""
         X = np.ascontiguousarray(vectors, dtype=np.float32)
@@ -478,6 +481,7 @@ class SPFresh:
             if self._len(p) >= self.max_posting:
                 queue.append(p)
 
+    @locked
     def delete(self, ids):
         """SPFresh::delete (src/spfresh.rs:863-871): tombstones."""
         for i in ids:
@@ -487,13 +491,16 @@ class SPFresh:
                 self.live -= 1
         self._sync()
 
+    @locked
     def is_deleted(self, id):  # noqa: A002
         return int(id) in self.deleted
 
+    @locked
     def get_vector(self, id):  # noqa: A002
         id = int(id)  # noqa: A001
         return None if id >= self.next_id or id in self.deleted else self.raw[id].tolist()
 
+    @locked
     def gc(self):
         """Inner::gc (src/spfresh.rs:613-643): purge tombstones, merge small postings."""
         queue = []
@@ -518,6 +525,7 @@ class SPFresh:
         self._drain(queue)
         self._sync()
 
+    @locked
     def stats(self):
         sizes = [self._len(b) for b in range(len(self.live_b)) if self._is_live(b)]
         return {"live": self.live, "deleted": len(self.deleted), "postings": int(self.live_b.sum()),
@@ -566,6 +574,7 @@ class SPFresh:
         s._sync()
         return s
 
+    @locked
     def save(self, path=None):
         """SPFresh::save (src/spfresh.rs:852-859): the four files SPFresh::open reads.
 
@@ -682,6 +691,7 @@ class SPFresh:
         self._raw_synced = self.next_id
         self._del_synced = set(self.deleted)
 
+    @locked
     def close(self):
         if self._h is not None:
             lib().dg_spfresh_destroy(self._h)
@@ -694,6 +704,7 @@ class SPFresh:
             pass
 
     # ----------------------------------------------------------------- search
+    @locked
     def search_arrays(self, queries, k=10, n_probe=8, stream=None):
         """Batched search: numpy in -> numpy out (ids u64, dists f32, counts u32),
         or CUDA tensors in -> tensors out."""
