@@ -195,3 +195,4 @@ def test_quantized_base(small_data, oracle, quantizer):
         assert np.array_equal(x, y)
     back.close()
     ix.close()
+
