@@ -53,3 +53,47 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(ImportError):
         _lib.lib()
+
+
+_C_TYPES = {"uint32_t": ctypes.c_uint32, "uint64_t": ctypes.c_uint64, "int32_t": ctypes.c_int32,
+            "int64_t": ctypes.c_int64, "float": ctypes.c_float, "double": ctypes.c_double, "int": ctypes.c_int,
+            "size_t": ctypes.c_size_t, "DgStatus": ctypes.c_int}
+
+
+def _ctype(decl, is_return=False):
+    """ctypes class of one C parameter or return declaration."""
+    decl = " ".join(decl.split())
+    if "*" in decl:
+        return ctypes.c_char_p if is_return and decl.replace(" ", "") == "constchar*" else ctypes.c_void_p
+    words = [w for w in decl.split() if w != "const"]
+    base = words[0] if is_return else words[-2]
+    return _C_TYPES[base]
+
+
+def _prototypes():
+    out = {}
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", h)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            for ret, name, params in re.findall(r"DG_API\s+([^;()]+?)\s*\b(dg_\w+)\s*\(([^)]*)\)\s*;", src):
+                ps = [p for p in (x.strip() for x in params.split(",")) if p and p != "void"]
+                out[name] = (_ctype(ret, True), [_ctype(p) for p in ps])
+    return out
+
+
+def test_ctypes_signatures_match_header():
+    """Every prototype's return type and each parameter (pointers as void *)
+    equal the ctypes signature the package binds, so no call passes an
+    argument of the wrong width."""
+    from pydiskann_b200 import _lib
+
+    protos = _prototypes()
+    assert set(protos) == _declared()
+    sigs = _lib._signatures()
+    for name, (ret, args) in protos.items():
+        bret, bargs = sigs[name]
+        assert bret is ret, f"{name}: return type"
+        assert len(bargs) == len(args), f"{name}: {len(bargs)} arguments bound, {len(args)} declared"
+        for i, (b, a) in enumerate(zip(bargs, args)):
+            assert b is a, f"{name}: argument {i} bound as {b.__name__}, declared {a.__name__}"
