@@ -27,6 +27,7 @@ import os
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -129,17 +130,68 @@ def recall(ids, gt, k=K):
 
 
 # ------------------------------------------------------------ clock probe
+def _nvml_index(cuda_index):
+    """NVML's ordinal of a CUDA device (they differ under CUDA_VISIBLE_DEVICES)."""
+    try:
+        import torch
+
+        return int(torch.cuda._get_nvml_device_index(cuda_index))
+    except Exception:
+        return cuda_index
+
+
 class Clocks:
-    """Samples SM clocks and throttle reasons while the timed region runs."""
+    """Samples SM clocks and throttle reasons while the timed region runs.
+
+    nvidia-smi polls every 200 ms from 0.3 s before the region; a thread polls
+    NVML (read-only queries) about every half millisecond from the moment the
+    context is entered until it exits, so a timed region of a few milliseconds
+    still has samples taken under load.  Without NVML the nvidia-smi samples
+    are reported."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits (nvmlClocksThrottleReason*)
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, nvml=None):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.fast = []  # (SM MHz, reason bits) from NVML inside the region
+        self.fast_max = None
+        self._nvml = nvml  # a stand-in module for tests; pynvml otherwise
+        self._go = threading.Event()
+        self._stop = threading.Event()
+        self._thr = None
+
+    def _poll(self):
+        try:
+            nv = self._nvml
+            if nv is None:
+                import pynvml as nv
+            nv.nvmlInit()
+        except Exception:
+            return
+        try:
+            h = nv.nvmlDeviceGetHandleByIndex(_nvml_index(self.gpu) if self._nvml is None else self.gpu)
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.fast_max = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            if not self._go.wait(timeout=10.0):
+                return
+            while not self._stop.is_set():
+                self.fast.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(reasons(h))))
+                time.sleep(0.0005)
+        except Exception:
+            pass
+        finally:
+            try:
+                nv.nvmlShutdown()
+            except Exception:
+                pass
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -150,10 +202,20 @@ class Clocks:
                  "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        try:
+            self._thr = threading.Thread(target=self._poll, daemon=True)
+            self._thr.start()
+        except Exception:
+            self._thr = None
         time.sleep(0.3)
+        self._go.set()
         return self
 
     def __exit__(self, *exc):
+        self._stop.set()
+        self._go.set()
+        if self._thr is not None:
+            self._thr.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -181,10 +243,18 @@ class Clocks:
         finally:
             if self.path and os.path.exists(self.path):
                 os.remove(self.path)
+        fast = list(self.fast)
+        if fast:
+            for name, bit in self.REASON_BITS:
+                if any(r & bit for _, r in fast):
+                    reasons.add(name)
+            top = max(mx) if mx else self.fast_max
+            return {"sm_mhz": float(np.median([c for c, _ in fast])), "sm_max_mhz": top, "reasons": sorted(reasons),
+                    "samples": len(fast), "source": "nvml, inside the timed region"}
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 # ------------------------------------------------------------ GPU timing

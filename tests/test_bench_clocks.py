@@ -1,0 +1,66 @@
+"""bench.py's clock record (host logic, no GPU): NVML samples are taken only
+inside the timed region, throttle-reason bits map to their names, and a
+missing or failing NVML falls back to the nvidia-smi samples without raising."""
+import os
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+class FakeNVML:
+    """The read-only NVML queries the sampler makes."""
+
+    NVML_CLOCK_SM = 1
+
+    def __init__(self, reasons=0x4, fail_init=False):
+        self.reasons, self.fail_init = reasons, fail_init
+        self.first_call = None
+        self.shut = False
+
+    def nvmlInit(self):
+        if self.fail_init:
+            raise RuntimeError("NVML unavailable")
+
+    def nvmlShutdown(self):
+        self.shut = True
+
+    def nvmlDeviceGetHandleByIndex(self, i):
+        return ("gpu", i)
+
+    def nvmlDeviceGetMaxClockInfo(self, h, clock):
+        return 1965
+
+    def nvmlDeviceGetClockInfo(self, h, clock):
+        if self.first_call is None:
+            self.first_call = time.monotonic()
+        return 1950
+
+    def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+        return self.reasons
+
+
+def test_samples_inside_the_region_only():
+    nv = FakeNVML(reasons=0x4 | 0x8)
+    with bench.Clocks(0, nvml=nv) as ck:
+        entered = time.monotonic()
+        time.sleep(0.03)
+    s = ck.summary()
+    assert nv.first_call is not None and nv.first_call >= entered - 0.005
+    assert s["source"].startswith("nvml") and s["samples"] >= 2
+    assert s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] is not None
+    assert s["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    assert nv.shut
+
+
+def test_failing_nvml_falls_back():
+    nv = FakeNVML(fail_init=True)
+    with bench.Clocks(0, nvml=nv) as ck:
+        time.sleep(0.01)
+    s = ck.summary()
+    assert s.get("source") != "nvml, inside the timed region"
+    assert set(s) >= {"sm_mhz", "sm_max_mhz", "reasons", "samples"}
