@@ -1,6 +1,7 @@
-"""bench.py's clock record (host logic, no GPU): NVML samples are taken only
-inside the timed region, throttle-reason bits map to their names, and a
-missing or failing NVML falls back to the nvidia-smi samples without raising."""
+"""bench.py's host logic (no GPU).  The clock record: NVML samples are taken
+only inside the timed region, throttle-reason bits map to their names, and a
+missing or failing NVML falls back to the nvidia-smi samples without raising.
+The reference arm: only rank 0 works."""
 import os
 import sys
 import time
@@ -64,3 +65,15 @@ def test_failing_nvml_falls_back():
     s = ck.summary()
     assert s.get("source") != "nvml, inside the timed region"
     assert set(s) >= {"sm_mhz", "sm_max_mhz", "reasons", "samples"}
+
+
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
+    """Under torchrun the reference arm's other ranks exit 0 without work and
+    print nothing; rank 0 alone times the CPU search and prints the line."""
+    def no_work(*a, **k):
+        raise AssertionError("a rank other than 0 built the workload")
+
+    monkeypatch.setattr(bench, "workload", no_work)
+    monkeypatch.setenv("RANK", "1")
+    assert bench.reference_arm(None) == 0
+    assert capsys.readouterr().out == ""
