@@ -5,7 +5,8 @@ program -- the program the kernels run -- agree on every label vector.
 Edge cases the reference defines: a field past the vector's labels is false
 (`labels.get(field).map_or(false, ..)`), And([]) is true and Or([]) false,
 In with no values is false, Range with min > max is false, Filter::None
-nested inside And / Or is true, and values at 0 and 2^64 - 1.
+nested inside And / Or is true, and values at 0 and 2^64 - 1.  Per-query
+programs packed into one array (pack_filters) keep each query's meaning.
 """
 import numpy as np
 import pytest
@@ -67,3 +68,26 @@ def test_reference_edge_cases(oracle):
         ops, pool = f.program()
         assert f.matches(lab) is want, f
         assert oracle.filter_matches(ops, pool, lab) is want, f
+
+
+def test_packed_per_query_programs(oracle):
+    """pack_filters: query q's slice ops[offs[q]:offs[q+1]] of the packed
+    program, with IN offsets rebased into the shared value pool, evaluates as
+    that query's own filter (the layout dg_search_batch reads through
+    filter_offsets)."""
+    from pydiskann_b200 import pack_filters
+
+    rng = np.random.default_rng(11)
+    nf = 3
+    filters = [_tree(rng, nf, 3) for _ in range(300)]
+    pk = pack_filters(filters)
+    assert pk.n == 300 and len(pk.offs) == 301 and pk.offs[0] == 0
+    assert np.all(np.diff(pk.offs.astype(np.int64)) >= 0)
+    ops = [(o.op, o.field, o.a, o.b) for o in pk.arr]
+    pool = [int(v) for v in pk.pool[: pk.plen]]
+    for q, f in enumerate(filters):
+        mine = ops[pk.offs[q]: pk.offs[q + 1]]
+        assert len(mine) == len(f.program()[0])
+        for _ in range(6):
+            lab = [VALUES[int(rng.integers(0, len(VALUES)))] for _ in range(nf)]
+            assert oracle.filter_matches(mine, pool, lab) == f.matches(lab), (q, f, lab)
