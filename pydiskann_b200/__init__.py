@@ -34,7 +34,8 @@ from ._lib import PAD, DgError, check, lib, ptr  # noqa: F401  (DgError is publi
 __all__ = [
     "DiskANN", "QuantizedDiskANN", "FilteredDiskANN", "IncrementalDiskANN", "SPFresh", "Filter", "build_graph",
     "medoid",
-    "pq_train", "pq_encode", "exact_knn", "read_fvecs", "write_fvecs", "read_ivecs",
+    "pq_train", "pq_encode", "exact_knn", "read_fvecs", "write_fvecs", "read_ivecs", "read_bvecs_as_f32",
+    "simd_info",
 ]
 
 _METRICS = {"l2": _lib.L2SQ, "cosine": _lib.COSINE, "dot": _lib.DOT, "euclidean": _lib.L2}
@@ -781,21 +782,57 @@ def rabitq_params(vectors, seed=0):
 
 
 # ----------------------------------------------------------------- formats
+def _read_vecs(path, dtype):
+    """Records of a little-endian u32 count followed by that many elements (the
+    fvecs / ivecs / bvecs layout, src/formats.rs:7-113), as numpy arrays.
+    Records may differ in length.  As with read_exact there, a trailing length
+    field of 1-3 bytes ends the file, and a record cut short is an I/O error."""
+    dt = np.dtype(dtype)
+    try:
+        buf = np.fromfile(path, dtype=np.uint8)
+    except OSError as e:
+        raise RuntimeError(f"I/O error: {e.strerror} (os error {e.errno})") from None
+    n = buf.size
+    if n >= 4:  # every record the same length: one reshape
+        d = int(buf[:4].view("<u4")[0])
+        rec = 4 + d * dt.itemsize
+        if n % rec == 0:
+            recs = buf.reshape(-1, rec)
+            if np.all(np.ascontiguousarray(recs[:, :4]).view("<u4") == d):
+                return list(np.ascontiguousarray(recs[:, 4:]).view(dt).reshape(len(recs), d))
+    out, pos = [], 0
+    while n - pos >= 4:
+        d = int(buf[pos:pos + 4].view("<u4")[0])
+        pos += 4
+        end = pos + d * dt.itemsize
+        if end > n:
+            raise RuntimeError("I/O error: failed to fill whole buffer")
+        out.append(buf[pos:end].view(dt))
+        pos = end
+    return out
+
+
 def read_fvecs(path):
-    """fvecs reader (src/formats.rs:7-47)."""
-    raw = np.fromfile(path, dtype=np.int32)
-    if raw.size == 0:
-        return []
-    d = raw[0]
-    return raw.reshape(-1, d + 1)[:, 1:].view(np.float32).tolist()
+    """fvecs reader (src/formats.rs:7-47): a list of float lists."""
+    return [v.tolist() for v in _read_vecs(path, "<f4")]
 
 
 def read_ivecs(path):
-    raw = np.fromfile(path, dtype=np.int32)
-    if raw.size == 0:
-        return []
-    d = raw[0]
-    return raw.reshape(-1, d + 1)[:, 1:].tolist()
+    """ivecs reader (src/formats.rs:50-90): a list of int lists."""
+    return [v.tolist() for v in _read_vecs(path, "<i4")]
+
+
+def read_bvecs_as_f32(path):
+    """bvecs reader with each byte scaled to [0, 1] as b / 255 in f32
+    (src/formats.rs:93-122)."""
+    return [(v.astype(np.float32) / np.float32(255.0)).tolist() for v in _read_vecs(path, np.uint8)]
+
+
+def simd_info():
+    """The reference reports which CPU SIMD sets its distance kernels use
+    (src/metric.rs:41-60).  Here distances run in CUDA kernels for sm_100a
+    (tensor-core MMAs for int8 and FP8), so this names that path."""
+    return f"CUDA sm_100a kernels, libdgann ABI {_lib.lib().dg_version()}"
 
 
 def write_fvecs(path, vectors):

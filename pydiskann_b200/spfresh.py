@@ -526,6 +526,17 @@ class SPFresh:
         self._sync()
 
     @locked
+    def compact(self):
+        """SPFresh::compact (src/spfresh.rs:645-669, 916-918).  The reference
+        rebuilds its centroid graph over the live postings and renumbers
+        their centroid ids 0..n-1, because it routes a query by a beam search
+        over that graph.  This mirror routes exactly, over the live
+        centroids on the device, and numbers live postings consecutively at
+        every save, so no routing state goes stale: compact publishes the
+        pending posting changes to the device and leaves results unchanged."""
+        self._sync()
+
+    @locked
     def stats(self):
         sizes = [self._len(b) for b in range(len(self.live_b)) if self._is_live(b)]
         return {"live": self.live, "deleted": len(self.deleted), "postings": int(self.live_b.sum()),

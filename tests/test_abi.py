@@ -97,3 +97,36 @@ def test_ctypes_signatures_match_header():
         assert len(bargs) == len(args), f"{name}: {len(bargs)} arguments bound, {len(args)} declared"
         for i, (b, a) in enumerate(zip(bargs, args)):
             assert b is a, f"{name}: argument {i} bound as {b.__name__}, declared {a.__name__}"
+
+
+# Methods and getters of each class of the reference binding
+# (python/src/lib.rs:53-389).  SPFresh.snapshot / restore copy an index to and
+# from an object store (remote storage, not the search path) and are not here.
+BINDING = {
+    "Filter": ["none", "eq", "in_", "lt", "gt", "range", "and_", "or_", "matches"],
+    "DiskANN": ["build", "open", "from_bytes", "search", "search_with_dists", "search_batch", "get_vector",
+                "num_vectors", "dim", "max_degree"],
+    "IncrementalDiskANN": ["build", "open", "from_bytes", "add_vectors", "add_vectors_with_labels",
+                           "delete_vectors", "is_deleted", "search", "search_with_dists", "search_filtered",
+                           "search_batch", "get_vector", "should_compact", "compact", "stats"],
+    "FilteredDiskANN": ["build", "open", "from_bytes", "search", "search_filtered", "search_filtered_with_dists",
+                        "search_filtered_batch", "count_matching", "get_labels", "num_vectors", "num_fields"],
+    "QuantizedDiskANN": ["build", "open", "save_quantized", "from_bytes", "search", "search_with_dists",
+                         "search_batch", "num_vectors", "dim"],
+    "SPFresh": ["build", "open", "save", "insert", "delete", "is_deleted", "search", "search_with_dists",
+                "search_batch", "get_vector", "gc", "compact", "stats"],
+}
+MODULE_FUNCTIONS = ["read_fvecs", "read_ivecs", "read_bvecs_as_f32", "write_fvecs", "simd_info"]
+
+
+def test_binding_surface():
+    import pydiskann_b200 as dg
+    from pydiskann_b200.spfresh import SPFresh
+
+    for cls, names in BINDING.items():
+        missing = [n for n in names if not hasattr(getattr(dg, cls), n)]
+        assert not missing, f"{cls} lacks {missing}"
+    assert not [f for f in MODULE_FUNCTIONS if not callable(getattr(dg, f, None))]
+    # dim is an instance attribute of the updatable indexes
+    assert SPFresh(4, device=None).dim == 4
+    assert dg.simd_info().startswith("CUDA sm_100a")

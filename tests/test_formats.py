@@ -316,3 +316,58 @@ def test_spfresh_save_open_host(tmp_path, quantizer):
     t.save(str(tmp_path / "again"))
     for suffix in ("spf", "postings", "vectors"):
         assert (tmp_path / f"again.{suffix}").read_bytes() == (tmp_path / f"sp.{suffix}").read_bytes()
+
+
+def _vecs_bytes(rows, fmt):
+    out = b""
+    for r in rows:
+        out += struct.pack("<I", len(r)) + b"".join(struct.pack(fmt, x) for x in r)
+    return out
+
+
+def test_vecs_readers(tmp_path):
+    """read_fvecs / read_ivecs / read_bvecs_as_f32 (src/formats.rs:7-122):
+    records of a u32 count and that many elements, lengths may differ; a 1-3
+    byte tail ends the file; a record cut short is an I/O error."""
+    import pydiskann_b200 as dg
+
+    rows = [[1.5, -2.0, 3.25], [], [7.0], [0.5, 0.25, 0.125, 2.0 ** 100]]
+    p = tmp_path / "ragged.fvecs"
+    p.write_bytes(_vecs_bytes(rows, "<f"))
+    assert dg.read_fvecs(str(p)) == rows
+    X = np.arange(20, dtype=np.float32).reshape(5, 4) - 7.5
+    dg.write_fvecs(str(tmp_path / "u.fvecs"), X)
+    assert dg.read_fvecs(str(tmp_path / "u.fvecs")) == X.tolist()
+    (tmp_path / "tail.fvecs").write_bytes(_vecs_bytes(rows, "<f") + b"\x03\x00")
+    assert dg.read_fvecs(str(tmp_path / "tail.fvecs")) == rows
+    (tmp_path / "cut.fvecs").write_bytes(_vecs_bytes(rows, "<f")[:-2])
+    with pytest.raises(RuntimeError, match="I/O error: failed to fill whole buffer"):
+        dg.read_fvecs(str(tmp_path / "cut.fvecs"))
+    with pytest.raises(RuntimeError, match="I/O error"):
+        dg.read_fvecs(str(tmp_path / "absent.fvecs"))
+    (tmp_path / "empty.ivecs").write_bytes(b"")
+    assert dg.read_ivecs(str(tmp_path / "empty.ivecs")) == []
+    irows = [[1, -2, 2147483647], [-2147483648], []]
+    (tmp_path / "g.ivecs").write_bytes(_vecs_bytes(irows, "<i"))
+    assert dg.read_ivecs(str(tmp_path / "g.ivecs")) == irows
+    brows = [[0, 1, 128, 255], [17]]
+    (tmp_path / "b.bvecs").write_bytes(_vecs_bytes(brows, "<B"))
+    got = dg.read_bvecs_as_f32(str(tmp_path / "b.bvecs"))
+    want = [[float(np.float32(b) / np.float32(255.0)) for b in r] for r in brows]
+    assert got == want and got[0][3] == 1.0 and got[0][0] == 0.0
+
+
+def test_spfresh_compact_host():
+    """compact keeps the index's state and answers: routing here is exact over
+    the live centroids, so there is no centroid graph to go stale."""
+    from pydiskann_b200.spfresh import SPFresh
+
+    rng = np.random.default_rng(5)
+    X = rng.integers(-8, 8, size=(500, 8)).astype(np.float32)
+    s = SPFresh.build(X, metric="l2", max_posting_size=24, device=None)
+    s.delete(range(0, 500, 9))
+    s.gc()
+    before = (s.stats(), [ids.copy() for ids in s.ids])
+    s.compact()
+    assert s.stats() == before[0]
+    assert all(np.array_equal(a, b) for a, b in zip(s.ids, before[1]))

@@ -54,7 +54,8 @@ def test_locked_excludes_and_reenters():
 @pytest.mark.parametrize("cls, names", [
     (IncrementalDiskANN, ["_add", "delete_vectors", "is_deleted", "search_arrays", "enable_bf16", "get_vector",
                           "should_compact", "compact", "stats", "to_bytes", "close"]),
-    (SPFresh, ["insert", "delete", "is_deleted", "get_vector", "gc", "stats", "save", "close", "search_arrays"]),
+    (SPFresh, ["insert", "delete", "is_deleted", "get_vector", "gc", "compact", "stats", "save", "close",
+               "search_arrays"]),
 ])
 def test_public_methods_are_locked(cls, names):
     for n in names:
