@@ -130,3 +130,76 @@ def test_binding_surface():
     # dim is an instance attribute of the updatable indexes
     assert SPFresh(4, device=None).dim == 4
     assert dg.simd_info().startswith("CUDA sm_100a")
+
+
+# Parameter names and defaults of the reference binding's methods, from their
+# #[pyo3(signature = ...)] attributes (python/src/lib.rs:84-356); REQ marks a
+# parameter without a default.
+REQ = object()
+_SEARCH = [("query", REQ), ("k", 10), ("beam_width", 128)]
+_BATCH = [("queries", REQ), ("k", 10), ("beam_width", 128)]
+_OPEN = [("path", REQ), ("metric", "l2")]
+_BYTES = [("data", REQ), ("metric", "l2")]
+SIGNATURES = {
+    ("DiskANN", "build"): [("vectors", REQ), ("path", REQ), ("metric", "l2"), ("max_degree", 64),
+                           ("build_beam_width", 128), ("alpha", 1.2)],
+    ("DiskANN", "open"): _OPEN, ("DiskANN", "from_bytes"): _BYTES, ("DiskANN", "search"): _SEARCH,
+    ("DiskANN", "search_with_dists"): _SEARCH, ("DiskANN", "search_batch"): _BATCH,
+    ("IncrementalDiskANN", "build"): [("vectors", REQ), ("path", REQ), ("metric", "l2"), ("labels", None),
+                                      ("quantizer", None), ("rerank_size", 0), ("pq_subspaces", 8),
+                                      ("delta_threshold", 10_000), ("tombstone_ratio", 0.1)],
+    ("IncrementalDiskANN", "open"): _OPEN, ("IncrementalDiskANN", "from_bytes"): _BYTES,
+    ("IncrementalDiskANN", "search"): _SEARCH, ("IncrementalDiskANN", "search_with_dists"): _SEARCH,
+    ("IncrementalDiskANN", "search_filtered"): [("query", REQ), ("filter", REQ), ("k", 10), ("beam_width", 128)],
+    ("IncrementalDiskANN", "search_batch"): _BATCH,
+    ("FilteredDiskANN", "build"): [("vectors", REQ), ("labels", REQ), ("path", REQ), ("metric", "l2"),
+                                   ("max_degree", 64), ("build_beam_width", 128), ("alpha", 1.2)],
+    ("FilteredDiskANN", "open"): _OPEN, ("FilteredDiskANN", "from_bytes"): _BYTES,
+    ("FilteredDiskANN", "search"): _SEARCH,
+    ("FilteredDiskANN", "search_filtered"): [("query", REQ), ("filter", REQ), ("k", 10), ("beam_width", 128)],
+    ("FilteredDiskANN", "search_filtered_with_dists"): [("query", REQ), ("filter", REQ), ("k", 10),
+                                                        ("beam_width", 128)],
+    ("FilteredDiskANN", "search_filtered_batch"): [("queries", REQ), ("filter", REQ), ("k", 10),
+                                                   ("beam_width", 128)],
+    ("QuantizedDiskANN", "build"): [("vectors", REQ), ("path", REQ), ("quantizer", "f16"), ("metric", "l2"),
+                                    ("rerank_size", 0), ("pq_subspaces", 8), ("max_degree", 64),
+                                    ("build_beam_width", 128), ("alpha", 1.2)],
+    ("QuantizedDiskANN", "open"): [("base_path", REQ), ("quantized_path", REQ), ("metric", "l2"),
+                                   ("rerank_size", 0)],
+    ("QuantizedDiskANN", "from_bytes"): [("data", REQ), ("metric", "l2"), ("rerank_size", 0)],
+    ("QuantizedDiskANN", "search"): _SEARCH, ("QuantizedDiskANN", "search_with_dists"): _SEARCH,
+    ("QuantizedDiskANN", "search_batch"): _BATCH,
+    ("SPFresh", "build"): [("vectors", REQ), ("path", REQ), ("metric", "l2"), ("quantizer", None),
+                           ("rerank_size", 0), ("pq_subspaces", 8), ("max_posting_size", 128),
+                           ("min_posting_size", 16), ("reassign_neighbors", 16), ("probe_ratio", float("inf"))],
+    ("SPFresh", "open"): _OPEN,
+    ("SPFresh", "search"): [("query", REQ), ("k", 10), ("n_probe", 8)],
+    ("SPFresh", "search_with_dists"): [("query", REQ), ("k", 10), ("n_probe", 8)],
+    ("SPFresh", "search_batch"): [("queries", REQ), ("k", 10), ("n_probe", 8)],
+}
+
+
+@pytest.mark.parametrize("cls, method", list(SIGNATURES))
+def test_binding_signatures(cls, method):
+    """Each reference parameter sits at the same position under the same name
+    with the same default, so positional and keyword calls written against the
+    reference binding work unchanged.  (A parameter the reference requires may
+    be optional here, e.g. `path`; parameters added after the reference's
+    ones must have defaults.)"""
+    import inspect
+
+    import pydiskann_b200 as dg
+    from pydiskann_b200.spfresh import SPFresh
+
+    owner = SPFresh if cls == "SPFresh" else getattr(dg, cls)
+    f = inspect.getattr_static(owner, method)
+    f = f.__func__ if isinstance(f, (staticmethod, classmethod)) else f
+    f = getattr(f, "__wrapped__", f)
+    ps = [p for p in inspect.signature(f).parameters.values() if p.name != "self"]
+    want = SIGNATURES[(cls, method)]
+    assert len(ps) >= len(want), f"{cls}.{method} takes {len(ps)} parameters"
+    for p, (name, default) in zip(ps, want):
+        assert p.name == name, f"{cls}.{method}: {p.name} where the reference has {name}"
+        if default is not REQ:
+            assert p.default == default, f"{cls}.{method}({name}=) defaults to {p.default!r}, not {default!r}"
+    assert all(p.default is not inspect.Parameter.empty for p in ps[len(want):])
