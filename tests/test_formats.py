@@ -370,4 +370,5 @@ def test_spfresh_compact_host():
     before = (s.stats(), [ids.copy() for ids in s.ids])
     s.compact()
     assert s.stats() == before[0]
+    assert set(before[0]) == {"live", "deleted", "postings", "max_posting"}  # python/src/lib.rs:341-344
     assert all(np.array_equal(a, b) for a, b in zip(s.ids, before[1]))
