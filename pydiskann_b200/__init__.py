@@ -791,7 +791,7 @@ def _read_vecs(path, dtype):
     try:
         buf = np.fromfile(path, dtype=np.uint8)
     except OSError as e:
-        raise RuntimeError(f"I/O error: {e.strerror} (os error {e.errno})") from None
+        raise _fmt.io_error(e) from None
     n = buf.size
     if n >= 4:  # every record the same length: one reshape
         d = int(buf[:4].view("<u4")[0])

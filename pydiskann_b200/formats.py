@@ -62,6 +62,14 @@ def _index_error(msg):
     return RuntimeError(f"Index error: {msg}")
 
 
+def io_error(e: OSError) -> RuntimeError:
+    """DiskAnnError::Io as the binding raises it: `I/O error: ` and Rust's
+    io::Error text, e.g. `No such file or directory (os error 2)`."""
+    if e.strerror and e.errno is not None:
+        return RuntimeError(f"I/O error: {e.strerror} (os error {e.errno})")
+    return RuntimeError(f"I/O error: {e}")
+
+
 def _ser_error(msg):
     return RuntimeError(f"Serialization error: {msg}")
 
@@ -243,7 +251,7 @@ def read_core(path):
     try:
         buf = np.memmap(path, dtype=np.uint8, mode="r")
     except OSError as e:
-        raise RuntimeError(f"I/O error: {e}") from None
+        raise io_error(e) from None
     except ValueError as e:  # empty file
         raise _index_error(f"Invalid metadata length (file size 0): {e}") from None
     return parse_core(buf)
@@ -408,7 +416,7 @@ def read_sidecar(path, num_vectors=None):
         with open(path, "rb") as f:
             data = f.read()
     except OSError as e:
-        raise RuntimeError(f"I/O error: {e}") from None
+        raise io_error(e) from None
     return parse_sidecar(data, num_vectors)
 
 
@@ -450,7 +458,7 @@ def read_labels(path) -> np.ndarray:
         with open(path, "rb") as f:
             data = f.read()
     except OSError as e:
-        raise RuntimeError(f"I/O error: {e}") from None
+        raise io_error(e) from None
     return parse_labels(data)
 
 

@@ -759,11 +759,13 @@ class SPFresh:
 
 
 def _read(path):
+    from . import formats as F
+
     try:
         with open(path, "rb") as f:
             return f.read()
     except OSError as e:
-        raise RuntimeError(f"I/O error: {e}") from None
+        raise F.io_error(e) from None
 
 
 def _codec_params(q):

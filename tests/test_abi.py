@@ -203,3 +203,34 @@ def test_binding_signatures(cls, method):
         if default is not REQ:
             assert p.default == default, f"{cls}.{method}({name}=) defaults to {p.default!r}, not {default!r}"
     assert all(p.default is not inspect.Parameter.empty for p in ps[len(want):])
+
+
+def test_errors_raised_before_any_device_work(tmp_path):
+    """The binding's error classes and messages (python/src/lib.rs:25-49): an
+    unknown metric or quantizer is a ValueError, a missing file a RuntimeError
+    carrying DiskAnnError::Io's text.  All of them are raised on the host,
+    before any device work."""
+    import numpy as np
+
+    import pydiskann_b200 as dg
+    from pydiskann_b200.spfresh import SPFresh
+
+    X = np.zeros((4, 2), np.float32)
+    bad_metric = [lambda: dg.DiskANN.build(X, None, metric="m"), lambda: dg.DiskANN.open("x", metric="m"),
+                  lambda: dg.QuantizedDiskANN.build(X, None, metric="m"),
+                  lambda: dg.FilteredDiskANN.build(X, np.zeros((4, 1), np.uint64), None, metric="m"),
+                  lambda: dg.IncrementalDiskANN.build(X, None, metric="m"), lambda: SPFresh.build(X, None, metric="m"),
+                  lambda: SPFresh.open("x", metric="m")]
+    for f in bad_metric:
+        with pytest.raises(ValueError, match="^unknown metric: m$"):
+            f()
+    for f in (lambda: dg.QuantizedDiskANN.build(X, None, quantizer="q"),
+              lambda: dg.IncrementalDiskANN.build(X, None, quantizer="q"), lambda: SPFresh.build(X, None, quantizer="q")):
+        with pytest.raises(ValueError, match="^unknown quantizer: q$"):
+            f()
+    gone = str(tmp_path / "absent")
+    for f in (lambda: dg.DiskANN.open(gone), lambda: dg.FilteredDiskANN.open(gone),
+              lambda: dg.QuantizedDiskANN.open(gone, gone + ".q"), lambda: dg.IncrementalDiskANN.open(gone),
+              lambda: SPFresh.open(gone), lambda: dg.read_fvecs(gone)):
+        with pytest.raises(RuntimeError, match=r"^I/O error: No such file or directory \(os error 2\)$"):
+            f()
