@@ -58,7 +58,16 @@ def _check_recorded_metric(meta, metric):
 
 
 def _f32(x, dim=None) -> np.ndarray:
-    a = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    try:
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    except ValueError:
+        # rows of different lengths: the reference's check (src/lib.rs:416-424)
+        rows = list(x)
+        d0 = len(rows[0])
+        for i, r in enumerate(rows):
+            if len(r) != d0:
+                raise RuntimeError(f"Index error: Vector {i} has dimension {len(r)} but expected {d0}") from None
+        raise
     if a.ndim == 1 and dim is not None:
         a = a.reshape(1, -1)
     return a

@@ -234,3 +234,21 @@ def test_errors_raised_before_any_device_work(tmp_path):
               lambda: SPFresh.open(gone), lambda: dg.read_fvecs(gone)):
         with pytest.raises(RuntimeError, match=r"^I/O error: No such file or directory \(os error 2\)$"):
             f()
+
+
+def test_build_validation_messages():
+    """DiskAnnError::IndexError texts of the builders' input checks
+    (src/lib.rs:412-424, src/filtered.rs:181-186), raised on the host."""
+    import numpy as np
+
+    import pydiskann_b200 as dg
+
+    E, X = np.zeros((0, 3), np.float32), np.zeros((4, 3), np.float32)
+    for f in (lambda: dg.DiskANN.build(E, None), lambda: dg.QuantizedDiskANN.build(E, None),
+              lambda: dg.FilteredDiskANN.build(E, np.zeros((0, 1), np.uint64), None)):
+        with pytest.raises(RuntimeError, match="^Index error: No vectors provided$"):
+            f()
+    with pytest.raises(RuntimeError, match="^Index error: Vector 2 has dimension 2 but expected 3$"):
+        dg.DiskANN.build([[1, 2, 3], [4, 5, 6], [7, 8]], None)
+    with pytest.raises(RuntimeError, match=r"^Index error: vectors.len\(\) \(4\) != labels.len\(\) \(3\)$"):
+        dg.FilteredDiskANN.build(X, np.zeros((3, 1), np.uint64), None)
