@@ -733,7 +733,7 @@ class FilteredDiskANN(_Index):
     def get_labels(self, id: int):  # noqa: A002
         if id < 0 or id >= self.num_vectors:
             return None
-        return self._labels[id].astype(np.int64).tolist()
+        return [int(v) for v in self._labels[id]]  # u64 values, as Vec<u64>
 
     def count_matching(self, filter: Filter) -> int:  # noqa: A002
         ops, pool = filter.program()
