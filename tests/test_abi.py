@@ -104,14 +104,14 @@ def test_ctypes_signatures_match_header():
 # from an object store (remote storage, not the search path) and are not here.
 BINDING = {
     "Filter": ["none", "eq", "in_", "lt", "gt", "range", "and_", "or_", "matches"],
-    "DiskANN": ["build", "open", "from_bytes", "search", "search_with_dists", "search_batch", "get_vector",
-                "num_vectors", "dim", "max_degree"],
-    "IncrementalDiskANN": ["build", "open", "from_bytes", "add_vectors", "add_vectors_with_labels",
+    "DiskANN": ["build", "open", "from_bytes", "to_bytes", "search", "search_with_dists", "search_batch",
+                "get_vector", "num_vectors", "dim", "max_degree"],
+    "IncrementalDiskANN": ["build", "open", "from_bytes", "to_bytes", "add_vectors", "add_vectors_with_labels",
                            "delete_vectors", "is_deleted", "search", "search_with_dists", "search_filtered",
                            "search_batch", "get_vector", "should_compact", "compact", "stats"],
-    "FilteredDiskANN": ["build", "open", "from_bytes", "search", "search_filtered", "search_filtered_with_dists",
+    "FilteredDiskANN": ["build", "open", "from_bytes", "to_bytes", "search", "search_filtered", "search_filtered_with_dists",
                         "search_filtered_batch", "count_matching", "get_labels", "num_vectors", "num_fields"],
-    "QuantizedDiskANN": ["build", "open", "save_quantized", "from_bytes", "search", "search_with_dists",
+    "QuantizedDiskANN": ["build", "open", "save_quantized", "from_bytes", "to_bytes", "search", "search_with_dists",
                          "search_batch", "num_vectors", "dim"],
     "SPFresh": ["build", "open", "save", "insert", "delete", "is_deleted", "search", "search_with_dists",
                 "search_batch", "get_vector", "gc", "compact", "stats"],
