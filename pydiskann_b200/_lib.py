@@ -184,3 +184,23 @@ def locked(fn):
             return fn(self, *args, **kwargs)
 
     return run
+
+
+def rows_f32(vectors, dim, message):
+    """Vectors for an insert into an index of dimension `dim`, as f32[n, dim].
+    The first vector of another length (ragged lists included) raises
+    RuntimeError(message(i, its_length)), the text of the reference's check."""
+    try:
+        X = np.ascontiguousarray(vectors, dtype=np.float32)
+    except ValueError:
+        for i, v in enumerate(vectors):
+            if len(v) != dim:
+                raise RuntimeError(message(i, len(v))) from None
+        raise
+    if X.size == 0:
+        return X.reshape(0, dim)
+    if X.ndim == 1:
+        X = X.reshape(1, -1)
+    if X.ndim != 2 or X.shape[1] != dim:
+        raise RuntimeError(message(0, X.shape[-1]))
+    return X

@@ -205,24 +205,22 @@ class IncrementalDiskANN:
     # ------------------------------------------------------------ updates
     def add_vectors(self, vectors):
         """add_vectors (src/incremental.rs:829-857): new ids 2^48 + local index."""
-        X = np.ascontiguousarray(vectors, dtype=np.float32)
-        if X.size == 0:
+        if len(vectors) == 0:
             return []
-        X = X.reshape(len(X), -1) if X.ndim == 2 else X.reshape(1, -1)
-        if X.shape[1] != self.dim:
-            raise RuntimeError(f"Index error: Vector 0 has dimension {X.shape[1]} but index expects {self.dim}")
+        X = _lib.rows_f32(vectors, self.dim, self._dim_error)
         return self._add(X, None)
+
+    def _dim_error(self, i, n):
+        return f"Index error: Vector {i} has dimension {n} but index expects {self.dim}"
 
     def add_vectors_with_labels(self, vectors, labels):
         """add_vectors_with_labels (src/incremental.rs:859-906)."""
-        X = np.ascontiguousarray(vectors, dtype=np.float32)
-        if X.size == 0:
+        if len(vectors) == 0:
             return []
         lab = [list(map(int, l)) for l in labels]
-        if len(lab) != len(X):
-            raise RuntimeError(f"Index error: vectors.len() ({len(X)}) != labels.len() ({len(lab)})")
-        if X.shape[1] != self.dim:
-            raise RuntimeError(f"Index error: Vector 0 has dimension {X.shape[1]} but index expects {self.dim}")
+        if len(lab) != len(vectors):
+            raise RuntimeError(f"Index error: vectors.len() ({len(vectors)}) != labels.len() ({len(lab)})")
+        X = _lib.rows_f32(vectors, self.dim, self._dim_error)
         for i, l in enumerate(lab):
             if self._nf > 0 and len(l) != self._nf:
                 raise RuntimeError(f"Index error: Label {i} has {len(l)} fields, expected {self._nf}")

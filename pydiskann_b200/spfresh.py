@@ -355,11 +355,7 @@ class SPFresh:
     @locked
     def insert(self, vectors):
         """Inner::insert (src/spfresh.rs:416-476); returns the new ids."""
-        X = np.ascontiguousarray(vectors, dtype=np.float32)
-        if X.size == 0:
-            X = X.reshape(0, self.dim)
-        if X.ndim != 2 or X.shape[1] != self.dim:
-            raise RuntimeError(f"Index error: Vector dim {X.shape[-1]} != index dim {self.dim}")
+        X = _lib.rows_f32(vectors, self.dim, lambda i, n: f"Index error: Vector dim {n} != index dim {self.dim}")
         ids = self._insert(X)
         self._sync()
         return ids

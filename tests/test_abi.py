@@ -252,3 +252,27 @@ def test_build_validation_messages():
         dg.DiskANN.build([[1, 2, 3], [4, 5, 6], [7, 8]], None)
     with pytest.raises(RuntimeError, match=r"^Index error: vectors.len\(\) \(4\) != labels.len\(\) \(3\)$"):
         dg.FilteredDiskANN.build(X, np.zeros((3, 1), np.uint64), None)
+
+
+def test_insert_dimension_checks():
+    """Inserts name the first vector of the wrong length, ragged lists
+    included, with the reference's texts (SPFresh: src/spfresh.rs:417-421;
+    IncrementalDiskANN: src/incremental.rs:834-843), and leave the index as it
+    was (python/tests/test_spfresh.py:239-243)."""
+    import numpy as np
+
+    from pydiskann_b200 import _lib
+    from pydiskann_b200.spfresh import SPFresh
+
+    s = SPFresh.build(np.random.default_rng(0).standard_normal((300, 8)).astype(np.float32), None,
+                      max_posting_size=24, device=None)
+    st = s.stats()
+    for bad, n in (([[0.0] * 9], 9), ([[0.0] * 8, [0.0] * 7], 7), (np.zeros((2, 9), np.float32), 9)):
+        with pytest.raises(RuntimeError, match=f"^Index error: Vector dim {n} != index dim 8$"):
+            s.insert(bad)
+    assert s.stats() == st
+    msg = lambda i, n: f"Index error: Vector {i} has dimension {n} but index expects 8"  # noqa: E731
+    with pytest.raises(RuntimeError, match="^Index error: Vector 2 has dimension 3 but index expects 8$"):
+        _lib.rows_f32([[0.0] * 8, [1.0] * 8, [2.0] * 3], 8, msg)
+    assert _lib.rows_f32(np.zeros((0, 8)), 8, msg).shape == (0, 8)
+    assert _lib.rows_f32([1.0] * 8, 8, msg).shape == (1, 8)
