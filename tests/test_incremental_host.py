@@ -92,3 +92,34 @@ def test_incremental_bytes_with_base_labels_tombstones():
     assert (cs, rr, st2.kind, st2.scale, st2.offset) == (2, 7, "int8", 0.5, -1.0) and np.array_equal(c2, codes.ravel())
     with pytest.raises(RuntimeError, match="Unsupported incremental format version: 1"):
         F.parse_incremental(struct.pack("<II", 0x494E4352, 1) + raw[8:])
+
+
+def test_should_compact_rule():
+    """IncrementalDiskANN::should_compact (src/incremental.rs:1100-1122): the
+    delta threshold, or tombstones / (base + delta) >= the ratio in f32.  The
+    object is made without its device mirror; the rule reads only sizes."""
+    import threading
+
+    from pydiskann_b200.incremental import IncrementalDiskANN
+
+    class Sized:
+        def __init__(self, n):
+            self.n = n
+
+        def __len__(self):
+            return self.n
+
+    def ix(base, delta, tomb, threshold=10_000, ratio=0.1):
+        o = object.__new__(IncrementalDiskANN)
+        o._lock = threading.RLock()
+        o._bX, o._dn, o.tombstones = Sized(base), delta, Sized(tomb)
+        o.delta_threshold, o.tombstone_ratio = threshold, ratio
+        return o
+
+    assert ix(100, 10_000, 0).should_compact()
+    assert not ix(100, 9_999, 0).should_compact()
+    assert ix(90, 10, 10).should_compact() and not ix(90, 10, 9).should_compact()
+    assert not ix(0, 0, 0).should_compact()
+    # 99 999 999 / 10^9 is below 0.1 in f64 but rounds to 0.1f in f32, so it compacts
+    assert ix(10**9, 0, 99_999_999).should_compact()
+    assert 99_999_999 / 10**9 < 0.1
