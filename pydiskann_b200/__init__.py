@@ -492,7 +492,7 @@ class DiskANN(_Index):
         return [i for i, _ in self.search_with_dists(query, k, beam_width)]
 
     def search_batch(self, queries, k=10, beam_width=128):
-        ids, ds, cnt = self.search_arrays(_f32(queries).reshape(-1, self.dim), k, beam_width)
+        ids, ds, cnt = self.search_arrays(_lib.query_rows(queries, self.dim), k, beam_width)
         return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
 
 
@@ -647,7 +647,7 @@ class QuantizedDiskANN(_Index):
         return [i for i, _ in self.search_with_dists(query, k, beam_width)]
 
     def search_batch(self, queries, k=10, beam_width=128):
-        ids, ds, cnt = self.search_arrays(_f32(queries).reshape(-1, self.dim), k, beam_width)
+        ids, ds, cnt = self.search_arrays(_lib.query_rows(queries, self.dim), k, beam_width)
         return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
 
     def search_filtered_with_dists(self, query, k, beam_width, labels, filter):  # noqa: A002
@@ -755,7 +755,7 @@ class FilteredDiskANN(_Index):
         return [i for i, _ in self.search_filtered_with_dists(query, filter, k, beam_width)]
 
     def search_filtered_batch(self, queries, filter, k=10, beam_width=128):  # noqa: A002
-        ids, ds, cnt = self.search_arrays(_f32(queries).reshape(-1, self.dim), k, beam_width,
+        ids, ds, cnt = self.search_arrays(_lib.query_rows(queries, self.dim), k, beam_width,
                                           filters=filter)
         return [ids[i, : cnt[i]].astype(np.int64).tolist() for i in range(len(cnt))]
 

@@ -204,3 +204,25 @@ def rows_f32(vectors, dim, message):
     if X.ndim != 2 or X.shape[1] != dim:
         raise RuntimeError(message(0, X.shape[-1]))
     return X
+
+
+def query_rows(queries, dim):
+    """Host queries as f32[nq, dim].  A query of another length (ragged lists
+    included) raises ValueError with the text of the reference's assertion
+    (src/lib.rs:684-690); a batch is never reinterpreted by reshaping it."""
+    try:
+        Q = np.ascontiguousarray(queries, dtype=np.float32)
+    except ValueError:
+        for q in queries:
+            if len(q) != dim:
+                raise ValueError(f"Query dim {len(q)} != index dim {dim}") from None
+        raise
+    if Q.size == 0 and Q.ndim <= 2 and (Q.ndim < 2 or Q.shape[1] in (0, dim)):
+        return Q.reshape(0, dim)
+    if Q.ndim == 1:
+        Q = Q.reshape(1, -1)
+    if Q.ndim != 2:
+        raise ValueError(f"queries must be one query or a 2-D batch, not shape {Q.shape}")
+    if Q.shape[1] != dim:
+        raise ValueError(f"Query dim {Q.shape[1]} != index dim {dim}")
+    return Q

@@ -285,7 +285,7 @@ class IncrementalDiskANN:
         """Batched search: (ids u64[nq, k], dists f32[nq, k], counts u32[nq]).
         A filter only applies to an index with labels, as in
         search_filtered_with_dists (src/incremental.rs:1020-1030)."""
-        Q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, self.dim)
+        Q = _lib.query_rows(queries, self.dim)
         if filters is not None and not self._nf:
             filters = None
         if traversal is None:  # the quantizer's codes unless a label filter is given (:1020-1070)

@@ -731,7 +731,7 @@ class SPFresh:
             p.flags = _lib.FLAG_DEVICE_PTRS | _lib.FLAG_STREAM
             p.stream = stream if stream is not None else torch.cuda.current_stream(Q.device).cuda_stream
         else:
-            Q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, self.dim)
+            Q = _lib.query_rows(queries, self.dim)
             nq = Q.shape[0]
             out = (np.empty((nq, k), dtype=np.uint64), np.empty((nq, k), dtype=np.float32),
                    np.empty(nq, dtype=np.uint32))

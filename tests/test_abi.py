@@ -276,3 +276,21 @@ def test_insert_dimension_checks():
         _lib.rows_f32([[0.0] * 8, [1.0] * 8, [2.0] * 3], 8, msg)
     assert _lib.rows_f32(np.zeros((0, 8)), 8, msg).shape == (0, 8)
     assert _lib.rows_f32([1.0] * 8, 8, msg).shape == (1, 8)
+
+
+def test_query_shapes():
+    """Host queries of the wrong length raise the reference's assertion text
+    (src/lib.rs:684-690) as ValueError; a batch is never reshaped into other
+    queries."""
+    import numpy as np
+
+    from pydiskann_b200 import _lib
+
+    for bad, n in ((np.zeros((2, 3)), 3), ([[0.0] * 4, [0.0] * 3], 3), (np.zeros(8), 8)):
+        with pytest.raises(ValueError, match=f"^Query dim {n} != index dim 4$"):
+            _lib.query_rows(bad, 4)
+    with pytest.raises(ValueError, match="2-D batch"):
+        _lib.query_rows(np.zeros((2, 2, 4)), 4)
+    assert _lib.query_rows(np.zeros(4), 4).shape == (1, 4)
+    assert _lib.query_rows([], 4).shape == (0, 4) and _lib.query_rows(np.zeros((0, 4)), 4).shape == (0, 4)
+    assert _lib.query_rows(np.ones((3, 4)), 4).shape == (3, 4)
