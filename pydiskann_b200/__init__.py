@@ -133,7 +133,7 @@ def fp8_encode(vectors, device=0):
 def exact_knn(vectors, queries, k=10, metric="l2", device=0):
     """Brute-force k nearest neighbours (FP64 accumulation) -> (ids, dists)."""
     X = _f32(vectors)
-    Q = _f32(queries).reshape(-1, X.shape[1])
+    Q = _lib.query_rows(queries, X.shape[1])
     ids = np.empty((Q.shape[0], k), dtype=np.uint32)
     ds = np.empty((Q.shape[0], k), dtype=np.float32)
     check(lib().dg_exact_knn(ptr(X), X.shape[0], X.shape[1], ptr(Q), Q.shape[0], k, _metric(metric),

@@ -76,7 +76,7 @@ class Server:
     def submit(self, query, k=10, beam_width=64, rerank_size=0, traversal=None, filter=None):  # noqa: A002
         q = np.ascontiguousarray(query, dtype=np.float32).reshape(-1)
         if q.shape[0] != self.index.dim:
-            raise ValueError(f"query has dimension {q.shape[0]}, index has {self.index.dim}")
+            raise ValueError(f"Query dim {q.shape[0]} != index dim {self.index.dim}")
         r = _lib.Request(k, beam_width, rerank_size, _trav(self.index, traversal))
         keep = []
         if filter is not None and not filter.is_none():
@@ -118,7 +118,7 @@ class Server:
         Returns a dict with per-request `ids` / `dists` (trimmed to counts),
         `latency_us` (scheduled arrival to result) and `wall_us`.
         """
-        Q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, self.index.dim)
+        Q = _lib.query_rows(queries, self.index.dim)
         n = Q.shape[0]
         arr = np.ascontiguousarray(arrival_us, dtype=np.float64)
         if arr.shape != (n,):
