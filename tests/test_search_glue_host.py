@@ -41,14 +41,16 @@ def test_spfresh_search_glue(monkeypatch):
     monkeypatch.setattr(spf_mod, "lib", lambda: fake)
     s = SPFresh(4, device=None)
     s._h = object()  # stands in for the device mirror
-    assert s.search_batch(np.zeros((3, 4), np.float32), k=2, n_probe=5) == [[0], [10, 11], [20, 21]]
-    assert fake.calls[-1] == (3, 2)
-    assert s.search_with_dists([0.0] * 4, k=3) == [(0, 0.0)]
-    for bad in ([0.0] * 8, np.zeros((2, 3)), [[0.0] * 4, [0.0] * 3]):
-        with pytest.raises(ValueError, match="Query dim"):
-            s.search_batch(bad, k=2)
-    assert len(fake.calls) == 2
-    s._h = None
+    try:
+        assert s.search_batch(np.zeros((3, 4), np.float32), k=2, n_probe=5) == [[0], [10, 11], [20, 21]]
+        assert fake.calls[-1] == (3, 2)
+        assert s.search_with_dists([0.0] * 4, k=3) == [(0, 0.0)]
+        for bad in ([0.0] * 8, np.zeros((2, 3)), [[0.0] * 4, [0.0] * 3]):
+            with pytest.raises(ValueError, match="Query dim"):
+                s.search_batch(bad, k=2)
+        assert len(fake.calls) == 2
+    finally:
+        s._h = None
 
 
 def test_incremental_search_glue(monkeypatch):
