@@ -404,7 +404,9 @@ class _Index:
                 p.filter_ops, p.filter_offsets = C.cast(arr, C.c_void_p), ptr(offs)
                 p.filter_pool, p.filter_pool_len = ptr(pool), plen
         if per_query_beam is not None:
-            pl = np.ascontiguousarray(per_query_beam, dtype=np.uint32)
+            pl = np.ascontiguousarray(per_query_beam, dtype=np.uint32).reshape(-1)
+            if len(pl) != nq:  # the library reads one beam width per query
+                raise ValueError(f"one beam width per query expected: {len(pl)} for {nq} queries")
             keep.append(pl)
             p.per_query_beam = ptr(pl)
         return p, Q, nq, out, stats, keep

@@ -77,3 +77,50 @@ def test_incremental_search_glue(monkeypatch):
         with pytest.raises(ValueError, match="Query dim"):
             o.search_batch(bad, k=2)
     assert len(seen) == 2
+
+
+def _read(p, dtype, n):
+    import ctypes as C
+
+    if not p:
+        return None
+    return np.frombuffer((C.c_char * (n * np.dtype(dtype).itemsize)).from_address(int(p)), dtype=dtype).copy()
+
+
+def test_search_params_packing():
+    """_Index._params (every host-side search and the autotuner): per-query
+    filter programs arrive as ops + offsets[nq + 1] + one value pool, one
+    program as ops without offsets, Filter.none() as no program, and one beam
+    width per query -- never fewer (the library reads nq of them)."""
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import Filter
+
+    op_dt = np.dtype({"names": ["op", "field", "a", "b"], "formats": [np.uint32, np.uint32, np.uint64, np.uint64],
+                      "offsets": [0, 4, 8, 16], "itemsize": 24})
+    ix = object.__new__(dg._Index)
+    ix._X = np.zeros((1, 4), np.float32)  # dim 4; nothing reaches a device
+    Q = np.zeros((3, 4), np.float32)
+    fl = [Filter.in_(0, [5, 6]), Filter.none(), Filter.or_([Filter.eq(1, 2), Filter.in_(2, [9])])]
+    p, _, nq, _, _, keep = ix._params(Q, 10, 32, 0, 0, fl, [8, 16, 24], None, None, False)
+    offs = _read(p.filter_offsets, np.uint32, nq + 1)
+    ops = _read(p.filter_ops, op_dt, int(offs[-1]))
+    pool = _read(p.filter_pool, np.uint64, p.filter_pool_len)
+    for q, f in enumerate(fl):
+        mine = [tuple(int(x) for x in o) for o in ops[offs[q]:offs[q + 1]]]
+        want, wpool = f.program()
+        assert len(mine) == len(want)
+        for (op, field, a, b), (wop, wfield, wa, wb) in zip(mine, want):
+            assert (op, field) == (wop, wfield)
+            if op == 2:  # IN: offsets rebased into the shared pool
+                assert pool[a:a + b].tolist() == wpool[wa:wa + wb]
+            else:
+                assert (a, b) == (wa, wb)
+    assert _read(p.per_query_beam, np.uint32, 3).tolist() == [8, 16, 24]
+    p1, *_ = ix._params(Q, 10, 32, 0, 0, Filter.eq(0, 1), None, None, None, False)
+    assert p1.filter_nops == 1 and not p1.filter_offsets
+    p0, *_ = ix._params(Q, 10, 32, 0, 0, Filter.none(), None, None, None, False)
+    assert p0.filter_nops == 0 and not p0.filter_ops
+    with pytest.raises(ValueError, match="one beam width per query"):
+        ix._params(Q, 10, 32, 0, 0, None, [8, 16], None, None, False)
+    with pytest.raises(ValueError, match="one filter per query"):
+        ix._params(Q, 10, 32, 0, 0, fl[:2], None, None, None, False)
