@@ -276,6 +276,21 @@ def _pack_programs(progs):
     return arr, np.asarray(offs, dtype=np.uint32), np.asarray(pool if pool else [0], dtype=np.uint64), len(pool)
 
 
+def _check_out(out, nq, k, dev):
+    """Caller-given result buffers (ids, dists, counts): the library writes
+    nq * k ids and distances and nq counts of 4 bytes each, contiguously,
+    into device memory for CUDA queries and host memory otherwise."""
+    for a, need, name in zip(out, (nq * k, nq * k, nq), ("ids", "dists", "counts")):
+        tensor = hasattr(a, "data_ptr")
+        size = a.numel() if tensor else np.asarray(a).size
+        item = a.element_size() if tensor else a.itemsize
+        contiguous = a.is_contiguous() if tensor else a.flags.c_contiguous
+        on_device = tensor and getattr(a, "is_cuda", False)
+        if size < need or item != 4 or not contiguous or on_device != dev or (not tensor and not a.flags.writeable):
+            raise ValueError(f"out[{name}] must be a writable contiguous {'CUDA' if dev else 'host'} array of "
+                             f">= {need} 4-byte elements")
+
+
 # ------------------------------------------------------------------- index
 class _Index:
     """A device-resident graph index (one libdgann DgIndex handle)."""
@@ -384,6 +399,7 @@ class _Index:
             if stream is not None:
                 p.flags = _lib.FLAG_STREAM
                 p.stream = stream
+        _check_out(out, nq, k, dev)
         if isinstance(filters, PackedFilters):
             if filters.n != nq:
                 raise ValueError("one filter per query expected")

@@ -124,3 +124,20 @@ def test_search_params_packing():
         ix._params(Q, 10, 32, 0, 0, None, [8, 16], None, None, False)
     with pytest.raises(ValueError, match="one filter per query"):
         ix._params(Q, 10, 32, 0, 0, fl[:2], None, None, None, False)
+
+
+def test_out_buffers_are_checked():
+    """Result buffers given by the caller must hold what the library writes:
+    nq * k ids and distances and nq counts, 4 bytes each, contiguous."""
+    import pydiskann_b200 as dg
+
+    ix = object.__new__(dg._Index)
+    ix._X = np.zeros((1, 4), np.float32)
+    Q = np.zeros((3, 4), np.float32)
+    good = (np.empty((3, 10), np.uint32), np.empty((3, 10), np.float32), np.empty(3, np.uint32))
+    assert ix._params(Q, 10, 32, 0, 0, None, None, good, None, False)[3] is good
+    bad = [(np.empty((3, 9), np.uint32), good[1], good[2]), (good[0], np.empty((3, 10), np.float64), good[2]),
+           (good[0], good[1], np.empty(2, np.uint32)), (good[0], np.empty((10, 3), np.float32).T, good[2])]
+    for out in bad:
+        with pytest.raises(ValueError, match="must be a writable contiguous host array"):
+            ix._params(Q, 10, 32, 0, 0, None, None, out, None, False)
