@@ -374,9 +374,15 @@ class _Index:
             import torch
 
             Q = queries.contiguous()
-            nq = Q.shape[0]
-            if Q.dtype != torch.float32 or Q.shape[1] != self.dim:
+            if Q.dim() == 1:
+                Q = Q.reshape(1, -1)
+            if Q.dim() != 2:
+                raise ValueError(f"queries must be one query or a 2-D batch, not shape {tuple(Q.shape)}")
+            if Q.shape[1] != self.dim:
                 raise ValueError(f"Query dim {Q.shape[1]} != index dim {self.dim}")
+            if Q.dtype != torch.float32:
+                raise ValueError(f"CUDA queries must be float32, not {Q.dtype}")
+            nq = Q.shape[0]
             if out is None:
                 out = (torch.empty((nq, k), dtype=torch.int32, device=Q.device),
                        torch.empty((nq, k), dtype=torch.float32, device=Q.device),

@@ -724,6 +724,14 @@ class SPFresh:
             import torch
 
             Q = queries.contiguous()
+            if Q.dim() == 1:
+                Q = Q.reshape(1, -1)
+            if Q.dim() != 2:
+                raise ValueError(f"queries must be one query or a 2-D batch, not shape {tuple(Q.shape)}")
+            if Q.shape[1] != self.dim:
+                raise ValueError(f"Query dim {Q.shape[1]} != index dim {self.dim}")
+            if Q.dtype != torch.float32:
+                raise ValueError(f"CUDA queries must be float32, not {Q.dtype}")
             nq = Q.shape[0]
             out = (torch.empty((nq, k), dtype=torch.int64, device=Q.device),
                    torch.empty((nq, k), dtype=torch.float32, device=Q.device),

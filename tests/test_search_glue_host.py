@@ -141,3 +141,57 @@ def test_out_buffers_are_checked():
     for out in bad:
         with pytest.raises(ValueError, match="must be a writable contiguous host array"):
             ix._params(Q, 10, 32, 0, 0, None, None, out, None, False)
+
+
+class _AsCuda:
+    """A CPU tensor that reports itself as CUDA, to reach the device-query
+    checks, which run before anything is allocated or launched."""
+
+    is_cuda = True
+
+    def __init__(self, t):
+        self.t = t
+
+    def data_ptr(self):
+        return self.t.data_ptr()
+
+    def contiguous(self):
+        return self
+
+    def dim(self):
+        return self.t.dim()
+
+    def reshape(self, *s):
+        return _AsCuda(self.t.reshape(*s))
+
+    @property
+    def shape(self):
+        return self.t.shape
+
+    @property
+    def dtype(self):
+        return self.t.dtype
+
+
+def test_device_query_checks():
+    import torch
+
+    import pydiskann_b200 as dg
+
+    ix = object.__new__(dg._Index)
+    ix._X = np.zeros((1, 4), np.float32)
+    s = SPFresh(4, device=None)
+    s._h = object()
+    try:
+        for call in (lambda q: ix._params(q, 10, 32, 0, 0, None, None, None, None, False),
+                     lambda q: s.search_arrays(q, 10, 4)):
+            with pytest.raises(ValueError, match="^Query dim 3 != index dim 4$"):
+                call(_AsCuda(torch.zeros(3)))
+            with pytest.raises(ValueError, match="^Query dim 3 != index dim 4$"):
+                call(_AsCuda(torch.zeros((2, 3))))
+            with pytest.raises(ValueError, match="2-D batch"):
+                call(_AsCuda(torch.zeros((2, 2, 4))))
+            with pytest.raises(ValueError, match="must be float32"):
+                call(_AsCuda(torch.zeros((2, 4), dtype=torch.float64)))
+    finally:
+        s._h = None
