@@ -225,14 +225,22 @@ DG_API DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const f
  * this library.  It allocates nothing: its scratch (the search's work counter
  * and copies of the filter programs and per-query beams) lives in a
  * file-scope device array of 256 KiB that every GPU loading the library keeps
- * until the process exits.  Requires DG_FLAG_DEVICE_PTRS (queries and outputs
- * in device memory, no host staging) and returns after enqueueing on the
- * stream.  Per-call parameters larger than the array (about 10k filter ops or
- * 60k per-query beams) are rejected with DG_EINVAL.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  Every call reuses the same array, so
- * calls that overlap on the GPU (any device, any stream, any handle) race:
- * order them on one stream or wait between them.  out_stats is not written. */
+ * until the process exits.  Requires DG_FLAG_DEVICE_PTRS: queries and outputs
+ * are device memory.  The filter programs (filter_ops, filter_offsets,
+ * filter_pool) and per_query_beam stay HOST memory, as in dg_search_batch:
+ * they are validated on the host and copied into the array with
+ * cudaMemcpyAsync on the call's stream, so pinned arrays must stay valid
+ * until the stream has passed the call.  Returns after enqueueing.  Per-call
+ * parameters larger than the array (about 10k filter ops or 60k per-query
+ * beams) are rejected with DG_EINVAL.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Each device has its own copy of the array:
+ * calls that overlap on the same device (any stream, any handle) share it
+ * and race, so order them on one stream or wait between them; calls on
+ * different devices do not interact.  Like dg_search_batch, the call records
+ * its completion on one of the index's 16 completion events (blocking while
+ * all 16 are in flight), so later row, adjacency, label and tombstone
+ * updates and dg_index_destroy wait for it.  out_stats is not written. */
 DG_API DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p, const float *queries,
                                        uint32_t nq, uint32_t *out_ids, float *out_dists,
                                        uint32_t *out_counts);

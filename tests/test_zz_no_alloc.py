@@ -17,7 +17,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _static_search(index, Qd, k, L, traversal, rerank=0, filt=None, beams=None):
+def _static_search(index, Qd, k, L, traversal, rerank=0, filt=None, beams=None, sync=True):
     import torch
 
     import pydiskann_b200 as dg
@@ -43,6 +43,8 @@ def _static_search(index, Qd, k, L, traversal, rerank=0, filt=None, beams=None):
         p.per_query_beam = _lib.ptr(b)
     st = _lib.lib().dg_search_batch_static(index._h, C.byref(p), _lib.ptr(Qd), nq, _lib.ptr(ids), _lib.ptr(ds),
                                            _lib.ptr(cnt))
+    if not sync:
+        return st, (ids, ds, cnt)
     torch.cuda.synchronize()
     return st, ids.cpu().numpy().view(np.uint32), ds.cpu().numpy(), cnt.cpu().numpy().view(np.uint32)
 
@@ -61,17 +63,39 @@ def setup():
     idx = dg.FilteredDiskANN(X, adj, med, labels)
     idx.enable_bf16()
     Qd = torch.from_numpy(Q).cuda()
-    yield dg, idx, Q, Qd
-    idx.close()
+    # code traversals: int8 and PQ codes with an FP32 rerank
+    q8 = dg.QuantizedDiskANN(X, adj, med)
+    q8.attach_int8(*dg.int8_params(X))
+    qpq = dg.QuantizedDiskANN(X, adj, med)
+    qpq.attach_pq(dg.pq_train(X, 16, 256, 4, 3000, seed=5))
+    # a base + delta shaped index: two entry points and tombstoned rows
+    tomb = dg.DiskANN.from_graph(X, adj, med)
+    dead = np.arange(7, len(X), 11, dtype=np.uint32)
+    _lib_check(tomb, "dg_index_set_tombstones", dead, len(dead), 1, len(dead))
+    _lib_check(tomb, "dg_index_set_entry_points", np.array([med, (med + 1234) % len(X)], dtype=np.uint32), 2)
+    yield dg, {"main": idx, "int8": q8, "pq": qpq, "tomb": tomb}, Q, Qd
+    for ix in (idx, q8, qpq, tomb):
+        ix.close()
 
 
-@pytest.mark.parametrize("case", ["fp32", "bf16_rerank", "filtered", "uneven_beams"])
-def test_static_matches_allocating_entry_point(setup, case):
-    dg, idx, Q, Qd = setup
+def _lib_check(index, name, arr, *args):
     from pydiskann_b200 import _lib
 
-    trav = _lib.TRAVERSE_BF16 if case == "bf16_rerank" else _lib.TRAVERSE_F32
-    rerank = 48 if case == "bf16_rerank" else 0
+    st = getattr(_lib.lib(), name)(index._h, _lib.ptr(arr), *args)
+    assert st == _lib.DG_OK, _lib.lib().dg_last_error()
+
+
+@pytest.mark.parametrize("case", ["fp32", "bf16_rerank", "filtered", "uneven_beams", "int8_rerank",
+                                  "pq_rerank", "tombstones_two_seeds"])
+def test_static_matches_allocating_entry_point(setup, case):
+    dg, ixs, Q, Qd = setup
+    from pydiskann_b200 import _lib
+
+    idx = {"int8_rerank": ixs["int8"], "pq_rerank": ixs["pq"], "tombstones_two_seeds": ixs["tomb"]}.get(case,
+                                                                                                    ixs["main"])
+    trav = {"bf16_rerank": _lib.TRAVERSE_BF16, "int8_rerank": _lib.TRAVERSE_CODES,
+            "pq_rerank": _lib.TRAVERSE_CODES}.get(case, _lib.TRAVERSE_F32)
+    rerank = 48 if case in ("bf16_rerank", "int8_rerank", "pq_rerank") else 0
     filt = dg.Filter.or_([dg.Filter.eq(0, 1), dg.Filter.range(1, 2, 4)]) if case == "filtered" else None
     beams = np.random.default_rng(3).integers(4, 120, size=len(Q)) if case == "uneven_beams" else None
     want = idx.search_arrays(Q, 10, 48, traversal=trav, rerank_size=rerank, filters=filt, per_query_beam=beams)
@@ -84,7 +108,8 @@ def test_static_matches_allocating_entry_point(setup, case):
 
 
 def test_static_rejects_parameters_beyond_its_array(setup):
-    dg, idx, Q, Qd = setup
+    dg, ixs, Q, Qd = setup
+    idx = ixs["main"]
     from pydiskann_b200 import _lib
 
     import torch
@@ -94,3 +119,38 @@ def test_static_rejects_parameters_beyond_its_array(setup):
     st, _, _, _ = _static_search(idx, big, 10, 32, _lib.TRAVERSE_F32, beams=beams)
     assert st == _lib.DG_EINVAL
     assert b"static scratch" in _lib.lib().dg_last_error()
+
+
+def test_updates_and_destroy_wait_for_a_static_search():
+    """A static search still running on its own stream when the caller
+    tombstones rows, rewrites rows and destroys the index (no synchronisation
+    in between) returns the results of the index as it was: every update and
+    the destroy wait for the search's completion event."""
+    import torch
+
+    import oracle
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import _lib, synth
+
+    X = synth.mixture(6000, 128, 16, seed=41)
+    Q = synth.mixture(3000, 128, 16, seed=41, stream=synth.STREAM_QUERY)
+    adj, med = dg.build_graph(X, 32, 64, 1.2, seed=6)
+    want = oracle.OracleIndex(X, adj, med).search(Q, 10, 200)
+    idx = dg.DiskANN.from_graph(X, adj, med)
+    Qd = torch.from_numpy(Q).cuda()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        st, (ids, ds, cnt) = _static_search(idx, Qd, 10, 200, _lib.TRAVERSE_F32, sync=False)
+    assert st == _lib.DG_OK, _lib.lib().dg_last_error()
+    # the nearest results of every query: tombstoned, then moved far away
+    hit = np.unique(want[0][:, :3]).astype(np.uint32)
+    _lib_check(idx, "dg_index_set_tombstones", hit, len(hit), 1, len(hit))
+    far = np.full((1, X.shape[1]), 1e6, dtype=np.float32)
+    for r in hit[:50]:
+        assert _lib.lib().dg_index_update_rows(idx._h, int(r), 1, _lib.ptr(far), None, None) == _lib.DG_OK
+    idx.close()
+    torch.cuda.synchronize()
+    assert np.array_equal(cnt.cpu().numpy().view(np.uint32), want[2])
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), want[0])
+    assert np.array_equal(ds.cpu().numpy(), want[1])
