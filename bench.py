@@ -1,23 +1,27 @@
 #!/usr/bin/env python
-"""QPS at recall@10 >= 0.95 on the 1M x 128 PQ workload, on one B200 (or N replicas).
+"""QPS at recall@10 >= 0.95 on the 1M x 128 workload, plain FP32 vs BF16 + FP32
+rerank, on one B200 (or N replicas).
 
 Workload: 1M x 128 FP32 base vectors from a 256-centre clipped Gaussian mixture
 (seeded synthetic data with the configuration's shapes and value distribution),
-10k queries per batch, Vamana graph R=64, L_build=128, alpha=1.2 (built on the
-GPU), PQ M=16 x K=256 trained with 25 Lloyd iterations on a 100k sample, k=10.
-A step is one batched search of the 10k queries.  Three variants are swept over
-the beam width L and each is timed at the smallest L whose recall@10 against
-the exact FP64 ground truth reaches 0.95:
-  fp32       -- plain FP32 beam search (DiskANN::search)
-  bf16_rerank-- BF16 rows during the search, FP32 rerank of the top L
-  int8_rerank-- int8 SQ codes (global scale/offset, src/sq.rs) during the
-                search, FP32 rerank of the top L
-  pq_rerank  -- PQ ADC during the search, FP32 rerank of the top L
-The headline `value` is the fastest variant at recall >= 0.95; a variant that
-does not reach it within the swept beams is reported with its best recall.
+10k queries per batch, Vamana graph R=64, L_build=128, alpha=1.2, PQ M=16 x
+K=256 trained with 25 Lloyd iterations on a 100k sample, k=10.  A step is one
+batched search of the 10k queries.  Each variant is timed at the smallest beam
+L whose recall@10 against the exact FP64 ground truth reaches 0.95:
+  bf16_rerank-- BF16 rows during the search, FP32 rerank of the top L: the
+                headline `value`
+  fp32       -- plain FP32 beam search (DiskANN::search), reported beside it
+  int8_rerank-- int8 SQ codes (global scale/offset, src/sq.rs) + FP32 rerank
+  fp8_rerank -- e4m3 rows with per-vector scales + FP32 rerank
+  pq_rerank  -- PQ ADC + FP32 rerank of the top L
+The graph, codebooks and ground truth are inputs of the search: `--prepare`
+builds them once into a cache, in a process of its own that loads only the
+index-construction library (libdgbuild.so), and both arms read that cache.
 
 `--impl reference` times the CPU restatement of the reference search (the
-oracle, all host threads) on the same graph, codes and queries.
+oracle, all host threads) on the same graph, queries and variant: BF16 rows
+during the traversal and an FP32 rerank of the top L, at the beam the oracle's
+own recall sweep picks.
 """
 from __future__ import annotations
 
@@ -39,6 +43,9 @@ if ROOT not in sys.path:
 CACHE = os.environ.get("DGANN_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "dgann_bench_cache"))
 R, L_BUILD, ALPHA, M, K_PQ, PQ_ITERS, PQ_SAMPLE, K = 64, 128, 1.2, 16, 256, 25, 100_000, 10
 L_SWEEP = (16, 24, 32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256, 384, 512, 768, 1024)
+METRIC = "QPS @ recall@10=0.95, plain FP32 vs BF16+FP32-rerank, 1 B200; p99 ms"
+HEADLINE = "bf16_rerank"
+PARITY_QUERIES = 1000  # queries of the batch compared with the oracle for every timed variant
 
 
 def log(*a):
@@ -51,11 +58,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--prepare", action="store_true",
+                    help="only build the cached graph, codebooks and ground truth (index-construction library)")
+    ap.add_argument("--device", type=int, default=0, help="device of --prepare")
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--target-recall", type=float, default=0.95)
-    ap.add_argument("--variants", default="fp32,bf16_rerank,fp8_rerank,int8_rerank,pq_rerank")
+    ap.add_argument("--variants", default="bf16_rerank,fp32,fp8_rerank,int8_rerank,pq_rerank")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
@@ -77,56 +87,94 @@ def parse():
 
 
 # ------------------------------------------------------------------ setup
-def workload(args, device=0, build=True):
-    """Data (regenerated), graph, codebooks and ground truth (cached on disk)."""
-    from pydiskann_b200 import synth
-
-    t0 = time.time()
-    X, Q = synth.pq_config(args.n, args.nq, 128, args.seed)
-    log(f"[setup] data {X.shape} + {Q.shape} in {time.time() - t0:.1f}s")
+def _cache_files(args):
     key = f"pq_n{args.n}_q{args.nq}_R{R}_L{L_BUILD}_a{ALPHA}_M{M}_s{args.seed}"
     d = os.path.join(CACHE, key)
-    files = {k: os.path.join(d, k + ".npy") for k in ("adj", "meta", "cb", "codes", "gt")}
-    if all(os.path.exists(f) for f in files.values()):
-        adj = np.load(files["adj"])
-        med = int(np.load(files["meta"])[0])
-        cb = np.load(files["cb"])
-        codes = np.load(files["codes"])
-        gt = np.load(files["gt"])
-        log(f"[setup] graph/codebooks/ground truth from cache {d}")
-        return X, Q, adj, med, (cb, codes), gt, {"cached": True}
-    if not build:
-        return None
+    return d, {k: os.path.join(d, k + ".npy") for k in ("adj", "meta", "cb", "codes", "gt")}
+
+
+def prepare(args):
+    """Builds the cached inputs of the search (graph, medoid, PQ codebooks and
+    codes, FP64 ground truth) with the index-construction library only."""
+    from pydiskann_b200 import synth
+
     import pydiskann_b200 as dg
 
+    d, files = _cache_files(args)
+    if all(os.path.exists(f) for f in files.values()):
+        return {"cached": True}
+    X, Q = synth.pq_config(args.n, args.nq, 128, args.seed)
+    dev = args.device
     times = {}
     t0 = time.time()
-    med = dg.medoid(X, device=device)
-    times["medoid_s"] = time.time() - t0
+    med = dg.medoid(X, device=dev)
+    times["medoid_s"] = round(time.time() - t0, 2)
     t0 = time.time()
-    adj, _ = dg.build_graph(X, R, L_BUILD, ALPHA, seed=args.seed, medoid_id=med, device=device)
-    times["graph_build_s"] = time.time() - t0
-    log(f"[setup] GPU Vamana build {times['graph_build_s']:.1f}s")
+    adj, _ = dg.build_graph(X, R, L_BUILD, ALPHA, seed=args.seed, medoid_id=med, device=dev)
+    times["graph_build_s"] = round(time.time() - t0, 2)
     t0 = time.time()
-    cb = dg.pq_train(X, M, K_PQ, PQ_ITERS, PQ_SAMPLE, seed=args.seed, device=device)
-    times["pq_train_s"] = time.time() - t0
-    codes = dg.pq_encode(X, cb, device=device)
+    cb = dg.pq_train(X, M, K_PQ, PQ_ITERS, PQ_SAMPLE, seed=args.seed, device=dev)
+    times["pq_train_s"] = round(time.time() - t0, 2)
+    codes = dg.pq_encode(X, cb, device=dev)
     t0 = time.time()
-    gt, _ = dg.exact_knn(X, Q, K, device=device)
-    times["ground_truth_s"] = time.time() - t0
-    log(f"[setup] PQ train {times['pq_train_s']:.1f}s, exact kNN {times['ground_truth_s']:.1f}s")
+    gt, _ = dg.exact_knn(X, Q, K, device=dev)
+    times["ground_truth_s"] = round(time.time() - t0, 2)
     os.makedirs(d, exist_ok=True)
     for k, v in (("adj", adj), ("meta", np.array([med])), ("cb", cb), ("codes", codes), ("gt", gt)):
         tmp = files[k] + f".tmp{os.getpid()}.npy"
         np.save(tmp, v)
         os.replace(tmp, files[k])
-    return X, Q, adj, med, (cb, codes), gt, times
+    with open(os.path.join(d, "setup.json"), "w") as f:
+        json.dump(times, f)
+    return times
+
+
+def _run_prepare(args, device):
+    """`bench.py --prepare` in a child process (it loads libdgbuild.so only)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--prepare", "--device", str(device), "--n", str(args.n),
+           "--nq", str(args.nq), "--seed", str(args.seed)]
+    t0 = time.time()
+    subprocess.run(cmd, check=True)
+    log(f"[setup] prepared the cached graph, codebooks and ground truth in {time.time() - t0:.1f}s")
+
+
+def workload(args, device=0, build=True):
+    """Data (regenerated from the seed) and the cached graph, codebooks and
+    ground truth; builds the cache first (in a child process) when missing."""
+    from pydiskann_b200 import synth
+
+    d, files = _cache_files(args)
+    if not all(os.path.exists(f) for f in files.values()):
+        if not build:
+            return None
+        _run_prepare(args, device)
+    t0 = time.time()
+    X, Q = synth.pq_config(args.n, args.nq, 128, args.seed)
+    log(f"[setup] data {X.shape} + {Q.shape} in {time.time() - t0:.1f}s")
+    adj = np.load(files["adj"])
+    med = int(np.load(files["meta"])[0])
+    cb = np.load(files["cb"])
+    codes = np.load(files["codes"])
+    gt = np.load(files["gt"])
+    setup = {"cache": d}
+    try:
+        setup.update(json.load(open(os.path.join(d, "setup.json"))))
+    except (OSError, ValueError):
+        pass
+    return X, Q, adj, med, (cb, codes), gt, setup
 
 
 def recall(ids, gt, k=K):
     ids = np.asarray(ids)[:, :k]
     hits = sum(len(set(ids[i].tolist()) & set(gt[i, :k].tolist())) for i in range(len(gt)))
     return hits / (len(gt) * k)
+
+
+def config_of(args, world, L):
+    """The `config` object both arms print (same workload, variant and beam)."""
+    return {"workload": f"pq-1Mx128 M={M} R={R} L_build={L_BUILD} alpha={ALPHA} k={K} nq={args.nq} n={args.n}",
+            "variant": HEADLINE, "L": L, "global_batch": args.nq * world, "parallelism": f"replicas{world}",
+            "l2_policy": "inputs larger than L2 (512 MB f32 + 256 MB bf16 rows + 256 MB adjacency)"}
 
 
 # ------------------------------------------------------------ clock probe
@@ -258,10 +306,11 @@ class Clocks:
 
 
 # ------------------------------------------------------------ GPU timing
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
-# ncu capture of this bench's own command, keyed by (variant, L, queries, base
-# vectors); profiles/beam_search_int8_1Mx128.md, section 1.
-NCU_TRAFFIC = {("int8_rerank", 40, 10_000, 1_000_000): 1204.7e6 + 29.3e6}
+# DRAM bytes per launch of the dominant kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum), measured by one ncu capture of this bench's own
+# command, keyed by (variant, L, queries, base vectors).
+NCU_TRAFFIC = {}
+NCU_TRAFFIC_SOURCE = ""
 
 VARIANTS = {
     # name: (traversal, rerank = L?)
@@ -326,29 +375,73 @@ def distance_error(X, Q, ids, ds):
     return {"max": float(e.max()) if e.size else 0.0, "mean": float(e.mean()) if e.size else 0.0}
 
 
-def algorithmic_bytes(name, stats, L, d=128):
-    """Bytes the algorithm must read per launch: adjacency rows, distance
-    operands, rerank rows, queries and results (per query E·4R + N·bytes per
-    evaluation + L·4d + 4d + 8k)."""
-    E = stats[:, 0].astype(np.float64).sum()
-    N = stats[:, 1].astype(np.float64).sum()
-    nq = stats.shape[0]
+def algorithmic_bytes(name, nq, L, E, N, d=128):
+    """Bytes the algorithm must read per launch of nq queries: adjacency rows,
+    distance operands, rerank rows, queries and results (per query E*4R +
+    N*bytes per evaluation + L*4d + 4d + 8k).  E (expansions) and N (distance
+    evaluations) are per-query means of an exact visited set (the oracle's
+    counts); the kernel's own N also counts ids its small visited table forgot
+    and evaluated again."""
     adj = E * 4 * R
     if name == "fp32":
         dist, rr = N * 4 * d, 0.0
     elif name == "bf16_rerank":
-        dist, rr = N * 2 * d, nq * L * 4 * d
+        dist, rr = N * 2 * d, L * 4 * d
     elif name == "int8_rerank":
-        dist, rr = N * d, nq * L * 4 * d
+        dist, rr = N * d, L * 4 * d
     elif name == "fp8_rerank":
-        dist, rr = N * (d + 8), nq * L * 4 * d  # e4m3 row + (scale, norm)
+        dist, rr = N * (d + 8), L * 4 * d  # e4m3 row + (scale, norm)
     else:
-        dist, rr = N * M, nq * L * 4 * d
-    return adj + dist + rr + nq * 4 * d + nq * K * 8, {"expansions_per_query": E / nq, "dist_evals_per_query": N / nq}
+        dist, rr = N * M, L * 4 * d
+    return nq * (adj + dist + rr + 4 * d + 8 * K)
+
+
+def _oracle_variant(X, adj, med, pq, name):
+    """The oracle index of a variant (test infrastructure, run only as the checker
+    of the parity leg and as the CPU baseline)."""
+    import oracle
+
+    o = oracle.OracleIndex(X, adj, med)
+    if name == "pq_rerank":
+        o.set_pq(*pq)
+    elif name == "int8_rerank":
+        from pydiskann_b200 import int8_params
+
+        sc, off = int8_params(X)
+        o.set_int8(sc, off, oracle.int8_encode(X, sc, off))
+    elif name == "bf16_rerank":
+        o.set_bf16()
+    elif name == "fp8_rerank":
+        o.set_fp8(*oracle.fp8_encode(X))
+    return o
+
+
+def _oracle_run(o, name, Qs, L, threads, with_stats=False):
+    if name == "fp32":
+        return o.search(Qs, K, L, threads=threads, with_stats=with_stats)
+    return o.search(Qs, K, L, rerank=L, use_codes=True, threads=threads, with_stats=with_stats)
+
+
+def parity_leg(X, Q, adj, med, pq, name, L, got, threads):
+    """Compares the GPU's results for the first PARITY_QUERIES queries of the
+    batch with the oracle's search of the same variant and beam: positions
+    whose id or distance differ, and queries whose result count differs.  Also
+    returns the oracle's per-query expansions and distance evaluations (an
+    exact visited set)."""
+    nq = min(PARITY_QUERIES, len(Q))
+    o = _oracle_variant(X, adj, med, pq, name)
+    oi, od, oc, st = _oracle_run(o, name, Q[:nq], L, threads, with_stats=True)
+    gi, gd, gc = (np.asarray(a)[:nq] for a in got)
+    return ({"queries": nq, "id_mismatch": int((gi != oi).sum()), "dist_mismatch": int((gd != od).sum()),
+             "count_mismatch": int((gc != oc).sum())},
+            {"expansions": float(st[:, 0].mean()), "dist_evals": float(st[:, 1].mean())})
 
 
 def main():
     args = parse()
+    if args.prepare:
+        log(f"[prepare] {json.dumps(prepare(args))}")
+        return 0
     if args.impl == "reference":
         return reference_arm(args)
     import torch
@@ -397,7 +490,7 @@ def main():
 
     # ---- recall sweep: smallest L reaching the target for each variant
     chosen, curves = {}, {}
-    for name in args.variants.split(","):
+    for name in wanted:
         curves[name] = []
         for L in L_SWEEP:
             ids, _, _ = run_variant(idx, qidx, name, Qd, L)
@@ -411,7 +504,7 @@ def main():
 
     # ---- timing per variant (device-resident queries and results), after the
     # autotuner picked the visited-table size for this exact search
-    results = {}
+    results, outs = {}, {}
     tuned = {}
     for name, (L, rec) in chosen.items():
         tuned[name] = autotune_variant(idx, qidx, name, Qd, L)
@@ -437,33 +530,53 @@ def main():
         total_ms = t_start.elapsed_time(t_end)
         steps_ms = np.array([a.elapsed_time(b) for a, b in ev])
         total_ms = max_over_ranks(total_ms, dist, dev)
-        ri, rd, _, st = run_variant(idx, qidx, name, Qd, L, with_stats=True)
+        outs[name] = tuple(t.cpu().numpy() for t in out)
+        outs[name] = (outs[name][0].view(np.uint32), outs[name][1], outs[name][2].view(np.uint32))
+        _, _, _, st = run_variant(idx, qidx, name, Qd, L, with_stats=True)
         stats = st.cpu().numpy().view(np.uint32)
-        alg_bytes, work = algorithmic_bytes(name, stats, L)
         # accuracy against the FP64 oracle: returned distances, the traversal's
         # own distances (rerank off) and the recall shortfall
         ti, td, _ = run_variant(idx, qidx, name, Qd, L, rerank=False)
-        acc = {"dist_rel_err": distance_error(X, Q, ri.cpu().numpy().view(np.uint32), rd.cpu().numpy()),
+        acc = {"dist_rel_err": distance_error(X, Q, outs[name][0], outs[name][1]),
                "traversal_dist_rel_err": distance_error(X, Q, ti.cpu().numpy().view(np.uint32), td.cpu().numpy()),
                "recall_delta_vs_fp64": round(1.0 - rec, 4)}
         results[name] = {
             "L": L, "recall_at_10": round(rec, 4), "qps": world * args.nq * args.steps / (total_ms / 1e3),
             "ms_per_step": total_ms / args.steps, "p50_ms": float(np.percentile(steps_ms, 50)),
             "p99_ms": float(np.percentile(steps_ms, 99)), "launch_ms": float(steps_ms.mean()),
-            "alg_bytes_per_launch": alg_bytes, **work, **acc, "visited_table_bits": tuned[name]["hbits"],
-            "clocks": ck.summary(),
+            "kernel_expansions_per_query": float(stats[:, 0].mean()),
+            "kernel_dist_evals_per_query": float(stats[:, 1].mean()),
+            **acc, "visited_table_bits": tuned[name]["hbits"], "clocks": ck.summary(),
         }
         log(f"[time] {name}: {json.dumps(results[name])}")
 
-    head = max(results, key=lambda n: results[n]["qps"]) if results else None
+    # ---- parity with the oracle on the first queries of the batch (rank 0),
+    # and the oracle's exact-visited work counts for the algorithmic bytes
+    parity = {}
+    if rank == 0:
+        threads = os.cpu_count() or 1
+        for name, r in results.items():
+            parity[name], work = parity_leg(X, Q, adj, med, (cb, codes), name, r["L"], outs[name], threads)
+            r["expansions_per_query"] = work["expansions"]
+            r["dist_evals_per_query"] = work["dist_evals"]
+            r["alg_bytes_per_launch"] = algorithmic_bytes(name, args.nq, r["L"], work["expansions"],
+                                                          work["dist_evals"])
+            log(f"[parity] {name}: {parity[name]} {work}")
+
+    head = HEADLINE if HEADLINE in results else (max(results, key=lambda n: results[n]["qps"]) if results else None)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
+    extra = {n: {"qps": r["qps"], "L": r["L"], "recall_at_10": r["recall_at_10"]} for n, r in results.items()
+             if n not in (HEADLINE, "fp32")}
+    for n in extra:
+        if n in ("int8_rerank",):
+            extra[n]["note"] = "int8 codes are lossless on this integer-valued 0-255 data (scale 1, offset 0)"
     line = {
-        "metric": "QPS @ recall@10=0.95, plain FP32 vs BF16+FP32-rerank, 1 B200; p99 ms",
+        "metric": METRIC,
         "value": results[head]["qps"] if head else None,
         "unit": "queries/s",
         "n_gpus": world,
@@ -476,10 +589,12 @@ def main():
         "dtype": {"fp32": "f32", "bf16_rerank": "bf16+f32", "int8_rerank": "u8+f32",
                   "fp8_rerank": "e4m3+f32"}.get(head, "u8-pq+f32"),
         "data": "synthetic (seeded 256-centre Gaussian mixture, 1M x 128, 10k queries)",
-        "config": {"workload": f"pq-1Mx128 M={M} R={R} L_build={L_BUILD} alpha={ALPHA} k={K} "
-                               f"nq={args.nq} n={args.n}", "variant": head,
-                   "L": results[head]["L"] if head else None, "global_batch": args.nq * world,
-                   "parallelism": f"replicas{world}", "l2_policy": "inputs larger than L2 (768 MB index)"},
+        "config": config_of(args, world, results[head]["L"] if head else None),
+        "fp32_qps": results["fp32"]["qps"] if "fp32" in results else None,
+        "bf16_rerank_over_fp32": (round(results[HEADLINE]["qps"] / results["fp32"]["qps"], 3)
+                                  if HEADLINE in results and "fp32" in results else None),
+        "extra_variants": extra,
+        "parity_vs_oracle": parity,
         "variants": results,
         "recall_curves": curves,
         "p99_ms": results[head]["p99_ms"] if head else None,
@@ -487,24 +602,27 @@ def main():
     }
     if head:
         r = results[head]
-        ach = r["alg_bytes_per_launch"] / (r["launch_ms"] / 1e3) / 1e9
-        line["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                            "frac": round(ach / hbm, 4),
-                            "traffic": NCU_TRAFFIC.get((head, r["L"], args.nq, args.n)),
-                            "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650"}
+        if "alg_bytes_per_launch" in r:
+            ach = r["alg_bytes_per_launch"] / (r["launch_ms"] / 1e3) / 1e9
+            tr = NCU_TRAFFIC.get((head, r["L"], args.nq, args.n))
+            line["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                                "frac": round(ach / hbm, 4), "traffic": tr,
+                                "traffic_source": NCU_TRAFFIC_SOURCE if tr else None,
+                                "peak_source": ("measured: MEASURED_PEAKS.json hbm_gbs (burst)" if peaks
+                                                else "fallback 6650 GB/s"),
+                                "kernel": f"beam_search_kernel {head} L={r['L']}",
+                                "alg_bytes_per_launch": r["alg_bytes_per_launch"]}
         line["clocks"] = r["clocks"]
         line["gpu_launches"] = args.steps
         line["e2e"] = e2e(args, idx, qidx, head, r["L"], Q, gt, dist, world, dev)
         if not args.no_serving:
             line["serving"] = {n: serving(args, idx, qidx, n, results[n]["L"], Q, gt)
-                               for n in dict.fromkeys(["fp32", head]) if n in results}
+                               for n in dict.fromkeys([head, "fp32"]) if n in results}
             # headline p99: the highest Poisson load (the saturation run measures queue drain)
-            loaded = [r for r in line["serving"][head]["rates"] if r["offered_rps"]]
+            loaded = [x for x in line["serving"][head]["rates"] if x["offered_rps"]]
             if loaded:
                 line["p99_ms"] = loaded[-1]["p99_ms"]
                 line["p99_load_rps"] = loaded[-1]["offered_rps"]
-        if "fp32" in results:
-            line["speedup_vs_fp32"] = round(r["qps"] / results["fp32"]["qps"], 2)
         if not args.no_filtered:
             line["filtered"] = filtered(args, X, Q, adj, med, dev, dist)
         if args.cosine and rank == 0:
@@ -900,35 +1018,14 @@ def serving(args, idx, qidx, name, L, Q, gt):
 
 
 # ------------------------------------------------------------ CPU legs
-def _oracle_index(X, adj, med, pq, name):
-    import oracle
-
-    o = oracle.OracleIndex(X, adj, med)
-    if name == "pq_rerank":
-        o.set_pq(*pq)
-    elif name == "int8_rerank":
-        import pydiskann_b200 as dg
-
-        sc, off = dg.int8_params(X)
-        o.set_int8(sc, off, oracle.int8_encode(X, sc, off))
-    return o
-
-
-def _oracle_run(o, name, Qs, L, threads):
-    # bf16_rerank runs as its FP32 equivalent on the CPU: the BF16 copy of
-    # integer-valued rows is exact, so both give the same ids and distances
-    if name in ("fp32", "bf16_rerank"):
-        return o.search(Qs, K, L, threads=threads)
-    return o.search(Qs, K, L, rerank=L, use_codes=True, threads=threads)
-
-
 def cpu_baseline(args, X, Q, adj, med, pq, name, L, threads=None):
+    """The oracle's search of the same variant and beam on the host cores, over
+    about cpu_seconds of queries (the batch, cycled)."""
     threads = threads or os.cpu_count() or 1
-    o = _oracle_index(X, adj, med, pq, name)
+    o = _oracle_variant(X, adj, med, pq, name)
     t0 = time.time()
     _oracle_run(o, name, Q[:200], L, threads)
     rate = 200 / max(time.time() - t0, 1e-6)
-    # about cpu_seconds of work: the query set, repeated when one pass is shorter
     ns = int(min(20 * len(Q), max(200, rate * args.cpu_seconds)))
     Qs = Q[np.arange(ns) % len(Q)]
     t0 = time.time()
@@ -936,63 +1033,55 @@ def cpu_baseline(args, X, Q, adj, med, pq, name, L, threads=None):
     dt = time.time() - t0
     return {"value": ns / dt, "unit": "queries/s", "cores": threads, "kind": "port",
             "sample": f"{ns} queries (the {len(Q)} bench queries, cycled), variant {name} at L={L}, "
-                      f"same graph/codes", "seconds": round(dt, 2)}
+                      f"same graph and rows", "seconds": round(dt, 2)}
 
 
 def reference_arm(args):
-    """The reference's plain search (DiskANN::search, CPU restatement, all host
-    threads) at the smallest beam reaching the recall target, on the workload
-    of the GPU arm.  Under torchrun only rank 0 works."""
+    """The reference search (CPU restatement, all host threads) of the headline
+    variant -- BF16 rows during the traversal, FP32 rerank of the top L -- at
+    the smallest beam whose recall@10 over the whole batch reaches the target,
+    on the workload of the GPU arm.  A step searches the whole batch.  This
+    process loads the oracle library only; a missing workload cache is built
+    by `bench.py --prepare` in a child process.  Under torchrun only rank 0
+    works."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    wl = workload(args, 0, build=False)
-    if wl is None:
-        # the graph and codebooks are inputs of the search; they are built once
-        # with the GPU builder and cached for both arms
-        wl = workload(args, 0, build=True)
-    X, Q, adj, med, pq, gt, _ = wl
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    X, Q, adj, med, pq, gt, _ = workload(args, int(os.environ.get("LOCAL_RANK", "0")))
     threads = os.cpu_count() or 1
-    name = "fp32"
-    o = _oracle_index(X, adj, med, pq, name)
-    # beam sweep on a 1000-query sample
-    ns = min(1000, len(Q))
-    L = L_SWEEP[-1]
+    name = HEADLINE
+    o = _oracle_variant(X, adj, med, pq, name)
+    L, curve = L_SWEEP[-1], []
     for Lc in L_SWEEP:
-        ids, _, _ = _oracle_run(o, name, Q[:ns], Lc, threads)
-        if recall(ids, gt[:ns]) >= args.target_recall:
+        ids, _, _ = _oracle_run(o, name, Q, Lc, threads)
+        rec = recall(ids, gt)
+        curve.append((Lc, round(rec, 4)))
+        if rec >= args.target_recall:
             L = Lc
             break
-    t0 = time.time()
-    _oracle_run(o, name, Q[:200], L, threads)
-    rate = 200 / max(time.time() - t0, 1e-6)
-    per_step = int(min(len(Q), max(100, rate * 6.0)))
     for _ in range(args.warmup):
-        _oracle_run(o, name, Q[:min(per_step, 200)], L, threads)
-    t0 = time.time()
-    ids_all = []
-    for s in range(args.steps):
-        lo = (s * per_step) % len(Q)
-        qs = Q[lo:lo + per_step]
-        ids, _, _ = _oracle_run(o, name, qs, L, threads)
-        ids_all.append((lo, ids))
-    dt = time.time() - t0
-    nq_done = sum(len(ids) for _, ids in ids_all)
-    qps = nq_done / dt
-    rec = float(np.mean([recall(ids, gt[lo:lo + len(ids)]) for lo, ids in ids_all]))
+        _oracle_run(o, name, Q[:1000], L, threads)
+    step_s = []
+    for _ in range(args.steps):
+        t0 = time.time()
+        ids, _, _ = _oracle_run(o, name, Q, L, threads)
+        step_s.append(time.time() - t0)
+    dt = float(np.sum(step_s))
+    qps = len(Q) * args.steps / dt
+    rec = recall(ids, gt)
     line = {
-        "impl": "reference",
-        "metric": "QPS @ recall@10=0.95, plain FP32 vs BF16+FP32-rerank, 1 B200; p99 ms",
-        "value": qps, "unit": "queries/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32",
         "data": "synthetic (seeded 256-centre Gaussian mixture, 1M x 128, 10k queries)",
-        "config": {"workload": f"pq-1Mx128 M={M} R={R} L_build={L_BUILD} alpha={ALPHA} k={K} "
-                               f"nq={args.nq} n={args.n}", "variant": name, "L": L,
-                   "recall_at_10": round(rec, 4)},
+        "config": config_of(args, world, L),
+        "recall_at_10": round(rec, 4), "recall_curve": curve,
+        "p99_ms": float(np.percentile(np.array(step_s) * 1e3, 99)),
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
-                         "sample": f"{per_step} queries per step, plain FP32 beam search (CPU restatement "
-                                   f"of the reference search, OpenMP over queries)"},
+                         "sample": f"the {len(Q)}-query batch per step: BF16 traversal + FP32 rerank of the top "
+                                   f"{L} (CPU restatement of the reference's quantized search, OpenMP over "
+                                   f"queries)"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _SO = os.path.join(_HERE, "_build", "libdgoracle.so")
 
 L2SQ, L2, COSINE, DOT = 0, 1, 2, 3
-Q_NONE, Q_PQ, Q_INT8, Q_RABITQ, Q_F16, Q_FP8 = 0, 1, 2, 3, 4, 5
+Q_NONE, Q_PQ, Q_INT8, Q_RABITQ, Q_F16, Q_FP8, Q_BF16 = 0, 1, 2, 3, 4, 5, 6
 PAD = 0xFFFFFFFF
 METRICS = {"l2": L2SQ, "l2sq": L2SQ, "euclidean": L2, "cosine": COSINE, "dot": DOT}
 
@@ -104,6 +104,7 @@ def _declare(L):
         "dgo_int8_encode": (None, [vp, u64, u32, f32, f32, vp]),
         "dgo_int8_distance": (f32, [vp, vp, u32, f32]),
         "dgo_f16_encode": (None, [vp, u64, u32, vp]),
+        "dgo_bf16_encode": (None, [vp, u64, u32, vp]),
         "dgo_fp8_encode": (None, [vp, u64, u32, vp, vp]),
         "dgo_e4m3_encode": (C.c_uint8, [C.c_float]),
         "dgo_e4m3_decode": (C.c_float, [C.c_uint8]),
@@ -233,6 +234,13 @@ class OracleIndex:
         self._keep.append(codes)
         self.s.quant, self.s.codes, self.s.code_size = Q_F16, _p(codes), codes.shape[1] * 2
 
+    def set_bf16(self, codes=None):
+        """BF16 rows (bf16_encode of the vectors unless given) for the BF16
+        traversal: search(..., use_codes=True, rerank=...)."""
+        codes = bf16_encode(self.vectors) if codes is None else np.ascontiguousarray(codes, dtype=np.uint16)
+        self._keep.append(codes)
+        self.s.quant, self.s.codes, self.s.code_size = Q_BF16, _p(codes), codes.shape[1] * 2
+
     def set_fp8(self, codes, scales):
         codes = np.ascontiguousarray(codes, dtype=np.uint8)
         sc = _f32(scales)
@@ -346,6 +354,14 @@ def f16_encode(X):
     X = _f32(X)
     out = np.empty(X.shape, dtype=np.uint16)
     lib().dgo_f16_encode(_p(X), X.size // X.shape[-1], X.shape[-1], _p(out))
+    return out
+
+
+def bf16_encode(X):
+    """f32 -> BF16 bits (u16), rounded to nearest even."""
+    X = _f32(X)
+    out = np.empty(X.shape, dtype=np.uint16)
+    lib().dgo_bf16_encode(_p(X), X.size // X.shape[-1], X.shape[-1], _p(out))
     return out
 
 

@@ -530,6 +530,21 @@ float fp8_row(const float *x, uint32_t d, uint8_t *code) {  // -> scale
   return s;
 }
 
+// ---------------------------------------------------------------- BF16
+static uint16_t f32_to_bf16(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);  // quiet NaN
+  u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest, ties to even
+  return (uint16_t)(u >> 16);
+}
+static float bf16_to_f32(uint16_t h) {
+  const uint32_t u = (uint32_t)h << 16;
+  float x;
+  std::memcpy(&x, &u, 4);
+  return x;
+}
+
 struct Prepared {
   std::vector<float> lut;
   std::vector<uint8_t> u8;
@@ -609,6 +624,15 @@ float quantized_distance(const DgoIndex &I, const float *q, uint32_t id, const P
         return r > 0.0f ? r : 0.0f;
       }
     }
+  }
+  if (I.quant == DGO_Q_BF16) {  // the metric of the f32 query against the decoded row
+    scratch.resize(I.d);
+    for (uint32_t i = 0; i < I.d; ++i) {
+      uint16_t u;
+      std::memcpy(&u, code + 2 * i, 2);
+      scratch[i] = bf16_to_f32(u);
+    }
+    return metric_eval(I.metric, q, scratch.data(), I.d);
   }
   if (I.metric != DGO_L2SQ && I.metric != DGO_L2) {
     scratch.resize(I.d);
@@ -1003,6 +1027,10 @@ void dgo_f16_encode(const float *X, uint64_t n, uint32_t d, uint16_t *codes) {
   for (uint64_t i = 0; i < n * d; ++i) codes[i] = f32_to_f16(X[i]);
 }
 float dgo_f16_distance(const uint16_t *q, const uint16_t *c, uint32_t d) { return f16_dist(q, c, d); }
+void dgo_bf16_encode(const float *X, uint64_t n, uint32_t d, uint16_t *codes) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)(n * d); ++i) codes[i] = f32_to_bf16(X[i]);
+}
 uint8_t dgo_e4m3_encode(float x) { return e4m3_encode(x); }
 float dgo_e4m3_decode(uint8_t c) { return e4m3_decode(c); }
 void dgo_fp8_encode(const float *X, uint64_t n, uint32_t d, uint8_t *codes, float *scales) {

@@ -30,7 +30,7 @@ extern "C" {
 #endif
 
 enum { DGO_L2SQ = 0, DGO_L2 = 1, DGO_COSINE = 2, DGO_DOT = 3 };
-enum { DGO_Q_NONE = 0, DGO_Q_PQ = 1, DGO_Q_INT8 = 2, DGO_Q_RABITQ = 3, DGO_Q_F16 = 4, DGO_Q_FP8 = 5 };
+enum { DGO_Q_NONE = 0, DGO_Q_PQ = 1, DGO_Q_INT8 = 2, DGO_Q_RABITQ = 3, DGO_Q_F16 = 4, DGO_Q_FP8 = 5, DGO_Q_BF16 = 6 };
 enum {
   DGO_F_TRUE = 0, DGO_F_EQ = 1, DGO_F_IN = 2, DGO_F_LT = 3, DGO_F_GT = 4,
   DGO_F_RANGE = 5, DGO_F_AND = 6, DGO_F_OR = 7
@@ -132,6 +132,12 @@ void dgo_int8_encode(const float *X, uint64_t n, uint32_t d, float scale, float 
 float dgo_int8_distance(const uint8_t *q, const uint8_t *c, uint32_t d, float scale);
 void dgo_f16_encode(const float *X, uint64_t n, uint32_t d, uint16_t *codes);
 float dgo_f16_distance(const uint16_t *q, const uint16_t *c, uint32_t d);
+
+/* ---- BF16 rows (the product's BF16 traversal; no counterpart in the
+ *      reference): each f32 rounded to nearest even in BF16 (NaN stays NaN),
+ *      code_size = 2*d; the traversal evaluates the metric of the f32 query
+ *      against the decoded row, exactly as over the f32 rows ---- */
+void dgo_bf16_encode(const float *X, uint64_t n, uint32_t d, uint16_t *codes);
 
 /* ---- FP8 e4m3 with per-vector scales (the product's FP8 traversal; no
  *      counterpart in the reference): s = max|x| / 448, codes e4m3(x / s)

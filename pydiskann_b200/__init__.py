@@ -78,7 +78,8 @@ def medoid(vectors, metric: str = "l2", device: int = 0) -> int:
     """calculate_medoid (src/lib.rs:748-768) on the GPU."""
     X = _f32(vectors)
     out = C.c_uint32()
-    check(lib().dg_medoid(ptr(X), X.shape[0], X.shape[1], _metric(metric), device, C.byref(out)))
+    B = _lib.builder()
+    check(B.dg_medoid(ptr(X), X.shape[0], X.shape[1], _metric(metric), device, C.byref(out)), B)
     return out.value
 
 
@@ -92,8 +93,9 @@ def build_graph(vectors, max_degree=64, build_beam_width=128, alpha=1.2, metric=
     if medoid_id is None:
         medoid_id = medoid(X, metric, device)
     adj = np.empty((X.shape[0], max_degree), dtype=np.uint32)
-    check(lib().dg_build_vamana(ptr(X), X.shape[0], X.shape[1], m, max_degree, build_beam_width,
-                                float(alpha), seed, medoid_id, device, ptr(adj)))
+    B = _lib.builder()
+    check(B.dg_build_vamana(ptr(X), X.shape[0], X.shape[1], m, max_degree, build_beam_width,
+                            float(alpha), seed, medoid_id, device, ptr(adj)), B)
     return adj, medoid_id
 
 
@@ -105,8 +107,9 @@ def pq_train(vectors, num_subspaces=8, num_centroids=256, kmeans_iterations=20,
     if X.shape[0] == 0:
         raise RuntimeError("Index error: No vectors to train on")
     cb = np.empty((M, K, X.shape[1] // max(M, 1)), dtype=np.float32)
-    check(lib().dg_pq_train(ptr(X), X.shape[0], X.shape[1], M, K, kmeans_iterations,
-                            training_sample_size, seed, device, ptr(cb)))
+    B = _lib.builder()
+    check(B.dg_pq_train(ptr(X), X.shape[0], X.shape[1], M, K, kmeans_iterations,
+                        training_sample_size, seed, device, ptr(cb)), B)
     return cb
 
 
@@ -116,7 +119,8 @@ def pq_encode(vectors, codebooks, device=0) -> np.ndarray:
     cb = _f32(codebooks)
     M, K, _ = cb.shape
     codes = np.empty((X.shape[0], M), dtype=np.uint8)
-    check(lib().dg_pq_encode(ptr(X), X.shape[0], X.shape[1], M, K, ptr(cb), device, ptr(codes)))
+    B = _lib.builder()
+    check(B.dg_pq_encode(ptr(X), X.shape[0], X.shape[1], M, K, ptr(cb), device, ptr(codes)), B)
     return codes
 
 
@@ -126,7 +130,8 @@ def fp8_encode(vectors, device=0):
     n, d = X.shape
     codes = np.empty((n, d), dtype=np.uint8)
     scales = np.empty(n, dtype=np.float32)
-    check(lib().dg_fp8_encode(ptr(X), n, d, device, ptr(codes), ptr(scales)))
+    B = _lib.builder()
+    check(B.dg_fp8_encode(ptr(X), n, d, device, ptr(codes), ptr(scales)), B)
     return codes, scales
 
 
@@ -136,8 +141,9 @@ def exact_knn(vectors, queries, k=10, metric="l2", device=0):
     Q = _lib.query_rows(queries, X.shape[1])
     ids = np.empty((Q.shape[0], k), dtype=np.uint32)
     ds = np.empty((Q.shape[0], k), dtype=np.float32)
-    check(lib().dg_exact_knn(ptr(X), X.shape[0], X.shape[1], ptr(Q), Q.shape[0], k, _metric(metric),
-                             device, ptr(ids), ptr(ds)))
+    B = _lib.builder()
+    check(B.dg_exact_knn(ptr(X), X.shape[0], X.shape[1], ptr(Q), Q.shape[0], k, _metric(metric),
+                         device, ptr(ids), ptr(ds)), B)
     return ids, ds
 
 

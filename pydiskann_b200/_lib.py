@@ -132,7 +132,16 @@ def _signatures():
 
 EXPORTED = tuple(_signatures().keys())
 
+# The index-construction subset of the ABI, also linked on its own into
+# libdgbuild.so (medoid, Vamana build, PQ training and encodes, exact kNN):
+# a process that only prepares an index loads that library, not the search
+# library.
+BUILDER = ("dg_medoid", "dg_build_vamana", "dg_pq_train", "dg_pq_encode", "dg_fp8_encode", "dg_exact_knn",
+           "dg_last_error", "dg_version")
+BUILD_LIB_PATH = os.environ.get("DGANN_BUILD_LIBRARY", os.path.join(HERE, "libdgbuild.so"))
+
 _lib = None
+_builder = None
 
 
 def lib():
@@ -152,9 +161,29 @@ def lib():
     return _lib
 
 
-def check(status):
+def builder():
+    """Load libdgbuild.so (the index-construction library); raises when it has
+    not been built."""
+    global _builder
+    if _builder is None:
+        if not os.path.exists(BUILD_LIB_PATH):
+            raise ImportError(
+                f"libdgbuild.so not found at {BUILD_LIB_PATH}; build it with `python -m pydiskann_b200.build`"
+            )
+        L = C.CDLL(BUILD_LIB_PATH)
+        sig = _signatures()
+        for name in BUILDER:
+            f = getattr(L, name)
+            f.restype, f.argtypes = sig[name]
+        _builder = L
+    return _builder
+
+
+def check(status, library=None):
+    """Raise for a non-OK status with the error text of `library` (the
+    library that returned it; default libdgann)."""
     if status != DG_OK:
-        msg = lib().dg_last_error().decode(errors="replace")
+        msg = (library or lib()).dg_last_error().decode(errors="replace")
         if status == DG_EINVAL:
             raise ValueError(msg)
         raise DgError(status, msg)

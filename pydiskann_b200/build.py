@@ -4,7 +4,10 @@ Usage: python -m pydiskann_b200.build [--force] [-j N]
 
 Every translation unit under csrc/ is compiled by nvcc for sm_100a in
 parallel and linked into pydiskann_b200/libdgann.so, next to this file, so
-the library travels with the source tree.
+the library travels with the source tree.  The index-construction units
+(medoid, Vamana build, PQ training and encodes, exact kNN) are also linked on
+their own into libdgbuild.so, which a process that only prepares an index
+loads instead of the search library.
 """
 from __future__ import annotations
 
@@ -19,6 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdgann.so")
+BUILD_LIB = os.path.join(HERE, "libdgbuild.so")
+BUILD_UNITS = ("dg_errors", "dg_build", "dg_vamana")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -85,11 +90,15 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False, d
         jobs = jobs or min(len(todo), os.cpu_count() or 4)
         with cf.ThreadPoolExecutor(jobs) as ex:
             list(ex.map(compile_one, todo))
-    if force or todo or _stale(LIB_, objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB_] + objs + ["-lcudart"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+    links = [(LIB_, objs)]
+    if lib_path is None:
+        links.append((BUILD_LIB, [o for o in objs if os.path.basename(o)[:-2] in BUILD_UNITS]))
+    for target, parts in links:
+        if force or todo or _stale(target, parts):
+            cmd = [nvcc] + ARCH + ["-shared", "-o", target] + parts + ["-lcudart", "-Xlinker", "--no-undefined"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"link of {os.path.basename(target)} failed:\n{r.stderr[-4000:]}")
     return LIB_
 
 

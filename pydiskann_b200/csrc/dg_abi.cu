@@ -11,22 +11,6 @@
 
 namespace dg {
 
-static thread_local std::string g_err;
-
-void set_error(const std::string &msg) { g_err = msg; }
-DgStatus fail(DgStatus st, const std::string &msg) {
-  g_err = msg;
-  return st;
-}
-DgStatus cuda_fail(cudaError_t e, const char *what) {
-  g_err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
-  return e == cudaErrorMemoryAllocation ? DG_ENOMEM : DG_EDEVICE;
-}
-
-// Rows are padded to a multiple of 32 dimensions: every 16-byte chunk
-// geometry of the gather kernels then divides the row exactly.
-uint32_t dpad_of(uint32_t d) { return (d + 31u) & ~31u; }
-
 DgStatus dev_alloc(DgIndex *idx, void **p, size_t bytes) {
   if (idx->hbm_budget && idx->hbm_used + bytes > idx->hbm_budget)
     return fail(DG_ENOMEM, "index exceeds its HBM budget (" + std::to_string(idx->hbm_budget) + " bytes)");
@@ -61,18 +45,6 @@ DgStatus to_device(DgIndex *idx, void **dst, const void *src, size_t bytes) {
   return DG_OK;
 }
 
-DgStatus upload_rows_f32(const float *host, uint64_t n, uint32_t d, uint32_t dpad, float *dev,
-                         cudaStream_t st) {
-  if (d == dpad) {
-    DG_CUDA(cudaMemcpyAsync(dev, host, n * d * sizeof(float), cudaMemcpyHostToDevice, st));
-    return DG_OK;
-  }
-  DG_CUDA(cudaMemsetAsync(dev, 0, n * dpad * sizeof(float), st));
-  DG_CUDA(cudaMemcpy2DAsync(dev, dpad * sizeof(float), host, d * sizeof(float), d * sizeof(float), n,
-                            cudaMemcpyHostToDevice, st));
-  return DG_OK;
-}
-
 static int met_kind(int32_t metric) {
   return metric == DG_DOT ? MET_DOT : metric == DG_COSINE ? MET_COS : MET_L2;
 }
@@ -89,9 +61,6 @@ static int lanes_per_row(uint32_t chunks) {
 using namespace dg;
 
 extern "C" {
-
-const char *dg_last_error(void) { return g_err.c_str(); }
-int32_t dg_version(void) { return DGANN_VERSION; }
 
 DgStatus dg_index_create(const DgIndexDesc *desc, DgIndex **out) {
   if (!desc || !out) return fail(DG_EINVAL, "null argument");
@@ -1089,12 +1058,21 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
                                     (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2);
   LaunchInfo info;
   switch (trav) {
-    case TRAV_F32: return launch_search_f32(a, Ly, met, lpr, lcap, filt, st, &info);
-    case TRAV_BF16: return launch_search_bf16(a, Ly, met, lpr, lcap, filt, st, &info);
-    case TRAV_F16: return launch_search_f16(a, Ly, met, lpr, lcap, filt, st, &info);
-    case TRAV_INT8: return launch_search_int8(a, Ly, met, lpr, lcap, filt, st, &info);
-    case TRAV_PQ: return launch_search_pq(a, Ly, met, lpr, lcap, filt, st, &info);
-    case TRAV_FP8: return launch_search_fp8(a, Ly, met, lpr, lcap, filt, st, &info);
-    default: return launch_search_rabitq(a, Ly, met, lpr, lcap, filt, st, &info);
+    case TRAV_F32: s = launch_search_f32(a, Ly, met, lpr, lcap, filt, st, &info); break;
+    case TRAV_BF16: s = launch_search_bf16(a, Ly, met, lpr, lcap, filt, st, &info); break;
+    case TRAV_F16: s = launch_search_f16(a, Ly, met, lpr, lcap, filt, st, &info); break;
+    case TRAV_INT8: s = launch_search_int8(a, Ly, met, lpr, lcap, filt, st, &info); break;
+    case TRAV_PQ: s = launch_search_pq(a, Ly, met, lpr, lcap, filt, st, &info); break;
+    case TRAV_FP8: s = launch_search_fp8(a, Ly, met, lpr, lcap, filt, st, &info); break;
+    default: s = launch_search_rabitq(a, Ly, met, lpr, lcap, filt, st, &info); break;
   }
+  if (s != DG_OK) return s;
+  // Record the search's completion on a slot event (created with the index,
+  // so nothing is allocated here): updates of rows, adjacency, labels or
+  // tombstones and dg_index_destroy wait for it, as they do for dg_search_batch.
+  DgIndex::Slot *slp = nullptr;
+  DG_CUDA(take_slot(idx, &slp));
+  DG_CUDA(cudaEventRecord(slp->done, st));
+  slp->pending = true;
+  return DG_OK;
 }

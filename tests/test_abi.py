@@ -32,6 +32,18 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_builder_library_exports_the_construction_subset():
+    """libdgbuild.so (index construction only) exports the construction entry
+    points and the error text, and none of the search or index calls."""
+    from pydiskann_b200 import _lib
+
+    lib = ctypes.CDLL(_lib.BUILD_LIB_PATH)
+    assert all(hasattr(lib, n) for n in _lib.BUILDER)
+    assert set(_lib.BUILDER) <= _declared()
+    for n in ("dg_index_create", "dg_search_batch", "dg_server_create", "dg_spfresh_search_batch"):
+        assert not hasattr(lib, n), n
+
+
 def test_binding_covers_header():
     from pydiskann_b200 import _lib
 
