@@ -574,8 +574,8 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
   if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
   if (reranked && !filt && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
-  // visited table: 2^hbits words of two 16-bit tags (about 3 tags per
-  // visited node at these beams), or the size dg_index_autotune measured
+  // visited table: 2^hbits words as buckets of eight 16-bit tags (about 3
+  // tags per visited node at these beams), or the size dg_index_autotune measured
   // fastest for this kind of search; DG_HBITS overrides both
   const uint32_t hbits = visited_bits(idx, trav, lcap, filt, maxL);
   uint32_t hB = 1;

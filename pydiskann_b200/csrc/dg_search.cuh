@@ -121,18 +121,24 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
 __device__ __forceinline__ uint32_t lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
 // ------------------------------------------------------------ visited set
-// A per-query table of 2^bbits 32-bit words in shared memory.  Ids are mixed
-// by a multiply with an odd constant modulo 2^B (a bijection on the B-bit ids,
-// n <= 2^B); the top bbits bits of the mix pick a word, the remaining B-bbits
-// bits (+1, 0 = empty) form a 16-bit tag, and each word holds the two most
-// recent tags of its bucket.  (word, tag) identifies an id uniquely, so the
-// table never reports an unvisited id as visited; it may forget an id when a
-// bucket overflows, which only costs a recomputed distance.  When B-bbits
-// exceeds 15 bits the words hold whole ids instead (direct mapped).
+// A per-query table of 2^bbits 32-bit words in shared memory, used as
+// 2^(bbits-2) buckets of eight 16-bit tags (16 bytes each).  Ids are mixed by a
+// multiply with an odd constant modulo 2^B (a bijection on the B-bit ids,
+// n <= 2^B); the top bits of the mix pick a bucket and the remaining bits (+1,
+// 0 = empty) form the tag.  A bucket keeps its eight most recent tags (a new
+// tag shifts the oldest out).  (bucket, tag) identifies an id uniquely, so
+// the table never reports an unvisited id as visited; it may forget an id
+// when a bucket overflows, which only costs a recomputed distance.  Eight
+// ways per bucket forget far fewer ids than two ways in the same bytes.  When
+// the tag would need more than 15 bits the words hold whole ids instead
+// (direct mapped).  Two lanes inserting into one bucket in the same
+// instruction may lose one insertion (a forgotten id), never invent a tag:
+// both stores carry the same shifted words and differ only in the new tag.
 struct Visited {
   uint32_t *w;
   uint32_t bbits, B;
-  __device__ __forceinline__ bool tagged() const { return B - bbits <= 15; }
+  __device__ __forceinline__ uint32_t tag_bits() const { return B - (bbits - 2); }
+  __device__ __forceinline__ bool tagged() const { return tag_bits() <= 15; }
   __device__ __forceinline__ uint32_t mix(uint32_t id) const {
     const uint32_t h = id * 0x9E3779B1u;
     return B >= 32 ? h : (h & ((1u << B) - 1u));
@@ -144,12 +150,15 @@ struct Visited {
   // True when `id` is recorded; otherwise records it.
   __device__ __forceinline__ bool test_and_set(uint32_t id) const {
     if (tagged()) {
+      const uint32_t tb = tag_bits();
       const uint32_t h = mix(id);
-      const uint32_t slot = h >> (B - bbits);
-      const uint32_t tag = (h & ((1u << (B - bbits)) - 1u)) + 1u;
-      const uint32_t v = w[slot];
-      if ((v & 0xffffu) == tag || (v >> 16) == tag) return true;
-      w[slot] = (v << 16) | tag;
+      const uint32_t tag = (h & ((1u << tb) - 1u)) + 1u;
+      uint4 *bucket = reinterpret_cast<uint4 *>(w) + (h >> tb);
+      const uint4 v = *bucket;
+      const uint32_t t2 = tag * 0x10001u;
+      if (__vcmpeq2(v.x, t2) | __vcmpeq2(v.y, t2) | __vcmpeq2(v.z, t2) | __vcmpeq2(v.w, t2)) return true;
+      *bucket = make_uint4((v.x << 16) | tag, __funnelshift_l(v.x, v.y, 16), __funnelshift_l(v.y, v.z, 16),
+                           __funnelshift_l(v.z, v.w, 16));
       return false;
     }
     const uint32_t slot = (id * 0x9E3779B1u) >> (32 - bbits);

@@ -803,9 +803,50 @@ __global__ void k_pm_items(const uint32_t *pcount, const uint32_t *pstart, const
   }
 }
 
+// Tensor-core form of the tile's dot products.  Every value of an
+// integer-valued row with |x| < 2^16 splits exactly into two BF16 parts, hi =
+// bf16(x) and lo = x - hi, so q.x = qh.xh + qh.xl + ql.xh + ql.xl with every
+// product exact; when every partial sum stays below 2^24 (d * max|q| * max|x|
+// < 2^24) the FP32 accumulation is exact too, and the tensor cores return the
+// dot products the FMA chain below returns, bit for bit.  A tile or a query
+// set outside those bounds takes the FMA chain.
+constexpr float kPmExactSum = 16777216.0f;  // 2^24
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], uint32_t addr) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(addr));
+}
+
+__device__ __forceinline__ void mma_bf16_16x8x16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};"
+               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Writes the exact BF16 split (hi, lo) of x and returns whether x is an
+// integer of magnitude below 2^15 (so that the split is exact).
+__device__ __forceinline__ bool bf16_split(float x, uint16_t &hi, uint16_t &lo) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  const __nv_bfloat16 l = __float2bfloat16_rn(__fsub_rn(x, __bfloat162float(h)));
+  hi = __bfloat16_as_ushort(h);
+  lo = __bfloat16_as_ushort(l);
+  return x == rintf(x) && fabsf(x) < 32768.0f;
+}
+
+// Shared-memory row stride (in BF16 elements) of the split copies: dk + 8, so
+// that the eight 16-byte rows one ldmatrix reads fall in distinct banks.
+__host__ __device__ inline uint32_t pm_ks(uint32_t d) { return ((d + 15u) & ~15u) + 8u; }
+// Capacity of a pair's k-best list: k rounded up to 32 (at most kPmK).
+__host__ __device__ inline uint32_t pm_kcap(uint32_t k) { return (k + 31u) & ~31u; }
+
 // One CTA (8 warps) per work item at a time: the item's queries and a tile of
 // the posting's entries in shared memory; warp w scores queries w, w+8, ...
-// against two entries per lane and keeps each query's k best.
+// against two entries per lane and keeps each query's k best.  The dot
+// products of a tile come from the tensor cores (the warps split the 64 x 32
+// tile into 16 x 16 blocks) when the tile and the queries meet the exactness
+// bounds above, else from an FMA chain per pair.
 __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4 *items, const uint32_t *n_items,
                                                           uint32_t *item_counter, const uint32_t *pair_q,
                                                           uint64_t *pair_keys, uint32_t *pair_cnt, uint32_t k) {
@@ -814,18 +855,28 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
   // query rows dpad floats; tile rows d + 4 floats: 16-byte rows whose float4
   // columns fall in distinct banks within each quarter warp
   const uint32_t dq = a.dpad, dt = a.d + 4, d4 = a.d / 4;
+  const uint32_t ks = pm_ks(a.d), dk = ks - 8, kc = pm_kcap(k);
   float *qsm = reinterpret_cast<float *>(smem);                              // [kPmQ][dpad]
   float *tile = qsm + kPmQ * dq;                                             // [kPmT][d + 4]
   uint32_t *tid = reinterpret_cast<uint32_t *>(tile + kPmT * dt);            // [kPmT] ids
   float *xn = reinterpret_cast<float *>(tid + kPmT);                         // [kPmT] |x|^2
   float *qn = xn + kPmT;                                                     // [kPmQ] |q|^2
-  uint64_t *lists = reinterpret_cast<uint64_t *>(qn + kPmQ);                 // [kPmQ][2][kPmK]
-  uint64_t *cst = lists + (size_t)kPmQ * 2 * kPmK;                           // [8][32]
-  __shared__ uint32_t s_item;
+  uint64_t *lists = reinterpret_cast<uint64_t *>(qn + kPmQ);                 // [kPmQ][2][kc]
+  uint64_t *cst = lists + (size_t)kPmQ * 2 * kc;                             // [8][32]
+  uint16_t *qhl = reinterpret_cast<uint16_t *>(cst + 8 * 32);                // [2][kPmQ][ks] BF16 hi, lo
+  uint16_t *thl = qhl + 2 * kPmQ * ks;                                       // [2][kPmT][ks]
+  // [kPmQ][kPmT] tensor-core dot products, over the f32 tile once it is split
+  float *dm = tile;
+  __shared__ uint32_t s_item, s_qbad, s_tbad, s_qmax, s_tmax;
   const uint32_t total = *n_items;
   const bool sq = a.metric == DG_L2;
+  const uint32_t qhl_s = (uint32_t)__cvta_generic_to_shared(qhl), thl_s = (uint32_t)__cvta_generic_to_shared(thl);
   while (true) {
-    if (threadIdx.x == 0) s_item = atomicAdd(item_counter, 1u);
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(item_counter, 1u);
+      s_qbad = 0u;
+      s_qmax = 0u;
+    }
     __syncthreads();
     const uint32_t it = s_item;
     __syncthreads();
@@ -835,6 +886,21 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
     for (uint32_t t = threadIdx.x; t < m * dq; t += blockDim.x) {
       const uint32_t j = t / dq, i = t % dq;
       qsm[t] = i < a.d ? __ldg(a.Q + (size_t)pair_q[p0 + j] * a.d + i) : 0.0f;
+    }
+    {  // BF16 split of the queries (rows past m and columns past d are zero)
+      bool bad = false;
+      float mx = 0.0f;
+      for (uint32_t t = threadIdx.x; t < kPmQ * dk; t += blockDim.x) {
+        const uint32_t j = t / dk, i = t % dk;
+        const float x = (j < m && i < a.d) ? __ldg(a.Q + (size_t)pair_q[p0 + j] * a.d + i) : 0.0f;
+        uint16_t h, l;
+        bad |= !bf16_split(x, h, l);
+        mx = fmaxf(mx, fabsf(x));
+        qhl[j * ks + i] = h;
+        qhl[(kPmQ + j) * ks + i] = l;
+      }
+      if (__syncthreads_or(bad) && threadIdx.x == 0) s_qbad = 1u;
+      if (mx > 0.0f) atomicMax(&s_qmax, __float_as_uint(mx));
     }
     __syncthreads();
     if (threadIdx.x < m) {
@@ -861,6 +927,10 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         }
         tid[r] = id;
       }
+      if (threadIdx.x == 0) {
+        s_tbad = 0u;
+        s_tmax = 0u;
+      }
       __syncthreads();
       if (threadIdx.x < ne) {
         const float *row = tile + threadIdx.x * dt;
@@ -868,22 +938,79 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         for (uint32_t i = 0; i < a.d; ++i) s2 = fmaf(row[i], row[i], s2);
         xn[threadIdx.x] = s2;
       }
+      {  // BF16 split of the tile (rows past ne and columns past d are zero)
+        bool bad = false;
+        float mx = 0.0f;
+        for (uint32_t t = threadIdx.x; t < kPmT * dk; t += blockDim.x) {
+          const uint32_t r = t / dk, i = t % dk;
+          const float x = (r < ne && i < a.d) ? tile[r * dt + i] : 0.0f;
+          uint16_t h, l;
+          bad |= !bf16_split(x, h, l);
+          mx = fmaxf(mx, fabsf(x));
+          thl[r * ks + i] = h;
+          thl[(kPmT + r) * ks + i] = l;
+        }
+        if (__syncthreads_or(bad) && threadIdx.x == 0) s_tbad = 1u;
+        if (mx > 0.0f) atomicMax(&s_tmax, __float_as_uint(mx));
+      }
       __syncthreads();
+      // (the dot products overwrite the f32 tile, which must hold kPmQ x kPmT floats)
+      const bool tc = !s_qbad && !s_tbad && dt >= (uint32_t)kPmQ &&
+                      (float)a.d * __uint_as_float(s_qmax) * __uint_as_float(s_tmax) < kPmExactSum;
       float acc[4][2];
 #pragma unroll
       for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = 0.0f;
-      const float4 *e0p = reinterpret_cast<const float4 *>(tile + (size_t)lane * dt);
-      const float4 *e1p = reinterpret_cast<const float4 *>(tile + (size_t)(lane + 32) * dt);
-#pragma unroll 2
-      for (uint32_t c = 0; c < d4; ++c) {
-        const float4 x0 = e0p[c], x1 = e1p[c];
+      if (tc) {
+        // warp w: entries 16 (w % 4) .. +15 against queries 16 (w / 4) .. +15
+        const uint32_t e16 = 16u * (warp & 3), q16 = 16u * (warp >> 2);
+        float c[2][4] = {{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
+        const uint32_t arow = e16 + (lane & 15), acol = (lane >> 4) * 8;
+        const uint32_t brow = q16 + (lane >> 4) * 8 + (lane & 7), bcol = ((lane >> 3) & 1) * 8;
+        for (uint32_t k0 = 0; k0 < dk; k0 += 16) {
+          uint32_t ah[4], al[4], bh[4], bl[4];
+          ldsm_x4(ah, thl_s + 2u * (arow * ks + k0 + acol));
+          ldsm_x4(al, thl_s + 2u * ((kPmT + arow) * ks + k0 + acol));
+          ldsm_x4(bh, qhl_s + 2u * (brow * ks + k0 + bcol));
+          ldsm_x4(bl, qhl_s + 2u * ((kPmQ + brow) * ks + k0 + bcol));
+#pragma unroll
+          for (int nt = 0; nt < 2; ++nt) {
+            mma_bf16_16x8x16(c[nt], ah, bh[2 * nt], bh[2 * nt + 1]);
+            mma_bf16_16x8x16(c[nt], ah, bl[2 * nt], bl[2 * nt + 1]);
+            mma_bf16_16x8x16(c[nt], al, bh[2 * nt], bh[2 * nt + 1]);
+            mma_bf16_16x8x16(c[nt], al, bl[2 * nt], bl[2 * nt + 1]);
+          }
+        }
+        // lane (g, t) holds entries g, g + 8 x queries 2t, 2t + 1 of each 8-query tile
+        const uint32_t g = lane >> 2, t2 = 2 * (lane & 3);
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+          const uint32_t qc = q16 + 8 * nt + t2;
+          dm[qc * kPmT + e16 + g] = c[nt][0];
+          dm[(qc + 1) * kPmT + e16 + g] = c[nt][1];
+          dm[qc * kPmT + e16 + g + 8] = c[nt][2];
+          dm[(qc + 1) * kPmT + e16 + g + 8] = c[nt][3];
+        }
+        __syncthreads();
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const uint32_t j = warp + 8 * u;
-          if (j < m) {
-            const float4 qv = reinterpret_cast<const float4 *>(qsm + j * dq)[c];
-            acc[u][0] = fmaf(qv.w, x0.w, fmaf(qv.z, x0.z, fmaf(qv.y, x0.y, fmaf(qv.x, x0.x, acc[u][0]))));
-            acc[u][1] = fmaf(qv.w, x1.w, fmaf(qv.z, x1.z, fmaf(qv.y, x1.y, fmaf(qv.x, x1.x, acc[u][1]))));
+          acc[u][0] = dm[j * kPmT + lane];
+          acc[u][1] = dm[j * kPmT + lane + 32];
+        }
+      } else {
+        const float4 *e0p = reinterpret_cast<const float4 *>(tile + (size_t)lane * dt);
+        const float4 *e1p = reinterpret_cast<const float4 *>(tile + (size_t)(lane + 32) * dt);
+#pragma unroll 2
+        for (uint32_t c = 0; c < d4; ++c) {
+          const float4 x0 = e0p[c], x1 = e1p[c];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t j = warp + 8 * u;
+            if (j < m) {
+              const float4 qv = reinterpret_cast<const float4 *>(qsm + j * dq)[c];
+              acc[u][0] = fmaf(qv.w, x0.w, fmaf(qv.z, x0.z, fmaf(qv.y, x0.y, fmaf(qv.x, x0.x, acc[u][0]))));
+              acc[u][1] = fmaf(qv.w, x1.w, fmaf(qv.z, x1.z, fmaf(qv.y, x1.y, fmaf(qv.x, x1.x, acc[u][1]))));
+            }
           }
         }
       }
@@ -892,7 +1019,7 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
       for (int u = 0; u < 4; ++u) {
         const uint32_t j = warp + 8 * u;
         if (j >= m) continue;  // warp-uniform
-        uint64_t *const bufs[2] = {lists + (size_t)j * 2 * kPmK, lists + (size_t)j * 2 * kPmK + kPmK};
+        uint64_t *const bufs[2] = {lists + (size_t)j * 2 * kc, lists + (size_t)j * 2 * kc + kc};
         // |q - x|^2 = |q|^2 + |x|^2 - 2 q.x (exact on integer-valued data)
         const float qq = qn[j];
         const float s0 = fmaxf(__fsub_rn(__fadd_rn(qq, xn[lane]), __fmul_rn(2.0f, acc[u][0])), 0.0f);
@@ -908,7 +1035,7 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
     for (int u = 0; u < 4; ++u) {
       const uint32_t j = warp + 8 * u;
       if (j >= m) continue;
-      const uint64_t *lst = lists + (size_t)j * 2 * kPmK + (size_t)cur[u] * kPmK;
+      const uint64_t *lst = lists + (size_t)j * 2 * kc + (size_t)cur[u] * kc;
       for (int i = lane; i < size[u]; i += 32) pair_keys[(size_t)(p0 + j) * k + i] = lst[i];
       if (lane == 0) pair_cnt[p0 + j] = (uint32_t)size[u];
     }
@@ -945,9 +1072,9 @@ __global__ void __launch_bounds__(128) k_pm_merge(const uint32_t *probe_cnt, con
   }
 }
 
-static size_t pm_smem(uint32_t d, uint32_t dpad) {
-  return ((size_t)kPmQ * dpad + (size_t)kPmT * (d + 4)) * 4 + (2 * kPmT + kPmQ) * 4 + (size_t)kPmQ * 2 * kPmK * 8 +
-         8 * 32 * 8;
+static size_t pm_smem(uint32_t d, uint32_t dpad, uint32_t k) {
+  return ((size_t)kPmQ * dpad + (size_t)kPmT * (d + 4)) * 4 + (2 * kPmT + kPmQ) * 4 +
+         (size_t)kPmQ * 2 * pm_kcap(k) * 8 + 8 * 32 * 8 + (size_t)2 * (kPmQ + kPmT) * pm_ks(d) * 2;
 }
 
 // Posting-major scan of one chunk whose routing matrix is in ac.route: probes
@@ -997,7 +1124,7 @@ static DgStatus pm_scan_chunk(DgSpfresh *s, const SpfArgs &ac, uint32_t nprobe, 
                                    (uint32_t *)s->pos_of.p);
   k_pm_items<<<(nb + 255) / 256, 256, 0, st>>>(pcount, pstart, istart, nb, (uint4 *)s->items.p);
   DG_CUDA(cudaGetLastError());
-  const size_t smem = pm_smem(s->d, s->dpad);
+  const size_t smem = pm_smem(s->d, s->dpad, k);
   DG_CUDA(cudaFuncSetAttribute(k_pm_scan_postings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0, sms = 0;
   DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pm_scan_postings, 256, smem));
@@ -1315,7 +1442,7 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
   const bool posting_major = s->nblocks >= 512 && s->quant == DG_Q_NONE &&
                              (s->metric == DG_L2 || s->metric == DG_L2SQ) && p->k <= (uint32_t)kPmK && nq >= 256 &&
                              (uint64_t)nq * nprobe >= 16ull * s->nblocks && s->nblocks < (1u << 22) && s->d % 4 == 0 &&
-                             pm_smem(s->d, s->dpad) <= 200 * 1024;
+                             pm_smem(s->d, s->dpad, p->k) <= 200 * 1024;
   if (s->nblocks >= 512) {
     // many postings: route all queries of a chunk in one tiled kernel (the
     // matrix of a chunk stays below 1 GiB), then scan the chunk

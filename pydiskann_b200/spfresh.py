@@ -187,7 +187,10 @@ class SPFresh:
         self.live_b = np.zeros(0, dtype=bool)
         self.ids = []      # per slot: np.uint64 array of entry ids
         self.codes = []    # per slot: u8 [len, code_size]
+        # freed slots with the epoch that freed them; a slot is reused only in
+        # a later epoch (an insert chunk or a gc), src/spfresh.rs:380-415
         self.free = []
+        self.epoch = 1
         self.raw = np.zeros((0, dim), dtype=np.float32)
         self.next_id = 0
         self.deleted = set()
@@ -303,9 +306,19 @@ class SPFresh:
         keep = np.array([int(i) not in self.deleted for i in ids], dtype=bool) if len(ids) else np.zeros(0, bool)
         return ids[keep], codes[keep]
 
+    def _alloc_free(self):
+        """Inner::alloc (src/spfresh.rs:380-393): the first freed slot of an
+        earlier epoch, taken out by swap-remove; None when there is none."""
+        for i, (b, e) in enumerate(self.free):
+            if e < self.epoch:
+                self.free[i] = self.free[-1]
+                self.free.pop()
+                return b
+        return None
+
     def _new_posting(self, centroid):
-        if self.free:
-            b = self.free.pop()
+        b = self._alloc_free()
+        if b is not None:
             self.cent[b] = centroid
         else:
             b = len(self.live_b)
@@ -324,7 +337,7 @@ class SPFresh:
         self.live_b[b] = False
         self.ids[b] = np.zeros(0, dtype=np.uint64)
         self.codes[b] = np.zeros((0, self.codec.size), dtype=np.uint8)
-        self.free.append(b)
+        self.free.append((b, self.epoch))
         self._dirty.add(b)
 
     def _rewrite(self, b, ids, codes):
@@ -371,6 +384,7 @@ class SPFresh:
         self.live += len(X)
         for c0 in range(0, len(X), CHUNK):
             chunk = X[c0:c0 + CHUNK]
+            self.epoch += 1
             self.created = []
             live = np.nonzero(self.live_b)[0]
             if len(live):
@@ -499,6 +513,7 @@ class SPFresh:
     @locked
     def gc(self):
         """Inner::gc (src/spfresh.rs:613-643): purge tombstones, merge small postings."""
+        self.epoch += 1
         queue = []
         for b in range(len(self.live_b)):
             if not self._is_live(b):
@@ -564,7 +579,7 @@ class SPFresh:
         s.live_b = live
         s.ids = [ids if live[b] else ids[:0] for b, (ids, _) in enumerate(posts)]
         s.codes = [codes if live[b] else codes[:0] for b, (_, codes) in enumerate(posts)]
-        s.free = [int(b) for b in np.nonzero(~live)[0]]
+        s.free = [(int(b), 0) for b in np.nonzero(~live)[0]]  # src/spfresh.rs:834-840
         n = meta.next_id
         for b, ids in enumerate(s.ids):
             if len(ids) and int(ids.max()) >= n:
