@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--no-filtered", action="store_true")
     ap.add_argument("--no-spfresh", action="store_true")
     ap.add_argument("--spfresh-n", type=int, default=2_000_000)
+    ap.add_argument("--spfresh-batches", type=int, default=3,
+                    help="update batches (1%% inserts, 0.5%% deletes, then searches at n_probe 64) after the load")
     ap.add_argument("--filtered-queries", type=int, default=5000)
     ap.add_argument("--cosine", action="store_true",
                     help="also run the quantized cosine workload (1M x 768, 20k queries, uneven beams)")
@@ -976,9 +978,62 @@ def spfresh_scan(args, dev, dist):
         if rec >= args.target_recall:
             break
     out["curve"] = curve
+    out["stream"] = spfresh_stream(args, s, Xs, Qs, Qd, dev)
     log(f"[spfresh] {json.dumps(out)}")
     s.close()
     return out
+
+
+def spfresh_stream(args, s, Xs, Qs, Qd, dev, nprobe=64):
+    """The update stream of the SPFresh workload: each batch inserts 1 % fresh
+    vectors of the same mixture and deletes 0.5 % of the live ids (uniformly),
+    then searches the query batch at n_probe 64 (device-timed); recall@10 is
+    against exact kNN over the live vectors after the batch."""
+    import torch
+
+    import pydiskann_b200 as dg
+    from pydiskann_b200 import synth
+
+    stream = torch.cuda.current_stream(dev)
+    n0 = len(Xs)
+    rng = np.random.default_rng([args.seed, 0x5F])
+    allX = [Xs]
+    rows = []
+    for b in range(args.spfresh_batches):
+        new = synth.mixture(n0 // 100, Xs.shape[1], 1024, args.seed, stream=synth.STREAM_MISC + 100 + b, clip=False,
+                            zipf=1.1)
+        t0 = time.time()
+        s.insert(new)
+        t_ins = time.time() - t0
+        allX.append(new)
+        live = np.setdiff1d(np.arange(s.next_id, dtype=np.int64), np.fromiter(s.deleted, dtype=np.int64))
+        gone = rng.choice(live, size=n0 // 200, replace=False)
+        t0 = time.time()
+        s.delete(gone.tolist())
+        t_del = time.time() - t0
+        live = np.setdiff1d(live, gone)
+        X = np.concatenate(allX)
+        gt, _ = dg.exact_knn(X[live], Qs, K, device=dev.index)
+        gt = live[gt.astype(np.int64)]
+        ids, _, _ = s.search_arrays(Qd, K, nprobe)
+        for _ in range(args.warmup):
+            s.search_arrays(Qd, K, nprobe)
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            s.search_arrays(Qd, K, nprobe)
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(e) / args.steps
+        st = s.stats()
+        row = {"batch": b, "inserted": len(new), "deleted": len(gone), "insert_s": round(t_ins, 2),
+               "delete_s": round(t_del, 3), "live": st["live"], "postings": st["postings"], "nprobe": nprobe,
+               "qps": len(Qs) / (ms / 1e3), "ms_per_step": ms,
+               "recall_at_10": round(recall(ids.cpu().numpy().astype(np.int64), gt), 4)}
+        rows.append(row)
+        log(f"[spfresh stream] {json.dumps(row)}")
+    return rows
 
 
 def serving(args, idx, qidx, name, L, Q, gt):

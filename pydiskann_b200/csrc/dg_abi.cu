@@ -140,7 +140,9 @@ DgStatus dg_index_enable_bf16(DgIndex *idx) {
   if (idx->bf16) return DG_OK;
   DgStatus s = dev_alloc(idx, (void **)&idx->bf16, idx->n * idx->dpad * 2);
   if (s != DG_OK) return s;
-  if ((s = encode_bf16_device(idx->vec, idx->n, idx->dpad, idx->bf16, idx->stream)) != DG_OK) return s;
+  if ((s = dev_alloc(idx, (void **)&idx->bf16_n2, idx->n * 4)) != DG_OK) return s;
+  if ((s = encode_bf16_device(idx->vec, idx->n, idx->dpad, idx->bf16, idx->stream, idx->bf16_n2)) != DG_OK)
+    return s;
   DG_CUDA(cudaStreamSynchronize(idx->stream));
   return DG_OK;
 }
@@ -366,7 +368,8 @@ DgStatus dg_index_update_rows(DgIndex *idx, uint64_t first, uint64_t count, cons
   if (vectors) {
     float *rows = idx->vec + first * idx->dpad;
     if ((s = upload_rows_f32(vectors, count, idx->d, idx->dpad, rows, idx->stream)) != DG_OK) return s;
-    if (idx->bf16 && (s = encode_bf16_device(rows, count, idx->dpad, idx->bf16 + first * idx->dpad, idx->stream)) != DG_OK)
+    if (idx->bf16 && (s = encode_bf16_device(rows, count, idx->dpad, idx->bf16 + first * idx->dpad, idx->stream,
+                                             idx->bf16_n2 + first)) != DG_OK)
       return s;
     if (idx->fp8 && (s = encode_fp8_device(rows, count, idx->d, idx->dpad, idx->fp8 + first * idx->dpad,
                                            idx->fp8_sn + first, idx->stream)) != DG_OK)
@@ -599,6 +602,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   a.metric = idx->metric;
   a.vec_f32 = idx->vec;
   a.vec_bf16 = idx->bf16;
+  a.bf16_n2 = idx->bf16_n2;
   a.adj = idx->adj;
   a.codes = idx->codes;
   a.code_stride = idx->code_stride;
@@ -996,6 +1000,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   a.metric = idx->metric;
   a.vec_f32 = idx->vec;
   a.vec_bf16 = idx->bf16;
+  a.bf16_n2 = idx->bf16_n2;
   a.adj = idx->adj;
   a.codes = idx->codes;
   a.code_stride = idx->code_stride;

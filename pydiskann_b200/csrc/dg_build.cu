@@ -226,9 +226,27 @@ static int grid_for(uint64_t work, int threads) {
   return (int)std::min<uint64_t>(std::max<uint64_t>(g, 1), 148ull * 64);
 }
 
-DgStatus encode_bf16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_t *out, cudaStream_t st) {
+// Squared norm of every BF16 row, summed in coordinate order in FP32.
+__global__ void k_bf16_norms(const uint16_t *rows, uint64_t n, uint32_t dpad, float *out) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint16_t *x = rows + r * dpad;
+    float s2 = 0.0f;
+    for (uint32_t i = 0; i < dpad; ++i) {
+      const float v = __uint_as_float((uint32_t)x[i] << 16);
+      s2 = __fadd_rn(s2, __fmul_rn(v, v));
+    }
+    out[r] = s2;
+  }
+}
+
+DgStatus encode_bf16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_t *out, cudaStream_t st,
+                            float *norms) {
   k_bf16<<<grid_for(n * dpad, 256), 256, 0, st>>>(vec, n * dpad, out);
   DG_CUDA(cudaGetLastError());
+  if (norms) {
+    k_bf16_norms<<<grid_for(n, 128), 128, 0, st>>>(out, n, dpad, norms);
+    DG_CUDA(cudaGetLastError());
+  }
   return DG_OK;
 }
 DgStatus encode_f16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_t *out, cudaStream_t st) {

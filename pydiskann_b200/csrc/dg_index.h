@@ -16,6 +16,7 @@ struct DgIndex {
   // HBM layout: every row starts on a 128-byte boundary when dpad*4 >= 128.
   float *vec = nullptr;       // [n][dpad] f32, zero padded
   uint16_t *bf16 = nullptr;   // [n][dpad] bf16 copy (optional)
+  float *bf16_n2 = nullptr;   // [n] squared norms of the bf16 rows
   uint8_t *fp8 = nullptr;     // [n][dpad] e4m3 copy (optional)
   float2 *fp8_sn = nullptr;   // [n] (scale, |decoded|^2) of the e4m3 rows
   uint32_t *adj = nullptr;    // [n][R]
@@ -88,8 +89,10 @@ DgStatus encode_int8_device(const float *vec, uint64_t n, uint32_t d, uint32_t d
                             float offset, uint8_t *codes, uint32_t stride, cudaStream_t st);
 DgStatus encode_f16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_t *codes,
                            cudaStream_t st);
+// BF16 rows (round to nearest even) and, when norms is not null, the squared
+// norm of each BF16 row.
 DgStatus encode_bf16_device(const float *vec, uint64_t n, uint32_t dpad, uint16_t *out,
-                            cudaStream_t st);
+                            cudaStream_t st, float *norms = nullptr);
 DgStatus encode_rabitq_device(const float *vec, uint64_t n, uint32_t d, uint32_t dpad, uint32_t P,
                               const float *centroid, const float *signs, uint8_t *codes,
                               uint32_t stride, cudaStream_t st);

@@ -36,6 +36,7 @@ struct SearchArgs {
   int32_t metric;
   const float *vec_f32;   // [n][dpad] exact rows (rerank and FP32 traversal)
   const uint16_t *vec_bf16;  // [n][dpad] BF16 traversal rows (may be null)
+  const float *bf16_n2;      // [n] squared norms of the BF16 rows
   const uint32_t *adj;    // [n][R]
   // quantized codes
   const uint8_t *codes;
@@ -110,6 +111,7 @@ __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool 
   else if (trav == TRAV_RABITQ) p = 4 * (rq_padded / 64) * 8 + 32 + align16(rq_padded * 4);
   else if (trav == TRAV_F16) p = align16(dpad * 4);
   else if (trav == TRAV_FP8) p = 2 * dpad + 16;  // query hi / lo e4m3 codes, then (scale, |q|^2)
+  else if (trav == TRAV_BF16) p = 4 * dpad + 16;  // query hi / lo BF16 values, then |q|^2
   o += align16(p);
   L.aux = o;  // 64-key copy of the register-resident working list (beams <= 64)
   o += lcap == 64 && !filt ? 64 * 8 : 0;
@@ -581,6 +583,74 @@ __device__ __forceinline__ double int8_dot_mma(const uint8_t *__restrict__ codes
   }
   const int *S = T == 0 ? v[0] : v[1];
   return (double)S[0] * 16777216.0 + (double)S[1] * 65536.0 + (double)S[2] * 256.0 + (double)S[3];
+}
+
+// One warp-wide BF16 x BF16 -> f32 tensor-core step (16 rows x 16 dims x 8 columns).
+__device__ __forceinline__ void mma_bf16_16x8x16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                                 uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// q.x for up to 32 candidate BF16 rows x on the tensor cores (FP32
+// accumulate), in the tile and lane layout of int8_l2_mma: two 16-row tiles;
+// lane t of group g reads the 16-byte chunks t, t+4, ... of its rows g, g+8
+// (and g+16, g+24), and each chunk feeds two k steps (its first four values,
+// then its last four).  The query enters as two B columns, hi = bf16(q) and
+// lo = bf16(q - hi) (qhl: dpad hi values, then dpad lo values), so the result
+// is x.hi + x.lo for lane j's candidate.  Every product of two BF16 values is
+// exact in FP32; on integer-valued rows and queries (hi = q, lo = 0) the sums
+// are exact integers below 2^24 as well.
+__device__ __forceinline__ float bf16_dot_mma(const uint16_t *__restrict__ rows, uint32_t dpad,
+                                              const uint16_t *qhl, uint32_t cand, int cnt, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int nch = (int)(dpad >> 3);
+  const int J = (nch + 3) >> 2;
+  const uint32_t id0 = __shfl_sync(kFull, cand, 0);
+  const bool two = cnt > 16;
+  const uint4 *rp[4];
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const int row = g + 8 * h;
+    uint32_t id = __shfl_sync(kFull, cand, row);
+    id = row < cnt ? id : id0;
+    rp[h] = reinterpret_cast<const uint4 *>(rows + (size_t)id * dpad);
+  }
+  // B column 0 holds hi, column 1 lo (columns 2..7 stay zero)
+  const uint4 *pq = reinterpret_cast<const uint4 *>(qhl + (g == 1 ? dpad : 0));
+  const bool col = g < 2;
+  float c0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, c1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  const uint4 z = make_uint4(0, 0, 0, 0);
+  for (int j0 = 0; j0 < J; j0 += 2) {
+    uint4 x[2][4], qv[2];
+    // every load of this step (both tiles) before the first tensor-core op
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int ch = t + 4 * (j0 + u);
+      const bool ok = j0 + u < J && ch < nch;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) x[u][h] = (ok && (h < 2 || two)) ? __ldg(rp[h] + ch) : z;
+      qv[u] = ok && col ? pq[ch] : z;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      mma_bf16_16x8x16(c0, x[u][0].x, x[u][1].x, x[u][0].y, x[u][1].y, qv[u].x, qv[u].y);
+      mma_bf16_16x8x16(c0, x[u][0].z, x[u][1].z, x[u][0].w, x[u][1].w, qv[u].z, qv[u].w);
+      if (two) {
+        mma_bf16_16x8x16(c1, x[u][2].x, x[u][3].x, x[u][2].y, x[u][3].y, qv[u].x, qv[u].y);
+        mma_bf16_16x8x16(c1, x[u][2].z, x[u][3].z, x[u][2].w, x[u][3].w, qv[u].z, qv[u].w);
+      }
+    }
+  }
+  // lane 4 (r % 8) of tile T holds row r % 8 (c[0], c[1]) and row r % 8 + 8
+  // (c[2], c[3]) against columns hi, lo; candidate j = 16T + r
+  const float a0 = __fadd_rn(c0[0], c0[1]), a1 = __fadd_rn(c0[2], c0[3]);
+  const float b0 = __fadd_rn(c1[0], c1[1]), b1 = __fadd_rn(c1[2], c1[3]);
+  const int T = lane >> 4, r = lane & 15, src = (r & 7) << 2;
+  const float e0 = __shfl_sync(kFull, a0, src), e1 = __shfl_sync(kFull, a1, src);
+  const float f0 = __shfl_sync(kFull, b0, src), f1 = __shfl_sync(kFull, b1, src);
+  return T == 0 ? (r < 8 ? e0 : e1) : (r < 8 ? f0 : f1);
 }
 
 // One warp-wide e4m3 x e4m3 -> f32 tensor-core step (16 rows x 32 dims x 8 columns).

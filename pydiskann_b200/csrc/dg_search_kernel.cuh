@@ -44,8 +44,14 @@ __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *ws
     if (MET == MET_L2) return finish_metric(MET, sqrt_l2, fmaxf(qs2.y + sn.y - 2.0f * dot, 0.0f), 0.0f, qq);
     return finish_metric(MET, false, dot, sn.y, qq);
   } else if (TRAV == TRAV_BF16) {
-    return rows_distance<LPR, 1, MET>(reinterpret_cast<const uint8_t *>(a.vec_bf16), a.dpad * 2,
-                                      (a.dpad / 8) / LPR, qs, cand, cnt, lane, sqrt_l2, qq);
+    // |q - x|^2 = |q|^2 + |x|^2 - 2 q.x with q.x on the tensor cores
+    const uint16_t *qhl = reinterpret_cast<const uint16_t *>(wsm + Ly.prov);
+    const float q2 = *reinterpret_cast<const float *>(wsm + Ly.prov + 4 * a.dpad);
+    const float xx = lane < cnt ? __ldg(a.bf16_n2 + cand) : 0.0f;
+    const float dot = bf16_dot_mma(a.vec_bf16, a.dpad, qhl, cand, cnt, lane);
+    if (MET == MET_L2) return finish_metric(MET, sqrt_l2, fmaxf(__fsub_rn(__fadd_rn(q2, xx), 2.0f * dot), 0.0f),
+                                            0.0f, qq);
+    return finish_metric(MET, false, dot, xx, qq);
   } else if (TRAV == TRAV_F16) {
     // L2 compares the f16-rounded query (F16Quantizer::prepare, src/sq.rs:51-55);
     // other metrics decode the code against the f32 query (src/quantized.rs:28-36).
@@ -202,6 +208,20 @@ __device__ __forceinline__ void prepare_query(const SearchArgs &a, uint8_t *wsm,
       lo[i] = __nv_cvt_float_to_fp8(__fmul_rn(__fsub_rn(v, hv), 16.0f), __NV_SATFINITE, __NV_E4M3);
     }
     if (lane == 0) *reinterpret_cast<float2 *>(wsm + Ly.prov + 2 * a.dpad) = make_float2(sq, qn);
+  } else if (TRAV == TRAV_BF16) {
+    // hi = bf16(q), lo = bf16(q - hi), then |q|^2 of the f32 query
+    uint16_t *hi = reinterpret_cast<uint16_t *>(wsm + Ly.prov), *lo = hi + a.dpad;
+    float q2 = 0.0f;
+    for (uint32_t i = lane; i < a.dpad; i += 32) {
+      const float v = qs[i];
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      hi[i] = __bfloat16_as_ushort(h);
+      lo[i] = __bfloat16_as_ushort(__float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h))));
+      q2 = fmaf(v, v, q2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q2 += __shfl_xor_sync(kFull, q2, o);
+    if (lane == 0) *reinterpret_cast<float *>(wsm + Ly.prov + 4 * a.dpad) = q2;
   } else if (TRAV == TRAV_F16) {
     float *qh = reinterpret_cast<float *>(wsm + Ly.prov);
     for (uint32_t i = lane; i < a.dpad; i += 32) qh[i] = __half2float(__float2half_rn(qs[i]));

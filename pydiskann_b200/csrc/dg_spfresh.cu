@@ -803,14 +803,14 @@ __global__ void k_pm_items(const uint32_t *pcount, const uint32_t *pstart, const
   }
 }
 
-// Tensor-core form of the tile's dot products.  Every value of an
-// integer-valued row with |x| < 2^16 splits exactly into two BF16 parts, hi =
-// bf16(x) and lo = x - hi, so q.x = qh.xh + qh.xl + ql.xh + ql.xl with every
-// product exact; when every partial sum stays below 2^24 (d * max|q| * max|x|
-// < 2^24) the FP32 accumulation is exact too, and the tensor cores return the
-// dot products the FMA chain below returns, bit for bit.  A tile or a query
-// set outside those bounds takes the FMA chain.
+// Tensor-core form of the tile's dot products.  Integer-valued rows and
+// queries with |x| <= 2048 are exact in FP16, every FP16 x FP16 product is
+// exact in FP32, and when every partial sum stays below 2^24 (d * max|q| *
+// max|x| < 2^24) the FP32 accumulation is exact too: the tensor cores then
+// return the dot products of the FMA chain below bit for bit.  A tile or a query set outside those
+// bounds takes the FMA chain.
 constexpr float kPmExactSum = 16777216.0f;  // 2^24
+constexpr float kPmF16Int = 2048.0f;        // integers up to this magnitude are exact in FP16
 
 __device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], uint32_t addr) {
   asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
@@ -818,25 +818,21 @@ __device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], uint32_t addr) {
                : "r"(addr));
 }
 
-__device__ __forceinline__ void mma_bf16_16x8x16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+__device__ __forceinline__ void mma_f16_16x8x16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
                "{%0,%1,%2,%3};"
                : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
                : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Writes the exact BF16 split (hi, lo) of x and returns whether x is an
-// integer of magnitude below 2^15 (so that the split is exact).
-__device__ __forceinline__ bool bf16_split(float x, uint16_t &hi, uint16_t &lo) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(x);
-  const __nv_bfloat16 l = __float2bfloat16_rn(__fsub_rn(x, __bfloat162float(h)));
-  hi = __bfloat16_as_ushort(h);
-  lo = __bfloat16_as_ushort(l);
-  return x == rintf(x) && fabsf(x) < 32768.0f;
+// FP16 bits of x and whether x is an integer exact in FP16 (|x| <= 2048).
+__device__ __forceinline__ uint16_t f16_exact(float x, bool &ok) {
+  ok = x == rintf(x) && fabsf(x) <= kPmF16Int;
+  return __half_as_ushort(__float2half_rn(x));
 }
 
-// Shared-memory row stride (in BF16 elements) of the split copies: dk + 8, so
-// that the eight 16-byte rows one ldmatrix reads fall in distinct banks.
+// Shared-memory row stride (in FP16 elements) of the converted copies: dk + 8,
+// so that the eight 16-byte rows one ldmatrix reads fall in distinct banks.
 __host__ __device__ inline uint32_t pm_ks(uint32_t d) { return ((d + 15u) & ~15u) + 8u; }
 // Capacity of a pair's k-best list: k rounded up to 32 (at most kPmK).
 __host__ __device__ inline uint32_t pm_kcap(uint32_t k) { return (k + 31u) & ~31u; }
@@ -863,14 +859,14 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
   float *qn = xn + kPmT;                                                     // [kPmQ] |q|^2
   uint64_t *lists = reinterpret_cast<uint64_t *>(qn + kPmQ);                 // [kPmQ][2][kc]
   uint64_t *cst = lists + (size_t)kPmQ * 2 * kc;                             // [8][32]
-  uint16_t *qhl = reinterpret_cast<uint16_t *>(cst + 8 * 32);                // [2][kPmQ][ks] BF16 hi, lo
-  uint16_t *thl = qhl + 2 * kPmQ * ks;                                       // [2][kPmT][ks]
-  // [kPmQ][kPmT] tensor-core dot products, over the f32 tile once it is split
+  uint16_t *qh = reinterpret_cast<uint16_t *>(cst + 8 * 32);                 // [kPmQ][ks] FP16 queries
+  uint16_t *th = qh + kPmQ * ks;                                             // [kPmT][ks] FP16 tile
+  // [kPmQ][kPmT] tensor-core dot products, over the f32 tile once it is converted
   float *dm = tile;
   __shared__ uint32_t s_item, s_qbad, s_tbad, s_qmax, s_tmax;
   const uint32_t total = *n_items;
   const bool sq = a.metric == DG_L2;
-  const uint32_t qhl_s = (uint32_t)__cvta_generic_to_shared(qhl), thl_s = (uint32_t)__cvta_generic_to_shared(thl);
+  const uint32_t qh_s = (uint32_t)__cvta_generic_to_shared(qh), th_s = (uint32_t)__cvta_generic_to_shared(th);
   while (true) {
     if (threadIdx.x == 0) {
       s_item = atomicAdd(item_counter, 1u);
@@ -883,22 +879,20 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
     if (it >= total) break;
     const uint4 item = items[it];
     const uint32_t b = item.x, p0 = item.y, m = item.z;
-    for (uint32_t t = threadIdx.x; t < m * dq; t += blockDim.x) {
-      const uint32_t j = t / dq, i = t % dq;
-      qsm[t] = i < a.d ? __ldg(a.Q + (size_t)pair_q[p0 + j] * a.d + i) : 0.0f;
-    }
-    {  // BF16 split of the queries (rows past m and columns past d are zero)
+    {  // queries: f32 rows (zero padded to dpad) and FP16 rows (zero padded to dk, rows past m zero)
       bool bad = false;
       float mx = 0.0f;
       for (uint32_t t = threadIdx.x; t < kPmQ * dk; t += blockDim.x) {
         const uint32_t j = t / dk, i = t % dk;
         const float x = (j < m && i < a.d) ? __ldg(a.Q + (size_t)pair_q[p0 + j] * a.d + i) : 0.0f;
-        uint16_t h, l;
-        bad |= !bf16_split(x, h, l);
+        bool ok;
+        qh[j * ks + i] = f16_exact(x, ok);
+        bad |= !ok;
         mx = fmaxf(mx, fabsf(x));
-        qhl[j * ks + i] = h;
-        qhl[(kPmQ + j) * ks + i] = l;
+        if (j < m && i < dq) qsm[j * dq + i] = x;
       }
+      for (uint32_t t = threadIdx.x; t < m * dq; t += blockDim.x)
+        if (t % dq >= dk) qsm[t] = 0.0f;  // dpad beyond the FP16 width
       if (__syncthreads_or(bad) && threadIdx.x == 0) s_qbad = 1u;
       if (mx > 0.0f) atomicMax(&s_qmax, __float_as_uint(mx));
     }
@@ -914,22 +908,38 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
     for (uint32_t e0 = 0; e0 < n_e; e0 += kPmT) {
       const uint32_t ne = min((uint32_t)kPmT, n_e - e0);
       __syncthreads();  // the previous tile is consumed (and the queries are in place)
-      for (uint32_t t = threadIdx.x; t < ne * d4; t += blockDim.x) {
-        const uint32_t r = t / d4, c = t % d4;
-        reinterpret_cast<float4 *>(tile + r * dt)[c] =
-            __ldg(reinterpret_cast<const float4 *>(a.codes + (size_t)(b * a.cap + e0 + r) * a.code_stride) + c);
-      }
-      for (uint32_t r = threadIdx.x; r < kPmT; r += blockDim.x) {
-        uint32_t id = DG_PAD;
-        if (r < ne) {
-          id = __ldg(a.ids + b * a.cap + e0 + r);
-          if (is_deleted(a.deleted, id)) id = DG_PAD;
-        }
-        tid[r] = id;
-      }
       if (threadIdx.x == 0) {
         s_tbad = 0u;
         s_tmax = 0u;
+      }
+      {  // the tile: f32 rows and FP16 rows (rows past ne and columns past d are zero)
+        bool bad = false;
+        float mx = 0.0f;
+        const uint32_t k4 = dk / 4;
+        for (uint32_t t = threadIdx.x; t < kPmT * k4; t += blockDim.x) {
+          const uint32_t r = t / k4, c = t % k4;
+          float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          if (r < ne && c < d4) {
+            v = __ldg(reinterpret_cast<const float4 *>(a.codes + (size_t)(b * a.cap + e0 + r) * a.code_stride) + c);
+            reinterpret_cast<float4 *>(tile + r * dt)[c] = v;
+          }
+          bool o0, o1, o2, o3;
+          const uint32_t lo = f16_exact(v.x, o0) | ((uint32_t)f16_exact(v.y, o1) << 16);
+          const uint32_t hi = f16_exact(v.z, o2) | ((uint32_t)f16_exact(v.w, o3) << 16);
+          *reinterpret_cast<uint2 *>(th + r * ks + 4 * c) = make_uint2(lo, hi);
+          bad |= !(o0 && o1 && o2 && o3);
+          mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+        }
+        for (uint32_t r = threadIdx.x; r < kPmT; r += blockDim.x) {
+          uint32_t id = DG_PAD;
+          if (r < ne) {
+            id = __ldg(a.ids + b * a.cap + e0 + r);
+            if (is_deleted(a.deleted, id)) id = DG_PAD;
+          }
+          tid[r] = id;
+        }
+        if (__syncthreads_or(bad) && threadIdx.x == 0) s_tbad = 1u;
+        if (mx > 0.0f) atomicMax(&s_tmax, __float_as_uint(mx));
       }
       __syncthreads();
       if (threadIdx.x < ne) {
@@ -938,25 +948,10 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         for (uint32_t i = 0; i < a.d; ++i) s2 = fmaf(row[i], row[i], s2);
         xn[threadIdx.x] = s2;
       }
-      {  // BF16 split of the tile (rows past ne and columns past d are zero)
-        bool bad = false;
-        float mx = 0.0f;
-        for (uint32_t t = threadIdx.x; t < kPmT * dk; t += blockDim.x) {
-          const uint32_t r = t / dk, i = t % dk;
-          const float x = (r < ne && i < a.d) ? tile[r * dt + i] : 0.0f;
-          uint16_t h, l;
-          bad |= !bf16_split(x, h, l);
-          mx = fmaxf(mx, fabsf(x));
-          thl[r * ks + i] = h;
-          thl[(kPmT + r) * ks + i] = l;
-        }
-        if (__syncthreads_or(bad) && threadIdx.x == 0) s_tbad = 1u;
-        if (mx > 0.0f) atomicMax(&s_tmax, __float_as_uint(mx));
-      }
-      __syncthreads();
+      const float qm = __uint_as_float(s_qmax), tm = __uint_as_float(s_tmax);
       // (the dot products overwrite the f32 tile, which must hold kPmQ x kPmT floats)
-      const bool tc = !s_qbad && !s_tbad && dt >= (uint32_t)kPmQ &&
-                      (float)a.d * __uint_as_float(s_qmax) * __uint_as_float(s_tmax) < kPmExactSum;
+      const bool tc = !s_qbad && !s_tbad && dt >= (uint32_t)kPmQ && (float)a.d * qm * tm < kPmExactSum;
+      __syncthreads();  // xn read the f32 tile
       float acc[4][2];
 #pragma unroll
       for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = 0.0f;
@@ -967,18 +962,11 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         const uint32_t arow = e16 + (lane & 15), acol = (lane >> 4) * 8;
         const uint32_t brow = q16 + (lane >> 4) * 8 + (lane & 7), bcol = ((lane >> 3) & 1) * 8;
         for (uint32_t k0 = 0; k0 < dk; k0 += 16) {
-          uint32_t ah[4], al[4], bh[4], bl[4];
-          ldsm_x4(ah, thl_s + 2u * (arow * ks + k0 + acol));
-          ldsm_x4(al, thl_s + 2u * ((kPmT + arow) * ks + k0 + acol));
-          ldsm_x4(bh, qhl_s + 2u * (brow * ks + k0 + bcol));
-          ldsm_x4(bl, qhl_s + 2u * ((kPmQ + brow) * ks + k0 + bcol));
-#pragma unroll
-          for (int nt = 0; nt < 2; ++nt) {
-            mma_bf16_16x8x16(c[nt], ah, bh[2 * nt], bh[2 * nt + 1]);
-            mma_bf16_16x8x16(c[nt], ah, bl[2 * nt], bl[2 * nt + 1]);
-            mma_bf16_16x8x16(c[nt], al, bh[2 * nt], bh[2 * nt + 1]);
-            mma_bf16_16x8x16(c[nt], al, bl[2 * nt], bl[2 * nt + 1]);
-          }
+          uint32_t av[4], bv[4];
+          ldsm_x4(av, th_s + 2u * (arow * ks + k0 + acol));
+          ldsm_x4(bv, qh_s + 2u * (brow * ks + k0 + bcol));
+          mma_f16_16x8x16(c[0], av, bv[0], bv[1]);
+          mma_f16_16x8x16(c[1], av, bv[2], bv[3]);
         }
         // lane (g, t) holds entries g, g + 8 x queries 2t, 2t + 1 of each 8-query tile
         const uint32_t g = lane >> 2, t2 = 2 * (lane & 3);
@@ -1074,7 +1062,7 @@ __global__ void __launch_bounds__(128) k_pm_merge(const uint32_t *probe_cnt, con
 
 static size_t pm_smem(uint32_t d, uint32_t dpad, uint32_t k) {
   return ((size_t)kPmQ * dpad + (size_t)kPmT * (d + 4)) * 4 + (2 * kPmT + kPmQ) * 4 +
-         (size_t)kPmQ * 2 * pm_kcap(k) * 8 + 8 * 32 * 8 + (size_t)2 * (kPmQ + kPmT) * pm_ks(d) * 2;
+         (size_t)kPmQ * 2 * pm_kcap(k) * 8 + 8 * 32 * 8 + (size_t)(kPmQ + kPmT) * pm_ks(d) * 2;
 }
 
 // Posting-major scan of one chunk whose routing matrix is in ac.route: probes
