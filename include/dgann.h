@@ -194,6 +194,10 @@ typedef struct {
   const uint32_t *per_query_beam; /* optional u32[nq] host array of per-query L */
   uint32_t flags;                 /* DG_FLAG_* */
   void *stream;                   /* cudaStream_t; without DG_FLAG_STREAM, NULL = the handle's stream */
+  /* optional u32[nq] host array of per-query k, each in [1, k]: query q
+   * returns up to per_query_k[q] results in its output row, which stays k
+   * entries long (padded with 0xFFFFFFFF / +inf past its count) */
+  const uint32_t *per_query_k;
 } DgSearchParams;
 
 /* Batched search.  Stands in for DiskANN::search_with_dists (src/lib.rs:683-714),

@@ -55,7 +55,7 @@ struct DgIndex {
     size_t cap = 0;
   };
   struct Slot {
-    Buf q, ids, dists, cnt, stats, fops, foffs, fpool, perl;
+    Buf q, ids, dists, cnt, stats, fops, foffs, fpool, perl, perk;
     uint32_t *counter = nullptr;  // work counters of the persistent grid (one per pipeline chunk)
     cudaEvent_t done = nullptr;
     bool pending = false;

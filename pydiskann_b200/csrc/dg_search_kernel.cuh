@@ -242,9 +242,10 @@ template <int TRAV, int MET, int LPRF>
 __device__ inline void emit_results(const SearchArgs &a, uint32_t q, const uint64_t *src, int have,
                                     bool use_rerank, uint32_t search_k, uint64_t *tmp, const float *qs,
                                     float qq, uint32_t n_exp, uint32_t n_dist, int lane) {
-  const uint32_t k = a.k;
-  uint32_t *oid = a.out_ids + (size_t)q * k;
-  float *od = a.out_d + (size_t)q * k;
+  // this query's k; output rows are a.k apart and padded past k
+  const uint32_t k = a.perK ? a.perK[q] : a.k;
+  uint32_t *oid = a.out_ids + (size_t)q * a.k;
+  float *od = a.out_d + (size_t)q * a.k;
   int count;
   if (use_rerank) {
     const int nr = min(have, (int)search_k);
@@ -269,7 +270,7 @@ __device__ inline void emit_results(const SearchArgs &a, uint32_t q, const uint6
       od[i] = key_dist(src[i]);
     }
   }
-  for (int i = count + lane; i < (int)k; i += 32) {
+  for (int i = count + lane; i < (int)a.k; i += 32) {
     oid[i] = DG_PAD;
     od[i] = __int_as_float(0x7f800000);
   }
@@ -376,7 +377,7 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
   const Visited vt{reinterpret_cast<uint32_t *>(wsm + Ly.hash), a.hbits, a.hB};
   float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
   const int L = (int)(a.perL ? a.perL[q] : a.L);
-  const uint32_t k = a.k;
+  const uint32_t k = a.perK ? a.perK[q] : a.k;
   const bool use_rerank = TRAV != TRAV_F32 && a.rerank > 0;
   const uint32_t search_k = use_rerank ? max(a.rerank, k) : k;
 
@@ -473,7 +474,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
   float *qs = reinterpret_cast<float *>(wsm + Ly.qf);
 
   const uint32_t L = a.perL ? a.perL[q] : a.L;
-  const uint32_t k = a.k;
+  const uint32_t k = a.perK ? a.perK[q] : a.k;
   // every traversal other than exact FP32 can be reranked with FP32 rows
   const bool use_rerank = TRAV != TRAV_F32 && a.rerank > 0;
   const uint32_t search_k = use_rerank ? max(a.rerank, k) : k;
