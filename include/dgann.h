@@ -259,21 +259,26 @@ DG_API DgStatus dg_count_matching(DgIndex *idx, const DgFilterOp *ops, uint32_t 
  * batch as a rayon par_iter over such calls (src/lib.rs:709-714); its benches
  * time sequential request loops (benches/benchmark.rs:183-207).  Here requests
  * are queued one at a time and a dispatcher thread forms batches of pending
- * requests with the same k, traversal, rerank size and filter presence (beam
- * and filter program stay per request), launching each batch on the next free
- * stream slot.  Requests that arrive while batches run are admitted as soon as
- * a slot frees, and batches on different slots overlap on the device.  Each
- * slot's buffers are allocated at creation and charged against
- * hbm_budget_bytes, so `streams` is the admission limit.  A request returns
+ * requests with the same traversal, rerank size and filter presence (k, beam
+ * and filter program stay per request, so one launch carries uneven k, beams
+ * and filters), launching each batch on the next free stream slot.  Requests
+ * that arrive while batches run are admitted as soon as a slot and memory
+ * free up, and batches on different slots overlap on the device.  Memory is
+ * admitted per batch: the server allocates one device arena (and a pinned
+ * host arena) of hbm_budget_bytes at creation, and each batch takes a region
+ * sized by its own queries, results at its largest k, beams and k; a batch
+ * that does not fit is trimmed, and the dispatcher waits for regions of
+ * batches in flight when not even one request fits.  A request returns
  * exactly what dg_search_batch returns for it alone. */
 typedef struct DgServer DgServer;
 typedef struct {
   uint32_t max_batch;        /* requests per launch */
-  uint32_t streams;          /* batches in flight at once (one buffer set each) */
+  uint32_t streams;          /* batches in flight at once (one stream each) */
   uint32_t max_k;            /* largest k a request may ask for */
   uint32_t max_filter_ops;   /* largest filter program of one request */
   uint32_t max_wait_us;      /* how long a partial batch waits to fill; 0 = launch at once */
-  uint64_t hbm_budget_bytes; /* 0 = no limit; creation fails with DG_ENOMEM beyond it */
+  uint64_t hbm_budget_bytes; /* the batch arena; 0 = room for a full batch at max_k on every stream.
+                                creation fails with DG_ENOMEM when one request at max_k does not fit */
 } DgServerConfig;
 typedef struct {
   uint32_t k;

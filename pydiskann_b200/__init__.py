@@ -370,7 +370,7 @@ class _Index:
 
     # -- the batched entry point
     def _params(self, queries, k, beam_width, traversal, rerank_size, filters, per_query_beam, out, stream,
-                with_stats):
+                with_stats, per_query_k=None):
         """DgSearchParams and buffers of one batched call (see search_arrays)."""
         dev = hasattr(queries, "data_ptr") and getattr(queries, "is_cuda", False)
         p = _lib.SearchParams()
@@ -437,19 +437,26 @@ class _Index:
                 raise ValueError(f"one beam width per query expected: {len(pl)} for {nq} queries")
             keep.append(pl)
             p.per_query_beam = ptr(pl)
+        if per_query_k is not None:
+            pk = np.ascontiguousarray(per_query_k, dtype=np.uint32).reshape(-1)
+            if len(pk) != nq:  # the library reads one k per query
+                raise ValueError(f"one k per query expected: {len(pk)} for {nq} queries")
+            keep.append(pk)
+            p.per_query_k = ptr(pk)
         return p, Q, nq, out, stats, keep
 
     def search_arrays(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32,
                       rerank_size=0, filters=None, per_query_beam=None, out=None, stream=None,
-                      with_stats=False):
+                      with_stats=False, per_query_k=None):
         """Batched search over numpy arrays (host) or CUDA tensors (device).
 
         Returns (ids u32[nq,k], dists f32[nq,k], counts u32[nq]) of the same
         kind as `queries`; rows are padded with PAD / +inf past counts.
-        `filters` is one Filter for all queries or a list of one per query.
+        `filters` is one Filter for all queries or a list of one per query;
+        `per_query_k` (each in [1, k]) gives query i its own k in a row of k.
         """
         p, Q, nq, out, stats, keep = self._params(queries, k, beam_width, traversal, rerank_size, filters,
-                                                  per_query_beam, out, stream, with_stats)
+                                                  per_query_beam, out, stream, with_stats, per_query_k)
         check(lib().dg_search_batch(self._h, C.byref(p), ptr(Q), nq, ptr(out[0]), ptr(out[1]),
                                     ptr(out[2]), ptr(stats)))
         del keep

@@ -50,7 +50,7 @@ class SearchParams(C.Structure):
         ("traversal", C.c_int32), ("filter_ops", C.c_void_p), ("filter_nops", C.c_uint32),
         ("filter_offsets", C.c_void_p), ("filter_pool", C.c_void_p),
         ("filter_pool_len", C.c_uint32), ("per_query_beam", C.c_void_p), ("flags", C.c_uint32),
-        ("stream", C.c_void_p),
+        ("stream", C.c_void_p), ("per_query_k", C.c_void_p),
     ]
 
 

@@ -56,6 +56,29 @@ static int lanes_per_row(uint32_t chunks) {
   return 2;
 }
 
+// Grows every call slot's staging buffers for per-call parameters to hold a
+// batch of nq queries with `ops` filter instructions and `pool` IN values, so
+// that later calls of that size reallocate nothing (a reallocation synchronises
+// the device, a latency spike for every batch in flight).  Waits for slots
+// whose previous call is still running.
+DgStatus reserve_call_buffers(DgIndex *idx, uint32_t nq, size_t ops, size_t pool) {
+  std::lock_guard<std::mutex> lk(idx->mu);
+  DG_CUDA(cudaSetDevice(idx->device));
+  for (auto &sl : idx->slots) {
+    if (sl.pending) {
+      DG_CUDA(cudaEventSynchronize(sl.done));
+      sl.pending = false;
+    }
+    DgStatus s;
+    if ((s = buf_reserve(sl.fops, ops * sizeof(DgFilterOp))) != DG_OK) return s;
+    if ((s = buf_reserve(sl.foffs, ((size_t)nq + 1) * 4)) != DG_OK) return s;
+    if ((s = buf_reserve(sl.fpool, pool * 8)) != DG_OK) return s;
+    if ((s = buf_reserve(sl.perl, (size_t)nq * 4)) != DG_OK) return s;
+    if ((s = buf_reserve(sl.perk, (size_t)nq * 4)) != DG_OK) return s;
+  }
+  return DG_OK;
+}
+
 }  // namespace dg
 
 using namespace dg;
@@ -116,7 +139,7 @@ DgStatus dg_index_destroy(DgIndex *idx) {
       cudaEventDestroy(sl.done);
     }
     for (DgIndex::Buf *b : {&sl.q, &sl.ids, &sl.dists, &sl.cnt, &sl.stats, &sl.fops, &sl.foffs,
-                            &sl.fpool, &sl.perl})
+                            &sl.fpool, &sl.perl, &sl.perk})
       if (b->p) cudaFree(b->p);
     if (sl.counter) cudaFree(sl.counter);
   }
@@ -550,6 +573,10 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
       if (p->per_query_beam[i] == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
   }
   if (maxL == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
+  if (p->per_query_k)
+    for (uint32_t i = 0; i < nq; ++i)
+      if (p->per_query_k[i] == 0 || p->per_query_k[i] > p->k)
+        return fail(DG_EINVAL, "per_query_k must be in [1, k]");
   const uint32_t total_ops = p->filter_offsets ? p->filter_offsets[nq] : p->filter_nops;
   bool any_filter = false;
   if (p->filter_offsets) {
@@ -643,6 +670,10 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
     if ((s = stage_copy(sl.perl, p->per_query_beam, (size_t)nq * 4, st)) != DG_OK) return s;
     a.perL = (const uint32_t *)sl.perl.p;
   }
+  if (p->per_query_k) {
+    if ((s = stage_copy(sl.perk, p->per_query_k, (size_t)nq * 4, st)) != DG_OK) return s;
+    a.perK = (const uint32_t *)sl.perk.p;
+  }
   const size_t kq = (size_t)nq * p->k;
   // host calls of many queries: chunks whose copies overlap the other chunks' kernels
   const uint32_t chunks = devptr || nq < 4096 ? 1u : std::min<uint32_t>(DgIndex::kPipeChunks, nq / 2048);
@@ -715,6 +746,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
       ac.out_cnt = a.out_cnt + q0;
       if (a.out_stats) ac.out_stats = a.out_stats + 2 * q0;
       if (a.perL) ac.perL = a.perL + q0;
+      if (a.perK) ac.perK = a.perK + q0;
       if (a.foffs) ac.foffs = a.foffs + q0;
       ac.counter = sl.counter + c;
       cudaStream_t ks = idx->pipe_k[c & 1];
@@ -940,6 +972,10 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
     }
   }
   if (maxL == 0) return fail(DG_EINVAL, "beam_width must be >= 1");
+  if (p->per_query_k)
+    for (uint32_t i = 0; i < nq; ++i)
+      if (p->per_query_k[i] == 0 || p->per_query_k[i] > p->k)
+        return fail(DG_EINVAL, "per_query_k must be in [1, k]");
   const uint32_t total_ops = p->filter_offsets ? p->filter_offsets[nq] : p->filter_nops;
   bool any_filter = false;
   if (p->filter_offsets) {
@@ -972,13 +1008,14 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   while (hB < 32 && (1ull << hB) < idx->n) ++hB;
   hB = std::max(hB, hbits);
 
-  // scratch layout: [0, 256) work counter | filter ops | offsets | pool | beams
+  // scratch layout: [0, 256) work counter | filter ops | offsets | pool | beams | per-query k
   auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
   const size_t o_ops = 256;
   const size_t o_offs = o_ops + up16(any_filter ? (size_t)total_ops * sizeof(DgFilterOp) : 0);
   const size_t o_pool = o_offs + up16(any_filter && p->filter_offsets ? (size_t)(nq + 1) * 4 : 0);
   const size_t o_beam = o_pool + up16(any_filter ? (size_t)p->filter_pool_len * 8 : 0);
-  const size_t used = o_beam + up16(p->per_query_beam ? (size_t)nq * 4 : 0);
+  const size_t o_k = o_beam + up16(p->per_query_beam ? (size_t)nq * 4 : 0);
+  const size_t used = o_k + up16(p->per_query_k ? (size_t)nq * 4 : 0);
   if (used > kStaticScratchBytes)
     return fail(DG_EINVAL, "per-call parameters need " + std::to_string(used) + " bytes; the static scratch holds " +
                                std::to_string(kStaticScratchBytes) + " (fewer filter ops or per-query beams per call)");
@@ -1046,6 +1083,10 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   if (p->per_query_beam) {
     DG_CUDA(cudaMemcpyAsync(scratch + o_beam, p->per_query_beam, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
     a.perL = reinterpret_cast<const uint32_t *>(scratch + o_beam);
+  }
+  if (p->per_query_k) {
+    DG_CUDA(cudaMemcpyAsync(scratch + o_k, p->per_query_k, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
+    a.perK = reinterpret_cast<const uint32_t *>(scratch + o_k);
   }
   a.Q = queries;
   a.out_ids = out_ids;

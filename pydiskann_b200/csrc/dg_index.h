@@ -77,6 +77,9 @@ namespace dg {
 uint32_t dpad_of(uint32_t d);
 DgStatus dev_alloc(DgIndex *idx, void **p, size_t bytes);
 DgStatus buf_reserve(DgIndex::Buf &b, size_t bytes);
+// Sizes the per-call staging buffers of every call slot for batches of nq
+// queries with `ops` filter instructions and `pool` IN values.
+DgStatus reserve_call_buffers(DgIndex *idx, uint32_t nq, size_t ops, size_t pool);
 DgStatus to_device(DgIndex *idx, void **dst, const void *src, size_t bytes);
 // Rows of d floats from the host into [n][dpad] device rows, zero padded.
 DgStatus upload_rows_f32(const float *host, uint64_t n, uint32_t d, uint32_t dpad, float *dev,

@@ -2,14 +2,22 @@
 //
 // Requests (one query each, with its own k, beam, rerank, traversal and
 // filter) are queued by dg_server_submit.  A dispatcher thread forms batches
-// of pending requests that share (k, traversal, rerank) and launches each
-// batch on the next free stream slot; a request that arrives while other
-// batches are on the GPU goes into the next batch as soon as a slot is free,
-// and batches on different slots run concurrently on the device.  Every slot
-// owns preallocated pinned host and device buffers, sized at creation and
-// charged against the configured HBM budget, so the number of slots is the
-// admission limit.  A host function enqueued after each batch's result copy
-// completes its requests; dg_server_wait waits for a ticket with a bound.
+// of pending requests that share (traversal, rerank, filter presence) -- k,
+// beam and the filter program stay per request, so one launch carries uneven
+// k, beams and filters -- and launches each batch on the next free stream
+// slot; a request that arrives while other batches are on the GPU goes into
+// the next batch as soon as a slot and memory are free, and batches on
+// different slots run concurrently on the device.
+//
+// Admission by HBM budget: the server holds one device arena (and a pinned
+// host arena of the same size) of hbm_budget_bytes, allocated at creation.
+// Each batch takes a region sized by its own need -- its queries, its result
+// rows at the batch's largest k, its per-query beams and k -- first fit; a
+// batch that does not fit is trimmed to the requests that do, and when not
+// even one fits the dispatcher waits for batches in flight to return their
+// regions.  A host function enqueued after each batch's result copy completes
+// its requests and frees its region; dg_server_wait waits for a ticket with a
+// bound.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -38,6 +46,7 @@ struct ServeRequest {
   std::vector<uint64_t> pool;
   Clock::time_point arrival, done_at;
   bool done = false;
+  bool picked = false;  // taken into the batch being formed (under the server's mutex)
   DgStatus status = DG_OK;
   std::string err;  // dg_last_error of the dispatcher thread when status != DG_OK
   std::vector<uint32_t> ids;
@@ -45,17 +54,61 @@ struct ServeRequest {
   uint32_t count = 0;
 };
 
+// A batch's region of the arenas (offsets into the device and pinned host
+// arenas; the same layout in both):
+//   queries f32[nq*d] | ids u32[nq*k] dists f32[nq*k] counts u32[nq] | beams u32[nq] | k u32[nq]
+// with k the batch's largest; every part starts on 256 bytes.
+struct BatchLayout {
+  size_t q = 0, out = 0, beam = 0, kq = 0, bytes = 0;
+};
+inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+inline BatchLayout batch_layout(uint32_t nq, uint32_t d, uint32_t kmax) {
+  BatchLayout L;
+  L.q = 0;
+  L.out = up256((size_t)nq * d * 4);
+  L.beam = L.out + up256((size_t)nq * kmax * 8 + (size_t)nq * 4);
+  L.kq = L.beam + up256((size_t)nq * 4);
+  L.bytes = L.kq + up256((size_t)nq * 4);
+  return L;
+}
+
+// First-fit allocator over [0, cap) (under the server's mutex).
+struct Arena {
+  size_t cap = 0;
+  std::vector<std::pair<size_t, size_t>> used;  // (offset, bytes), sorted by offset
+  bool take(size_t bytes, size_t *off) {
+    size_t at = 0;
+    for (size_t i = 0; i <= used.size(); ++i) {
+      const size_t end = i < used.size() ? used[i].first : cap;
+      if (end >= at && end - at >= bytes) {
+        used.insert(used.begin() + i, {at, bytes});
+        *off = at;
+        return true;
+      }
+      if (i < used.size()) at = used[i].first + used[i].second;
+    }
+    return false;
+  }
+  void give(size_t off) {
+    for (size_t i = 0; i < used.size(); ++i)
+      if (used[i].first == off) {
+        used.erase(used.begin() + i);
+        return;
+      }
+  }
+  size_t in_use() const {
+    size_t t = 0;
+    for (auto &u : used) t += u.second;
+    return t;
+  }
+};
+
 struct ServeSlot {
   cudaStream_t stream = nullptr;
-  float *h_q = nullptr, *d_q = nullptr;
-  // results of a batch of nq requests with k each, in one buffer so that one
-  // copy brings them back: ids u32[nq*k] | dists f32[nq*k] | counts u32[nq]
-  uint8_t *h_out = nullptr, *d_out = nullptr;
-  uint32_t *h_beam = nullptr;  // pinned: the search stages it with an async copy
   bool busy = false;
   std::vector<ServeRequest *> batch;
-  uint32_t k = 0;
-  struct DgServerImpl *owner = nullptr;
+  uint32_t k = 0;       // result row stride: the batch's largest k
+  size_t off = 0;       // the batch's arena region
 };
 
 }  // namespace dg
@@ -64,6 +117,9 @@ struct DgServer {
   DgIndex *idx = nullptr;
   DgServerConfig cfg{};
   std::vector<dg::ServeSlot> slots;
+  dg::Arena arena;                          // under mu
+  uint8_t *d_arena = nullptr, *h_arena = nullptr;
+  size_t peak_bytes = 0;                    // largest arena use seen (under mu)
   std::mutex mu;
   std::condition_variable cv_submit, cv_done, cv_slot;
   std::deque<dg::ServeRequest *> pending;
@@ -131,9 +187,11 @@ static void CUDART_CB slot_done(void *arg) {
   // results into the requests' own buffers (sized at submission) without the
   // lock: a waiter reads them only after seeing `done`, which is set below
   const size_t nb = sl.batch.size(), nk = nb * (size_t)sl.k;
-  const uint32_t *ids = reinterpret_cast<const uint32_t *>(sl.h_out);
-  const float *ds = reinterpret_cast<const float *>(sl.h_out + nk * 4);
-  const uint32_t *cnt = reinterpret_cast<const uint32_t *>(sl.h_out + nk * 8);
+  const BatchLayout L = batch_layout((uint32_t)nb, s->idx->d, sl.k);
+  const uint8_t *h_out = s->h_arena + sl.off + L.out;
+  const uint32_t *ids = reinterpret_cast<const uint32_t *>(h_out);
+  const float *ds = reinterpret_cast<const float *>(h_out + nk * 4);
+  const uint32_t *cnt = reinterpret_cast<const uint32_t *>(h_out + nk * 8);
   for (size_t i = 0; i < nb; ++i) {
     ServeRequest *r = sl.batch[i];
     r->count = std::min(cnt[i], r->k);
@@ -149,6 +207,7 @@ static void CUDART_CB slot_done(void *arg) {
     s->served += nb;
     sl.batch.clear();
     sl.busy = false;
+    s->arena.give(sl.off);
     --s->in_flight;
   }
   s->cv_done.notify_all();
@@ -158,9 +217,18 @@ static void CUDART_CB slot_done(void *arg) {
 
 static bool same_class(const ServeRequest *a, const ServeRequest *b) {
   // a filtered search is a different traversal (expanded beam), so requests
-  // with and without a filter never share a batch
-  return a->k == b->k && a->traversal == b->traversal && a->rerank == b->rerank &&
-         a->ops.empty() == b->ops.empty();
+  // with and without a filter never share a batch; k, beam and the filter
+  // program are per query within a launch
+  return a->traversal == b->traversal && a->rerank == b->rerank && a->ops.empty() == b->ops.empty();
+}
+
+// Fails one request (under mu).
+static void fail_request(DgServer *s, ServeRequest *r, DgStatus st, const std::string &why) {
+  r->status = st;
+  r->err = why;
+  r->done = true;
+  r->done_at = Clock::now();
+  s->cv_done.notify_all();
 }
 
 static void dispatch_loop(DgServer *s) {
@@ -179,7 +247,7 @@ static void dispatch_loop(DgServer *s) {
       const auto deadline = s->pending.front()->arrival + std::chrono::microseconds(s->cfg.max_wait_us);
       s->cv_submit.wait_until(lk, deadline, [&] { return s->stop || s->pending.size() >= s->cfg.max_batch; });
     }
-    // a free slot (admission: every slot holds its own HBM reservation)
+    // a free slot (a stream for the batch)
     int slot = -1;
     s->cv_slot.wait(lk, [&] {
       for (size_t i = 0; i < s->slots.size(); ++i)
@@ -191,32 +259,62 @@ static void dispatch_loop(DgServer *s) {
     });
     if (slot < 0) break;
     ServeSlot &sl = s->slots[slot];
-    // oldest request fixes the class; take up to max_batch of that class in arrival order
+    // oldest request fixes the class; candidates: up to max_batch of that
+    // class in arrival order
     ServeRequest *head = s->pending.front();
     batch.clear();
-    for (auto it = s->pending.begin(); it != s->pending.end() && batch.size() < s->cfg.max_batch;) {
-      if (same_class(*it, head)) {
-        batch.push_back(*it);
-        it = s->pending.erase(it);
-      } else {
-        ++it;
-      }
+    for (auto it = s->pending.begin(); it != s->pending.end() && batch.size() < s->cfg.max_batch; ++it)
+      if (same_class(*it, head)) batch.push_back(*it);
+    // admission: the longest prefix of the candidates whose region fits
+    size_t off = 0;
+    uint32_t take = (uint32_t)batch.size(), kmax = 0;
+    while (take > 0) {
+      kmax = 0;
+      for (uint32_t i = 0; i < take; ++i) kmax = std::max(kmax, batch[i]->k);
+      if (s->arena.take(batch_layout(take, dim, kmax).bytes, &off)) break;
+      take = take > 8 ? take - take / 4 : take - 1;
     }
+    if (take == 0) {
+      if (s->in_flight == 0) {  // cannot fit even alone: the budget is too small for it
+        ServeRequest *r = head;
+        s->pending.erase(std::find(s->pending.begin(), s->pending.end(), r));
+        fail_request(s, r, DG_ENOMEM, "request needs more memory than the server's HBM budget");
+        continue;
+      }
+      // wait for a batch in flight to return its region
+      const uint64_t served0 = s->served.load();
+      s->cv_slot.wait(lk, [&] { return s->stop || s->served.load() != served0 || s->in_flight == 0; });
+      continue;
+    }
+    batch.resize(take);
+    for (ServeRequest *r : batch) r->picked = true;
+    s->pending.erase(std::remove_if(s->pending.begin(), s->pending.end(), [](ServeRequest *r) { return r->picked; }),
+                     s->pending.end());
+    for (ServeRequest *r : batch) r->picked = false;
     sl.busy = true;
+    sl.off = off;
+    s->peak_bytes = std::max(s->peak_bytes, s->arena.in_use());
     s->max_in_flight = std::max(s->max_in_flight, ++s->in_flight);
     sl.batch = batch;
-    sl.k = head->k;
+    sl.k = kmax;
     lk.unlock();
 
     const uint32_t nq = (uint32_t)batch.size();
+    const BatchLayout L = batch_layout(nq, dim, kmax);
+    float *h_q = reinterpret_cast<float *>(s->h_arena + off + L.q);
+    uint32_t *h_beam = reinterpret_cast<uint32_t *>(s->h_arena + off + L.beam);
+    uint32_t *h_k = reinterpret_cast<uint32_t *>(s->h_arena + off + L.kq);
+    float *d_q = reinterpret_cast<float *>(s->d_arena + off + L.q);
+    uint8_t *d_out = s->d_arena + off + L.out;
     offs.assign(1, 0);
     ops.clear();
     pool.clear();
     bool any_filter = false;
     for (uint32_t i = 0; i < nq; ++i) {
       ServeRequest *r = batch[i];
-      std::memcpy(sl.h_q + (size_t)i * dim, r->query.data(), dim * sizeof(float));
-      sl.h_beam[i] = r->beam;
+      std::memcpy(h_q + (size_t)i * dim, r->query.data(), dim * sizeof(float));
+      h_beam[i] = r->beam;
+      h_k[i] = r->k;
       const uint64_t base = pool.size();
       for (DgFilterOp o : r->ops) {
         if (o.op == DG_F_IN) o.a += base;
@@ -227,16 +325,17 @@ static void dispatch_loop(DgServer *s) {
       offs.push_back((uint32_t)ops.size());
     }
     DgStatus st = DG_OK;
-    if (cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)nq * dim * sizeof(float), cudaMemcpyHostToDevice, sl.stream) !=
+    if (cudaMemcpyAsync(d_q, h_q, (size_t)nq * dim * sizeof(float), cudaMemcpyHostToDevice, sl.stream) !=
         cudaSuccess)
       st = fail(DG_EDEVICE, "request copy failed");
     if (st == DG_OK) {
       DgSearchParams p{};
-      p.k = head->k;
+      p.k = kmax;
       p.beam_width = head->beam;
       p.rerank_size = head->rerank;
       p.traversal = head->traversal;
-      p.per_query_beam = sl.h_beam;
+      p.per_query_beam = h_beam;
+      p.per_query_k = h_k;
       if (any_filter) {
         p.filter_ops = ops.data();
         p.filter_offsets = offs.data();
@@ -245,15 +344,15 @@ static void dispatch_loop(DgServer *s) {
       }
       p.flags = DG_FLAG_DEVICE_PTRS | DG_FLAG_STREAM;
       p.stream = sl.stream;
-      const size_t nk = (size_t)nq * head->k;
-      st = dg_search_batch(s->idx, &p, sl.d_q, nq, reinterpret_cast<uint32_t *>(sl.d_out),
-                           reinterpret_cast<float *>(sl.d_out + nk * 4),
-                           reinterpret_cast<uint32_t *>(sl.d_out + nk * 8), nullptr);
+      const size_t nk = (size_t)nq * kmax;
+      st = dg_search_batch(s->idx, &p, d_q, nq, reinterpret_cast<uint32_t *>(d_out),
+                           reinterpret_cast<float *>(d_out + nk * 4), reinterpret_cast<uint32_t *>(d_out + nk * 8),
+                           nullptr);
     }
     if (st == DG_OK) {
-      const size_t kq = (size_t)nq * head->k;
-      if (cudaMemcpyAsync(sl.h_out, sl.d_out, kq * 8 + (size_t)nq * 4, cudaMemcpyDeviceToHost, sl.stream) !=
-              cudaSuccess ||
+      const size_t kq = (size_t)nq * kmax;
+      if (cudaMemcpyAsync(s->h_arena + off + L.out, d_out, kq * 8 + (size_t)nq * 4, cudaMemcpyDeviceToHost,
+                          sl.stream) != cudaSuccess ||
           cudaLaunchHostFunc(sl.stream, slot_done, new SlotDone{s, slot}) != cudaSuccess)
         st = fail(DG_EDEVICE, "result copy failed");
     }
@@ -269,6 +368,8 @@ static void dispatch_loop(DgServer *s) {
       }
       sl.batch.clear();
       sl.busy = false;
+      cudaStreamSynchronize(sl.stream);  // the region may be read by copies already issued
+      s->arena.give(off);
       --s->in_flight;
       s->cv_done.notify_all();
       s->cv_slot.notify_all();
@@ -322,11 +423,9 @@ DgStatus dg_server_destroy(DgServer *s) {
   for (ServeSlot &sl : s->slots) {
     if (sl.stream) cudaStreamSynchronize(sl.stream);
     if (sl.stream) cudaStreamDestroy(sl.stream);
-    for (void *p : {(void *)sl.h_q, (void *)sl.h_out, (void *)sl.h_beam})
-      if (p) cudaFreeHost(p);
-    for (void *p : {(void *)sl.d_q, (void *)sl.d_out})
-      if (p) cudaFree(p);
   }
+  if (s->h_arena) cudaFreeHost(s->h_arena);
+  if (s->d_arena) cudaFree(s->d_arena);
   for (ServeRequest *r : s->recs) delete r;
   delete s;
   return DG_OK;
@@ -337,26 +436,36 @@ DgStatus dg_server_create(DgIndex *idx, const DgServerConfig *cfg, DgServer **ou
   *out = nullptr;
   if (cfg->max_batch == 0 || cfg->streams == 0 || cfg->max_k == 0)
     return fail(DG_EINVAL, "max_batch, streams and max_k must be >= 1");
-  const size_t slot_bytes = (size_t)cfg->max_batch * (idx->d * 4 + (size_t)cfg->max_k * 8 + 4);
-  if (cfg->hbm_budget_bytes && slot_bytes * cfg->streams > cfg->hbm_budget_bytes)
-    return fail(DG_ENOMEM, "server slots (" + std::to_string(slot_bytes * cfg->streams) +
-                               " bytes) exceed the HBM budget");
+  // arena: the budget, or (without one) room for a full batch at max_k on every stream
+  const size_t full = batch_layout(cfg->max_batch, idx->d, cfg->max_k).bytes;
+  const size_t one = batch_layout(1, idx->d, cfg->max_k).bytes;
+  const size_t arena = cfg->hbm_budget_bytes ? (size_t)cfg->hbm_budget_bytes : full * cfg->streams;
+  if (arena < one)
+    return fail(DG_ENOMEM, "HBM budget (" + std::to_string(arena) + " bytes) below one request at max_k (" +
+                               std::to_string(one) + " bytes)");
   DG_CUDA(cudaSetDevice(idx->device));
   DgServer *s = new (std::nothrow) DgServer();
   if (!s) return fail(DG_ENOMEM, "host allocation failed");
   s->idx = idx;
   s->cfg = *cfg;
+  s->arena.cap = arena;
+  if (cudaMalloc(&s->d_arena, arena) != cudaSuccess || cudaMallocHost(&s->h_arena, arena) != cudaSuccess) {
+    dg_server_destroy(s);
+    return fail(DG_ENOMEM, "server arena allocation failed");
+  }
+  // the index's per-call staging at this server's largest batch, so no batch
+  // reallocates it (and synchronises the device) while others are in flight
+  DgStatus rs = reserve_call_buffers(idx, cfg->max_batch, (size_t)cfg->max_batch * cfg->max_filter_ops,
+                                     (size_t)cfg->max_batch * cfg->max_filter_ops);
+  if (rs != DG_OK) {
+    dg_server_destroy(s);
+    return rs;
+  }
   s->slots.resize(cfg->streams);
   for (ServeSlot &sl : s->slots) {
-    const size_t nq = cfg->max_batch, kq = nq * cfg->max_k;
-    bool ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sl.h_q, nq * idx->d * 4) == cudaSuccess && cudaMalloc(&sl.d_q, nq * idx->d * 4) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sl.h_out, kq * 8 + nq * 4) == cudaSuccess &&
-         cudaMalloc(&sl.d_out, kq * 8 + nq * 4) == cudaSuccess;
-    ok = ok && cudaMallocHost(&sl.h_beam, nq * 4) == cudaSuccess;
-    if (!ok) {
+    if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess) {
       dg_server_destroy(s);
-      return fail(DG_ENOMEM, "server slot allocation failed");
+      return fail(DG_EDEVICE, "server stream creation failed");
     }
   }
   s->dispatcher = std::thread(dispatch_loop, s);

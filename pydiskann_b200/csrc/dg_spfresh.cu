@@ -834,8 +834,9 @@ __device__ __forceinline__ uint16_t f16_exact(float x, bool &ok) {
 // Shared-memory row stride (in FP16 elements) of the converted copies: dk + 8,
 // so that the eight 16-byte rows one ldmatrix reads fall in distinct banks.
 __host__ __device__ inline uint32_t pm_ks(uint32_t d) { return ((d + 15u) & ~15u) + 8u; }
-// Capacity of a pair's k-best list: k rounded up to 32 (at most kPmK).
-__host__ __device__ inline uint32_t pm_kcap(uint32_t k) { return (k + 31u) & ~31u; }
+// Capacity of a pair's k-best list: k rounded up to 16 (at most kPmK), which
+// keeps the scan's shared memory at three CTAs per SM for d = 96, k <= 16.
+__host__ __device__ inline uint32_t pm_kcap(uint32_t k) { return (k + 15u) & ~15u; }
 
 // One CTA (8 warps) per work item at a time: the item's queries and a tile of
 // the posting's entries in shared memory; warp w scores queries w, w+8, ...

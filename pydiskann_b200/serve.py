@@ -42,8 +42,9 @@ class Server:
 
     max_batch requests per launch, `streams` batches in flight, requests up to
     max_k results and max_filter_ops filter ops; a partial batch waits at most
-    max_wait_us for more requests.  Slot buffers are charged against
-    hbm_budget_bytes (0 = no limit).
+    max_wait_us for more requests.  Batches mix k, beams and filters; each
+    batch is admitted by its own memory need into an arena of
+    hbm_budget_bytes (0 = a full batch at max_k per stream).
     """
 
     def __init__(self, index, max_batch=1024, streams=4, max_k=100, max_filter_ops=64, max_wait_us=0,

@@ -649,6 +649,21 @@ class SPFresh:
             codes[b, :n] = self.codes[b]
         return cent, live, lens, ids, codes
 
+    def _block_arrays(self, blocks):
+        """The slots in `blocks` (all below len(live_b)) as DgSpfreshDesc rows."""
+        m = len(blocks)
+        cent = np.ascontiguousarray(self.cent[blocks], dtype=np.float32)
+        live = np.ascontiguousarray(self.live_b[blocks], dtype=np.uint8)
+        lens = np.zeros(m, dtype=np.uint32)
+        ids = np.full((m, self.cap), np.uint64(_lib.PAD64), dtype=np.uint64)
+        codes = np.zeros((m, self.cap, self.codec.size), dtype=np.uint8)
+        for j, b in enumerate(blocks):
+            n = self._len(b)
+            lens[j] = n
+            ids[j, :n] = self.ids[b]
+            codes[j, :n] = self.codes[b]
+        return cent, live, lens, ids, codes
+
     def _sync(self):
         if self.device is None:  # host-only instance (update logic without a GPU mirror)
             return
@@ -657,11 +672,9 @@ class SPFresh:
             return
         if self._dirty:
             blocks = np.array(sorted(self._dirty), dtype=np.uint32)
-            cent, live, lens, ids, codes = self.host_arrays(self._dev_blocks)
-            check(lib().dg_spfresh_update_blocks(
-                self._h, ptr(blocks), len(blocks), ptr(np.ascontiguousarray(cent[blocks])),
-                ptr(np.ascontiguousarray(live[blocks])), ptr(np.ascontiguousarray(lens[blocks])),
-                ptr(np.ascontiguousarray(ids[blocks])), ptr(np.ascontiguousarray(codes[blocks]))))
+            cent, live, lens, ids, codes = self._block_arrays(blocks)
+            check(lib().dg_spfresh_update_blocks(self._h, ptr(blocks), len(blocks), ptr(cent), ptr(live), ptr(lens),
+                                                 ptr(ids), ptr(codes)))
             self._dirty.clear()
         if self.next_id > self._raw_synced:
             rows = np.ascontiguousarray(self.raw[self._raw_synced:self.next_id])

@@ -95,10 +95,52 @@ def test_overlapping_batches_and_submit_wait(qindex, small_data):
         assert np.array_equal(ri, ids[i, : cnt[i]]) and np.array_equal(rd, ds[i, : cnt[i]]) and lat > 0
 
 
+def test_mixed_k_in_one_launch(qindex, small_data):
+    """One batched call carries a k per query (k in {10, 100}, with and
+    without filters): every row equals the query's own search with its k."""
+    _, Q = small_data
+    n = 96
+    k = np.where(np.arange(n) % 2 == 0, 10, 100).astype(np.uint32)
+    filt = [FILTERS[i % 3] if i % 4 == 1 else None for i in range(n)]
+    ids, ds, cnt = qindex.search_arrays(Q[:n], 100, 64, traversal=_lib.TRAVERSE_BF16, filters=filt, per_query_k=k)
+    for i in range(n):
+        ai, ad = _alone(qindex, Q[i], k[i], 64, _lib.TRAVERSE_BF16, 0, filt[i])
+        assert cnt[i] == len(ai) <= k[i]
+        assert np.array_equal(ids[i, : cnt[i]], ai) and np.array_equal(ds[i, : cnt[i]], ad), i
+        assert (ids[i, cnt[i]:] == _lib.PAD).all() and np.isinf(ds[i, cnt[i]:]).all()
+    with pytest.raises(ValueError):
+        qindex.search_arrays(Q[:4], 10, 64, per_query_k=np.array([5, 11, 3, 2]))
+
+
+def test_serving_mixes_k_and_admits_by_memory(qindex, small_data):
+    """A burst of requests with k in {10, 100}: batches mix k (fewer batches
+    than one class per k would need), and under a budget that holds only a few
+    requests at once the dispatcher trims batches to what fits and waits for
+    memory; every result is the request's own search."""
+    _, Q = small_data
+    n = 256
+    Qn = Q[np.arange(n) % len(Q)]
+    k = np.where(np.arange(n) % 2 == 0, 10, 100)
+    with dg.Server(qindex, max_batch=64, streams=2, max_k=100) as srv:
+        out = srv.run_trace(Qn, np.zeros(n), k=k, beam_width=48, traversal=_lib.TRAVERSE_F32)
+        roomy = srv.stats()
+    per_request = 512 + 1024 + 256 + 256  # query, results at k = 100, beam, k (256-byte parts)
+    with dg.Server(qindex, max_batch=64, streams=2, max_k=100, hbm_budget_bytes=6 * per_request) as srv:
+        tight = srv.run_trace(Qn, np.zeros(n), k=k, beam_width=48, traversal=_lib.TRAVERSE_F32)
+        st = srv.stats()
+    assert roomy["served"] == st["served"] == n
+    assert roomy["batches"] <= n // 64 + 2  # k = 10 and k = 100 share launches
+    assert st["batches"] > roomy["batches"]  # trimmed to the budget
+    for res in (out, tight):
+        for i in range(n):
+            ai, ad = _alone(qindex, Qn[i], k[i], 48, _lib.TRAVERSE_F32, 0, None)
+            assert np.array_equal(res["ids"][i], ai) and np.array_equal(res["dists"][i], ad), i
+
+
 def test_server_errors(qindex, small_data):
     _, Q = small_data
-    with pytest.raises(dg.DgError) as e:  # slot buffers above the HBM budget
-        dg.Server(qindex, max_batch=1024, streams=4, hbm_budget_bytes=4096)
+    with pytest.raises(dg.DgError) as e:  # one request at max_k does not fit the budget
+        dg.Server(qindex, max_batch=1024, streams=4, max_k=100, hbm_budget_bytes=1024)
     assert e.value.status == _lib.DG_ENOMEM
     with dg.Server(qindex, max_batch=8, streams=1, max_k=10, max_wait_us=300_000) as srv:
         with pytest.raises(ValueError):
