@@ -213,14 +213,23 @@ DG_API DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const flo
 
 /* Launch-schedule autotuner (no counterpart in the reference): times this
  * exact search -- the caller's parameters and queries (host or device per
- * p->flags) -- with each per-query visited-table size from 2^8 to 2^13 words
- * (the table's shared memory sets how many queries an SM holds; a smaller
- * table recomputes the distances of ids it forgets, never changes results)
- * and keeps the fastest for later searches of the same traversal, working-set
- * capacity and filtering.  ms_per_call[6] (may be NULL) receives the mean time
- * per call of each size, -1 where the size did not fit in shared memory. */
+ * p->flags) -- under candidate launch schedules and keeps the fastest for
+ * later searches of the same traversal, working-set capacity and filtering.
+ * The axes, searched one after another: the per-query visited-table size
+ * from 2^8 to 2^13 words (its shared memory sets how many queries an SM
+ * holds; a smaller table recomputes the distances of ids it forgets), the
+ * order in which the persistent grid takes the queries (as given, or grouped
+ * by nearest pivot row so that queries in one region of the graph run
+ * together and share rows in L2), and the share of the resident CTAs per SM
+ * the grid uses (100, 75, 50 %).  No schedule changes a result.
+ * ms_per_call[6] (may be NULL) receives the mean time per call of each table
+ * size, -1 where the size did not fit in shared memory. */
 DG_API DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const float *queries, uint32_t nq,
                                   uint32_t reps, uint32_t *best_hbits, float *ms_per_call);
+/* The schedule the last dg_index_autotune chose: visited-table bits, query
+ * order (0 = as given, 1 = grouped by nearest pivot) and percent of the
+ * resident CTAs per SM.  No counterpart in the reference. */
+DG_API DgStatus dg_index_tuned_schedule(DgIndex *idx, uint32_t *hbits, uint32_t *order, uint32_t *occ_pct);
 
 /* dg_search_batch for callers that cannot have device memory allocated for
  * them (hosts whose device memory belongs to a separate pool manager,
@@ -397,6 +406,13 @@ DG_API DgStatus dg_pq_train(const float *X, uint64_t n, uint32_t dim, uint32_t M
 /* ProductQuantizer::encode (src/pq.rs:122-149) on the GPU. */
 DG_API DgStatus dg_pq_encode(const float *X, uint64_t n, uint32_t dim, uint32_t M, uint32_t K,
                       const float *codebooks, int32_t device, uint8_t *out_codes);
+/* RaBitQ::encode_with (src/rabitq.rs:218-256) on the GPU: codes of
+ * padded/8+8 bytes of every row of X as residuals against `centroid`
+ * (f32[dim]), with the quantizer's signs f32[3*padded].  SPFresh re-encodes
+ * the entries of a posting against its new centroid with it
+ * (Inner::encode, src/spfresh.rs:328-339). */
+DG_API DgStatus dg_rabitq_encode(const float *X, uint64_t n, uint32_t dim, uint32_t padded, const float *centroid,
+                                 const float *signs, int32_t device, uint8_t *out_codes);
 /* The FP8 encoding of dg_index_enable_fp8 on the GPU: codes u8[n*dim] (e4m3)
  * and scales f32[n].  No counterpart in the reference. */
 DG_API DgStatus dg_fp8_encode(const float *X, uint64_t n, uint32_t dim, int32_t device, uint8_t *out_codes,

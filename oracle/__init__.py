@@ -429,3 +429,73 @@ def spfresh_search(view: Spfresh, Q, k, nprobe, threads=0):
     lib().dgo_spfresh_search_batch(C.byref(view), _p(Q), nq, k, nprobe, _p(ids), _p(ds), _p(cnt),
                                    threads)
     return ids, ds, cnt
+
+
+def _draw(seed, a, b, c, n):
+    """floor(rand * n / 2^64): a uniform draw in [0, n) from the shared stream."""
+    return (rand(seed, a, b, c) * n) >> 64
+
+
+def pq_train(X, M, K, iterations, sample, seed):
+    """ProductQuantizer::train (src/pq.rs:51-119, 290-410) with the product's
+    seeded draws instead of thread_rng: a training sample of `sample` distinct
+    rows by a partial Fisher-Yates shuffle (stream 0x7371), per subspace
+    k-means++ seeding -- first centre from stream 0x6b6c, then D^2-weighted
+    draws (stream 0x6b6d; an all-zero weight draws uniformly from 0x6b6e) --
+    then `iterations` Lloyd steps: each row to its nearest centre (squared L2
+    summed in coordinate order in f32, the first centre on ties), each centre
+    to the f64 mean of its rows rounded to f32, an empty centre to a row drawn
+    from stream 0x6b6f + iteration.  Codebooks f32[M, K, d/M]."""
+    X = _f32(X)
+    n, d = X.shape
+    ds = d // M
+    if sample > 0 and n > sample:
+        perm = list(range(n))
+        for i in range(sample):
+            j = i + _draw(seed, 0x7371, i, 0, n - i)
+            perm[i], perm[j] = perm[j], perm[i]
+        rows = perm[:sample]
+    else:
+        rows = list(range(n))
+    S = X[rows]
+    ns = len(S)
+    cb = np.zeros((M, K, ds), dtype=np.float32)
+
+    def sqdist(x, c):  # x [r, ds], c [k, ds] -> f32 [r, k], sequential over ds
+        acc = np.zeros((x.shape[0], c.shape[0]), dtype=np.float32)
+        for j in range(ds):
+            t = (x[:, j:j + 1] - c[None, :, j]).astype(np.float32)
+            acc = (acc + (t * t).astype(np.float32)).astype(np.float32)
+        return acc
+
+    keff = min(K, ns)
+    for m in range(M):
+        Sm = S[:, m * ds:(m + 1) * ds]
+        cb[m, 0] = Sm[_draw(seed, 0x6b6c, m, 0, ns)]
+        mind = np.full(ns, np.float32(3.402823466e38), dtype=np.float32)
+        for c in range(1, keff):
+            mind = np.minimum(mind, sqdist(Sm, cb[m, c - 1:c])[:, 0])
+            tot = float(np.sum(mind.astype(np.float64)))
+            if tot <= 0.0:
+                chosen = _draw(seed, 0x6b6e, m, c, ns)
+            else:
+                u = (rand(seed, 0x6b6d, m, c) >> 11) * (1.0 / 9007199254740992.0)
+                cum = np.cumsum(mind.astype(np.float64))
+                hit = np.nonzero(cum >= u * tot)[0]
+                chosen = int(hit[0]) if len(hit) else ns - 1
+            cb[m, c] = Sm[chosen]
+        for c in range(keff, K):
+            cb[m, c] = cb[m, c % keff]
+    for it in range(iterations):
+        for m in range(M):
+            Sm = S[:, m * ds:(m + 1) * ds]
+            a = np.argmin(sqdist(Sm, cb[m]), axis=1)
+            new = cb[m].copy()
+            for c in range(K):
+                sel = Sm[a == c]
+                if len(sel):
+                    new[c] = (sel.astype(np.float64).sum(0) / len(sel)).astype(np.float32)
+                else:
+                    new[c] = Sm[_draw(seed, 0x6b6f + it, m, c, ns)]
+            cb[m] = new
+    return cb

@@ -124,6 +124,20 @@ def pq_encode(vectors, codebooks, device=0) -> np.ndarray:
     return codes
 
 
+def rabitq_encode(vectors, centroid, signs, padded=None, device=0):
+    """RaBitQ::encode_with (src/rabitq.rs:218-256) on the GPU: residual codes of
+    the rows against `centroid` (u8[n, padded/8 + 8])."""
+    X = _f32(vectors)
+    n, d = X.shape
+    P = padded or rabitq_padded(d)
+    cen = np.ascontiguousarray(centroid, dtype=np.float32).reshape(-1)
+    sg = np.ascontiguousarray(signs, dtype=np.float32).reshape(-1)
+    codes = np.empty((n, P // 8 + 8), dtype=np.uint8)
+    B = _lib.builder()
+    check(B.dg_rabitq_encode(ptr(X), n, d, P, ptr(cen), ptr(sg), device, ptr(codes)), B)
+    return codes
+
+
 def fp8_encode(vectors, device=0):
     """(codes u8[n, d] e4m3, scales f32[n]) as the FP8 traversal stores them."""
     X = _f32(vectors)
@@ -466,16 +480,21 @@ class _Index:
 
     def autotune(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32, rerank_size=0, filters=None,
                  per_query_beam=None, reps=3):
-        """Times this search (same arguments as search_arrays) with each
-        visited-table size and keeps the fastest for later searches of the same
-        kind (dg_index_autotune).  Returns {"hbits": chosen, "ms": {bits: ms per call}}."""
+        """Times this search (same arguments as search_arrays) under candidate
+        launch schedules -- visited-table size, query order, CTAs per SM -- and
+        keeps the fastest for later searches of the same kind
+        (dg_index_autotune).  Returns {"hbits", "order", "occ_pct": the chosen
+        schedule, "ms": {bits: ms per call of each table size}}."""
         p, Q, nq, _, _, keep = self._params(queries, k, beam_width, traversal, rerank_size, filters,
                                             per_query_beam, None, None, False)
         best = C.c_uint32()
         ms = (C.c_float * 6)()
         check(lib().dg_index_autotune(self._h, C.byref(p), ptr(Q), nq, reps, C.byref(best), ms))
         del keep
-        return {"hbits": best.value, "ms": {8 + i: round(ms[i], 4) for i in range(6) if ms[i] >= 0}}
+        hb, order, occ = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().dg_index_tuned_schedule(self._h, C.byref(hb), C.byref(order), C.byref(occ)))
+        return {"hbits": hb.value, "order": order.value, "occ_pct": occ.value,
+                "ms": {8 + i: round(ms[i], 4) for i in range(6) if ms[i] >= 0}}
 
     # -- reference-shaped helpers
     def _rows(self, ids, dists, cnt):

@@ -99,6 +99,7 @@ def _signatures():
         "dg_index_attach_labels": (st, [vp, u32, vp]),
         "dg_index_get_codes": (st, [vp, vp, u64, vp]),
         "dg_index_autotune": (st, [vp, vp, vp, u32, u32, vp, vp]),
+        "dg_index_tuned_schedule": (st, [vp, vp, vp, vp]),
         "dg_index_set_entry_points": (st, [vp, vp, u32]),
         "dg_index_set_code_limit": (st, [vp, u64]),
         "dg_index_set_tombstones": (st, [vp, vp, u64, i32, u64]),
@@ -124,6 +125,7 @@ def _signatures():
         "dg_pq_train": (st, [vp, u64, u32, u32, u32, u32, u64, u64, i32, vp]),
         "dg_pq_encode": (st, [vp, u64, u32, u32, u32, vp, i32, vp]),
         "dg_fp8_encode": (st, [vp, u64, u32, i32, vp, vp]),
+        "dg_rabitq_encode": (st, [vp, u64, u32, u32, vp, vp, i32, vp]),
         "dg_exact_knn": (st, [vp, u64, u32, vp, u32, u32, i32, i32, vp, vp]),
         "dg_last_error": (C.c_char_p, []),
         "dg_version": (i32, []),
@@ -136,8 +138,8 @@ EXPORTED = tuple(_signatures().keys())
 # libdgbuild.so (medoid, Vamana build, PQ training and encodes, exact kNN):
 # a process that only prepares an index loads that library, not the search
 # library.
-BUILDER = ("dg_medoid", "dg_build_vamana", "dg_pq_train", "dg_pq_encode", "dg_fp8_encode", "dg_exact_knn",
-           "dg_last_error", "dg_version")
+BUILDER = ("dg_medoid", "dg_build_vamana", "dg_pq_train", "dg_pq_encode", "dg_fp8_encode", "dg_rabitq_encode",
+           "dg_exact_knn", "dg_last_error", "dg_version")
 BUILD_LIB_PATH = os.environ.get("DGANN_BUILD_LIBRARY", os.path.join(HERE, "libdgbuild.so"))
 
 _lib = None

@@ -447,20 +447,30 @@ static uint32_t tune_key(int trav, int lcap, bool filt) {
   return ((uint32_t)trav << 20) | ((uint32_t)lcap << 1) | (filt ? 1u : 0u);
 }
 
-static uint32_t visited_bits(DgIndex *idx, int trav, int lcap, bool filt, uint32_t maxL) {
-  uint32_t hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
+// The launch schedule of this kind of search: the autotuner's choice, or the
+// defaults (a visited table sized by the beam, queries as given, every
+// resident CTA); DG_HBITS, DG_ORDER and DG_OCC_PCT override each axis.
+static DgIndex::Schedule schedule_of(DgIndex *idx, int trav, int lcap, bool filt, uint32_t maxL) {
+  DgIndex::Schedule sc;
+  sc.hbits = maxL <= 64 ? 10 : maxL <= 128 ? 11 : 12;
   {
     std::lock_guard<std::mutex> lk(idx->mu);
-    if (idx->hbits_force > 0) {
-      hbits = (uint32_t)idx->hbits_force;
+    if (idx->forcing) {
+      sc = idx->force;
       idx->last_key = tune_key(trav, lcap, filt);
     } else {
-      auto it = idx->tuned_hbits.find(tune_key(trav, lcap, filt));
-      if (it != idx->tuned_hbits.end()) hbits = it->second;
+      auto it = idx->tuned.find(tune_key(trav, lcap, filt));
+      if (it != idx->tuned.end()) sc = it->second;
     }
   }
-  if (const char *e = std::getenv("DG_HBITS")) hbits = (uint32_t)std::max(6, std::min(14, atoi(e)));
-  return hbits;
+  if (const char *e = std::getenv("DG_HBITS")) sc.hbits = (uint32_t)std::max(6, std::min(14, atoi(e)));
+  if (const char *e = std::getenv("DG_ORDER")) sc.order = atoi(e) != 0;
+  if (const char *e = std::getenv("DG_OCC_PCT")) sc.occ_pct = (uint32_t)std::max(1, std::min(100, atoi(e)));
+  return sc;
+}
+
+static uint32_t visited_bits(DgIndex *idx, int trav, int lcap, bool filt, uint32_t maxL) {
+  return schedule_of(idx, trav, lcap, filt, maxL).hbits;
 }
 
 static void index_state(const DgIndex *idx, SearchArgs &a) {
@@ -604,10 +614,12 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   int lcap = need <= 64 ? 64 : need <= 256 ? 256 : need <= 1024 ? 1024 : 0;
   if (!lcap) return fail(DG_ENOTSUP, "beam width / expanded beam above 1024 is not supported");
   if (reranked && !filt && search_k > 1024) return fail(DG_ENOTSUP, "rerank size above 1024");
-  // visited table: 2^hbits words as buckets of eight 16-bit tags (about 3
-  // tags per visited node at these beams), or the size dg_index_autotune measured
-  // fastest for this kind of search; DG_HBITS overrides both
-  const uint32_t hbits = visited_bits(idx, trav, lcap, filt, maxL);
+  // launch schedule: visited table of 2^hbits words as buckets of eight
+  // 16-bit tags (about 3 tags per visited node at these beams), query order
+  // and CTAs per SM, as dg_index_autotune measured fastest for this kind of
+  // search (defaults otherwise); DG_HBITS overrides the table size
+  const DgIndex::Schedule sched = schedule_of(idx, trav, lcap, filt, maxL);
+  const uint32_t hbits = sched.hbits;
   uint32_t hB = 1;
   while (hB < 32 && (1ull << hB) < idx->n) ++hB;
   hB = std::max(hB, hbits);
@@ -702,6 +714,20 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
     }
   }
   a.counter = sl.counter;
+  a.occ_pct = sched.occ_pct;
+  // query order: grouped by nearest pivot (per pipeline chunk) when the
+  // schedule asks for it and the pivots fit the ordering kernel
+  const bool ordered = sched.order && (size_t)pivot_count(idx->dpad) * idx->d * 4 <= 48 * 1024;
+  // scratch: perm [nq] | pivot of each query [nq] | bin counts [pipeline chunk][npiv]
+  uint32_t *perm = nullptr, *obin = nullptr, *ohist = nullptr;
+  if (ordered) {
+    if ((s = ensure_pivots(idx)) != DG_OK) return s;
+    if ((s = buf_reserve(sl.sched, ((size_t)2 * nq + (size_t)DgIndex::kPipeChunks * idx->npiv) * 4)) != DG_OK)
+      return s;
+    perm = (uint32_t *)sl.sched.p;
+    obin = perm + nq;
+    ohist = obin + nq;
+  }
 
   const int met = met_kind(idx->metric);
   int lpr = 1;
@@ -711,8 +737,15 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded,
                                     (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2);
-  auto launch = [&](const SearchArgs &aa, cudaStream_t ss) -> DgStatus {
+  auto launch = [&](const SearchArgs &a0, cudaStream_t ss) -> DgStatus {
     LaunchInfo info;
+    SearchArgs aa = a0;
+    if (ordered) {  // positions of this launch's queries (relative to aa.Q); chunk c counts with counter c
+      const size_t q0 = (size_t)(aa.Q - a.Q) / idx->d, c = (size_t)(aa.counter - a.counter);
+      DgStatus so = order_queries(idx, aa.Q, aa.nq, perm + q0, obin + q0, ohist + c * idx->npiv, ss);
+      if (so != DG_OK) return so;
+      aa.perm = perm + q0;
+    }
     DG_CUDA(cudaMemsetAsync(aa.counter, 0, 4, ss));
     switch (trav) {
       case TRAV_F32: return launch_search_f32(aa, Ly, met, lpr, lcap, filt, ss, &info);
@@ -818,47 +851,83 @@ DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const float *q
   DgSearchParams pp = *p;
   pp.flags = p->flags | DG_FLAG_DEVICE_PTRS | DG_FLAG_STREAM;
   pp.stream = sc.st;
-  float best_ms = 0.0f;
-  uint32_t best = 0, key = 0;
-  DgStatus result = DG_OK;
-  for (uint32_t hb = kTuneMinBits; hb <= kTuneMaxBits; ++hb) {
-    if (ms_per_call) ms_per_call[hb - kTuneMinBits] = -1.0f;
+  auto run = [&]() {
+    return dg_search_batch(idx, &pp, dq, nq, (uint32_t *)sc.p[1], (float *)sc.p[2], (uint32_t *)sc.p[3], nullptr);
+  };
+  // mean time per call of one schedule (a warm-up call first); DG_ENOTSUP when
+  // it does not fit (a visited table too large for shared memory)
+  auto time_schedule = [&](const DgIndex::Schedule &c, float *ms) -> DgStatus {
     {
       std::lock_guard<std::mutex> lk(idx->mu);
-      idx->hbits_force = (int)hb;
+      idx->forcing = true;
+      idx->force = c;
     }
-    auto run = [&]() {
-      return dg_search_batch(idx, &pp, dq, nq, (uint32_t *)sc.p[1], (float *)sc.p[2], (uint32_t *)sc.p[3],
-                             nullptr);
-    };
-    DgStatus s = run();  // warm-up; a table that does not fit in shared memory is skipped
-    if (s == DG_OK) {
-      cudaEventRecord(sc.e[0], sc.st);
-      for (uint32_t r = 0; r < reps && s == DG_OK; ++r) s = run();
-      cudaEventRecord(sc.e[1], sc.st);
+    DgStatus s = run();
+    if (s != DG_OK) return s;
+    cudaEventRecord(sc.e[0], sc.st);
+    for (uint32_t r = 0; r < reps && s == DG_OK; ++r) s = run();
+    cudaEventRecord(sc.e[1], sc.st);
+    if (s != DG_OK) return s;
+    DG_CUDA(cudaEventSynchronize(sc.e[1]));
+    DG_CUDA(cudaEventElapsedTime(ms, sc.e[0], sc.e[1]));
+    *ms /= (float)reps;
+    return DG_OK;
+  };
+  DgIndex::Schedule best{};
+  float best_ms = 0.0f;
+  bool have = false;
+  uint32_t key = 0;
+  DgStatus result = DG_OK;
+  auto consider = [&](const DgIndex::Schedule &c, float *ms_out) -> DgStatus {
+    float ms = 0.0f;
+    const DgStatus s = time_schedule(c, &ms);
+    if (s == DG_ENOTSUP) return DG_OK;
+    if (s != DG_OK) return s;
+    if (ms_out) *ms_out = ms;
+    if (!have || ms < best_ms) {
+      have = true;
+      best = c;
+      best_ms = ms;
+      std::lock_guard<std::mutex> lk(idx->mu);
+      key = idx->last_key;
     }
-    if (s == DG_OK && cudaEventSynchronize(sc.e[1]) == cudaSuccess) {
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, sc.e[0], sc.e[1]);
-      ms /= (float)reps;
-      if (ms_per_call) ms_per_call[hb - kTuneMinBits] = ms;
-      if (!best || ms < best_ms) {
-        best = hb;
-        best_ms = ms;
-        std::lock_guard<std::mutex> lk(idx->mu);
-        key = idx->last_key;
-      }
-    } else if (s != DG_ENOTSUP) {
-      result = s;
-      break;
-    }
+    return DG_OK;
+  };
+  // coordinate search: the visited-table size (queries as given, every
+  // resident CTA), then the query order, then the CTAs per SM
+  for (uint32_t hb = kTuneMinBits; hb <= kTuneMaxBits && result == DG_OK; ++hb) {
+    if (ms_per_call) ms_per_call[hb - kTuneMinBits] = -1.0f;
+    DgIndex::Schedule c;
+    c.hbits = hb;
+    result = consider(c, ms_per_call ? ms_per_call + (hb - kTuneMinBits) : nullptr);
+  }
+  if (result == DG_OK && have) {
+    DgIndex::Schedule c = best;
+    c.order = 1;
+    result = consider(c, nullptr);
+  }
+  for (uint32_t pct : {75u, 50u}) {
+    if (result != DG_OK || !have) break;
+    DgIndex::Schedule c = best;
+    c.occ_pct = pct;
+    result = consider(c, nullptr);
   }
   std::lock_guard<std::mutex> lk(idx->mu);
-  idx->hbits_force = 0;
+  idx->forcing = false;
   if (result != DG_OK) return result;
-  if (!best) return fail(DG_ENOTSUP, "no visited-table size fits this search");
-  idx->tuned_hbits[key] = best;
-  if (best_hbits) *best_hbits = best;
+  if (!have) return fail(DG_ENOTSUP, "no visited-table size fits this search");
+  idx->tuned[key] = best;
+  idx->last_tuned = best;
+  if (best_hbits) *best_hbits = best.hbits;
+  return DG_OK;
+}
+
+DgStatus dg_index_tuned_schedule(DgIndex *idx, uint32_t *hbits, uint32_t *order, uint32_t *occ_pct) {
+  if (!idx) return fail(DG_EINVAL, "null index");
+  std::lock_guard<std::mutex> lk(idx->mu);
+  if (hbits) *hbits = idx->last_tuned.hbits;
+  if (order) *order = idx->last_tuned.order;
+  if (occ_pct) *occ_pct = idx->last_tuned.occ_pct;
   return DG_OK;
 }
 

@@ -651,6 +651,37 @@ DgStatus dg_pq_encode(const float *X, uint64_t n, uint32_t dim, uint32_t M, uint
   return s;
 }
 
+DgStatus dg_rabitq_encode(const float *X, uint64_t n, uint32_t dim, uint32_t padded, const float *centroid,
+                          const float *signs, int32_t device, uint8_t *out_codes) {
+  if (!X || !centroid || !signs || !out_codes) return fail(DG_EINVAL, "null argument");
+  if (padded < 64 || (padded & (padded - 1)) || padded < dim) return fail(DG_EINVAL, "bad padded dimension");
+  if (n == 0) return DG_OK;
+  DG_CUDA(cudaSetDevice(device));
+  const uint32_t dpad = dpad_of(dim), cs = padded / 8 + 8;
+  cudaStream_t st;
+  DG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  float *v = nullptr, *cen = nullptr, *sg = nullptr;
+  uint8_t *codes = nullptr;
+  DgStatus s = DG_OK;
+  if (cudaMallocAsync(&v, n * dpad * 4, st) != cudaSuccess || cudaMallocAsync(&cen, (size_t)dim * 4, st) != cudaSuccess ||
+      cudaMallocAsync(&sg, (size_t)3 * padded * 4, st) != cudaSuccess ||
+      cudaMallocAsync(&codes, n * cs, st) != cudaSuccess)
+    s = fail(DG_ENOMEM, "rabitq encode staging");
+  if (s == DG_OK) s = upload_rows_f32(X, n, dim, dpad, v, st);
+  if (s == DG_OK && (cudaMemcpyAsync(cen, centroid, (size_t)dim * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                     cudaMemcpyAsync(sg, signs, (size_t)3 * padded * 4, cudaMemcpyHostToDevice, st) != cudaSuccess))
+    s = fail(DG_EDEVICE, "rabitq parameter upload");
+  if (s == DG_OK) s = encode_rabitq_device(v, n, dim, dpad, padded, cen, sg, codes, cs, st);
+  if (s == DG_OK && cudaMemcpyAsync(out_codes, codes, n * cs, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    s = fail(DG_EDEVICE, "code download");
+  cudaStreamSynchronize(st);
+  for (void *p : {(void *)v, (void *)cen, (void *)sg, (void *)codes})
+    if (p) cudaFreeAsync(p, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return s;
+}
+
 DgStatus dg_pq_train(const float *X, uint64_t n, uint32_t dim, uint32_t M, uint32_t K,
                      uint32_t iterations, uint64_t sample, uint64_t seed, int32_t device,
                      float *out_codebooks) {

@@ -39,11 +39,20 @@ struct DgIndex {
   std::vector<uint32_t> tomb_host;     // its host copy
   uint64_t ntomb = 0;                  // tombstone count the search config uses
   uint64_t code_limit = 0;             // rows >= code_limit have no codes (0 = every row has)
-  // visited-table size (log2 words per query) chosen by dg_index_autotune per
-  // (traversal, working-set capacity, filtered); hbits_force > 0 pins it while tuning
-  std::map<uint32_t, uint32_t> tuned_hbits;
-  int hbits_force = 0;
-  uint32_t last_key = 0;  // key of the last search run with hbits_force set
+  // Launch schedule of a kind of search (traversal, working-set capacity,
+  // filtered), chosen by dg_index_autotune: the visited-table size (log2 words
+  // per query), the query order (0 = as given, 1 = grouped by nearest pivot)
+  // and the share of the resident CTAs per SM the grid uses (percent).
+  struct Schedule {
+    uint32_t hbits = 0, order = 0, occ_pct = 100;
+  };
+  std::map<uint32_t, Schedule> tuned;
+  bool forcing = false;   // the autotuner pins `force` while it times a candidate
+  Schedule force{};
+  uint32_t last_key = 0;  // key of the last search run while forcing
+  Schedule last_tuned{};  // the schedule the last dg_index_autotune chose
+  float *pivots = nullptr;  // [npiv][dpad] rows spread over the ids (query ordering)
+  uint32_t npiv = 0;
   cudaStream_t stream = nullptr;
   uint64_t hbm_budget = 0, hbm_used = 0;
   std::mutex mu;
@@ -55,7 +64,7 @@ struct DgIndex {
     size_t cap = 0;
   };
   struct Slot {
-    Buf q, ids, dists, cnt, stats, fops, foffs, fpool, perl, perk;
+    Buf q, ids, dists, cnt, stats, fops, foffs, fpool, perl, perk, sched;
     uint32_t *counter = nullptr;  // work counters of the persistent grid (one per pipeline chunk)
     cudaEvent_t done = nullptr;
     bool pending = false;
@@ -80,6 +89,13 @@ DgStatus buf_reserve(DgIndex::Buf &b, size_t bytes);
 // Sizes the per-call staging buffers of every call slot for batches of nq
 // queries with `ops` filter instructions and `pool` IN values.
 DgStatus reserve_call_buffers(DgIndex *idx, uint32_t nq, size_t ops, size_t pool);
+// Query ordering by nearest pivot (dg_schedule.cu): pivots are set up once;
+// order_queries writes perm[nq] (positions -> query ids) using bin[nq] and
+// hist[npiv] as scratch.
+uint32_t pivot_count(uint32_t dpad);
+DgStatus ensure_pivots(DgIndex *idx);
+DgStatus order_queries(const DgIndex *idx, const float *Q, uint32_t nq, uint32_t *perm, uint32_t *bin,
+                       uint32_t *hist, cudaStream_t st);
 DgStatus to_device(DgIndex *idx, void **dst, const void *src, size_t bytes);
 // Rows of d floats from the host into [n][dpad] device rows, zero padded.
 DgStatus upload_rows_f32(const float *host, uint64_t n, uint32_t d, uint32_t dpad, float *dev,

@@ -1,5 +1,6 @@
 // dg_launch.cuh -- host-side launch of the beam-search kernel instantiations.
 #pragma once
+#include <algorithm>
 #include <mutex>
 #include <unordered_map>
 
@@ -69,6 +70,7 @@ DgStatus launch_persistent(K kernel, const SearchArgs &a, const WarpLayout &Ly, 
     nb = n_it->second;
   }
   if (nb <= 0) return fail(DG_ENOTSUP, "search kernel cannot be resident on an SM");
+  if (a.occ_pct > 0 && a.occ_pct < 100) nb = std::max(1, (int)((nb * a.occ_pct + 99) / 100));
   int grid = nb * sms;
   const int need = (int)((a.nq + 3) / 4);
   if (grid > need) grid = need;

@@ -77,6 +77,8 @@ struct SearchArgs {
   uint32_t *out_cnt;
   uint32_t *out_stats;
   uint32_t *counter;  // work counter, zero at launch
+  const uint32_t *perm;  // order in which the grid takes the queries (null = as given)
+  uint32_t occ_pct;      // share of the resident CTAs per SM the grid uses (percent; 0 = all)
 };
 
 enum TravKind { TRAV_F32 = 0, TRAV_BF16 = 1, TRAV_PQ = 2, TRAV_INT8 = 3, TRAV_RABITQ = 4, TRAV_F16 = 5, TRAV_FP8 = 6 };

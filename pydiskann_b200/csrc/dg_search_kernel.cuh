@@ -621,6 +621,7 @@ __global__ void __launch_bounds__(128, DG_SEARCH_MIN_BLOCKS) beam_search_kernel(
     if (lane == 0) q = atomicAdd(a.counter, 1u);
     q = __shfl_sync(kFull, q, 0);
     if (q >= a.nq) break;
+    if (a.perm) q = __ldg(a.perm + q);
     if (LCAP == 64 && !FILT)
       search_one_reg<TRAV, MET, LPR, LPRF>(a, q, wsm, Ly, lane);
     else

@@ -92,8 +92,9 @@ def _fht(v):
 class _Codec:
     """Code of a vector stored in a posting (Inner::encode, src/spfresh.rs:328-339)."""
 
-    def __init__(self, kind, dim, params):
+    def __init__(self, kind, dim, params, device=None):
         self.kind, self.dim, self.p = kind, dim, params
+        self.device = device  # RaBitQ residual codes are encoded on this GPU (None: on the host)
         if kind is None:
             self.size = 4 * dim
         elif kind == "f16":
@@ -129,6 +130,10 @@ class _Codec:
                 out[:, m] = d.argmin(1)
             return out
         # RaBitQ residual code against the posting centroid (src/rabitq.rs:218-256)
+        if self.device is not None:
+            import pydiskann_b200 as dg
+
+            return dg.rabitq_encode(V, centroid, self.p["signs"], self.p["padded"], self.device)
         P, signs = self.p["padded"], self.p["signs"].reshape(3, -1)
         r = np.zeros((len(V), P), dtype=np.float32)
         r[:, : self.dim] = V - centroid
@@ -179,7 +184,7 @@ class SPFresh:
         if metric not in _METRICS:
             raise ValueError(f"unknown metric: {metric}")
         self.dim, self.metric_name, self.metric = dim, metric, _METRICS[metric]
-        self.codec = _Codec(quantizer, dim, qparams or {})
+        self.codec = _Codec(quantizer, dim, qparams or {}, device)
         self.rerank_size, self.max_posting, self.min_posting = rerank_size, max_posting_size, min_posting_size
         self.reassign_neighbors, self.probe_ratio, self.device = reassign_neighbors, probe_ratio, device
         self.cap = 2 * max_posting_size  # block layout, src/spfresh.rs:109-111
@@ -446,19 +451,28 @@ class SPFresh:
         ids, codes = self._live_entries(frm)
         keep = np.array([int(i) not in mv for i in ids], dtype=bool)
         self._rewrite(frm, ids[keep], codes[keep])
-        for id_, code in zip(ids[~keep], codes[~keep]):
+        dest, added = [], {}  # target of each moved entry; entries pushed to a slot so far
+        for id_ in ids[~keep]:
             t = mv[int(id_)]
-            if not (self._is_live(t) and self._len(t) < 2 * self.max_posting):
+            if not (self._is_live(t) and self._len(t) + added.get(t, 0) < 2 * self.max_posting):
                 if frm not in queue:
                     queue.insert(0, frm)
                 if self._is_live(t):
                     queue.append(t)
                 t = frm
-            if self.codec.residual:
-                code = self._encode(self.raw[int(id_)], t)
-            self._push(t, int(id_), code)
-            if self._len(t) >= self.max_posting:
+            dest.append(t)
+            added[t] = added.get(t, 0) + 1
+            if self._len(t) + added[t] >= self.max_posting:
                 queue.append(t)
+        moved = codes[~keep]
+        if self.codec.residual and len(dest):  # re-encoded against the target's centroid, one call per target
+            moved = moved.copy()
+            dest_a = np.array(dest)
+            for t in np.unique(dest_a):
+                sel = np.nonzero(dest_a == t)[0]
+                moved[sel] = self.codec.encode(self.raw[ids[~keep][sel].astype(np.int64)], self.cent[t])
+        for id_, code, t in zip(ids[~keep], moved, dest):
+            self._push(t, int(id_), code)
 
     def _split(self, b, queue):
         # Splits converge for metric distances; a score such as 1 - dot on
@@ -475,11 +489,14 @@ class SPFresh:
         c1, c2, side = kmeans2(vs, self.metric)
         self._free_posting(b)
         nb = [self._new_posting(c1), self._new_posting(c2)]
+        if self.codec.residual:  # re-encoded against the new centroids, one call per new posting
+            codes = codes.copy()
+            for sd in (False, True):
+                sel = np.nonzero(side == sd)[0]
+                if len(sel):
+                    codes[sel] = self.codec.encode(vs[sel], self.cent[nb[int(sd)]])
         for id_, code, sd in zip(ids, codes, side):
-            t = nb[int(sd)]
-            if self.codec.residual:
-                code = self._encode(self.raw[int(id_)], t)
-            self._push(t, int(id_), code)
+            self._push(nb[int(sd)], int(id_), code)
         around = sorted({q for p in nb for q in self._neighbourhood(p)})
         for p in nb:
             self._relocate(p, self._local_moves(p, around), queue)

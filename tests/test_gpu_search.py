@@ -92,6 +92,19 @@ def test_pq_codes_and_search_match_oracle(oracle, small_data, small_graph):
     q.close()
 
 
+@pytest.mark.parametrize("sample,iters", [(2500, 4), (0, 3)])
+def test_pq_training_matches_oracle(oracle, small_data, sample, iters):
+    """The GPU k-means (sample, k-means++ seeding, Lloyd steps with f64 centre
+    sums) equals the oracle's restatement of ProductQuantizer::train
+    (src/pq.rs:290-410) from the same seed, codebooks bit for bit on
+    integer-valued data (every sum is exact)."""
+    X, _ = small_data
+    got = dg.pq_train(X, num_subspaces=16, num_centroids=256, kmeans_iterations=iters,
+                      training_sample_size=sample, seed=4)
+    want = oracle.pq_train(X, 16, 256, iters, sample, 4)
+    assert np.array_equal(got, want), np.argwhere(got != want)[:5]
+
+
 def test_int8_codes_and_search_match_oracle(oracle, small_data, small_graph):
     X, Q = small_data
     adj, med = small_graph
@@ -359,14 +372,50 @@ def test_autotune_keeps_results(oracle, small_data, small_graph):
         assert 8 <= t["hbits"] <= 13 and t["hbits"] in t["ms"] and len(t["ms"]) >= 3
         assert_same(q.search_arrays(Q, 10, 48, rerank_size=24, **kw),
                     o.search(Q, 10, 48, rerank=24, use_codes=True, **okw))
-    for hb in (8, 13):  # the extremes, forced: identical results
-        import os
-        os.environ["DG_HBITS"] = str(hb)
+    import os
+
+    # every schedule axis at its extremes, forced: identical results, with
+    # per-query beams and filters riding along with the reordered queries
+    beams = np.random.default_rng(2).integers(8, 64, len(Q)).astype(np.uint32)
+    filt = [FILTERS[i % len(FILTERS)] for i in range(len(Q))]
+    want_b = o.search(Q, 10, 48, rerank=24, use_codes=True, per_query_L=beams)
+    for env in ({"DG_HBITS": "8"}, {"DG_HBITS": "13"}, {"DG_ORDER": "1"}, {"DG_ORDER": "1", "DG_HBITS": "8"},
+                {"DG_OCC_PCT": "50"}, {"DG_OCC_PCT": "75", "DG_ORDER": "1"}):
+        os.environ.update(env)
         try:
             assert_same(q.search_arrays(Q, 10, 48, rerank_size=24), o.search(Q, 10, 48, rerank=24, use_codes=True))
+            assert_same(q.search_arrays(Q, 10, 48, rerank_size=24, per_query_beam=beams), want_b)
+            got = q.search_arrays(Q, 10, 48, rerank_size=24, filters=filt)
+            for i in range(0, len(Q), 7):
+                fo, fp = filt[i].program()
+                wi, wd, wc = o.search(Q[i:i + 1], 10, 48, rerank=24, use_codes=True, filter_ops=fo, filter_pool=fp)
+                assert got[2][i] == wc[0] and np.array_equal(got[0][i], wi[0]) and np.array_equal(got[1][i], wd[0])
         finally:
-            del os.environ["DG_HBITS"]
+            for k_ in env:
+                del os.environ[k_]
     q.close()
+
+
+def test_autotune_schedule_axes(oracle, small_data, small_graph):
+    """The tuner's choice covers the three axes (table size, query order,
+    CTAs per SM) and a device-pointer search of 3000 queries after tuning --
+    ordered or not -- returns the oracle's results."""
+    import torch
+
+    X, Q = small_data
+    adj, med = small_graph
+    ix = dg.DiskANN.from_graph(X, adj, med)
+    ix.enable_bf16()
+    Qb = np.concatenate([Q] * 15)
+    t = ix.autotune(Qb, 10, 40, traversal=_lib.TRAVERSE_BF16, rerank_size=40, reps=2)
+    assert 8 <= t["hbits"] <= 13 and t["order"] in (0, 1) and t["occ_pct"] in (50, 75, 100)
+    o = oracle.OracleIndex(X, adj, med)
+    o.set_bf16()
+    want = o.search(Qb, 10, 40, rerank=40, use_codes=True)
+    got = ix.search_arrays(torch.from_numpy(Qb).cuda(), 10, 40, traversal=_lib.TRAVERSE_BF16, rerank_size=40)
+    assert_same(tuple(g.cpu().numpy().view(np.uint32) if g.dtype != torch.float32 else g.cpu().numpy()
+                      for g in got), want)
+    ix.close()
 
 
 @pytest.mark.parametrize("d", [48, 96, 200, 768])

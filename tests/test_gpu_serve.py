@@ -101,10 +101,10 @@ def test_mixed_k_in_one_launch(qindex, small_data):
     _, Q = small_data
     n = 96
     k = np.where(np.arange(n) % 2 == 0, 10, 100).astype(np.uint32)
-    filt = [FILTERS[i % 3] if i % 4 == 1 else None for i in range(n)]
+    filt = [FILTERS[i % 3] if i % 4 == 1 else dg.Filter.none() for i in range(n)]
     ids, ds, cnt = qindex.search_arrays(Q[:n], 100, 64, traversal=_lib.TRAVERSE_BF16, filters=filt, per_query_k=k)
     for i in range(n):
-        ai, ad = _alone(qindex, Q[i], k[i], 64, _lib.TRAVERSE_BF16, 0, filt[i])
+        ai, ad = _alone(qindex, Q[i], k[i], 64, _lib.TRAVERSE_BF16, 0, None if filt[i].is_none() else filt[i])
         assert cnt[i] == len(ai) <= k[i]
         assert np.array_equal(ids[i, : cnt[i]], ai) and np.array_equal(ds[i, : cnt[i]], ad), i
         assert (ids[i, cnt[i]:] == _lib.PAD).all() and np.isinf(ds[i, cnt[i]:]).all()

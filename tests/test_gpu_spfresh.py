@@ -211,3 +211,26 @@ def test_posting_major_scan_matches_oracle(oracle, metric):
         oi, od, oc = oracle.spfresh_search(view, Q, 10, nprobe)
         assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od), nprobe
     s.close()
+
+
+def test_rabitq_postings_reencoded_on_the_gpu(oracle):
+    """RaBitQ posting codes are residuals against their posting's centroid, so
+    splits and relocations re-encode them (Inner::encode,
+    src/spfresh.rs:328-339).  The re-encode runs on the GPU encoder: after
+    inserts that split postings, every entry's code equals the oracle's
+    encode_with against its posting's current centroid."""
+    X = synth.mixture(3000, 32, 30, seed=14, clip=False)
+    s = dg.SPFresh.build(X, quantizer="rabitq", max_posting_size=40, min_posting_size=8, seed=3)
+    s.insert(synth.mixture(800, 32, 30, seed=15, clip=False))
+    s.delete(list(range(0, 3800, 13)))
+    s.gc()
+    P, signs = s.codec.p["padded"], s.codec.p["signs"]
+    checked = 0
+    for b in range(len(s.live_b)):
+        if not s.live_b[b] or not len(s.ids[b]):
+            continue
+        want = oracle.rabitq_encode(s.raw[s.ids[b].astype(np.int64)], P, s.cent[b], signs)
+        assert np.array_equal(s.codes[b], want), b
+        checked += 1
+    assert checked > 50
+    s.close()
