@@ -308,11 +308,13 @@ class Clocks:
 
 
 # ------------------------------------------------------------ GPU timing
-# DRAM bytes per launch of the dominant kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum), measured by one ncu capture of this bench's own
-# command, keyed by (variant, L, queries, base vectors).
-NCU_TRAFFIC = {}
-NCU_TRAFFIC_SOURCE = ""
+# DRAM bytes of one launch of the dominant kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum) from one ncu capture of this bench's command on a
+# smaller batch, keyed by (variant, L, base vectors): (queries captured,
+# bytes).  The line scales it to the batch by queries.
+NCU_TRAFFIC = {("bf16_rerank", 40, 1_000_000): (2000, 612.557568e6 + 4.95616e6)}
+NCU_TRAFFIC_SOURCE = ("scaled by queries from one ncu --set full capture of a 2000-query launch of the same "
+                      "kernel (python bench.py --nq 2000 --variants bf16_rerank ...)")
 
 VARIANTS = {
     # name: (traversal, rerank = L?)
@@ -548,7 +550,8 @@ def main():
             "p99_ms": float(np.percentile(steps_ms, 99)), "launch_ms": float(steps_ms.mean()),
             "kernel_expansions_per_query": float(stats[:, 0].mean()),
             "kernel_dist_evals_per_query": float(stats[:, 1].mean()),
-            **acc, "visited_table_bits": tuned[name]["hbits"], "clocks": ck.summary(),
+            **acc, "visited_table_bits": tuned[name]["hbits"],
+            "schedule": {k: v for k, v in tuned[name].items() if k != "ms"}, "clocks": ck.summary(),
         }
         log(f"[time] {name}: {json.dumps(results[name])}")
 
@@ -606,7 +609,8 @@ def main():
         r = results[head]
         if "alg_bytes_per_launch" in r:
             ach = r["alg_bytes_per_launch"] / (r["launch_ms"] / 1e3) / 1e9
-            tr = NCU_TRAFFIC.get((head, r["L"], args.nq, args.n))
+            cap = NCU_TRAFFIC.get((head, r["L"], args.n))
+            tr = cap[1] * args.nq / cap[0] if cap else None
             line["roofline"] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                                 "frac": round(ach / hbm, 4), "traffic": tr,
                                 "traffic_source": NCU_TRAFFIC_SOURCE if tr else None,

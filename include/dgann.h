@@ -380,6 +380,19 @@ DG_API DgStatus dg_spfresh_update_blocks(DgSpfresh *s, const uint32_t *blocks, u
 DG_API DgStatus dg_spfresh_put_raw(DgSpfresh *s, uint64_t first_id, const float *vectors, uint64_t n);
 /* SPFresh::delete tombstones (src/spfresh.rs:863-871); deleted = 0 clears. */
 DG_API DgStatus dg_spfresh_set_deleted(DgSpfresh *s, const uint64_t *ids, uint64_t n, int32_t deleted);
+/* The centroid and live flag of n posting slots, without their entries:
+ * SPFresh's update path publishes new and freed postings with it before it
+ * routes against them (Inner::new_posting / free_posting,
+ * src/spfresh.rs:395-415).  centroids f32[n*dim], live u8[n]. */
+DG_API DgStatus dg_spfresh_set_centroids(DgSpfresh *s, const uint32_t *blocks, uint32_t n, const float *centroids,
+                                         const uint8_t *live);
+/* Inner::nearest (src/spfresh.rs:358-378) for nv host vectors: the n (<= 64)
+ * nearest live postings of each, ascending by (distance, slot), with every
+ * distance summed in coordinate order in FP32 (brute force at every posting
+ * count); rows are padded with DG_PAD / +inf past the live postings.  The
+ * host update path routes its inserts, neighbourhoods and gc moves with it. */
+DG_API DgStatus dg_spfresh_nearest(DgSpfresh *s, const float *vectors, uint32_t nv, uint32_t n,
+                                   uint32_t *out_slots, float *out_dists);
 /* SPFresh::search_with_dists / search_batch (src/spfresh.rs:671-770,886-908):
  * out_ids u64[nq*k] (DG_PAD64 padded), out_dists f32[nq*k], out_counts u32[nq].
  * Searches of one handle share its scratch: each waits on the GPU for the

@@ -17,12 +17,9 @@ exact:
   * nearest() is brute force over the live postings at every size (the
     reference switches to its centroid graph above 4096 postings, a graph it
     builds non-deterministically) and orders equal distances by slot;
-  * a decision compares distances evaluated in f64 (the reference's
-    distance kernels come from numkong, whose f32 rounding no test pins):
-    nearest() and the pair distance of insert / kmeans2 sum (c - v)^2, the
-    per-chunk insert targets and local_moves use |v|^2 + |c|^2 - 2 v.c as a
-    matrix product; nearest() and the insert targets round the f64 value to
-    f32 before ordering, as the f32 values of the reference order.
+  * every distance is the f32 sum of squared differences in coordinate order,
+    the oracle's metric_eval (the reference's distances come from numkong,
+    f32 with an order no test pins).
 """
 from __future__ import annotations
 
@@ -32,18 +29,25 @@ CHUNK = 4096  # src/spfresh.rs:21
 
 
 def _l2_direct(v, C):
-    """f64 sum of squared differences of v against every row of C."""
-    d = C.astype(np.float64) - v.astype(np.float64)
-    return (d * d).sum(1)
+    """f32 coordinate-order squared L2 of v against every row of C."""
+    C = np.asarray(C, dtype=np.float32)
+    v = np.asarray(v, dtype=np.float32)
+    acc = np.zeros(len(C), dtype=np.float32)
+    for i in range(C.shape[1]):
+        t = v[i] - C[:, i]
+        acc = acc + t * t
+    return acc
 
 
 def _l2_matrix(V, C):
-    """f64 |v|^2 + |c|^2 - 2 v.c for every row pair, clamped at 0."""
-    V = np.asarray(V, dtype=np.float64)
-    C = np.asarray(C, dtype=np.float64)
-    if len(V) == 0 or len(C) == 0:
-        return np.zeros((len(V), len(C)))
-    return np.maximum((V * V).sum(1)[:, None] + (C * C).sum(1)[None, :] - 2.0 * (V @ C.T), 0.0)
+    """_l2_direct for every row of V: f32 [len(V), len(C)]."""
+    V = np.asarray(V, dtype=np.float32)
+    C = np.asarray(C, dtype=np.float32)
+    out = np.zeros((len(V), len(C)), dtype=np.float32)
+    for i in range(V.shape[1] if len(V) else 0):
+        t = V[:, i, None] - C[None, :, i]
+        out = out + t * t
+    return out
 
 
 class RefSpfresh:
@@ -117,7 +121,7 @@ class RefSpfresh:
         live = self.live_slots()
         if not live:
             return []
-        d = _l2_direct(v, np.stack([self.centroid[b] for b in live])).astype(np.float32)
+        d = _l2_direct(v, np.stack([self.centroid[b] for b in live]))
         order = sorted(range(len(live)), key=lambda i: (d[i], live[i]))[:n]
         return [(live[i], float(d[i])) for i in order]
 
@@ -138,7 +142,7 @@ class RefSpfresh:
             self.created = []
             live = self.live_slots()
             if live:
-                D = _l2_matrix(chunk, np.stack([self.centroid[b] for b in live])).astype(np.float32)
+                D = _l2_matrix(chunk, np.stack([self.centroid[b] for b in live]))
                 targets = [live[int(j)] for j in np.argmin(D, axis=1)]
             else:
                 targets = [None] * len(chunk)

@@ -119,6 +119,8 @@ def _signatures():
         "dg_spfresh_update_blocks": (st, [vp, vp, u32, vp, vp, vp, vp, vp]),
         "dg_spfresh_put_raw": (st, [vp, u64, vp, u64]),
         "dg_spfresh_set_deleted": (st, [vp, vp, u64, i32]),
+        "dg_spfresh_set_centroids": (st, [vp, vp, u32, vp, vp]),
+        "dg_spfresh_nearest": (st, [vp, vp, u32, u32, vp, vp]),
         "dg_spfresh_search_batch": (st, [vp, vp, vp, u32, vp, vp, vp]),
         "dg_medoid": (st, [vp, u64, u32, i32, i32, vp]),
         "dg_build_vamana": (st, [vp, u64, u32, i32, u32, u32, f32, u64, u32, i32, vp]),

@@ -55,6 +55,7 @@ struct DgSpfresh {
   std::vector<void *> allocs;
   DgIndex::Buf q, oids, od, ocnt, route;  // route: query x posting routing distances of one chunk
   DgIndex::Buf live_idx;                   // [0]: number of live postings, then their slot indices
+  DgIndex::Buf rnorm;                      // routing norms: |q|^2 of a chunk's queries, |c|^2 of the live centroids
   // posting-major scan of one chunk: probes per query, (query, posting) pairs
   // grouped by posting, work items, per-pair candidate lists
   DgIndex::Buf probe, probe_cnt, pcount, pstart, pfill, istart, pair_q, pos_of, items, pair_keys, pair_cnt, misc;
@@ -1031,6 +1032,170 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
   }
 }
 
+// ------------------------------------------------------ routing, tensor cores
+// Squared-L2 routing for many postings on the tensor cores.  k_route_tc
+// computes an approximation D~ = |q|^2 + |c|^2 - 2 q.c of every query x live
+// centroid pair, q.c as three BF16 products (qh.ch + qh.cl + ql.ch of the
+// two-term BF16 splits, FP32 accumulate), whose distance from the oracle's
+// coordinate-order FP32 sum is at most
+//   eps(q, c) = 1e-4 (|q|^2 + |c|^2) + 6e-4 |q| |c|
+// (dropped split terms < 3 * 2^-16 |q| |c|, accumulation < 600 * 2^-24 |q| |c|,
+// the norms and the oracle's own sum < 200 * 2^-24 (|q|^2 + |c|^2); a factor
+// of four above their sum).  k_route_fix then takes U, the n_probe-th
+// smallest upper bound D~ + eps of a query's row, and writes the exact
+// coordinate-order distance for every centroid whose lower bound D~ - eps is
+// at most U, and +inf for the rest.  Every centroid of the exact n_probe
+// nearest (ties included) has its lower bound at most U, so the selection
+// that follows picks exactly the postings exact routing picks.
+constexpr float kRouteRel = 1e-4f, kRouteCross = 6e-4f;
+constexpr int kRTK = 32;             // dimensions staged per step
+constexpr int kRTS = kRTK + 8;       // staged row stride (BF16 elements): conflict-free ldmatrix
+
+__device__ __forceinline__ float route_eps(float qq, float cc) {
+  return kRouteRel * (qq + cc) + kRouteCross * sqrtf(qq * cc);
+}
+
+// |q|^2 of every query and |c|^2 of every live centroid (FP32, coordinate order).
+__global__ void k_route_norms(const float *__restrict__ Q, uint32_t nq, uint32_t qstride, const float *__restrict__ C,
+                              const uint32_t *__restrict__ cidx, uint32_t d, uint32_t dpad, float *qn, float *cn) {
+  const uint32_t nl = __ldg(cidx);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nq + nl; t += gridDim.x * blockDim.x) {
+    const float *x = t < nq ? Q + (size_t)t * qstride : C + (size_t)__ldg(cidx + 1 + (t - nq)) * dpad;
+    float s2 = 0.0f;
+    for (uint32_t i = 0; i < d; ++i) s2 = __fadd_rn(s2, __fmul_rn(x[i], x[i]));
+    if (t < nq) qn[t] = s2;
+    else cn[t - nq] = s2;
+  }
+}
+
+// One block: 64 queries x 64 live centroids; warp w computes queries
+// 16 (w % 4) .. +15 against centroids 32 (w / 4) .. +31.
+__global__ void __launch_bounds__(256) k_route_tc(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
+                                                  const float *__restrict__ C, const uint32_t *__restrict__ cidx,
+                                                  uint32_t d, uint32_t dpad, const float *__restrict__ qn,
+                                                  const float *__restrict__ cn, float *__restrict__ D, uint32_t ldd) {
+  __shared__ __align__(16) uint16_t qs[2][kRT * kRTS], cs[2][kRT * kRTS];  // [hi, lo][row][k]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t q0 = blockIdx.y * kRT, c0 = blockIdx.x * kRT;
+  const uint32_t nl = __ldg(cidx);
+  if (c0 >= nl) return;  // the whole block: fewer live postings than slots
+  const uint32_t *col = cidx + 1;
+  const uint32_t m16 = 16u * (warp & 3), n32 = 32u * (warp >> 2);
+  float acc[4][4] = {};
+  const uint32_t qs_s[2] = {(uint32_t)__cvta_generic_to_shared(qs[0]), (uint32_t)__cvta_generic_to_shared(qs[1])};
+  const uint32_t cs_s[2] = {(uint32_t)__cvta_generic_to_shared(cs[0]), (uint32_t)__cvta_generic_to_shared(cs[1])};
+  const uint32_t arow = m16 + (lane & 15), acol = (lane >> 4) * 8;
+  const uint32_t brow = (lane >> 4) * 8 + (lane & 7), bcol = ((lane >> 3) & 1) * 8;
+  for (uint32_t k0 = 0; k0 < d; k0 += kRTK) {
+    for (uint32_t e = threadIdx.x; e < (uint32_t)kRT * kRTK; e += blockDim.x) {
+      const uint32_t r = e / kRTK, k = e % kRTK, kk = k0 + k;
+      const float xq = (q0 + r < nq && kk < d) ? __ldg(Q + (size_t)(q0 + r) * qstride + kk) : 0.0f;
+      const float xc = (c0 + r < nl && kk < d) ? __ldg(C + (size_t)__ldg(col + c0 + r) * dpad + kk) : 0.0f;
+      const __nv_bfloat16 hq = __float2bfloat16_rn(xq), hc = __float2bfloat16_rn(xc);
+      qs[0][r * kRTS + k] = __bfloat16_as_ushort(hq);
+      qs[1][r * kRTS + k] = __bfloat16_as_ushort(__float2bfloat16_rn(xq - __bfloat162float(hq)));
+      cs[0][r * kRTS + k] = __bfloat16_as_ushort(hc);
+      cs[1][r * kRTS + k] = __bfloat16_as_ushort(__float2bfloat16_rn(xc - __bfloat162float(hc)));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < kRTK; ks += 16) {
+      uint32_t ah[4], al[4], bh[2][4], bl[2][4];
+      ldsm_x4(ah, qs_s[0] + 2u * (arow * kRTS + ks + acol));
+      ldsm_x4(al, qs_s[1] + 2u * (arow * kRTS + ks + acol));
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        ldsm_x4(bh[h], cs_s[0] + 2u * ((n32 + 16 * h + brow) * kRTS + ks + bcol));
+        ldsm_x4(bl[h], cs_s[1] + 2u * ((n32 + 16 * h + brow) * kRTS + ks + bcol));
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const uint32_t(&bhh)[4] = bh[nt >> 1], (&bll)[4] = bl[nt >> 1];
+        const int o = 2 * (nt & 1);
+        mma_bf16_16x8x16(acc[nt], ah[0], ah[1], ah[2], ah[3], bhh[o], bhh[o + 1]);
+        mma_bf16_16x8x16(acc[nt], ah[0], ah[1], ah[2], ah[3], bll[o], bll[o + 1]);
+        mma_bf16_16x8x16(acc[nt], al[0], al[1], al[2], al[3], bhh[o], bhh[o + 1]);
+      }
+    }
+    __syncthreads();
+  }
+  // lane (g, t): queries g, g + 8 x centroids 2t, 2t + 1 of each 8-centroid tile
+  const uint32_t g = lane >> 2, t2 = 2 * (lane & 3);
+#pragma unroll
+  for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t q = q0 + m16 + g + (e >= 2 ? 8 : 0), c = c0 + n32 + 8 * nt + t2 + (e & 1);
+      if (q < nq && c < nl) D[(size_t)q * ldd + c] = __fsub_rn(__fadd_rn(qn[q], cn[c]), 2.0f * acc[nt][e]);
+    }
+}
+
+// Per query (one warp): U = the n_probe-th smallest upper bound of its row,
+// then the exact distance for every column whose lower bound is at most U,
+// +inf elsewhere.
+__global__ void __launch_bounds__(128) k_route_fix(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
+                                                   const float *__restrict__ C, const uint32_t *__restrict__ cidx,
+                                                   uint32_t d, uint32_t dpad, int metric, const float *__restrict__ qn,
+                                                   const float *__restrict__ cn, float *D, uint32_t ldd,
+                                                   uint32_t nprobe) {
+  __shared__ uint32_t hist_all[4][2048];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t *hist = hist_all[warp];
+  const uint32_t nl = __ldg(cidx);
+  const uint32_t *col = cidx + 1;
+  for (uint32_t q = blockIdx.x * 4 + warp; q < nq; q += gridDim.x * 4) {
+    float *rq = D + (size_t)q * ldd;
+    const float qq = qn[q];
+    float U = __int_as_float(0x7f800000);
+    if (nprobe < nl) {
+      uint32_t need = nprobe, prefix = 0, mask = 0;
+      auto ub_bits = [&](uint32_t j, bool &ok) {
+        ok = true;
+        return __float_as_uint(fmaxf(rq[j] + route_eps(qq, __ldg(cn + j)), 0.0f));
+      };
+      const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+      for (int ps = 0; ps < 3; ++ps) {
+        const uint32_t b = pm_radix_pass(hist, nl, ub_bits, prefix, mask, shifts[ps], widths[ps], need, lane);
+        prefix |= b << shifts[ps];
+        mask |= ((1u << widths[ps]) - 1u) << shifts[ps];
+      }
+      U = __uint_as_float(prefix);
+    }
+    const float *qr = Q + (size_t)q * qstride;
+    for (uint32_t j = lane; j < nl; j += 32) {
+      const float lb = rq[j] - route_eps(qq, __ldg(cn + j));
+      rq[j] = lb <= U ? seq_metric(qr, C + (size_t)__ldg(col + j) * dpad, d, metric) : __int_as_float(0x7f800000);
+    }
+    __syncwarp();
+  }
+}
+
+// The n nearest live postings of each row of an exact routing matrix (one
+// warp per row), as (distance, slot) keys in ascending order: slots, distances.
+__global__ void __launch_bounds__(128) k_route_topn(const float *__restrict__ D, uint32_t nv, uint32_t ldd,
+                                                    const uint32_t *__restrict__ cidx, uint32_t n,
+                                                    uint32_t *out_slots, float *out_d) {
+  __shared__ __align__(16) uint64_t lists[4][2][64];
+  __shared__ __align__(16) uint64_t cst[4][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t *const bufs[2] = {lists[warp][0], lists[warp][1]};
+  const uint32_t nl = __ldg(cidx);
+  for (uint32_t v = blockIdx.x * 4 + warp; v < nv; v += gridDim.x * 4) {
+    int cur = 0, size = 0;
+    for (uint32_t j0 = 0; j0 < nl; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      const uint64_t key = j < nl ? make_key(D[(size_t)v * ldd + j], __ldg(cidx + 1 + j)) : kKeyInvalid;
+      insert_batch(key, bufs, cur, size, (int)n, cst[warp], lane);
+    }
+    for (uint32_t i = lane; i < n; i += 32) {
+      const bool ok = (int)i < size;
+      out_slots[(size_t)v * n + i] = ok ? key_id(bufs[cur][i]) : DG_PAD;
+      out_d[(size_t)v * n + i] = ok ? key_dist(bufs[cur][i]) : __int_as_float(0x7f800000);
+    }
+    __syncwarp();
+  }
+}
+
 // Per query: the k best keys over its probed postings' pair lists.
 __global__ void __launch_bounds__(128) k_pm_merge(const uint32_t *probe_cnt, const uint32_t *pos_of, uint32_t nq,
                                                   uint32_t nprobe, const uint64_t *pair_keys,
@@ -1160,7 +1325,7 @@ DgStatus dg_spfresh_destroy(DgSpfresh *s) {
     cudaEventDestroy(s->searched);
   }
   for (void *p : s->allocs) cudaFree(p);
-  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx, &s->probe, &s->probe_cnt,
+  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx, &s->rnorm, &s->probe, &s->probe_cnt,
                           &s->pcount, &s->pstart, &s->pfill, &s->istart, &s->pair_q, &s->pos_of, &s->items,
                           &s->pair_keys, &s->pair_cnt, &s->misc})
     if (b->p) cudaFree(b->p);
@@ -1318,6 +1483,63 @@ DgStatus dg_spfresh_update_blocks(DgSpfresh *s, const uint32_t *blocks, uint32_t
   return DG_OK;
 }
 
+DgStatus dg_spfresh_set_centroids(DgSpfresh *s, const uint32_t *blocks, uint32_t nupd, const float *centroids,
+                                  const uint8_t *live) {
+  if (!s || (nupd && (!blocks || !centroids || !live))) return fail(DG_EINVAL, "null argument");
+  for (uint32_t u = 0; u < nupd; ++u)
+    if (blocks[u] >= s->nblocks) return fail(DG_EINVAL, "block index out of range");
+  std::lock_guard<std::mutex> lk(s->mu);
+  DG_CUDA(cudaSetDevice(s->device));
+  cudaStream_t ss = s->stream;
+  DG_CUDA(cudaStreamWaitEvent(ss, s->searched, 0));
+  for (uint32_t u = 0; u < nupd; ++u) {
+    const uint32_t b = blocks[u];
+    DgStatus st = upload_rows_f32(centroids + (size_t)u * s->d, 1, s->d, s->dpad, s->centroids + (size_t)b * s->dpad, ss);
+    if (st != DG_OK) return st;
+    DG_CUDA(cudaMemcpyAsync(s->live + b, live + u, 1, cudaMemcpyHostToDevice, ss));
+  }
+  DG_CUDA(cudaStreamSynchronize(ss));  // the host arrays may go once this returns
+  return DG_OK;
+}
+
+DgStatus dg_spfresh_nearest(DgSpfresh *s, const float *vectors, uint32_t nv, uint32_t n, uint32_t *out_slots,
+                            float *out_dists) {
+  if (!s || (nv && (!vectors || !out_slots || !out_dists))) return fail(DG_EINVAL, "null argument");
+  if (n == 0 || n > 64) return fail(DG_EINVAL, "n must be in [1, 64]");
+  if (nv == 0) return DG_OK;
+  std::lock_guard<std::mutex> lk(s->mu);
+  DG_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  DG_CUDA(cudaStreamWaitEvent(st, s->searched, 0));  // shares the search's scratch
+  DgStatus r;
+  const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nv, (1ull << 28) / s->nblocks));
+  if ((r = buf_reserve(s->q, (size_t)nv * s->d * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->route, (size_t)chunk * s->nblocks * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->live_idx, ((size_t)s->nblocks + 1) * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->oids, (size_t)nv * n * 4)) != DG_OK) return r;
+  if ((r = buf_reserve(s->od, (size_t)nv * n * 4)) != DG_OK) return r;
+  DG_CUDA(cudaMemcpyAsync(s->q.p, vectors, (size_t)nv * s->d * 4, cudaMemcpyHostToDevice, st));
+  uint32_t *lidx = (uint32_t *)s->live_idx.p;
+  DG_CUDA(cudaMemsetAsync(lidx, 0, 4, st));
+  k_live_idx<<<(s->nblocks + 255) / 256, 256, 0, st>>>(s->live, s->nblocks, lidx);
+  for (uint32_t v0 = 0; v0 < nv; v0 += chunk) {
+    const uint32_t vn = std::min(chunk, nv - v0);
+    const float *Qc = (const float *)s->q.p + (size_t)v0 * s->d;
+    dim3 grid((s->nblocks + kRT - 1) / kRT, (vn + kRT - 1) / kRT);
+    k_route<<<grid, 256, 0, st>>>(Qc, vn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric, (float *)s->route.p,
+                                  s->nblocks);
+    k_route_topn<<<(unsigned)std::min<uint32_t>((vn + 3) / 4, 148 * 16), 128, 0, st>>>(
+        (const float *)s->route.p, vn, s->nblocks, lidx, n, (uint32_t *)s->oids.p + (size_t)v0 * n,
+        (float *)s->od.p + (size_t)v0 * n);
+  }
+  DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaMemcpyAsync(out_slots, s->oids.p, (size_t)nv * n * 4, cudaMemcpyDeviceToHost, st));
+  DG_CUDA(cudaMemcpyAsync(out_dists, s->od.p, (size_t)nv * n * 4, cudaMemcpyDeviceToHost, st));
+  DG_CUDA(cudaEventRecord(s->searched, st));
+  DG_CUDA(cudaStreamSynchronize(st));
+  return DG_OK;
+}
+
 DgStatus dg_spfresh_put_raw(DgSpfresh *s, uint64_t first_id, const float *vectors, uint64_t n) {
   if (!s || (n && !vectors)) return fail(DG_EINVAL, "null argument");
   if (first_id + n > s->id_cap) return fail(DG_EINVAL, "raw rows beyond id_capacity");
@@ -1438,6 +1660,7 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
     const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nq, (1ull << 28) / s->nblocks));
     if ((r = buf_reserve(s->route, (size_t)chunk * s->nblocks * 4)) != DG_OK) return r;
     if ((r = buf_reserve(s->live_idx, ((size_t)s->nblocks + 1) * 4)) != DG_OK) return r;
+    if ((r = buf_reserve(s->rnorm, ((size_t)chunk + s->nblocks) * 4)) != DG_OK) return r;
     uint32_t *lidx = (uint32_t *)s->live_idx.p;
     DG_CUDA(cudaMemsetAsync(lidx, 0, 4, st));
     k_live_idx<<<(s->nblocks + 255) / 256, 256, 0, st>>>(s->live, s->nblocks, lidx);
@@ -1453,8 +1676,20 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
       ac.route = (const float *)s->route.p;
       ac.route_idx = lidx;
       dim3 grid((s->nblocks + kRT - 1) / kRT, (qn + kRT - 1) / kRT);
-      k_route<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric,
-                                    (float *)s->route.p, s->nblocks);
+      if (s->metric == DG_L2 || s->metric == DG_L2SQ) {
+        // tensor-core approximation, then exact distances for the candidates of each row
+        float *qnorm = (float *)s->rnorm.p, *cnorm = qnorm + chunk;
+        k_route_norms<<<(unsigned)std::min<size_t>(((size_t)qn + s->nblocks + 255) / 256, 148 * 16), 256, 0, st>>>(
+            ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, qnorm, cnorm);
+        k_route_tc<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, qnorm, cnorm,
+                                         (float *)s->route.p, s->nblocks);
+        k_route_fix<<<(unsigned)std::min<uint32_t>((qn + 3) / 4, 148 * 16), 128, 0, st>>>(
+            ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric, qnorm, cnorm, (float *)s->route.p,
+            s->nblocks, nprobe);
+      } else {
+        k_route<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric,
+                                      (float *)s->route.p, s->nblocks);
+      }
       DG_CUDA(cudaGetLastError());
       if (posting_major) {
         if ((r = pm_scan_chunk(s, ac, nprobe, p->k, pcap, rcap, st)) != DG_OK) return r;

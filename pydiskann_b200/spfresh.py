@@ -29,49 +29,49 @@ _METRICS = {"l2": _lib.L2SQ, "cosine": _lib.COSINE, "dot": _lib.DOT, "euclidean"
 CHUNK = 4096
 
 
-def _dist_rows(metric, v, C_):
-    """metric_eval(v, row) for every row of C_ (float64 accumulation)."""
-    v = v.astype(np.float64)
-    Cm = C_.astype(np.float64)
+def _seq_rows(metric, v, C_):
+    """metric_eval(v, c) for every row c of C_, summed in coordinate order in
+    f32: the arithmetic of the GPU routing kernels (seq_metric) and of the
+    oracle's metric_eval, i.e. the reference's f32 distances in a fixed order."""
+    Ct = np.ascontiguousarray(np.asarray(C_, dtype=np.float32).T)
+    v = np.asarray(v, dtype=np.float32).reshape(-1)
+    n = Ct.shape[1]
     if metric in (_lib.L2SQ, _lib.L2):
-        d = ((Cm - v) ** 2).sum(1)
-        return np.sqrt(d) if metric == _lib.L2 else d
-    ab = Cm @ v
+        acc = np.zeros(n, dtype=np.float32)
+        for i in range(len(v)):
+            t = v[i] - Ct[i]
+            acc = acc + t * t
+        return np.sqrt(acc) if metric == _lib.L2 else acc
+    ab = np.zeros(n, dtype=np.float32)
+    bb = np.zeros(n, dtype=np.float32)
+    aa = np.float32(0.0)
+    for i in range(len(v)):
+        ab = ab + v[i] * Ct[i]
+        aa = np.float32(aa + v[i] * v[i])
+        bb = bb + Ct[i] * Ct[i]
     if metric == _lib.DOT:
-        return 1.0 - ab
-    aa, bb = float(v @ v), (Cm * Cm).sum(1)
+        return np.float32(1.0) - ab
     with np.errstate(divide="ignore", invalid="ignore"):
-        r = 1.0 - ab / (np.sqrt(aa) * np.sqrt(bb))
-    r = np.where((aa == 0) & (bb == 0), 0.0, np.where(ab == 0, 1.0, r))
-    return np.maximum(r, 0.0)
+        r = np.float32(1.0) - ab / (np.sqrt(aa) * np.sqrt(bb))
+    r = np.where((aa == 0) & (bb == 0), np.float32(0.0), np.where(ab == 0, np.float32(1.0), r))
+    return np.maximum(r, np.float32(0.0)).astype(np.float32)
 
 
-def _dist_matrix(metric, V, C_):
-    """metric_eval(v, c) for every row v of V and row c of C_ (float64), as an
-    [len(V), len(C_)] matrix (squared L2 as |v|^2 + |c|^2 - 2 v.c), in blocks."""
-    V = np.asarray(V, dtype=np.float64)
-    Cm = np.asarray(C_, dtype=np.float64)
-    out = np.empty((len(V), len(Cm)), dtype=np.float64)
-    if len(V) == 0 or len(Cm) == 0:
+def _seq_matrix(metric, V, C_):
+    """_seq_rows for every row of V: an f32 [len(V), len(C_)] matrix."""
+    V = np.asarray(V, dtype=np.float32)
+    C_ = np.asarray(C_, dtype=np.float32)
+    out = np.empty((len(V), len(C_)), dtype=np.float32)
+    if len(V) == 0 or len(C_) == 0:
         return out
-    cc = (Cm * Cm).sum(1)[None, :]
-    step = max(1, (1 << 24) // max(1, len(Cm)))
-    for s in range(0, len(V), step):
-        blk = V[s:s + step]
-        if metric in (_lib.L2SQ, _lib.L2):
-            d = np.maximum((blk * blk).sum(1)[:, None] + cc - 2.0 * (blk @ Cm.T), 0.0)
-            out[s:s + step] = np.sqrt(d) if metric == _lib.L2 else d
-            continue
-        ab = blk @ Cm.T
-        if metric == _lib.DOT:
-            out[s:s + step] = 1.0 - ab
-            continue
-        aa = (blk * blk).sum(1)[:, None]
-        bb = (Cm * Cm).sum(1)[None, :]
-        with np.errstate(divide="ignore", invalid="ignore"):
-            r = 1.0 - ab / (np.sqrt(aa) * np.sqrt(bb))
-        r = np.where((aa == 0) & (bb == 0), 0.0, np.where(ab == 0, 1.0, r))
-        out[s:s + step] = np.maximum(r, 0.0)
+    if metric in (_lib.L2SQ, _lib.L2):
+        acc = np.zeros((len(V), len(C_)), dtype=np.float32)
+        for i in range(V.shape[1]):
+            t = V[:, i, None] - C_[None, :, i]
+            acc = acc + t * t
+        return np.sqrt(acc) if metric == _lib.L2 else acc
+    for r in range(len(V)):
+        out[r] = _seq_rows(metric, V[r], C_)
     return out
 
 
@@ -161,12 +161,12 @@ def kmeans2(vs, metric):
             out.append((sel.sum(0, dtype=np.float32) / np.float32(cnt)).astype(np.float32))
         return out
 
-    d0 = _dist_rows(metric, vs[0], vs[1:]) if n > 1 else np.zeros(0)
+    d0 = _seq_rows(metric, vs[0], vs[1:]) if n > 1 else np.zeros(0)
     far = int(np.argmax(d0)) + 1 if n > 1 else 0
     c = [vs[0].copy(), vs[far].copy()]
     side = np.zeros(n, dtype=bool)
     for _ in range(5):
-        side = _dist_rows(metric, c[1], vs) < _dist_rows(metric, c[0], vs)
+        side = _seq_rows(metric, c[1], vs) < _seq_rows(metric, c[0], vs)
         if side.all() or not side.any():
             break
         c = means(side)
@@ -203,6 +203,7 @@ class SPFresh:
         self.created = []
         self._h = None
         self._dirty = set()
+        self._cent_dirty = set()  # slots whose centroid or live flag the device mirror has not seen
         self._dev_blocks = 0
         self._dev_ids = 0
         self._raw_synced = 0
@@ -336,6 +337,7 @@ class SPFresh:
         self.codes[b] = np.zeros((0, self.codec.size), dtype=np.uint8)
         self.created.append(b)
         self._dirty.add(b)
+        self._cent_dirty.add(b)
         return b
 
     def _free_posting(self, b):
@@ -344,6 +346,7 @@ class SPFresh:
         self.codes[b] = np.zeros((0, self.codec.size), dtype=np.uint8)
         self.free.append((b, self.epoch))
         self._dirty.add(b)
+        self._cent_dirty.add(b)
 
     def _rewrite(self, b, ids, codes):
         self.ids[b], self.codes[b] = np.asarray(ids, dtype=np.uint64), np.asarray(codes, dtype=np.uint8).reshape(-1, self.codec.size)
@@ -357,17 +360,49 @@ class SPFresh:
     def _encode(self, v, b):
         return self.codec.encode(v, self.cent[b] if self.codec.residual else None)[0]
 
+    def _device_routing(self):
+        """True when the device mirror can route against the current postings:
+        it exists and holds every slot; new and freed postings are published
+        first (their centroids and live flags)."""
+        if self._h is None:
+            return False
+        if len(self.live_b) > self._dev_blocks:
+            self._create_device()
+            return True
+        if self._cent_dirty:
+            blocks = np.array(sorted(self._cent_dirty), dtype=np.uint32)
+            cent = np.ascontiguousarray(self.cent[blocks], dtype=np.float32)
+            live = np.ascontiguousarray(self.live_b[blocks], dtype=np.uint8)
+            check(lib().dg_spfresh_set_centroids(self._h, ptr(blocks), len(blocks), ptr(cent), ptr(live)))
+            self._cent_dirty.clear()
+        return True
+
+    def _nearest_many(self, V, n):
+        """Inner::nearest (src/spfresh.rs:358-378) for every row of V: the n
+        nearest live postings as (slots, distances), ascending by (distance,
+        slot), FP32 coordinate-order distances; on the GPU when the device
+        mirror is attached (dg_spfresh_nearest), else on the host."""
+        V = np.ascontiguousarray(V, dtype=np.float32).reshape(-1, self.dim)
+        live = np.nonzero(self.live_b)[0]
+        n = min(n, len(live))
+        if n == 0 or len(V) == 0:
+            return np.zeros((len(V), 0), np.int64), np.zeros((len(V), 0), np.float32)
+        if n <= 64 and self._device_routing():
+            slots = np.empty((len(V), n), dtype=np.uint32)
+            dists = np.empty((len(V), n), dtype=np.float32)
+            check(lib().dg_spfresh_nearest(self._h, ptr(V), len(V), n, ptr(slots), ptr(dists)))
+            return slots.astype(np.int64), dists
+        D = _seq_matrix(self.metric, V, self.cent[live])
+        order = np.lexsort((np.broadcast_to(live, D.shape), D), axis=1)[:, :n]
+        return live[order], np.take_along_axis(D, order, axis=1)
+
     def _nearest(self, v, n):
         """Live postings by (distance to centroid, slot), closest first (src/spfresh.rs:358-378)."""
-        live = np.nonzero(self.live_b)[0]
-        if len(live) == 0:
-            return []
-        d = _dist_rows(self.metric, v, self.cent[live]).astype(np.float32)
-        order = np.lexsort((live, d))[: max(n, 0)]
-        return [(int(live[i]), float(d[i])) for i in order]
+        slots, dists = self._nearest_many(v, n)
+        return [(int(b), float(d)) for b, d in zip(slots[0], dists[0])]
 
     def _dist(self, v, b):
-        return float(_dist_rows(self.metric, v, self.cent[b:b + 1])[0])
+        return float(_seq_rows(self.metric, v, self.cent[b:b + 1])[0])
 
     # --------------------------------------------------------------- updates
     @locked
@@ -391,13 +426,10 @@ class SPFresh:
             chunk = X[c0:c0 + CHUNK]
             self.epoch += 1
             self.created = []
-            live = np.nonzero(self.live_b)[0]
-            if len(live):
-                # nearest live posting per vector; f32 distances, lowest slot on ties
-                D = _dist_matrix(self.metric, chunk, self.cent[live]).astype(np.float32)
-                targets = [int(t) for t in live[np.argmin(D, axis=1)]]
-            else:
-                targets = [None] * len(chunk)
+            # nearest live posting per vector (lowest slot on ties), as the
+            # reference routes a chunk before inserting it
+            slots, _ = self._nearest_many(chunk, 1)
+            targets = [int(t) for t in slots[:, 0]] if slots.shape[1] else [None] * len(chunk)
             for j, v in enumerate(chunk):
                 id_ = first + c0 + j
                 t = targets[j]
@@ -407,7 +439,7 @@ class SPFresh:
                     best = nn[0] if nn else None
                 cr = [c for c in self.created if self._is_live(c)]
                 if cr:  # postings split off earlier in this chunk
-                    dc = _dist_rows(self.metric, v, self.cent[cr])
+                    dc = _seq_rows(self.metric, v, self.cent[cr])
                     for c, dd in zip(cr, dc):
                         if best is None or dd < best[1]:
                             best = (c, float(dd))
@@ -427,7 +459,7 @@ class SPFresh:
         if not cands or len(ids) == 0:
             return moves
         V = self.raw[ids.astype(np.int64)]
-        D = _dist_matrix(self.metric, V, self.cent[[p] + cands])
+        D = _seq_matrix(self.metric, V, self.cent[[p] + cands])
         best = np.argmin(D[:, 1:], axis=1)
         better = D[np.arange(len(ids)), 1 + best] < D[:, 0]
         for j in np.nonzero(better)[0]:
@@ -693,6 +725,7 @@ class SPFresh:
             check(lib().dg_spfresh_update_blocks(self._h, ptr(blocks), len(blocks), ptr(cent), ptr(live), ptr(lens),
                                                  ptr(ids), ptr(codes)))
             self._dirty.clear()
+            self._cent_dirty.clear()
         if self.next_id > self._raw_synced:
             rows = np.ascontiguousarray(self.raw[self._raw_synced:self.next_id])
             check(lib().dg_spfresh_put_raw(self._h, self._raw_synced, ptr(rows), len(rows)))
@@ -740,6 +773,7 @@ class SPFresh:
         self._h = h
         self._dev_blocks, self._dev_ids = nb, id_cap
         self._dirty.clear()
+        self._cent_dirty.clear()
         self._raw_synced = self.next_id
         self._del_synced = set(self.deleted)
 
@@ -867,7 +901,7 @@ def _centroid_graph(C_, metric, device):
     # host-only instance: exact nearest-centroid lists
     graph = []
     for c0 in range(0, n, 1024):
-        D = _dist_matrix(_METRICS[metric], C_[c0:c0 + 1024], C_)
+        D = _seq_matrix(_METRICS[metric], C_[c0:c0 + 1024], C_)
         for i in range(len(D)):
             D[i, c0 + i] = np.inf
         graph += np.argsort(D, axis=1, kind="stable")[:, : min(32, n - 1)].tolist()

@@ -17,7 +17,11 @@ from pydiskann_b200.spfresh import SPFresh
 
 
 def _arr(p, ctype, shape):
-    return np.ctypeslib.as_array(C.cast(C.c_void_p(p), C.POINTER(ctype)), shape).copy()
+    return _view(p, ctype, shape).copy()
+
+
+def _view(p, ctype, shape):
+    return np.ctypeslib.as_array(C.cast(C.c_void_p(p), C.POINTER(ctype)), shape)
 
 
 class FakeSpfLib:
@@ -32,6 +36,7 @@ class FakeSpfLib:
             "lens": _arr(d.block_len, C.c_uint32, (nb,)), "ids": _arr(d.entry_ids, C.c_uint64, (nb, cap)),
             "codes": _arr(d.entry_codes, C.c_uint8, (nb, cap, cs)), "raw": np.zeros((d.id_capacity, dim), np.float32),
             "deleted": _arr(d.deleted, C.c_uint8, (d.id_capacity,)).astype(bool), "cap": cap, "dim": dim, "cs": cs,
+            "metric": d.metric,
         }
         if d.num_raw:
             st["raw"][: d.num_raw] = _arr(d.raw, C.c_float, (d.num_raw, dim))
@@ -61,6 +66,24 @@ class FakeSpfLib:
     def dg_spfresh_put_raw(self, h, first, rows, n):
         st = self._st(h)
         st["raw"][first:first + n] = _arr(rows.value, C.c_float, (n, st["dim"]))
+        return 0
+
+    def dg_spfresh_set_centroids(self, h, blocks, n, cent, live):
+        st = self._st(h)
+        b = _arr(blocks.value, C.c_uint32, (n,))
+        st["cent"][b] = _arr(cent.value, C.c_float, (n, st["dim"]))
+        st["live"][b] = _arr(live.value, C.c_uint8, (n,))
+        return 0
+
+    def dg_spfresh_nearest(self, h, V, nv, n, slots, dists):
+        """Routes against this stand-in's own copy of the centroids, so a
+        centroid the host did not publish routes differently."""
+        st = self._st(h)
+        live = np.nonzero(st["live"])[0]
+        D = spf_mod._seq_matrix(st["metric"], _arr(V.value, C.c_float, (nv, st["dim"])), st["cent"][live])
+        order = np.lexsort((np.broadcast_to(live, D.shape), D), axis=1)[:, :n]
+        _view(slots.value, C.c_uint32, (nv, n))[:] = live[order]
+        _view(dists.value, C.c_float, (nv, n))[:] = np.take_along_axis(D, order, axis=1)
         return 0
 
     def dg_spfresh_set_deleted(self, h, ids, n, deleted):
