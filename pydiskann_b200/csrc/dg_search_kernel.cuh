@@ -25,8 +25,11 @@ struct QueryCtx {
   uint32_t fnops;
 };
 
-// Distances for the cnt staged candidates (lane j holds cand), per traversal kind.
-template <int TRAV, int MET, int LPR>
+// Distances for the cnt staged candidates (lane j holds cand), per traversal
+// kind.  TC selects tensor-core BF16 distances (the register-list kernel);
+// the general kernel, with more state per warp, computes them as packed FP32
+// FMAs, which measured faster there.
+template <int TRAV, int MET, int LPR, bool TC = true>
 __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *wsm,
                                                 const WarpLayout &Ly, uint32_t cand, int cnt,
                                                 int lane, float qq) {
@@ -43,6 +46,9 @@ __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *ws
     const float dot = sn.x * qs2.x * fp8_dot_mma(a.vec_fp8, a.dpad, qhl, cand, cnt, lane);
     if (MET == MET_L2) return finish_metric(MET, sqrt_l2, fmaxf(qs2.y + sn.y - 2.0f * dot, 0.0f), 0.0f, qq);
     return finish_metric(MET, false, dot, sn.y, qq);
+  } else if (TRAV == TRAV_BF16 && !TC) {
+    return rows_distance<LPR, 1, MET>(reinterpret_cast<const uint8_t *>(a.vec_bf16), a.dpad * 2,
+                                      (a.dpad / 8) / LPR, qs, cand, cnt, lane, sqrt_l2, qq);
   } else if (TRAV == TRAV_BF16) {
     // |q - x|^2 = |q|^2 + |x|^2 - 2 q.x with q.x on the tensor cores
     const uint16_t *qhl = reinterpret_cast<const uint16_t *>(wsm + Ly.prov);
@@ -549,7 +555,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     for (int g0 = 0; g0 < ns; g0 += 32) {
       const int cnt = min(32, ns - g0);
       const uint32_t cand = lane < cnt ? stage[g0 + lane] : DG_PAD;
-      float d = batch_distance<TRAV, MET, LPR>(a, wsm, Ly, cand, cnt, lane, qq);
+      float d = batch_distance<TRAV, MET, LPR, false>(a, wsm, Ly, cand, cnt, lane, qq);
       if (TRAV != TRAV_F32 && a.code_limit < a.n && lane < cnt && cand >= a.code_limit)
         d = exact_row_distance<MET>(a, qs, cand, qq);
       uint64_t key = lane < cnt ? make_key(d, cand) : kKeyInvalid;
