@@ -615,9 +615,6 @@ __device__ __forceinline__ void mma_bf16_16x8x16(float (&c)[4], uint32_t a0, uin
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-#ifndef DG_BF16_PREFETCH
-#define DG_BF16_PREFETCH 0
-#endif
 // q.x for up to 32 candidate BF16 rows x on the tensor cores (FP32
 // accumulate), in the tile and lane layout of int8_l2_mma: two 16-row tiles;
 // lane t of group g reads the 16-byte chunks t, t+4, ... of its rows g, g+8
@@ -645,15 +642,6 @@ __device__ __forceinline__ float bf16_dot_mma(const uint16_t *__restrict__ rows,
   // B column 0 holds hi, column 1 lo (columns 2..7 stay zero)
   const uint4 *pq = reinterpret_cast<const uint4 *>(qhl + (g == 1 ? dpad : 0));
   const bool col = g < 2;
-#if DG_BF16_PREFETCH
-  // the second 128-byte half of every candidate row into L2 now, so the
-  // second round of loads hits L2 instead of paying another DRAM trip
-  if (t == 0 && nch > 8) {
-#pragma unroll
-    for (int h = 0; h < 4; ++h)
-      if (h < 2 || two) asm volatile("prefetch.global.L2 [%0];" ::"l"(rp[h] + 8));
-  }
-#endif
   // two accumulators per tile (even and odd 16-byte chunk steps) halve the
   // chain of dependent tensor-core ops
   float c0[2][4] = {}, c1[2][4] = {};

@@ -18,6 +18,7 @@
 //      threshold changes after every insertion, so the warp computes a batch of
 //      candidates in parallel and replays the decisions entry by entry.
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1042,7 +1043,8 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
 // (dropped split terms < 3 * 2^-16 |q| |c|, accumulation < 600 * 2^-24 |q| |c|,
 // the norms and the oracle's own sum < 200 * 2^-24 (|q|^2 + |c|^2); a factor
 // of four above their sum).  k_route_fix then takes U, the n_probe-th
-// smallest upper bound D~ + eps of a query's row, and writes the exact
+// smallest upper bound D~ + eps of a query's row (n_probe <= 64; wider probes
+// route with the exact k_route), and writes the exact
 // coordinate-order distance for every centroid whose lower bound D~ - eps is
 // at most U, and +inf for the rest.  Every centroid of the exact n_probe
 // nearest (ties included) has its lower bound at most U, so the selection
@@ -1130,17 +1132,19 @@ __global__ void __launch_bounds__(256) k_route_tc(const float *__restrict__ Q, u
     }
 }
 
-// Per query (one warp): U = the n_probe-th smallest upper bound of its row,
-// then the exact distance for every column whose lower bound is at most U,
-// +inf elsewhere.
+// Per query (one warp): U = the n_probe-th smallest upper bound of its row
+// (n_probe <= 64: a sorted list of the smallest upper bounds, most columns
+// rejected by one compare against the list's worst), then the exact distance
+// for every column whose lower bound is at most U, +inf elsewhere.
 __global__ void __launch_bounds__(128) k_route_fix(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
                                                    const float *__restrict__ C, const uint32_t *__restrict__ cidx,
                                                    uint32_t d, uint32_t dpad, int metric, const float *__restrict__ qn,
                                                    const float *__restrict__ cn, float *D, uint32_t ldd,
                                                    uint32_t nprobe) {
-  __shared__ uint32_t hist_all[4][2048];
+  __shared__ __align__(16) uint64_t lists[4][2][64];
+  __shared__ __align__(16) uint64_t cst[4][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t *hist = hist_all[warp];
+  uint64_t *const bufs[2] = {lists[warp][0], lists[warp][1]};
   const uint32_t nl = __ldg(cidx);
   const uint32_t *col = cidx + 1;
   for (uint32_t q = blockIdx.x * 4 + warp; q < nq; q += gridDim.x * 4) {
@@ -1148,18 +1152,14 @@ __global__ void __launch_bounds__(128) k_route_fix(const float *__restrict__ Q, 
     const float qq = qn[q];
     float U = __int_as_float(0x7f800000);
     if (nprobe < nl) {
-      uint32_t need = nprobe, prefix = 0, mask = 0;
-      auto ub_bits = [&](uint32_t j, bool &ok) {
-        ok = true;
-        return __float_as_uint(fmaxf(rq[j] + route_eps(qq, __ldg(cn + j)), 0.0f));
-      };
-      const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
-      for (int ps = 0; ps < 3; ++ps) {
-        const uint32_t b = pm_radix_pass(hist, nl, ub_bits, prefix, mask, shifts[ps], widths[ps], need, lane);
-        prefix |= b << shifts[ps];
-        mask |= ((1u << widths[ps]) - 1u) << shifts[ps];
+      int cur = 0, size = 0;
+      for (uint32_t j0 = 0; j0 < nl; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        const uint64_t key =
+            j < nl ? make_key(fmaxf(rq[j] + route_eps(qq, __ldg(cn + j)), 0.0f), j) : kKeyInvalid;
+        insert_batch(key, bufs, cur, size, (int)nprobe, cst[warp], lane);
       }
-      U = __uint_as_float(prefix);
+      U = key_dist(bufs[cur][nprobe - 1]);
     }
     const float *qr = Q + (size_t)q * qstride;
     for (uint32_t j = lane; j < nl; j += 32) {
@@ -1676,7 +1676,9 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
       ac.route = (const float *)s->route.p;
       ac.route_idx = lidx;
       dim3 grid((s->nblocks + kRT - 1) / kRT, (qn + kRT - 1) / kRT);
-      if (s->metric == DG_L2 || s->metric == DG_L2SQ) {
+      // DG_SPF_EXACT_ROUTE=1 routes with the exact kernel only (a test knob)
+      static const bool exact_only = std::getenv("DG_SPF_EXACT_ROUTE") && atoi(std::getenv("DG_SPF_EXACT_ROUTE"));
+      if ((s->metric == DG_L2 || s->metric == DG_L2SQ) && nprobe <= 64 && !exact_only) {
         // tensor-core approximation, then exact distances for the candidates of each row
         float *qnorm = (float *)s->rnorm.p, *cnorm = qnorm + chunk;
         k_route_norms<<<(unsigned)std::min<size_t>(((size_t)qn + s->nblocks + 255) / 256, 148 * 16), 256, 0, st>>>(
