@@ -106,6 +106,28 @@ __device__ __forceinline__ float batch_distance(const SearchArgs &a, uint8_t *ws
   }
 }
 
+// Stages the unvisited neighbours of an expanded node (its adjacency row) into
+// stage[0..return), marking them visited.  The first 64 entries are loaded
+// before any is tested, so a row of up to 64 neighbours costs one DRAM round
+// trip instead of one per 32 entries.
+__device__ __forceinline__ int stage_neighbours(const SearchArgs &a, const uint32_t *row, const Visited &vt,
+                                                uint32_t *stage, int lane) {
+  const uint32_t n0 = (uint32_t)lane < a.R ? __ldg(row + lane) : DG_PAD;
+  const uint32_t n1 = (uint32_t)lane + 32 < a.R ? __ldg(row + lane + 32) : DG_PAD;
+  int ns = 0;
+  for (uint32_t j0 = 0; j0 < a.R; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const uint32_t nb = j0 == 0 ? n0 : j0 == 32 ? n1 : (j < a.R ? __ldg(row + j) : DG_PAD);
+    bool ok = nb != DG_PAD && nb < a.n;
+    if (ok) ok = !vt.test_and_set(nb);
+    const uint32_t m = __ballot_sync(kFull, ok);
+    if (ok) stage[ns + __popc(m & lanemask_lt(lane))] = nb;
+    ns += __popc(m);
+  }
+  __syncwarp();
+  return ns;
+}
+
 // Exact FP32 distance of lane j's candidate (rerank, src/quantized.rs:110-121).
 template <int MET, int LPRF>
 __device__ __forceinline__ float exact_distance(const SearchArgs &a, const float *qs, uint32_t cand,
@@ -426,18 +448,7 @@ __device__ inline void search_one_reg(const SearchArgs &a, uint32_t q, uint8_t *
     }
     ++n_exp;
     // stage unvisited neighbours
-    const uint32_t *row = a.adj + (size_t)key_id(best) * a.R;
-    int ns = 0;
-    for (uint32_t j0 = 0; j0 < a.R; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
-      bool ok = nb != DG_PAD && nb < a.n;
-      if (ok) ok = !vt.test_and_set(nb);
-      const uint32_t m = __ballot_sync(kFull, ok);
-      if (ok) stage[ns + __popc(m & lanemask_lt(lane))] = nb;
-      ns += __popc(m);
-    }
-    __syncwarp();
+    const int ns = stage_neighbours(a, a.adj + (size_t)key_id(best) * a.R, vt, stage, lane);
     n_dist += ns;
     // distances; keep only keys below the current worst (the rest cannot enter)
     int nsurv = 0;
@@ -592,19 +603,7 @@ __device__ inline void search_one(const SearchArgs &a, uint32_t q, uint8_t *wsm,
     ++n_exp;
 
     // ---- stage unvisited neighbours
-    const uint32_t node = key_id(best);
-    const uint32_t *row = a.adj + (size_t)node * a.R;
-    ns = 0;
-    for (uint32_t j0 = 0; j0 < a.R; j0 += 32) {
-      const uint32_t j = j0 + lane;
-      const uint32_t nb = j < a.R ? __ldg(row + j) : DG_PAD;
-      bool ok = nb != DG_PAD && nb < a.n;
-      if (ok) ok = !vt.test_and_set(nb);
-      const uint32_t m = __ballot_sync(kFull, ok);
-      if (ok) stage[ns + __popc(m & lanemask_lt(lane))] = nb;
-      ns += __popc(m);
-    }
-    __syncwarp();
+    ns = stage_neighbours(a, a.adj + (size_t)key_id(best) * a.R, vt, stage, lane);
   }
 
   // ---- emit
