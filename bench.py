@@ -400,12 +400,12 @@ def algorithmic_bytes(name, nq, L, E, N, d=128):
     return nq * (adj + dist + rr + 4 * d + 8 * K)
 
 
-def _oracle_variant(X, adj, med, pq, name):
+def _oracle_variant(X, adj, med, pq, name, native=False):
     """The oracle index of a variant (test infrastructure, run only as the checker
-    of the parity leg and as the CPU baseline)."""
+    of the parity leg and, built for the host's own CPU, as the CPU baseline)."""
     import oracle
 
-    o = oracle.OracleIndex(X, adj, med)
+    o = oracle.OracleIndex(X, adj, med, native=native)
     if name == "pq_rerank":
         o.set_pq(*pq)
     elif name == "int8_rerank":
@@ -1081,7 +1081,7 @@ def cpu_baseline(args, X, Q, adj, med, pq, name, L, threads=None):
     """The oracle's search of the same variant and beam on the host cores, over
     about cpu_seconds of queries (the batch, cycled)."""
     threads = threads or os.cpu_count() or 1
-    o = _oracle_variant(X, adj, med, pq, name)
+    o = _oracle_variant(X, adj, med, pq, name, native=True)
     t0 = time.time()
     _oracle_run(o, name, Q[:200], L, threads)
     rate = 200 / max(time.time() - t0, 1e-6)
@@ -1110,7 +1110,7 @@ def reference_arm(args):
     X, Q, adj, med, pq, gt, _ = workload(args, int(os.environ.get("LOCAL_RANK", "0")))
     threads = os.cpu_count() or 1
     name = HEADLINE
-    o = _oracle_variant(X, adj, med, pq, name)
+    o = _oracle_variant(X, adj, med, pq, name, native=True)
     L, curve = L_SWEEP[-1], []
     for Lc in L_SWEEP:
         ids, _, _ = _oracle_run(o, name, Q, Lc, threads)
@@ -1139,8 +1139,8 @@ def reference_arm(args):
         "p99_ms": float(np.percentile(np.array(step_s) * 1e3, 99)),
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
                          "sample": f"the {len(Q)}-query batch per step: BF16 traversal + FP32 rerank of the top "
-                                   f"{L} (CPU restatement of the reference's quantized search, OpenMP over "
-                                   f"queries)"},
+                                   f"{L} (CPU restatement of the reference's quantized search, -O3 -march=native, "
+                                   f"OpenMP over queries)"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

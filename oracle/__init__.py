@@ -34,6 +34,8 @@ def build() -> str:
 
 
 _lib = None
+_native = None
+_SO_NATIVE = os.path.join(_HERE, "_build", "libdgoracle_native.so")
 
 
 def lib():
@@ -46,6 +48,17 @@ def lib():
         _lib = C.CDLL(_SO)
         _declare(_lib)
     return _lib
+
+
+def lib_native():
+    """The same oracle compiled for the machine running it (-O3 -march=native),
+    built there on first use: the CPU timing legs of the bench use it."""
+    global _native
+    if _native is None:
+        subprocess.run(["make", "-s", "-C", _HERE, "native"], check=True)
+        _native = C.CDLL(_SO_NATIVE)
+        _declare(_native)
+    return _native
 
 
 class FilterOp(C.Structure):
@@ -202,7 +215,8 @@ def filter_matches(ops, pool, labels):
 class OracleIndex:
     """Holds numpy buffers alive for a DgoIndex view."""
 
-    def __init__(self, vectors, adjacency, medoid_id, metric=L2SQ):
+    def __init__(self, vectors, adjacency, medoid_id, metric=L2SQ, native=False):
+        self._L = lib_native() if native else lib()
         self.vectors = _f32(vectors)
         self.adj = np.ascontiguousarray(adjacency, dtype=np.uint32)
         self.s = Index()
@@ -277,7 +291,7 @@ class OracleIndex:
         cnt = np.zeros(nq, dtype=np.uint32)
         st = np.zeros((nq, 2), dtype=np.uint32)
         pl = None if per_query_L is None else np.ascontiguousarray(per_query_L, dtype=np.uint32)
-        lib().dgo_search_batch(C.byref(self.s), C.byref(p), _p(Q), nq, _p(pl), _p(ids), _p(ds),
+        self._L.dgo_search_batch(C.byref(self.s), C.byref(p), _p(Q), nq, _p(pl), _p(ids), _p(ds),
                                _p(cnt), _p(st), threads)
         if with_stats:
             return ids, ds, cnt, st
@@ -303,7 +317,7 @@ class OracleIndex:
         ds = np.zeros((nq, k), dtype=np.float32)
         cnt = np.zeros(nq, dtype=np.uint32)
         cl = self.s.n if code_limit is None else code_limit
-        lib().dgo_incremental_search_batch(C.byref(self.s), C.byref(p), _p(sd), len(sd), _p(dd), int(ntomb),
+        self._L.dgo_incremental_search_batch(C.byref(self.s), C.byref(p), _p(sd), len(sd), _p(dd), int(ntomb),
                                            int(cl), _p(Q), nq, _p(ids), _p(ds), _p(cnt), threads)
         return ids, ds, cnt
 
