@@ -736,7 +736,8 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
   const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded,
-                                    (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2);
+                                    (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2,
+                                    idx->R);
   auto launch = [&](const SearchArgs &a0, cudaStream_t ss) -> DgStatus {
     LaunchInfo info;
     SearchArgs aa = a0;
@@ -1170,7 +1171,8 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   else if (trav == TRAV_INT8) lpr = lanes_per_row(idx->code_stride / 16);
   const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded,
-                                    (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2);
+                                    (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2,
+                                    idx->R);
   LaunchInfo info;
   switch (trav) {
     case TRAV_F32: s = launch_search_f32(a, Ly, met, lpr, lcap, filt, st, &info); break;
