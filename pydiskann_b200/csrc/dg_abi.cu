@@ -737,7 +737,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded,
                                     (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2,
-                                    idx->R);
+                                    idx->R, true);
   auto launch = [&](const SearchArgs &a0, cudaStream_t ss) -> DgStatus {
     LaunchInfo info;
     SearchArgs aa = a0;
@@ -1172,7 +1172,7 @@ extern "C" DgStatus dg_search_batch_static(DgIndex *idx, const DgSearchParams *p
   const WarpLayout Ly = warp_layout(trav, lcap, filt, hbits, idx->dpad, idx->pq_M, idx->pq_K,
                                     idx->rq_padded,
                                     (trav == TRAV_RABITQ || trav == TRAV_INT8) && met_kind(idx->metric) != MET_L2,
-                                    idx->R);
+                                    idx->R, true);
   LaunchInfo info;
   switch (trav) {
     case TRAV_F32: s = launch_search_f32(a, Ly, met, lpr, lcap, filt, st, &info); break;

@@ -93,16 +93,24 @@ struct WarpLayout {
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 // `decode`: RaBitQ or int8 with a cosine / dot metric (RaBitQ: rotated query
 // and nibble table; int8: four signed digit columns of the query).
+// `reg_list`: the search kernel keeps this launch's working list in registers
+// (unfiltered, beams <= 64); its 32-key compaction buffer then shares the
+// first 256 bytes of w0, which that path only uses as a scatter buffer
+// written after every read of the compacted keys.
 __host__ __device__ inline WarpLayout warp_layout(int trav, uint32_t lcap, bool filt, uint32_t hbits,
                                                   uint32_t dpad, uint32_t pq_M, uint32_t pq_K,
                                                   uint32_t rq_padded, bool decode = false,
-                                                  uint32_t degree = kStageCap) {
+                                                  uint32_t degree = kStageCap, bool reg_list = false) {
   WarpLayout L{};
   uint32_t o = 0;
   L.w0 = o; o += lcap * 8;
   L.w1 = o; o += lcap * 8;
   L.res = o; o += filt ? lcap * 8 : 0;
-  L.cstage = o; o += 32 * 8;
+  if (reg_list && lcap == 64 && !filt) {
+    L.cstage = L.w0;
+  } else {
+    L.cstage = o; o += 32 * 8;
+  }
   L.stage = o; o += align16(max(degree, 2u) * 4);  // one adjacency row, or the two seeds
   L.hash = o; o += (1u << hbits) * 4;
   L.qf = o; o += align16(dpad * 4);

@@ -56,7 +56,7 @@ struct DgSpfresh {
   std::vector<void *> allocs;
   DgIndex::Buf q, oids, od, ocnt, route;  // route: query x posting routing distances of one chunk
   DgIndex::Buf live_idx;                   // [0]: number of live postings, then their slot indices
-  DgIndex::Buf rnorm;                      // routing norms: |q|^2 of a chunk's queries, |c|^2 of the live centroids
+  DgIndex::Buf fr;                         // tensor-core routing: centre, norms and scales, FP16 halves
   // posting-major scan of one chunk: probes per query, (query, posting) pairs
   // grouped by posting, work items, per-pair candidate lists
   DgIndex::Buf probe, probe_cnt, pcount, pstart, pfill, istart, pair_q, pos_of, items, pair_keys, pair_cnt, misc;
@@ -1034,138 +1034,427 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
 }
 
 // ------------------------------------------------------ routing, tensor cores
-// Squared-L2 routing for many postings on the tensor cores.  k_route_tc
-// computes an approximation D~ = |q|^2 + |c|^2 - 2 q.c of every query x live
-// centroid pair, q.c as three BF16 products (qh.ch + qh.cl + ql.ch of the
-// two-term BF16 splits, FP32 accumulate), whose distance from the oracle's
-// coordinate-order FP32 sum is at most
-//   eps(q, c) = 1e-4 (|q|^2 + |c|^2) + 6e-4 |q| |c|
-// (dropped split terms < 3 * 2^-16 |q| |c|, accumulation < 600 * 2^-24 |q| |c|,
-// the norms and the oracle's own sum < 200 * 2^-24 (|q|^2 + |c|^2); a factor
-// of four above their sum).  k_route_fix then takes U, the n_probe-th
-// smallest upper bound D~ + eps of a query's row (n_probe <= 64; wider probes
-// route with the exact k_route), and writes the exact
-// coordinate-order distance for every centroid whose lower bound D~ - eps is
-// at most U, and +inf for the rest.  Every centroid of the exact n_probe
-// nearest (ties included) has its lower bound at most U, so the selection
-// that follows picks exactly the postings exact routing picks.
-constexpr float kRouteRel = 1e-4f, kRouteCross = 6e-4f;
-constexpr int kRTK = 32;             // dimensions staged per step
-constexpr int kRTS = kRTK + 8;       // staged row stride (BF16 elements): conflict-free ldmatrix
+// Posting-major batches under L2 with n_probe <= 64 and d <= 128 route on the
+// tensor cores.  Queries and live centroids are centred on the mean m of (up
+// to) 1024 live centroids, scaled per vector by a power of two (largest
+// coordinate below 2^14) and split into FP16 halves x = hi + lo; k_route_tcm
+// writes A = |q'|^2 + |c'|^2 - 2 q'.c' for every query x live centroid pair
+// (q' = q - m, c' = c - m; q'.c' as qh.ch + qh.cl + ql.ch, FP32 accumulate).
+// A is within
+//     E(q) = 4e-4 (|q'|^2 + max_c |c'|^2)
+// of the oracle's coordinate-order FP32 sum: the dropped lo.lo term and the
+// split leave < 3 * 2^-22 |q'||c'|, the accumulation < 3 d * 2^-23 |q'||c'|,
+// the norms, the centring and the oracle's own rounding < 3 (d + 4) * 2^-24
+// (|q'|^2 + |c'|^2); for d <= 128 all together stay below a quarter of E.
+// k_fr_select (a warp per query) then finds an upper bound U of the query's
+// n_probe-th smallest A (the n_probe-th smallest of the four smallest values
+// each lane saw), keeps every centroid with A <= U + 2 E(q) -- which holds
+// for every centroid of the exact n_probe nearest, ties included -- computes
+// their exact coordinate-order distances and takes the n_probe smallest
+// (distance, slot) keys in ascending order: the probes, and the order, of the
+// exact selection.  A query with more candidates than its list holds falls
+// back to exact distances for every live centroid.
+constexpr int kFrMeanRows = 1024;  // live centroids averaged for the centre
+constexpr int kFrC = 64;           // centroids per staged tile (k_route_tcm)
+constexpr int kFrTiles = 16;       // tiles per block of k_route_tcm
+constexpr int kFrCap = 256;        // candidate list of a query (k_fr_select)
+constexpr float kFrEps = 4e-4f;
 
-__device__ __forceinline__ float route_eps(float qq, float cc) {
-  return kRouteRel * (qq + cc) + kRouteCross * sqrtf(qq * cc);
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+
+__device__ __forceinline__ float ordered_float(uint32_t u) {
+  u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+  return __uint_as_float(u);
 }
 
-// |q|^2 of every query and |c|^2 of every live centroid (FP32, coordinate order).
-__global__ void k_route_norms(const float *__restrict__ Q, uint32_t nq, uint32_t qstride, const float *__restrict__ C,
-                              const uint32_t *__restrict__ cidx, uint32_t d, uint32_t dpad, float *qn, float *cn) {
+// The power-of-two scale that brings a vector whose largest |coordinate| is
+// mx below 2^14 (1 for a zero vector), and its inverse.
+__device__ __forceinline__ float2 fr_scale(float mx) {
+  if (!(mx > 0.0f)) return make_float2(1.0f, 1.0f);
+  int e;
+  frexpf(mx, &e);  // mx < 2^e
+  return make_float2(ldexpf(1.0f, 14 - e), ldexpf(1.0f, e - 14));
+}
+
+// The centre: mean of the first min(live, 1024) live centroids (one block of
+// 1024 threads, d <= 128); also clears the largest-norm word.
+__global__ void __launch_bounds__(1024) k_fr_mean(const float *__restrict__ C, const uint32_t *__restrict__ cidx,
+                                                  uint32_t d, uint32_t dpad, float *mu, uint32_t *maxcc_bits) {
+  __shared__ float part[8][128];
+  const uint32_t nl = __ldg(cidx), m = min(nl, (uint32_t)kFrMeanRows);
+  const uint32_t i = threadIdx.x & 127, rg = threadIdx.x >> 7;
+  float acc = 0.0f;
+  if (i < d)
+    for (uint32_t j = rg; j < m; j += 8) acc += __ldg(C + (size_t)__ldg(cidx + 1 + j) * dpad + i);
+  part[rg][i] = acc;
+  __syncthreads();
+  if (rg == 0 && i < d) {
+    float t = 0.0f;
+    for (int r = 0; r < 8; ++r) t += part[r][i];
+    mu[i] = m ? t / (float)m : 0.0f;
+  }
+  if (threadIdx.x == 0) *maxcc_bits = 0u;
+}
+
+// Per live centroid j (a warp each): c' = c - m, |c'|^2, FP16 hi / lo halves of
+// c' s in rows of kd halves (zero padded past d), (|c'|^2, 1 / s), and the
+// largest |c'|^2 (as float bits: norms are non-negative).
+__global__ void __launch_bounds__(256) k_fr_centroids(const float *__restrict__ C, const uint32_t *__restrict__ cidx,
+                                                      uint32_t d, uint32_t dpad, uint32_t kd,
+                                                      const float *__restrict__ mu, __half *ch, __half *cl,
+                                                      float2 *cinfo, uint32_t *maxcc_bits) {
   const uint32_t nl = __ldg(cidx);
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nq + nl; t += gridDim.x * blockDim.x) {
-    const float *x = t < nq ? Q + (size_t)t * qstride : C + (size_t)__ldg(cidx + 1 + (t - nq)) * dpad;
-    float s2 = 0.0f;
-    for (uint32_t i = 0; i < d; ++i) s2 = __fadd_rn(s2, __fmul_rn(x[i], x[i]));
-    if (t < nq) qn[t] = s2;
-    else cn[t - nq] = s2;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nl; j += nw) {
+    const float *c = C + (size_t)__ldg(cidx + 1 + j) * dpad;
+    float v[4], s2 = 0.0f, mx = 0.0f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = lane + 32u * u;
+      v[u] = i < d ? __fsub_rn(__ldg(c + i), __ldg(mu + i)) : 0.0f;
+      s2 = fmaf(v[u], v[u], s2);
+      mx = fmaxf(mx, fabsf(v[u]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s2 += __shfl_xor_sync(kFull, s2, o);
+      mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+    }
+    const float2 sc = fr_scale(mx);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = lane + 32u * u;
+      if (i < kd) {
+        const float x = v[u] * sc.x;
+        const __half h = __float2half_rn(x);
+        ch[(size_t)j * kd + i] = h;
+        cl[(size_t)j * kd + i] = __float2half_rn(x - __half2float(h));
+      }
+    }
+    if (lane == 0) {
+      cinfo[j] = make_float2(s2, sc.y);
+      atomicMax(maxcc_bits, __float_as_uint(s2));
+    }
   }
 }
 
-// One block: 64 queries x 64 live centroids; warp w computes queries
-// 16 (w % 4) .. +15 against centroids 32 (w / 4) .. +31.
-__global__ void __launch_bounds__(256) k_route_tc(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
-                                                  const float *__restrict__ C, const uint32_t *__restrict__ cidx,
-                                                  uint32_t d, uint32_t dpad, const float *__restrict__ qn,
-                                                  const float *__restrict__ cn, float *__restrict__ D, uint32_t ldd) {
-  __shared__ __align__(16) uint16_t qs[2][kRT * kRTS], cs[2][kRT * kRTS];  // [hi, lo][row][k]
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t q0 = blockIdx.y * kRT, c0 = blockIdx.x * kRT;
-  const uint32_t nl = __ldg(cidx);
-  if (c0 >= nl) return;  // the whole block: fewer live postings than slots
-  const uint32_t *col = cidx + 1;
-  const uint32_t m16 = 16u * (warp & 3), n32 = 32u * (warp >> 2);
-  float acc[4][4] = {};
-  const uint32_t qs_s[2] = {(uint32_t)__cvta_generic_to_shared(qs[0]), (uint32_t)__cvta_generic_to_shared(qs[1])};
-  const uint32_t cs_s[2] = {(uint32_t)__cvta_generic_to_shared(cs[0]), (uint32_t)__cvta_generic_to_shared(cs[1])};
-  const uint32_t arow = m16 + (lane & 15), acol = (lane >> 4) * 8;
-  const uint32_t brow = (lane >> 4) * 8 + (lane & 7), bcol = ((lane >> 3) & 1) * 8;
-  for (uint32_t k0 = 0; k0 < d; k0 += kRTK) {
-    for (uint32_t e = threadIdx.x; e < (uint32_t)kRT * kRTK; e += blockDim.x) {
-      const uint32_t r = e / kRTK, k = e % kRTK, kk = k0 + k;
-      const float xq = (q0 + r < nq && kk < d) ? __ldg(Q + (size_t)(q0 + r) * qstride + kk) : 0.0f;
-      const float xc = (c0 + r < nl && kk < d) ? __ldg(C + (size_t)__ldg(col + c0 + r) * dpad + kk) : 0.0f;
-      const __nv_bfloat16 hq = __float2bfloat16_rn(xq), hc = __float2bfloat16_rn(xc);
-      qs[0][r * kRTS + k] = __bfloat16_as_ushort(hq);
-      qs[1][r * kRTS + k] = __bfloat16_as_ushort(__float2bfloat16_rn(xq - __bfloat162float(hq)));
-      cs[0][r * kRTS + k] = __bfloat16_as_ushort(hc);
-      cs[1][r * kRTS + k] = __bfloat16_as_ushort(__float2bfloat16_rn(xc - __bfloat162float(hc)));
-    }
-    __syncthreads();
-#pragma unroll
-    for (int ks = 0; ks < kRTK; ks += 16) {
-      uint32_t ah[4], al[4], bh[2][4], bl[2][4];
-      ldsm_x4(ah, qs_s[0] + 2u * (arow * kRTS + ks + acol));
-      ldsm_x4(al, qs_s[1] + 2u * (arow * kRTS + ks + acol));
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        ldsm_x4(bh[h], cs_s[0] + 2u * ((n32 + 16 * h + brow) * kRTS + ks + bcol));
-        ldsm_x4(bl[h], cs_s[1] + 2u * ((n32 + 16 * h + brow) * kRTS + ks + bcol));
-      }
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const uint32_t(&bhh)[4] = bh[nt >> 1], (&bll)[4] = bl[nt >> 1];
-        const int o = 2 * (nt & 1);
-        mma_bf16_16x8x16(acc[nt], ah[0], ah[1], ah[2], ah[3], bhh[o], bhh[o + 1]);
-        mma_bf16_16x8x16(acc[nt], ah[0], ah[1], ah[2], ah[3], bll[o], bll[o + 1]);
-        mma_bf16_16x8x16(acc[nt], al[0], al[1], al[2], al[3], bhh[o], bhh[o + 1]);
-      }
-    }
-    __syncthreads();
+// seq_metric for L2 / squared L2 between 16-byte aligned rows (d % 4 == 0):
+// the same coordinate-order arithmetic, four coordinates per load.
+__device__ __forceinline__ float seq_l2_rows4(const float *q, const float *x, uint32_t d, int metric) {
+  const float4 *q4 = reinterpret_cast<const float4 *>(q), *x4 = reinterpret_cast<const float4 *>(x);
+  float acc = 0.0f;
+#pragma unroll 4
+  for (uint32_t i = 0; i < d / 4; ++i) {
+    const float4 a = __ldg(q4 + i), b = __ldg(x4 + i);
+    float t = __fsub_rn(a.x, b.x);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(a.y, b.y);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(a.z, b.z);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
+    t = __fsub_rn(a.w, b.w);
+    acc = __fadd_rn(acc, __fmul_rn(t, t));
   }
-  // lane (g, t): queries g, g + 8 x centroids 2t, 2t + 1 of each 8-centroid tile
-  const uint32_t g = lane >> 2, t2 = 2 * (lane & 3);
-#pragma unroll
-  for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const uint32_t q = q0 + m16 + g + (e >= 2 ? 8 : 0), c = c0 + n32 + 8 * nt + t2 + (e & 1);
-      if (q < nq && c < nl) D[(size_t)q * ldd + c] = __fsub_rn(__fadd_rn(qn[q], cn[c]), 2.0f * acc[nt][e]);
-    }
+  return metric == DG_L2 ? __fsqrt_rn(acc) : acc;
 }
 
-// Per query (one warp): U = the n_probe-th smallest upper bound of its row
-// (n_probe <= 64: a sorted list of the smallest upper bounds, most columns
-// rejected by one compare against the list's worst), then the exact distance
-// for every column whose lower bound is at most U, +inf elsewhere.
-__global__ void __launch_bounds__(128) k_route_fix(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
-                                                   const float *__restrict__ C, const uint32_t *__restrict__ cidx,
-                                                   uint32_t d, uint32_t dpad, int metric, const float *__restrict__ qn,
-                                                   const float *__restrict__ cn, float *D, uint32_t ldd,
-                                                   uint32_t nprobe) {
-  __shared__ __align__(16) uint64_t lists[4][2][64];
-  __shared__ __align__(16) uint64_t cst[4][32];
+// Per query q of a chunk (a warp each): q' = q - m, |q'|^2, FP16 hi / lo halves
+// of q' s in rows of kd halves, and (|q'|^2, -2 / s, E(q), 0).
+__global__ void __launch_bounds__(256) k_fr_queries(const float *__restrict__ Q, uint32_t nq, uint32_t qstride,
+                                                    uint32_t d, uint32_t kd, const float *__restrict__ mu,
+                                                    const uint32_t *__restrict__ maxcc_bits, __half *qh, __half *ql,
+                                                    float4 *qinfo) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const float maxcc = __uint_as_float(__ldg(maxcc_bits));
+  for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nq; q += nw) {
+    float v[4], s2 = 0.0f, mx = 0.0f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = lane + 32u * u;
+      v[u] = i < d ? __fsub_rn(__ldg(Q + (size_t)q * qstride + i), __ldg(mu + i)) : 0.0f;
+      s2 = fmaf(v[u], v[u], s2);
+      mx = fmaxf(mx, fabsf(v[u]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s2 += __shfl_xor_sync(kFull, s2, o);
+      mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+    }
+    const float2 sc = fr_scale(mx);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = lane + 32u * u;
+      if (i < kd) {
+        const float x = v[u] * sc.x;
+        const __half h = __float2half_rn(x);
+        qh[(size_t)q * kd + i] = h;
+        ql[(size_t)q * kd + i] = __float2half_rn(x - __half2float(h));
+      }
+    }
+    if (lane == 0) qinfo[q] = make_float4(s2, -2.0f * sc.y, __fmul_ru(kFrEps, __fadd_ru(s2, maxcc)), 0.0f);
+  }
+}
+
+// A for 64 queries (4 warps x 16) x kFrTiles tiles of 64 live centroids per
+// block, into D (rows ldd floats apart, ldd a multiple of 4).  Query
+// fragments come straight from the hi / lo rows into registers; centroid
+// tiles are staged in shared memory (double-buffered asynchronous copies) and
+// read with ldmatrix.
+template <int KS>
+__global__ void __launch_bounds__(128) k_route_tcm(const __half *__restrict__ qh, const __half *__restrict__ ql,
+                                                   const float4 *__restrict__ qinfo, uint32_t nq,
+                                                   const __half *__restrict__ ch, const __half *__restrict__ cl,
+                                                   const float2 *__restrict__ cinfo,
+                                                   const uint32_t *__restrict__ cidx, float *__restrict__ D,
+                                                   uint32_t ldd) {
+  constexpr int KD = 16 * KS, RS = KD + 8;  // staged row stride (halves): conflict-free ldmatrix
+  constexpr int CH = KD / 8;                // 16-byte chunks per row
+  extern __shared__ __align__(16) uint8_t smem[];
+  __half *tiles = reinterpret_cast<__half *>(smem);                         // [stage][hi, lo][kFrC][RS]
+  float2 *tinfo = reinterpret_cast<float2 *>(smem + 2 * 2 * kFrC * RS * 2);  // [stage][kFrC]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint64_t *const bufs[2] = {lists[warp][0], lists[warp][1]};
+  const int g = lane >> 2, t = lane & 3;
   const uint32_t nl = __ldg(cidx);
+  const int t0 = blockIdx.y * kFrTiles;
+  const int ntile = min(kFrTiles, (int)((nl + kFrC - 1) / kFrC) - t0);
+  if (ntile <= 0) return;  // the whole block: past the live centroids
+  const uint32_t qa = blockIdx.x * 64 + warp * 16 + g, qb = qa + 8;
+  // A fragments: rows g, g + 8; k = 2t, 2t + 1 (+8) of each 16-dimension step
+  uint32_t ah[KS][4], al[KS][4];
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks) {
+    const uint32_t *ra = reinterpret_cast<const uint32_t *>(qh + (size_t)min(qa, nq - 1) * KD + 16 * ks + 2 * t);
+    const uint32_t *rb = reinterpret_cast<const uint32_t *>(qh + (size_t)min(qb, nq - 1) * KD + 16 * ks + 2 * t);
+    const uint32_t *la = reinterpret_cast<const uint32_t *>(ql + (size_t)min(qa, nq - 1) * KD + 16 * ks + 2 * t);
+    const uint32_t *lb = reinterpret_cast<const uint32_t *>(ql + (size_t)min(qb, nq - 1) * KD + 16 * ks + 2 * t);
+    ah[ks][0] = __ldg(ra);
+    ah[ks][1] = __ldg(rb);
+    ah[ks][2] = __ldg(ra + 4);
+    ah[ks][3] = __ldg(rb + 4);
+    al[ks][0] = __ldg(la);
+    al[ks][1] = __ldg(lb);
+    al[ks][2] = __ldg(la + 4);
+    al[ks][3] = __ldg(lb + 4);
+  }
+  const float4 ia = __ldg(qinfo + min(qa, nq - 1)), ib = __ldg(qinfo + min(qb, nq - 1));
+  auto stage = [&](int tt, int sb) {
+    const uint32_t j0 = (uint32_t)(t0 + tt) * kFrC;
+    for (int e = threadIdx.x; e < 2 * kFrC * CH; e += 128) {
+      const int hl = e / (kFrC * CH), rem = e - hl * (kFrC * CH), r = rem / CH, c = rem - r * CH;
+      const uint32_t j = j0 + r;
+      const __half *src = (hl ? cl : ch) + (j < nl ? (size_t)j * KD + c * 8 : 0);
+      cp_async16(tiles + ((size_t)(sb * 2 + hl) * kFrC + r) * RS + c * 8, src, j < nl ? 16u : 0u);
+    }
+    if (threadIdx.x < kFrC / 2) {
+      const uint32_t j = j0 + 2 * threadIdx.x;
+      cp_async16(tinfo + sb * kFrC + 2 * threadIdx.x, cinfo + (j < nl ? j : 0), j + 1 < nl ? 16u : (j < nl ? 8u : 0u));
+    }
+    cp_async_commit();
+  };
+  stage(0, 0);
+  const uint32_t bo = 2u * (((lane >> 4) * 8 + (lane & 7)) * RS + ((lane >> 3) & 1) * 8);
+  for (int tt = 0; tt < ntile; ++tt) {
+    const int sb = tt & 1;
+    if (tt + 1 < ntile) {
+      stage(tt + 1, sb ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+    const uint32_t th_s = (uint32_t)__cvta_generic_to_shared(tiles + (size_t)(sb * 2) * kFrC * RS);
+    const uint32_t tl_s = th_s + 2u * kFrC * RS;
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        uint32_t bh[4], bl[4];
+        const uint32_t off = bo + 2u * (16 * h * RS + 16 * ks);
+        ldsm_x4(bh, th_s + off);
+        ldsm_x4(bl, tl_s + off);
+#pragma unroll
+        for (int o = 0; o < 2; ++o) {
+          float(&c)[4] = acc[2 * h + o];
+          mma_f16_16x8x16(c, ah[ks], bh[2 * o], bh[2 * o + 1]);
+          mma_f16_16x8x16(c, ah[ks], bl[2 * o], bl[2 * o + 1]);
+          mma_f16_16x8x16(c, al[ks], bh[2 * o], bh[2 * o + 1]);
+        }
+      }
+    }
+    // lane (g, t): queries qa, qb x centroids 2t, 2t + 1 of each 8-centroid n-tile
+    const uint32_t j0 = (uint32_t)(t0 + tt) * kFrC;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const int cc = 8 * nt + 2 * t;
+      const uint32_t j = j0 + cc;
+      const float2 c0 = tinfo[sb * kFrC + cc], c1 = tinfo[sb * kFrC + cc + 1];
+      if (j < nl) {  // j even, ldd a multiple of 4: the pair is 8-byte aligned (column j + 1 may be padding)
+        if (qa < nq)
+          *reinterpret_cast<float2 *>(D + (size_t)qa * ldd + j) =
+              make_float2(fmaf(ia.y * c0.y, acc[nt][0], __fadd_rn(ia.x, c0.x)),
+                          fmaf(ia.y * c1.y, acc[nt][1], __fadd_rn(ia.x, c1.x)));
+        if (qb < nq)
+          *reinterpret_cast<float2 *>(D + (size_t)qb * ldd + j) =
+              make_float2(fmaf(ib.y * c0.y, acc[nt][2], __fadd_rn(ib.x, c0.x)),
+                          fmaf(ib.y * c1.y, acc[nt][3], __fadd_rn(ib.x, c1.x)));
+      }
+    }
+    __syncthreads();  // every warp is done with this stage before it is refilled
+  }
+}
+
+static size_t fr_tcm_smem(int ks) { return 2 * 2 * kFrC * (16 * (size_t)ks + 8) * 2 + 2 * kFrC * 8; }
+
+// Probes of each query from its row of A (a warp per query, 4 per block):
+// U = the n-th smallest of the four smallest values of every lane (U is at
+// least the row's n-th smallest A), the live indices with A <= U + 2 E(q)
+// into a list, their exact distances, the n smallest (distance, slot) keys,
+// the probe_ratio cut of the query-major selection.
+__global__ void __launch_bounds__(128) k_fr_select(const float *__restrict__ D, uint32_t ldd, uint32_t nq,
+                                                   const float4 *__restrict__ qinfo, const float *__restrict__ Q,
+                                                   uint32_t qstride, uint32_t d, const float *__restrict__ C,
+                                                   uint32_t dpad, const uint32_t *__restrict__ cidx, int metric,
+                                                   uint32_t nprobe, float probe_ratio, uint32_t *probe_out,
+                                                   uint32_t *probe_cnt) {
+  __shared__ uint32_t lists[4][kFrCap];
+  __shared__ __align__(16) uint64_t keys[4][kFrCap];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t n = max(nprobe, 1u), nl = __ldg(cidx);
   const uint32_t *col = cidx + 1;
+  uint32_t *lst = lists[warp];
+  uint64_t *K = keys[warp];
+  const float inf = __int_as_float(0x7f800000);
   for (uint32_t q = blockIdx.x * 4 + warp; q < nq; q += gridDim.x * 4) {
-    float *rq = D + (size_t)q * ldd;
-    const float qq = qn[q];
-    float U = __int_as_float(0x7f800000);
-    if (nprobe < nl) {
+    const float *row = D + (size_t)q * ldd;
+    const float4 *row4 = reinterpret_cast<const float4 *>(row);
+    const uint32_t n4 = nl / 4;
+    float bound = inf;
+    if (nl > n) {
+      // the four smallest values this lane sees
+      float t0 = inf, t1 = inf, t2 = inf, t3 = inf;
+      auto see = [&](float v) {
+        if (v < t3) {
+          t3 = v;
+          if (t3 < t2) { const float x = t2; t2 = t3; t3 = x; }
+          if (t2 < t1) { const float x = t1; t1 = t2; t2 = x; }
+          if (t1 < t0) { const float x = t0; t0 = t1; t1 = x; }
+        }
+      };
+      for (uint32_t i = lane; i < n4; i += 32) {
+        const float4 v = __ldg(row4 + i);
+        see(v.x);
+        see(v.y);
+        see(v.z);
+        see(v.w);
+      }
+      if (4 * n4 + lane < nl) see(__ldg(row + 4 * n4 + lane));
+      // U: the n-th smallest of the 128 kept values (ordered bits, bisection)
+      const uint32_t u0 = ordered_bits(t0), u1 = ordered_bits(t1), u2 = ordered_bits(t2), u3 = ordered_bits(t3);
+      uint32_t lo = 0, hi = 0xffffffffu;
+      while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        const uint32_t c = __reduce_add_sync(kFull, (uint32_t)(u0 <= mid) + (u1 <= mid) + (u2 <= mid) + (u3 <= mid));
+        if (c >= n) hi = mid;
+        else lo = mid + 1;
+      }
+      bound = __fadd_ru(ordered_float(lo), 2.0f * __ldg(qinfo + q).z);
+    }
+    // the candidates: every live index with A <= bound (all of them when nl <= n)
+    int m = 0;
+    for (uint32_t i0 = 0; i0 < n4 + 1; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      float4 v = make_float4(inf, inf, inf, inf);
+      if (i < n4) v = __ldg(row4 + i);
+      else if (i == n4) {
+        if (4 * n4 < nl) v.x = __ldg(row + 4 * n4);
+        if (4 * n4 + 1 < nl) v.y = __ldg(row + 4 * n4 + 1);
+        if (4 * n4 + 2 < nl) v.z = __ldg(row + 4 * n4 + 2);
+      }
+      const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t j = 4 * i + u;
+        const bool keep = j < nl && (vv[u] <= bound || nl <= n);
+        const uint32_t km = __ballot_sync(kFull, keep);
+        const int pos = m + __popc(km & lanemask_lt(lane));
+        if (keep && pos < kFrCap) lst[pos] = j;
+        m += __popc(km);
+      }
+    }
+    __syncwarp();
+    const float *qg = Q + (size_t)q * qstride;
+    int np;
+    const uint64_t *sorted;
+    if (m <= kFrCap) {
+      constexpr int PL = kFrCap / 32;
+      uint64_t kk[PL];
+#pragma unroll
+      for (int u = 0; u < PL; ++u) {
+        const int x = lane + 32 * u;
+        kk[u] = kKeyInvalid;
+        if (x < m) {
+          const uint32_t slot = __ldg(col + lst[x]);
+          kk[u] = make_key(seq_l2_rows4(qg, C + (size_t)slot * dpad, d, metric), slot);
+          K[x] = kk[u];
+        }
+      }
+      __syncwarp();
+      int rk[PL];
+#pragma unroll
+      for (int u = 0; u < PL; ++u) {
+        rk[u] = 0;
+        if (lane + 32 * u < m)
+          for (int x = 0; x < m; ++x) rk[u] += K[x] < kk[u] ? 1 : 0;
+      }
+      __syncwarp();
+      np = min((int)n, m);
+#pragma unroll
+      for (int u = 0; u < PL; ++u)
+        if (lane + 32 * u < m && rk[u] < np) K[rk[u]] = kk[u];
+      __syncwarp();
+      sorted = K;
+    } else {  // too many candidates: exact distances of every live centroid, a sorted list of n
+      uint64_t *const P[2] = {K, K + 64};
+      uint64_t *cst = K + 128;
       int cur = 0, size = 0;
       for (uint32_t j0 = 0; j0 < nl; j0 += 32) {
         const uint32_t j = j0 + lane;
-        const uint64_t key =
-            j < nl ? make_key(fmaxf(rq[j] + route_eps(qq, __ldg(cn + j)), 0.0f), j) : kKeyInvalid;
-        insert_batch(key, bufs, cur, size, (int)nprobe, cst[warp], lane);
+        uint64_t key = kKeyInvalid;
+        if (j < nl) {
+          const uint32_t slot = __ldg(col + j);
+          key = make_key(seq_l2_rows4(qg, C + (size_t)slot * dpad, d, metric), slot);
+        }
+        insert_batch(key, P, cur, size, (int)n, cst, lane);
       }
-      U = key_dist(bufs[cur][nprobe - 1]);
+      np = size;
+      sorted = P[cur];
     }
-    const float *qr = Q + (size_t)q * qstride;
-    for (uint32_t j = lane; j < nl; j += 32) {
-      const float lb = rq[j] - route_eps(qq, __ldg(cn + j));
-      rq[j] = lb <= U ? seq_metric(qr, C + (size_t)__ldg(col + j) * dpad, d, metric) : __int_as_float(0x7f800000);
+    // probe_ratio cut, as the query-major selection
+    if (np > 0 && isfinite(probe_ratio)) {
+      const float d0 = key_dist(sorted[0]);
+      if (d0 >= 0.0f) {
+        const float lim = __fmul_rn(d0, fmaxf(probe_ratio, 1.0f));
+        int first_out = np;
+        for (int i = lane; i < np; i += 32)
+          if (key_dist(sorted[i]) > lim) first_out = min(first_out, i);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) first_out = min(first_out, __shfl_xor_sync(kFull, first_out, o));
+        np = first_out;
+      }
     }
+    for (int i = lane; i < np; i += 32) probe_out[(size_t)q * nprobe + i] = key_id(sorted[i]);
+    if (lane == 0) probe_cnt[q] = (uint32_t)np;
     __syncwarp();
   }
 }
@@ -1234,8 +1523,85 @@ static size_t pm_smem(uint32_t d, uint32_t dpad, uint32_t k) {
 // Posting-major scan of one chunk whose routing matrix is in ac.route: probes
 // (the query-major kernel stops after selecting them), pairs grouped by
 // posting, the scan, the per-query merge.
+// Tensor-core routing state of one search (the live list fixed): the centre,
+// the largest centred norm, per live centroid (|c'|^2, 1 / s) and FP16 halves,
+// per query of a chunk (|q'|^2, -2 / s, E, 0) and FP16 halves, the A matrix.
+struct FrPrep {
+  float *mu;
+  uint32_t *maxcc;
+  float2 *cinfo;
+  __half *ch, *cl, *qh, *ql;
+  float4 *qinfo;
+  float *D;
+  uint32_t ldd;
+  int ks;  // 16-dimension steps of the padded rows (2, 4, 6 or 8)
+};
+
+static DgStatus fr_prepare(DgSpfresh *s, const uint32_t *lidx, uint32_t chunk, cudaStream_t st, FrPrep *fp) {
+  const int ks = s->d <= 32 ? 2 : s->d <= 64 ? 4 : s->d <= 96 ? 6 : 8;
+  const size_t kd = 16 * (size_t)ks, nb = s->nblocks;
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t o_max = up(128 * 4), o_info = o_max + 256, o_h = o_info + up(nb * 8), o_l = o_h + up(nb * kd * 2),
+               o_qi = o_l + up(nb * kd * 2), o_qh = o_qi + up((size_t)chunk * 16), o_ql = o_qh + up((size_t)chunk * kd * 2),
+               total = o_ql + up((size_t)chunk * kd * 2);
+  fp->ldd = (uint32_t)((nb + 3) & ~(size_t)3);
+  DgStatus r;
+  if ((r = buf_reserve(s->fr, total)) != DG_OK) return r;
+  if ((r = buf_reserve(s->route, (size_t)chunk * fp->ldd * 4)) != DG_OK) return r;
+  uint8_t *base = (uint8_t *)s->fr.p;
+  fp->mu = (float *)base;
+  fp->maxcc = (uint32_t *)(base + o_max);
+  fp->cinfo = (float2 *)(base + o_info);
+  fp->ch = (__half *)(base + o_h);
+  fp->cl = (__half *)(base + o_l);
+  fp->qinfo = (float4 *)(base + o_qi);
+  fp->qh = (__half *)(base + o_qh);
+  fp->ql = (__half *)(base + o_ql);
+  fp->D = (float *)s->route.p;
+  fp->ks = ks;
+  k_fr_mean<<<1, 1024, 0, st>>>(s->centroids, lidx, s->d, s->dpad, fp->mu, fp->maxcc);
+  k_fr_centroids<<<(unsigned)std::min<size_t>((nb + 7) / 8, 148 * 16), 256, 0, st>>>(
+      s->centroids, lidx, s->d, s->dpad, (uint32_t)kd, fp->mu, fp->ch, fp->cl, fp->cinfo, fp->maxcc);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+template <int KS>
+static DgStatus fr_matrix(const SpfArgs &ac, const FrPrep &fp, uint32_t nblocks, cudaStream_t st) {
+  const size_t smem = fr_tcm_smem(KS);
+  DG_CUDA(cudaFuncSetAttribute(k_route_tcm<KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const uint32_t ntiles = (nblocks + kFrC - 1) / kFrC;
+  dim3 grid((ac.nq + 63) / 64, std::max(1u, (ntiles + kFrTiles - 1) / kFrTiles));
+  k_route_tcm<KS><<<grid, 128, smem, st>>>(fp.qh, fp.ql, fp.qinfo, ac.nq, fp.ch, fp.cl, fp.cinfo, ac.route_idx,
+                                           fp.D, fp.ldd);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
+// The probes of a chunk's queries: query halves, the A matrix, the selection.
+static DgStatus fr_route(const SpfArgs &ac, const FrPrep &fp, uint32_t nprobe, uint32_t nblocks, uint32_t *probe,
+                         uint32_t *pcnt, cudaStream_t st) {
+  const uint32_t kd = 16u * (uint32_t)fp.ks;
+  k_fr_queries<<<(unsigned)std::min<size_t>(((size_t)ac.nq + 7) / 8, 148 * 16), 256, 0, st>>>(
+      ac.Q, ac.nq, ac.d, ac.d, kd, fp.mu, fp.maxcc, fp.qh, fp.ql, fp.qinfo);
+  DG_CUDA(cudaGetLastError());
+  DgStatus r;
+  switch (fp.ks) {
+    case 2: r = fr_matrix<2>(ac, fp, nblocks, st); break;
+    case 4: r = fr_matrix<4>(ac, fp, nblocks, st); break;
+    case 6: r = fr_matrix<6>(ac, fp, nblocks, st); break;
+    default: r = fr_matrix<8>(ac, fp, nblocks, st); break;
+  }
+  if (r != DG_OK) return r;
+  k_fr_select<<<(unsigned)std::min<uint32_t>((ac.nq + 3) / 4, 148 * 16), 128, 0, st>>>(
+      fp.D, fp.ldd, ac.nq, fp.qinfo, ac.Q, ac.d, ac.d, ac.centroids, ac.dpad, ac.route_idx, ac.metric, nprobe,
+      ac.probe_ratio, probe, pcnt);
+  DG_CUDA(cudaGetLastError());
+  return DG_OK;
+}
+
 static DgStatus pm_scan_chunk(DgSpfresh *s, const SpfArgs &ac, uint32_t nprobe, uint32_t k, uint32_t pcap,
-                              uint32_t rcap, cudaStream_t st) {
+                              uint32_t rcap, cudaStream_t st, const FrPrep *fp) {
   DgStatus r;
   const uint32_t qn = ac.nq, nb = s->nblocks;
   const size_t npairs = (size_t)qn * nprobe;
@@ -1260,6 +1626,9 @@ static DgStatus pm_scan_chunk(DgSpfresh *s, const SpfArgs &ac, uint32_t nprobe, 
     k_pm_select<<<(unsigned)std::min<uint32_t>((qn + 3) / 4, 148 * 16), 128, 0, st>>>(
         ac.route, ac.route_idx, qn, nb, nprobe, ac.probe_ratio, probe, pcnt);
     DG_CUDA(cudaGetLastError());
+  } else if (fp) {
+    // tensor-core routing: the A matrix, then exact distances near the cut
+    if ((r = fr_route(ac, *fp, nprobe, nb, probe, pcnt, st)) != DG_OK) return r;
   } else {
     // the query-major kernel's selection, stopped before its scan
     SpfArgs ap = ac;
@@ -1325,7 +1694,7 @@ DgStatus dg_spfresh_destroy(DgSpfresh *s) {
     cudaEventDestroy(s->searched);
   }
   for (void *p : s->allocs) cudaFree(p);
-  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx, &s->rnorm, &s->probe, &s->probe_cnt,
+  for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx, &s->fr, &s->probe, &s->probe_cnt,
                           &s->pcount, &s->pstart, &s->pfill, &s->istart, &s->pair_q, &s->pos_of, &s->items,
                           &s->pair_keys, &s->pair_cnt, &s->misc})
     if (b->p) cudaFree(b->p);
@@ -1654,17 +2023,23 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
                              (s->metric == DG_L2 || s->metric == DG_L2SQ) && p->k <= (uint32_t)kPmK && nq >= 256 &&
                              (uint64_t)nq * nprobe >= 16ull * s->nblocks && s->nblocks < (1u << 22) && s->d % 4 == 0 &&
                              pm_smem(s->d, s->dpad, p->k) <= 200 * 1024;
+  // DG_SPF_EXACT_ROUTE=1 routes with the exact FP32 kernel only (an A/B knob)
+  static const bool exact_only = std::getenv("DG_SPF_EXACT_ROUTE") && atoi(std::getenv("DG_SPF_EXACT_ROUTE"));
+  // posting-major batches under L2 with n_probe <= 64 and d <= 128 route on the
+  // tensor cores (exact distances only near each query's cut)
+  const bool tc_route = posting_major && nprobe <= 64 && s->d <= 128 && ((uintptr_t)a.Q & 15) == 0 && !exact_only;
   if (s->nblocks >= 512) {
     // many postings: route all queries of a chunk in one tiled kernel (the
     // matrix of a chunk stays below 1 GiB), then scan the chunk
     const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nq, (1ull << 28) / s->nblocks));
-    if ((r = buf_reserve(s->route, (size_t)chunk * s->nblocks * 4)) != DG_OK) return r;
+    if (!tc_route && (r = buf_reserve(s->route, (size_t)chunk * s->nblocks * 4)) != DG_OK) return r;
     if ((r = buf_reserve(s->live_idx, ((size_t)s->nblocks + 1) * 4)) != DG_OK) return r;
-    if ((r = buf_reserve(s->rnorm, ((size_t)chunk + s->nblocks) * 4)) != DG_OK) return r;
     uint32_t *lidx = (uint32_t *)s->live_idx.p;
     DG_CUDA(cudaMemsetAsync(lidx, 0, 4, st));
     k_live_idx<<<(s->nblocks + 255) / 256, 256, 0, st>>>(s->live, s->nblocks, lidx);
     DG_CUDA(cudaGetLastError());
+    FrPrep fp{};
+    if (tc_route && (r = fr_prepare(s, lidx, chunk, st, &fp)) != DG_OK) return r;
     for (uint32_t q0 = 0; q0 < nq; q0 += chunk) {
       const uint32_t qn = std::min(chunk, nq - q0);
       SpfArgs ac = a;
@@ -1673,28 +2048,16 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
       ac.out_ids = a.out_ids + (size_t)q0 * p->k;
       ac.out_d = a.out_d + (size_t)q0 * p->k;
       ac.out_cnt = a.out_cnt + q0;
-      ac.route = (const float *)s->route.p;
+      ac.route = tc_route ? nullptr : (const float *)s->route.p;
       ac.route_idx = lidx;
-      dim3 grid((s->nblocks + kRT - 1) / kRT, (qn + kRT - 1) / kRT);
-      // DG_SPF_EXACT_ROUTE=1 routes with the exact kernel only (a test knob)
-      static const bool exact_only = std::getenv("DG_SPF_EXACT_ROUTE") && atoi(std::getenv("DG_SPF_EXACT_ROUTE"));
-      if ((s->metric == DG_L2 || s->metric == DG_L2SQ) && nprobe <= 64 && !exact_only) {
-        // tensor-core approximation, then exact distances for the candidates of each row
-        float *qnorm = (float *)s->rnorm.p, *cnorm = qnorm + chunk;
-        k_route_norms<<<(unsigned)std::min<size_t>(((size_t)qn + s->nblocks + 255) / 256, 148 * 16), 256, 0, st>>>(
-            ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, qnorm, cnorm);
-        k_route_tc<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, qnorm, cnorm,
-                                         (float *)s->route.p, s->nblocks);
-        k_route_fix<<<(unsigned)std::min<uint32_t>((qn + 3) / 4, 148 * 16), 128, 0, st>>>(
-            ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric, qnorm, cnorm, (float *)s->route.p,
-            s->nblocks, nprobe);
-      } else {
+      if (!tc_route) {
+        dim3 grid((s->nblocks + kRT - 1) / kRT, (qn + kRT - 1) / kRT);
         k_route<<<grid, 256, 0, st>>>(ac.Q, qn, s->d, s->centroids, lidx, s->d, s->dpad, s->metric,
                                       (float *)s->route.p, s->nblocks);
+        DG_CUDA(cudaGetLastError());
       }
-      DG_CUDA(cudaGetLastError());
       if (posting_major) {
-        if ((r = pm_scan_chunk(s, ac, nprobe, p->k, pcap, rcap, st)) != DG_OK) return r;
+        if ((r = pm_scan_chunk(s, ac, nprobe, p->k, pcap, rcap, st, tc_route ? &fp : nullptr)) != DG_OK) return r;
       } else if ((r = scan(ac)) != DG_OK) {
         return r;
       }

@@ -234,3 +234,51 @@ def test_rabitq_postings_reencoded_on_the_gpu(oracle):
         checked += 1
     assert checked > 50
     s.close()
+
+
+@pytest.mark.parametrize("d,metric", [(96, "l2"), (96, "euclidean"), (128, "l2"), (20, "l2")])
+def test_tensor_core_routing_matches_oracle(oracle, d, metric):
+    """Posting-major batches with n_probe <= 64 route on the tensor cores (FP16
+    hi/lo products of centred, scaled vectors), then compute exact
+    coordinate-order distances for every centroid within the error bound of
+    each query's cut.  The probes, and so ids, counts and distances, equal the
+    oracle's exact routing for several widths and a probe_ratio cut."""
+    X = synth.mixture(30000, d, 64, seed=41, clip=False)
+    Q = synth.mixture(600, d, 64, seed=41, stream=synth.STREAM_QUERY, clip=False)
+    s = dg.SPFresh.bulk_load(X, metric=metric, max_posting_size=32, seed=8)
+    assert s.stats()["postings"] >= 512
+    s.delete(list(range(0, 30000, 29)))
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 16), (10, 64), (32, 33), (1, 1)):
+        if 600 * nprobe < 16 * s.stats()["postings"]:
+            continue  # below the posting-major threshold
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
+    s.probe_ratio = 1.3
+    view, keep = oracle_view(oracle, s)
+    gi, gd, gc = s.search_arrays(Q, 10, 64)
+    oi, od, oc = oracle.spfresh_search(view, Q, 10, 64)
+    assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od)
+    s.close()
+
+
+def test_tensor_core_routing_wide_bound_falls_back_exactly(oracle):
+    """Two clusters 2e5 apart along one axis: after centring, every norm is
+    about 1e10, so the tensor-core error bound covers every centroid of a
+    query's half and the candidates outgrow a query's list.  Those queries
+    fall back to exact distances for every live centroid; results still equal
+    the oracle's."""
+    rng = np.random.default_rng(5)
+    X = synth.mixture(30000, 32, 64, seed=43, clip=False)
+    X[:, 0] += np.where(rng.random(30000) < 0.5, -1e5, 1e5).astype(np.float32)
+    Q = synth.mixture(600, 32, 64, seed=43, stream=synth.STREAM_QUERY, clip=False)
+    Q[:, 0] += np.where(rng.random(600) < 0.5, -1e5, 1e5).astype(np.float32)
+    s = dg.SPFresh.bulk_load(X, metric="l2", max_posting_size=32, seed=9)
+    assert s.stats()["postings"] >= 512
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 64), (10, 40)):
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
+    s.close()
