@@ -91,6 +91,8 @@ struct SpfArgs {
   const uint32_t *route_idx; // [1 + live] count, then the live slots the columns of `route` belong to
   uint32_t *probe_out;       // non-null: write each query's probed slots ([nq][nprobe]) and stop
   uint32_t *probe_cnt;       // [nq] number of probed slots
+  const uint32_t *probe_in;  // non-null: each query's probed slots ([nq][nprobe], ascending keys), routing done
+  const uint32_t *probe_in_cnt;
 };
 
 enum SpfKind { SPF_RAW = 0, SPF_PQ = 1, SPF_INT8 = 2, SPF_F16 = 3, SPF_RABITQ = 4 };
@@ -396,7 +398,11 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
     // ---- 1. routing
     const int nprobe = (int)max(a.nprobe, 1u);
     int pcur = 0, psize = 0;
-    if (a.route) {
+    if (a.probe_in) {  // routed already (probes after the probe_ratio cut)
+      psize = (int)a.probe_in_cnt[q];
+      for (int i = lane; i < psize; i += 32) P[0][i] = make_key(0.0f, a.probe_in[(size_t)q * a.nprobe + i]);
+      __syncwarp();
+    } else if (a.route) {
       // precomputed distances: the loads of 8 batches go out before their
       // (in-order) insertions
       const float *rq = a.route + (size_t)q * a.nblocks;
@@ -423,7 +429,7 @@ __global__ void __launch_bounds__(128, 4) spfresh_kernel(SpfArgs a, SpfLayout Ly
     }
     // ---- 2. probe_ratio cut
     int np = psize;
-    if (np > 0 && isfinite(a.probe_ratio)) {
+    if (np > 0 && isfinite(a.probe_ratio) && !a.probe_in) {
       const float d0 = key_dist(P[pcur][0]);
       if (d0 >= 0.0f) {
         const float lim = __fmul_rn(d0, fmaxf(a.probe_ratio, 1.0f));
@@ -2025,9 +2031,10 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
                              pm_smem(s->d, s->dpad, p->k) <= 200 * 1024;
   // DG_SPF_EXACT_ROUTE=1 routes with the exact FP32 kernel only (an A/B knob)
   static const bool exact_only = std::getenv("DG_SPF_EXACT_ROUTE") && atoi(std::getenv("DG_SPF_EXACT_ROUTE"));
-  // posting-major batches under L2 with n_probe <= 64 and d <= 128 route on the
-  // tensor cores (exact distances only near each query's cut)
-  const bool tc_route = posting_major && nprobe <= 64 && s->d <= 128 && ((uintptr_t)a.Q & 15) == 0 && !exact_only;
+  // batches of >= 256 queries under L2 with n_probe <= 64 and d <= 128 route on
+  // the tensor cores (exact distances only near each query's cut)
+  const bool tc_route = s->nblocks >= 512 && (s->metric == DG_L2 || s->metric == DG_L2SQ) && nq >= 256 &&
+                        nprobe <= 64 && s->d <= 128 && s->d % 4 == 0 && ((uintptr_t)a.Q & 15) == 0 && !exact_only;
   if (s->nblocks >= 512) {
     // many postings: route all queries of a chunk in one tiled kernel (the
     // matrix of a chunk stays below 1 GiB), then scan the chunk
@@ -2058,6 +2065,14 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
       }
       if (posting_major) {
         if ((r = pm_scan_chunk(s, ac, nprobe, p->k, pcap, rcap, st, tc_route ? &fp : nullptr)) != DG_OK) return r;
+      } else if (tc_route) {  // probes first, then the query-major scan of them
+        if ((r = buf_reserve(s->probe, (size_t)qn * nprobe * 4)) != DG_OK) return r;
+        if ((r = buf_reserve(s->probe_cnt, (size_t)qn * 4)) != DG_OK) return r;
+        if ((r = fr_route(ac, fp, nprobe, s->nblocks, (uint32_t *)s->probe.p, (uint32_t *)s->probe_cnt.p, st)) != DG_OK)
+          return r;
+        ac.probe_in = (const uint32_t *)s->probe.p;
+        ac.probe_in_cnt = (const uint32_t *)s->probe_cnt.p;
+        if ((r = scan(ac)) != DG_OK) return r;
       } else if ((r = scan(ac)) != DG_OK) {
         return r;
       }

@@ -258,7 +258,9 @@ class SPFresh:
         max_posting_size split by the same 2-means as an insert-time split
         (without relocating neighbours).  The result satisfies the index's
         invariants, so inserts, deletes and searches continue as after build();
-        it is for large loads, where per-vector insertion is host-bound."""
+        it is for large loads, where per-vector insertion is host-bound.
+        Quantizer parameters default as in build() (int8 range, PQ with 8
+        subspaces, RaBitQ rotation signs and centroid)."""
         import pydiskann_b200 as dg
 
         X = np.ascontiguousarray(vectors, dtype=np.float32)
@@ -269,6 +271,11 @@ class SPFresh:
         qp = dict(qparams or {})
         if quantizer == "int8" and not qp:
             qp["scale"], qp["offset"] = dg.int8_params(X)
+        elif quantizer == "pq" and not qp:
+            qp["codebooks"] = dg.pq_train(X, 8, 256, 20, 50_000, seed, device)
+        elif quantizer == "rabitq" and not qp:
+            cen, signs = dg.rabitq_params(X, seed)
+            qp["padded"], qp["signs"], qp["centroid"] = dg.rabitq_padded(X.shape[1]), signs, cen
         s = SPFresh(X.shape[1], metric, quantizer, qp, rerank_size, max_posting_size, min_posting_size,
                     reassign_neighbors, probe_ratio, device)
         n = len(X)

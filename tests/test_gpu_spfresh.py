@@ -282,3 +282,25 @@ def test_tensor_core_routing_wide_bound_falls_back_exactly(oracle):
         oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
         assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
     s.close()
+
+
+@pytest.mark.parametrize("quant,metric", [("int8", "l2"), ("pq", "l2"), ("rabitq", "l2"), ("rabitq", "euclidean"),
+                                          (None, "euclidean")])
+def test_tensor_core_routing_feeds_query_major_scan(oracle, quant, metric):
+    """Batches of >= 256 queries that probe too few postings for the
+    posting-major scan still route on the tensor cores; the query-major scan
+    then takes the probes as given.  Quantized postings (codes scanned, exact
+    re-check or rerank as configured) give the oracle's results bit for bit."""
+    X = synth.mixture(30000, 48, 64, seed=45, clip=False)
+    Q = synth.mixture(300, 48, 64, seed=45, stream=synth.STREAM_QUERY, clip=False)
+    kw = {} if quant is None else {"quantizer": quant}
+    s = dg.SPFresh.bulk_load(X, metric=metric, max_posting_size=32, seed=10, **kw)
+    assert s.stats()["postings"] >= 512
+    s.delete(list(range(0, 30000, 31)))
+    view, keep = oracle_view(oracle, s)
+    for k, nprobe in ((10, 4), (10, 20)):
+        assert 300 * nprobe < 16 * s.stats()["postings"]  # query-major
+        gi, gd, gc = s.search_arrays(Q, k, nprobe)
+        oi, od, oc = oracle.spfresh_search(view, Q, k, nprobe)
+        assert np.array_equal(gc, oc) and np.array_equal(gi, oi) and np.array_equal(gd, od), (k, nprobe)
+    s.close()
