@@ -60,6 +60,7 @@ struct DgSpfresh {
   // posting-major scan of one chunk: probes per query, (query, posting) pairs
   // grouped by posting, work items, per-pair candidate lists
   DgIndex::Buf probe, probe_cnt, pcount, pstart, pfill, istart, pair_q, pos_of, items, pair_keys, pair_cnt, misc;
+  DgIndex::Buf qthr;  // posting-major scan: per query, a bound of its k-th distance
 };
 
 namespace dg {
@@ -96,6 +97,12 @@ struct SpfArgs {
 };
 
 enum SpfKind { SPF_RAW = 0, SPF_PQ = 1, SPF_INT8 = 2, SPF_F16 = 3, SPF_RABITQ = 4 };
+
+// The float whose ordered bits (ordered_bits) are u.
+__device__ __forceinline__ float ordered_float(uint32_t u) {
+  u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+  return __uint_as_float(u);
+}
 
 // metric_eval of the oracle with its rounding (sequential sums).
 __device__ __forceinline__ float seq_metric(const float *q, const float *x, uint32_t d, int metric) {
@@ -689,11 +696,25 @@ __global__ void __launch_bounds__(128) k_pm_select(const float *route, const uin
   for (uint32_t q = blockIdx.x * 4 + warp; q < nq; q += gridDim.x * 4) {
     const float *rq = route + (size_t)q * nblocks;
     const uint32_t take = min(nprobe, nl);
-    // the nearest distance, for the probe_ratio cut
+    // the nearest distance, for the probe_ratio cut, and a column holding it
     float d0 = __int_as_float(0x7f800000);
-    for (uint32_t j = lane; j < nl; j += 32) d0 = fminf(d0, __ldg(rq + j));
+    uint32_t j0min = 0xffffffffu;
+    for (uint32_t j = lane; j < nl; j += 32) {
+      const float v = __ldg(rq + j);
+      if (v < d0) {
+        d0 = v;
+        j0min = j;
+      }
+    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) d0 = fminf(d0, __shfl_xor_sync(kFull, d0, o));
+    for (int o = 16; o > 0; o >>= 1) {
+      const float od = __shfl_xor_sync(kFull, d0, o);
+      const uint32_t oj = __shfl_xor_sync(kFull, j0min, o);
+      if (od < d0 || (od == d0 && oj < j0min)) {
+        d0 = od;
+        j0min = oj;
+      }
+    }
     uint32_t tbits = 0xffffffffu, tslot = 0xffffffffu;  // cut-off key (all keys when take == nl)
     if (take > 0 && take < nl) {
       uint32_t need = take, prefix = 0, mask = 0;
@@ -723,7 +744,7 @@ __global__ void __launch_bounds__(128) k_pm_select(const float *route, const uin
     }
     const bool cut = isfinite(probe_ratio) && d0 >= 0.0f;
     const float lim = cut ? __fmul_rn(d0, fmaxf(probe_ratio, 1.0f)) : __int_as_float(0x7f800000);
-    uint32_t n_out = 0;
+    uint32_t n_out = 0, near_at = 0;
     for (uint32_t j0 = 0; j0 < nl; j0 += 32) {
       const uint32_t j = j0 + lane;
       bool sel = false;
@@ -735,8 +756,20 @@ __global__ void __launch_bounds__(128) k_pm_select(const float *route, const uin
         sel = (bits < tbits || (bits == tbits && slot <= tslot)) && !(dv > lim);
       }
       const uint32_t m = __ballot_sync(kFull, sel);
-      if (sel) probe_out[(size_t)q * nprobe + n_out + __popc(m & lanemask_lt(lane))] = slot;
+      const uint32_t at = n_out + __popc(m & lanemask_lt(lane));
+      if (sel) probe_out[(size_t)q * nprobe + at] = slot;
+      const uint32_t hm = __ballot_sync(kFull, sel && j == j0min);
+      if (hm) near_at = __shfl_sync(kFull, at, __ffs(hm) - 1);
       n_out += __popc(m);
+    }
+    __syncwarp();
+    // the nearest probe first (the posting-major bound starts from it; the
+    // scan does not depend on the order of the probes)
+    if (lane == 0 && near_at > 0 && near_at < n_out) {
+      uint32_t *po = probe_out + (size_t)q * nprobe;
+      const uint32_t t = po[0];
+      po[0] = po[near_at];
+      po[near_at] = t;
     }
     if (lane == 0) probe_cnt[q] = n_out;
     __syncwarp();
@@ -852,9 +885,87 @@ __host__ __device__ inline uint32_t pm_kcap(uint32_t k) { return (k + 15u) & ~15
 // products of a tile come from the tensor cores (the warps split the 64 x 32
 // tile into 16 x 16 blocks) when the tile and the queries meet the exactness
 // bounds above, else from an FMA chain per pair.
+// qthr[q] for each query of a posting-major chunk (a warp each): an upper
+// bound of the query's k-th smallest scan distance, from the live entries of
+// its first probe (the nearest one).  B, the k-th smallest of their
+// coordinate-order squared distances, is within (d + 2) 2^-24 B of the exact
+// value; the scan's |q|^2 + |x|^2 - 2 q.x differs from the exact value by at
+// most (2d + 6) 2^-24 (|q|^2 + |x|^2).  So
+//     B (1 + (d + 2) 2^-23) + 4 (d + 4) 2^-24 (|q|^2 + max |x|^2)
+// (rounded up; its square root, rounded up, for euclidean) bounds the k-th
+// smallest scan distance over the probes.  All ones when the first probe has
+// fewer than k live entries.
+__global__ void __launch_bounds__(128) k_pm_bound(SpfArgs a, const uint32_t *probe, const uint32_t *pcnt,
+                                                  uint32_t nprobe, uint32_t k, uint32_t *qthr) {
+  extern __shared__ float bsm[];  // [4][cap] squared distances
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float *sv = bsm + (size_t)warp * a.cap;
+  for (uint32_t q = blockIdx.x * 4 + warp; q < a.nq; q += gridDim.x * 4) {
+    uint32_t tb = 0xffffffffu;
+    if (pcnt[q] > 0) {
+      const uint32_t b = probe[(size_t)q * nprobe];
+      const uint32_t n_e = min(a.len[b], a.cap);
+      const float *qg = a.Q + (size_t)q * a.d;
+      float qq = 0.0f, xxm = 0.0f;
+      for (uint32_t i = lane; i < a.d; i += 32) qq = fmaf(__ldg(qg + i), __ldg(qg + i), qq);
+      int live = 0;
+      for (uint32_t e0 = 0; e0 < n_e; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        const bool ok = e < n_e && !is_deleted(a.deleted, __ldg(a.ids + (size_t)b * a.cap + e));
+        float sd = 0.0f, xx = 0.0f;
+        if (ok) {
+          const float *x = reinterpret_cast<const float *>(a.codes + ((size_t)b * a.cap + e) * a.code_stride);
+#pragma unroll 8
+          for (uint32_t i = 0; i < a.d; ++i) {
+            const float xv = __ldg(x + i), t = __fsub_rn(__ldg(qg + i), xv);
+            sd = __fadd_rn(sd, __fmul_rn(t, t));
+            xx = fmaf(xv, xv, xx);
+          }
+        }
+        const uint32_t msk = __ballot_sync(kFull, ok);
+        if (ok) sv[live + __popc(msk & lanemask_lt(lane))] = sd;
+        live += __popc(msk);
+        xxm = fmaxf(xxm, xx);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        qq += __shfl_xor_sync(kFull, qq, o);
+        xxm = fmaxf(xxm, __shfl_xor_sync(kFull, xxm, o));
+      }
+      __syncwarp();
+      if (live >= (int)k) {
+        uint32_t lo = 0, hi = 0xffffffffu;  // the k-th smallest: smallest v with #{ <= v} >= k
+        while (lo < hi) {
+          const uint32_t mid = lo + ((hi - lo) >> 1);
+          uint32_t c = 0;
+          for (int i = lane; i < live; i += 32) c += ordered_bits(sv[i]) <= mid ? 1u : 0u;
+          c = __reduce_add_sync(kFull, c);
+          if (c >= k) hi = mid;
+          else lo = mid + 1;
+        }
+        const float fd = (float)a.d;
+        const float c1 = __fmul_ru(fd + 2.0f, 1.1920928955078125e-7f);  // (d + 2) 2^-23
+        const float c2 = __fmul_ru(4.0f * (fd + 4.0f), 5.9604644775390625e-8f);  // 4 (d + 4) 2^-24
+        float bound = __fadd_ru(__fmul_ru(ordered_float(lo), __fadd_ru(1.0f, c1)), __fmul_ru(c2, __fadd_ru(qq, xxm)));
+        if (a.metric == DG_L2) bound = __fsqrt_ru(bound);
+        tb = ordered_bits(bound);
+      }
+      __syncwarp();
+    }
+    if (lane == 0) qthr[q] = tb;
+    __syncwarp();
+  }
+}
+
+// qthr[q] (ordered distance bits) is an upper bound of query q's final k-th
+// distance: k_pm_bound's, lowered to the k-th distance of any of its pair
+// lists that holds k keys.  Entries farther than it cannot reach the result, so
+// they are dropped before the pair-list insertion (keys at the bound stay,
+// ties included); the result does not depend on when bounds arrive.
 __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4 *items, const uint32_t *n_items,
                                                           uint32_t *item_counter, const uint32_t *pair_q,
-                                                          uint64_t *pair_keys, uint32_t *pair_cnt, uint32_t k) {
+                                                          uint64_t *pair_keys, uint32_t *pair_cnt, uint32_t k,
+                                                          uint32_t *qthr) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // query rows dpad floats; tile rows d + 4 floats: 16-byte rows whose float4
@@ -1017,15 +1128,20 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         const uint32_t j = warp + 8 * u;
         if (j >= m) continue;  // warp-uniform
         uint64_t *const bufs[2] = {lists + (size_t)j * 2 * kc, lists + (size_t)j * 2 * kc + kc};
+        uint32_t *qt = qthr + pair_q[p0 + j];
+        const uint32_t tb = *reinterpret_cast<volatile uint32_t *>(qt);
         // |q - x|^2 = |q|^2 + |x|^2 - 2 q.x (exact on integer-valued data)
         const float qq = qn[j];
         const float s0 = fmaxf(__fsub_rn(__fadd_rn(qq, xn[lane]), __fmul_rn(2.0f, acc[u][0])), 0.0f);
         const float s1 = fmaxf(__fsub_rn(__fadd_rn(qq, xn[lane + 32]), __fmul_rn(2.0f, acc[u][1])), 0.0f);
         const float d0 = sq ? __fsqrt_rn(s0) : s0, d1 = sq ? __fsqrt_rn(s1) : s1;
-        insert_batch(id0 != DG_PAD ? make_key(d0, id0) : kKeyInvalid, bufs, cur[u], size[u], (int)k,
-                     cst + warp * 32, lane);
-        insert_batch(id1 != DG_PAD ? make_key(d1, id1) : kKeyInvalid, bufs, cur[u], size[u], (int)k,
-                     cst + warp * 32, lane);
+        const bool k0 = id0 != DG_PAD && ordered_bits(d0) <= tb, k1 = id1 != DG_PAD && ordered_bits(d1) <= tb;
+        insert_batch(k0 ? make_key(d0, id0) : kKeyInvalid, bufs, cur[u], size[u], (int)k, cst + warp * 32, lane);
+        insert_batch(k1 ? make_key(d1, id1) : kKeyInvalid, bufs, cur[u], size[u], (int)k, cst + warp * 32, lane);
+        if (size[u] >= (int)k && lane == 0) {
+          const uint32_t nb = key_hi(bufs[cur[u]][k - 1]);
+          if (nb < tb) atomicMin(qt, nb);
+        }
       }
     }
 #pragma unroll
@@ -1074,10 +1190,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
 
-__device__ __forceinline__ float ordered_float(uint32_t u) {
-  u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
-  return __uint_as_float(u);
-}
 
 // The power-of-two scale that brings a vector whose largest |coordinate| is
 // mx below 2^14 (1 for a zero vector), and its inverse.
@@ -1357,7 +1469,20 @@ __global__ void __launch_bounds__(128) k_fr_select(const float *__restrict__ D, 
           if (t1 < t0) { const float x = t0; t0 = t1; t1 = x; }
         }
       };
-      for (uint32_t i = lane; i < n4; i += 32) {
+      uint32_t i = lane;
+      for (; i + 96 < n4; i += 128) {  // four loads in flight per lane
+        float4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = __ldg(row4 + i + 32 * u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          see(v[u].x);
+          see(v[u].y);
+          see(v[u].z);
+          see(v[u].w);
+        }
+      }
+      for (; i < n4; i += 32) {
         const float4 v = __ldg(row4 + i);
         see(v.x);
         see(v.y);
@@ -1378,24 +1503,32 @@ __global__ void __launch_bounds__(128) k_fr_select(const float *__restrict__ D, 
     }
     // the candidates: every live index with A <= bound (all of them when nl <= n)
     int m = 0;
-    for (uint32_t i0 = 0; i0 < n4 + 1; i0 += 32) {
-      const uint32_t i = i0 + lane;
-      float4 v = make_float4(inf, inf, inf, inf);
-      if (i < n4) v = __ldg(row4 + i);
-      else if (i == n4) {
-        if (4 * n4 < nl) v.x = __ldg(row + 4 * n4);
-        if (4 * n4 + 1 < nl) v.y = __ldg(row + 4 * n4 + 1);
-        if (4 * n4 + 2 < nl) v.z = __ldg(row + 4 * n4 + 2);
-      }
-      const float vv[4] = {v.x, v.y, v.z, v.w};
+    for (uint32_t i0 = 0; i0 < n4 + 1; i0 += 128) {  // four loads in flight per lane
+      float4 v[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const uint32_t j = 4 * i + u;
-        const bool keep = j < nl && (vv[u] <= bound || nl <= n);
-        const uint32_t km = __ballot_sync(kFull, keep);
-        const int pos = m + __popc(km & lanemask_lt(lane));
-        if (keep && pos < kFrCap) lst[pos] = j;
-        m += __popc(km);
+      for (int w = 0; w < 4; ++w) {
+        const uint32_t i = i0 + 32 * w + lane;
+        v[w] = make_float4(inf, inf, inf, inf);
+        if (i < n4) v[w] = __ldg(row4 + i);
+        else if (i == n4) {
+          if (4 * n4 < nl) v[w].x = __ldg(row + 4 * n4);
+          if (4 * n4 + 1 < nl) v[w].y = __ldg(row + 4 * n4 + 1);
+          if (4 * n4 + 2 < nl) v[w].z = __ldg(row + 4 * n4 + 2);
+        }
+      }
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        const uint32_t i = i0 + 32 * w + lane;
+        const float vv[4] = {v[w].x, v[w].y, v[w].z, v[w].w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const uint32_t j = 4 * i + u;
+          const bool keep = j < nl && (vv[u] <= bound || nl <= n);
+          const uint32_t km = __ballot_sync(kFull, keep);
+          const int pos = m + __popc(km & lanemask_lt(lane));
+          if (keep && pos < kFrCap) lst[pos] = j;
+          m += __popc(km);
+        }
       }
     }
     __syncwarp();
@@ -1624,6 +1757,7 @@ static DgStatus pm_scan_chunk(DgSpfresh *s, const SpfArgs &ac, uint32_t nprobe, 
   if ((r = buf_reserve(s->pair_keys, npairs * k * 8)) != DG_OK) return r;
   if ((r = buf_reserve(s->pair_cnt, npairs * 4)) != DG_OK) return r;
   if ((r = buf_reserve(s->misc, 16)) != DG_OK) return r;
+  if ((r = buf_reserve(s->qthr, (size_t)qn * 4)) != DG_OK) return r;
   uint32_t *probe = (uint32_t *)s->probe.p, *pcnt = (uint32_t *)s->probe_cnt.p;
   uint32_t *pcount = (uint32_t *)s->pcount.p, *pstart = (uint32_t *)s->pstart.p, *pfill = (uint32_t *)s->pfill.p;
   uint32_t *istart = (uint32_t *)s->istart.p, *counter = (uint32_t *)s->misc.p;
@@ -1659,9 +1793,18 @@ static DgStatus pm_scan_chunk(DgSpfresh *s, const SpfArgs &ac, uint32_t nprobe, 
   DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pm_scan_postings, 256, smem));
   DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
   if (per_sm < 1) return fail(DG_ENOTSUP, "posting-major scan does not fit on an SM");
+  uint32_t *qthr = (uint32_t *)s->qthr.p;
+  const size_t bsmem = (size_t)4 * s->cap * 4;
+  if (bsmem <= 160 * 1024) {
+    DG_CUDA(cudaFuncSetAttribute(k_pm_bound, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem));
+    k_pm_bound<<<(unsigned)std::min<uint32_t>((qn + 3) / 4, 148 * 16), 128, bsmem, st>>>(ac, probe, pcnt, nprobe,
+                                                                                           k, qthr);
+  } else {
+    DG_CUDA(cudaMemsetAsync(qthr, 0xff, (size_t)qn * 4, st));  // no bound: every entry goes to its pair list
+  }
   k_pm_scan_postings<<<per_sm * sms, 256, smem, st>>>(ac, (const uint4 *)s->items.p, istart + nb, counter,
                                                       (const uint32_t *)s->pair_q.p, (uint64_t *)s->pair_keys.p,
-                                                      (uint32_t *)s->pair_cnt.p, k);
+                                                      (uint32_t *)s->pair_cnt.p, k, qthr);
   k_pm_merge<<<(unsigned)std::min<uint32_t>((qn + 3) / 4, 148 * 16), 128, 0, st>>>(
       pcnt, (const uint32_t *)s->pos_of.p, qn, nprobe, (const uint64_t *)s->pair_keys.p,
       (const uint32_t *)s->pair_cnt.p, k, ac.out_ids, ac.out_d, ac.out_cnt);
@@ -1702,7 +1845,7 @@ DgStatus dg_spfresh_destroy(DgSpfresh *s) {
   for (void *p : s->allocs) cudaFree(p);
   for (DgIndex::Buf *b : {&s->q, &s->oids, &s->od, &s->ocnt, &s->route, &s->live_idx, &s->fr, &s->probe, &s->probe_cnt,
                           &s->pcount, &s->pstart, &s->pfill, &s->istart, &s->pair_q, &s->pos_of, &s->items,
-                          &s->pair_keys, &s->pair_cnt, &s->misc})
+                          &s->pair_keys, &s->pair_cnt, &s->misc, &s->qthr})
     if (b->p) cudaFree(b->p);
   if (s->counter) cudaFree(s->counter);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -2037,8 +2180,8 @@ DgStatus dg_spfresh_search_batch(DgSpfresh *s, const DgSpfreshParams *p, const f
                         nprobe <= 64 && s->d <= 128 && s->d % 4 == 0 && ((uintptr_t)a.Q & 15) == 0 && !exact_only;
   if (s->nblocks >= 512) {
     // many postings: route all queries of a chunk in one tiled kernel (the
-    // matrix of a chunk stays below 1 GiB), then scan the chunk
-    const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nq, (1ull << 28) / s->nblocks));
+    // matrix of a chunk stays below 2 GiB), then scan the chunk
+    const uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nq, (1ull << 29) / s->nblocks));
     if (!tc_route && (r = buf_reserve(s->route, (size_t)chunk * s->nblocks * 4)) != DG_OK) return r;
     if ((r = buf_reserve(s->live_idx, ((size_t)s->nblocks + 1) * 4)) != DG_OK) return r;
     uint32_t *lidx = (uint32_t *)s->live_idx.p;
