@@ -43,6 +43,7 @@ if ROOT not in sys.path:
 CACHE = os.environ.get("DGANN_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "dgann_bench_cache"))
 R, L_BUILD, ALPHA, M, K_PQ, PQ_ITERS, PQ_SAMPLE, K = 64, 128, 1.2, 16, 256, 25, 100_000, 10
 L_SWEEP = (16, 24, 32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256, 384, 512, 768, 1024)
+COSINE_SWEEP = (256, 384, 512, 768, 1024)  # fixed beams of the cosine recall-target sweep
 METRIC = "QPS @ recall@10=0.95, plain FP32 vs BF16+FP32-rerank, 1 B200; p99 ms"
 HEADLINE = "bf16_rerank"
 PARITY_QUERIES = 1000  # queries of the batch compared with the oracle for every timed variant
@@ -65,6 +66,10 @@ def parse():
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--target-recall", type=float, default=0.95)
+    ap.add_argument("--beam", type=int, default=0,
+                    help="time this beam instead of sweeping for the target recall (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="time the default launch schedule (profiling runs: fewer launches before the timed ones)")
     ap.add_argument("--variants", default="bf16_rerank,fp32,fp8_rerank,int8_rerank,pq_rerank")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -82,7 +87,9 @@ def parse():
                     help="also run the quantized cosine workload (1M x 768, 20k queries, uneven beams)")
     ap.add_argument("--cosine-n", type=int, default=1_000_000)
     ap.add_argument("--filtered-serving", action="store_true",
-                    help="also run the filtered serving workload (1M x 256, labels, R=48, Poisson 5k-200k req/s)")
+                    help="run the filtered serving workload (1M x 256, labels, R=48, Poisson 5k-200k req/s) on its "
+                         "whole grid (k in {10, 100} x L in {64, 200} x 5 rates); by default a short grid runs")
+    ap.add_argument("--no-filtered-serving", action="store_true")
     ap.add_argument("--fs-n", type=int, default=1_000_000)
     ap.add_argument("--cosine-nq", type=int, default=20_000)
     return ap.parse_args()
@@ -496,12 +503,12 @@ def main():
     chosen, curves = {}, {}
     for name in wanted:
         curves[name] = []
-        for L in L_SWEEP:
+        for L in ((args.beam,) if args.beam else L_SWEEP):
             ids, _, _ = run_variant(idx, qidx, name, Qd, L)
             torch.cuda.synchronize()
             rec = recall(ids.cpu().numpy().view(np.uint32), gt)
             curves[name].append((L, round(rec, 4)))
-            if rec >= args.target_recall:
+            if rec >= args.target_recall or args.beam:
                 chosen[name] = (L, rec)
                 break
         log(f"[sweep] {name}: {chosen.get(name)} curve {curves[name]}")
@@ -511,7 +518,9 @@ def main():
     results, outs = {}, {}
     tuned = {}
     for name, (L, rec) in chosen.items():
-        tuned[name] = autotune_variant(idx, qidx, name, Qd, L)
+        tuned[name] = ({"hbits": 10 if L <= 64 else 11 if L <= 128 else 12, "order": 0, "occ_pct": 100,
+                        "warps_per_cta": 4, "default": True}
+                       if args.no_autotune else autotune_variant(idx, qidx, name, Qd, L))
         log(f"[autotune] {name}: {tuned[name]}")
         out = run_variant(idx, qidx, name, Qd, L)
         for _ in range(args.warmup):
@@ -633,8 +642,12 @@ def main():
             line["filtered"] = filtered(args, X, Q, adj, med, dev, dist)
         if args.cosine and rank == 0:
             line["quantized_cosine"] = quantized_cosine(args, dev)
-        if args.filtered_serving and rank == 0:
-            line["filtered_serving"] = filtered_serving(args, dev)
+        if not args.no_filtered_serving and rank == 0:
+            try:
+                line["filtered_serving"] = filtered_serving(args, dev, full=args.filtered_serving)
+            except Exception as e:  # a secondary workload: keep the headline line
+                line["filtered_serving"] = {"error": repr(e)[:400]}
+                log(f"[filtered serving] failed: {e!r}")
         if not args.no_spfresh and rank == 0:
             # one replica is enough for this secondary measurement (it stages
             # several GB of posting blocks on the host)
@@ -786,15 +799,16 @@ def filtered(args, X, Q, adj, med, dev, dist):
     return out
 
 
-def filtered_serving(args, dev):
+def filtered_serving(args, dev, full=True):
     """The filtered serving workload: 1M x 256 Gaussian mixture (512 centres),
     each vector with 1-3 of 100 labels drawn Zipf(1.0); a Vamana graph with
     R = 48 (the reference has no filter-aware build); queries ask Or(Eq(0, l),
     Eq(1, l), Eq(2, l)) for a uniform label l (selectivity ~0.5 % to ~35 %).
     Requests with their own filters arrive as Poisson streams at 5k-200k req/s
-    through the serving loop, for k in {10, 100} and L in {64, 200}, FP32 and
-    BF16 + FP32 rerank; p50 / p99 latency, achieved QPS and recall@10 against
-    exact kNN inside each label's subset."""
+    through the serving loop, for k in {10, 100} and L in {64, 200} (full) or
+    for (k, L) = (10, 64) and (100, 200) at 5k, 50k and 200k req/s (short), FP32
+    and BF16 + FP32 rerank; p50 / p99 latency, achieved QPS and recall@10
+    against exact kNN inside each label's subset."""
     import pydiskann_b200 as dg
     from pydiskann_b200 import _lib, synth
 
@@ -816,30 +830,31 @@ def filtered_serving(args, dev):
     log(f"[filtered serving] setup {setup}")
     ix = dg.FilteredDiskANN(X, adj, med, labels, device=dev.index or 0)
     ix.enable_bf16()
-    out = {"n": len(X), "dim": 256, "R": 48, "queries": nq, "setup": setup, "runs": []}
-    rates = (5_000, 20_000, 50_000, 100_000, 200_000)
+    out = {"n": len(X), "dim": 256, "R": 48, "queries": nq, "setup": setup, "grid": "full" if full else "short",
+           "runs": []}
+    rates = (5_000, 20_000, 50_000, 100_000, 200_000) if full else (5_000, 50_000, 200_000)
+    kls = [(k, L) for k in (10, 100) for L in (64, 200)] if full else [(10, 64), (100, 200)]
     for name, trav in (("fp32", _lib.TRAVERSE_F32), ("bf16_rerank", _lib.TRAVERSE_BF16)):
-        for k in (10, 100):
-            for L in (64, 200):
-                rr = L if name != "fp32" else 0
-                tune = ix.autotune(Q[:2000], k, L, traversal=trav, rerank_size=rr, filters=flist[:2000], reps=1)
-                with dg.Server(ix, max_batch=512, streams=16, max_k=100) as srv:
-                    srv.run_trace(Q[:1000], np.zeros(1000), k=k, beam_width=L, rerank_size=rr, traversal=trav,
-                                  filters=flist[:1000])
-                    for rate in rates:
-                        n = int(max(2000, rate * 1.0))
-                        qi = np.arange(n) % nq
-                        res = srv.run_trace(Q[qi], dg.poisson_arrivals(n, rate, seed=rate), k=k, beam_width=L,
-                                            rerank_size=rr, traversal=trav, filters=[flist[i] for i in qi])
-                        lat = res["latency_us"] / 1e3
-                        hits = [len(set(res["ids"][i][:K].tolist()) & set(gt[qi[i]].tolist()))
-                                for i in range(0, n, max(1, n // 2000))]
-                        r = {"variant": name, "k": k, "L": L, "offered_rps": rate,
-                             "achieved_qps": round(n / (res["wall_us"] / 1e6)), "p50_ms": round(float(np.percentile(lat, 50)), 3),
-                             "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                             "recall_at_10": round(float(np.mean(hits)) / K, 4), "visited_table_bits": tune["hbits"]}
-                        out["runs"].append(r)
-                        log(f"[filtered serving] {json.dumps(r)}")
+        for k, L in kls:
+            rr = L if name != "fp32" else 0
+            tune = ix.autotune(Q[:2000], k, L, traversal=trav, rerank_size=rr, filters=flist[:2000], reps=1)
+            with dg.Server(ix, max_batch=512, streams=16, max_k=100) as srv:
+                srv.run_trace(Q[:1000], np.zeros(1000), k=k, beam_width=L, rerank_size=rr, traversal=trav,
+                              filters=flist[:1000])
+                for rate in rates:
+                    n = int(max(2000, rate * 1.0))
+                    qi = np.arange(n) % nq
+                    res = srv.run_trace(Q[qi], dg.poisson_arrivals(n, rate, seed=rate), k=k, beam_width=L,
+                                        rerank_size=rr, traversal=trav, filters=[flist[i] for i in qi])
+                    lat = res["latency_us"] / 1e3
+                    hits = [len(set(res["ids"][i][:K].tolist()) & set(gt[qi[i]].tolist()))
+                            for i in range(0, n, max(1, n // 2000))]
+                    r = {"variant": name, "k": k, "L": L, "offered_rps": rate,
+                         "achieved_qps": round(n / (res["wall_us"] / 1e6)), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                         "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                         "recall_at_10": round(float(np.mean(hits)) / K, 4), "visited_table_bits": tune["hbits"]}
+                    out["runs"].append(r)
+                    log(f"[filtered serving] {json.dumps(r)}")
     ix.close()
     return out
 
@@ -938,6 +953,39 @@ def quantized_cosine(args, dev):
             "visited_table_bits": tune["hbits"],
         }
         log(f"[cosine] {name}: {json.dumps(out['variants'][name])}")
+    # The per-query beams above (32..256) stop near recall 0.38 on this spectrum;
+    # one fixed beam for the whole batch is swept upwards to the smallest that
+    # reaches the target recall, then timed there.
+    out["at_target"] = {"target_recall": args.target_recall, "variants": {}}
+    for name, ix, trav, rr in variants[:4]:
+        curve, hit = [], None
+        for L in COSINE_SWEEP:
+            ids = ix.search_arrays(Qd, K, L, traversal=trav, rerank_size=rr)[0]
+            torch.cuda.synchronize()
+            rec = recall(ids.cpu().numpy().view(np.uint32), gt)
+            curve.append((L, round(rec, 4)))
+            if rec >= args.target_recall:
+                hit = (L, rec)
+                break
+        row = {"recall_curve": curve}
+        if hit:
+            L = hit[0]
+            tune = ix.autotune(Qd, K, L, traversal=trav, rerank_size=rr, reps=1)
+            res = ix.search_arrays(Qd, K, L, traversal=trav, rerank_size=rr)
+            for _ in range(max(args.warmup, 1)):
+                ix.search_arrays(Qd, K, L, traversal=trav, rerank_size=rr, out=res)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                ix.search_arrays(Qd, K, L, traversal=trav, rerank_size=rr, out=res)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / args.steps
+            row.update({"L": L, "recall_at_10": round(hit[1], 4), "qps": len(Q) / (ms / 1e3), "ms_per_step": ms,
+                        "visited_table_bits": tune["hbits"]})
+        out["at_target"]["variants"][name] = row
+        log(f"[cosine] at target {name}: {json.dumps(row)}")
     for ix in (base, q8, rq):
         ix.close()
     return out

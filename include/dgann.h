@@ -220,16 +220,21 @@ DG_API DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const flo
  * holds; a smaller table recomputes the distances of ids it forgets), the
  * order in which the persistent grid takes the queries (as given, or grouped
  * by nearest pivot row so that queries in one region of the graph run
- * together and share rows in L2), and the share of the resident CTAs per SM
- * the grid uses (100, 75, 50 %).  No schedule changes a result.
+ * together and share rows in L2), the share of the resident CTAs per SM
+ * the grid uses (100, 75, 50 %), and the warps (queries in flight) per CTA
+ * (4, 2, 1: a query with a large state -- long beams, wide rows -- packs an
+ * SM's shared memory more finely in smaller CTAs).  No schedule changes a
+ * result.
  * ms_per_call[6] (may be NULL) receives the mean time per call of each table
  * size, -1 where the size did not fit in shared memory. */
 DG_API DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const float *queries, uint32_t nq,
                                   uint32_t reps, uint32_t *best_hbits, float *ms_per_call);
 /* The schedule the last dg_index_autotune chose: visited-table bits, query
- * order (0 = as given, 1 = grouped by nearest pivot) and percent of the
- * resident CTAs per SM.  No counterpart in the reference. */
-DG_API DgStatus dg_index_tuned_schedule(DgIndex *idx, uint32_t *hbits, uint32_t *order, uint32_t *occ_pct);
+ * order (0 = as given, 1 = grouped by nearest pivot), percent of the
+ * resident CTAs per SM and warps per CTA (each out pointer may be NULL).  No
+ * counterpart in the reference. */
+DG_API DgStatus dg_index_tuned_schedule(DgIndex *idx, uint32_t *hbits, uint32_t *order, uint32_t *occ_pct,
+                                        uint32_t *warps_per_cta);
 
 /* dg_search_batch for callers that cannot have device memory allocated for
  * them (hosts whose device memory belongs to a separate pool manager,

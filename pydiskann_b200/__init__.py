@@ -481,19 +481,20 @@ class _Index:
     def autotune(self, queries, k=10, beam_width=128, traversal=_lib.TRAVERSE_F32, rerank_size=0, filters=None,
                  per_query_beam=None, reps=3):
         """Times this search (same arguments as search_arrays) under candidate
-        launch schedules -- visited-table size, query order, CTAs per SM -- and
-        keeps the fastest for later searches of the same kind
-        (dg_index_autotune).  Returns {"hbits", "order", "occ_pct": the chosen
-        schedule, "ms": {bits: ms per call of each table size}}."""
+        launch schedules -- visited-table size, query order, CTAs per SM, warps
+        per CTA -- and keeps the fastest for later searches of the same kind
+        (dg_index_autotune).  Returns {"hbits", "order", "occ_pct",
+        "warps_per_cta": the chosen schedule, "ms": {bits: ms per call of each
+        table size}}."""
         p, Q, nq, _, _, keep = self._params(queries, k, beam_width, traversal, rerank_size, filters,
                                             per_query_beam, None, None, False)
         best = C.c_uint32()
         ms = (C.c_float * 6)()
         check(lib().dg_index_autotune(self._h, C.byref(p), ptr(Q), nq, reps, C.byref(best), ms))
         del keep
-        hb, order, occ = C.c_uint32(), C.c_uint32(), C.c_uint32()
-        check(lib().dg_index_tuned_schedule(self._h, C.byref(hb), C.byref(order), C.byref(occ)))
-        return {"hbits": hb.value, "order": order.value, "occ_pct": occ.value,
+        hb, order, occ, wpb = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib().dg_index_tuned_schedule(self._h, C.byref(hb), C.byref(order), C.byref(occ), C.byref(wpb)))
+        return {"hbits": hb.value, "order": order.value, "occ_pct": occ.value, "warps_per_cta": wpb.value,
                 "ms": {8 + i: round(ms[i], 4) for i in range(6) if ms[i] >= 0}}
 
     # -- reference-shaped helpers

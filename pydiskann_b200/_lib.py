@@ -99,7 +99,7 @@ def _signatures():
         "dg_index_attach_labels": (st, [vp, u32, vp]),
         "dg_index_get_codes": (st, [vp, vp, u64, vp]),
         "dg_index_autotune": (st, [vp, vp, vp, u32, u32, vp, vp]),
-        "dg_index_tuned_schedule": (st, [vp, vp, vp, vp]),
+        "dg_index_tuned_schedule": (st, [vp, vp, vp, vp, vp]),
         "dg_index_set_entry_points": (st, [vp, vp, u32]),
         "dg_index_set_code_limit": (st, [vp, u64]),
         "dg_index_set_tombstones": (st, [vp, vp, u64, i32, u64]),

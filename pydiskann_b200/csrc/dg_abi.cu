@@ -466,6 +466,7 @@ static DgIndex::Schedule schedule_of(DgIndex *idx, int trav, int lcap, bool filt
   if (const char *e = std::getenv("DG_HBITS")) sc.hbits = (uint32_t)std::max(6, std::min(14, atoi(e)));
   if (const char *e = std::getenv("DG_ORDER")) sc.order = atoi(e) != 0;
   if (const char *e = std::getenv("DG_OCC_PCT")) sc.occ_pct = (uint32_t)std::max(1, std::min(100, atoi(e)));
+  if (const char *e = std::getenv("DG_WPB")) sc.wpb = atoi(e) == 1 ? 1u : atoi(e) == 2 ? 2u : 4u;
   return sc;
 }
 
@@ -715,6 +716,7 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   }
   a.counter = sl.counter;
   a.occ_pct = sched.occ_pct;
+  a.wpb = sched.wpb;
   // query order: grouped by nearest pivot (per pipeline chunk) when the
   // schedule asks for it and the pivots fit the ordering kernel
   const bool ordered = sched.order && (size_t)pivot_count(idx->dpad) * idx->d * 4 <= 48 * 1024;
@@ -913,6 +915,12 @@ DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const float *q
     c.occ_pct = pct;
     result = consider(c, nullptr);
   }
+  for (uint32_t w : {2u, 1u}) {
+    if (result != DG_OK || !have) break;
+    DgIndex::Schedule c = best;
+    c.wpb = w;
+    result = consider(c, nullptr);
+  }
   std::lock_guard<std::mutex> lk(idx->mu);
   idx->forcing = false;
   if (result != DG_OK) return result;
@@ -923,12 +931,14 @@ DgStatus dg_index_autotune(DgIndex *idx, const DgSearchParams *p, const float *q
   return DG_OK;
 }
 
-DgStatus dg_index_tuned_schedule(DgIndex *idx, uint32_t *hbits, uint32_t *order, uint32_t *occ_pct) {
+DgStatus dg_index_tuned_schedule(DgIndex *idx, uint32_t *hbits, uint32_t *order, uint32_t *occ_pct,
+                                 uint32_t *warps_per_cta) {
   if (!idx) return fail(DG_EINVAL, "null index");
   std::lock_guard<std::mutex> lk(idx->mu);
   if (hbits) *hbits = idx->last_tuned.hbits;
   if (order) *order = idx->last_tuned.order;
   if (occ_pct) *occ_pct = idx->last_tuned.occ_pct;
+  if (warps_per_cta) *warps_per_cta = idx->last_tuned.wpb;
   return DG_OK;
 }
 

@@ -41,10 +41,12 @@ struct DgIndex {
   uint64_t code_limit = 0;             // rows >= code_limit have no codes (0 = every row has)
   // Launch schedule of a kind of search (traversal, working-set capacity,
   // filtered), chosen by dg_index_autotune: the visited-table size (log2 words
-  // per query), the query order (0 = as given, 1 = grouped by nearest pivot)
-  // and the share of the resident CTAs per SM the grid uses (percent).
+  // per query), the query order (0 = as given, 1 = grouped by nearest pivot),
+  // the share of the resident CTAs per SM the grid uses (percent) and the
+  // warps per CTA (4, 2 or 1: smaller CTAs pack an SM's shared memory more
+  // finely when each query holds a large state).
   struct Schedule {
-    uint32_t hbits = 0, order = 0, occ_pct = 100;
+    uint32_t hbits = 0, order = 0, occ_pct = 100, wpb = 4;  // wpb: warps (queries in flight) per CTA
   };
   std::map<uint32_t, Schedule> tuned;
   bool forcing = false;   // the autotuner pins `force` while it times a candidate

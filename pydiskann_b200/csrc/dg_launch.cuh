@@ -14,8 +14,9 @@ struct LaunchInfo {
   uint32_t smem = 0;
 };
 
-// Launch geometry: 4 warps per block, as many resident blocks as shared memory
-// allows on every SM, never more warps than queries.
+// Launch geometry: 4 warps per block (or the schedule's 2 or 1), as many
+// resident blocks as shared memory and registers allow on every SM, never more
+// warps than queries.
 // Resident blocks per SM of (device, kernel, shared-memory size), and the
 // largest dynamic shared memory already granted to (device, kernel): the
 // attribute and occupancy queries run once, not on every launch (a serving
@@ -34,7 +35,8 @@ inline LaunchGeometry &launch_geometry() {
 template <typename K>
 DgStatus launch_persistent(K kernel, const SearchArgs &a, const WarpLayout &Ly, cudaStream_t st,
                            LaunchInfo *info) {
-  const uint32_t smem = Ly.total * 4;
+  const uint32_t wpb = (a.wpb == 1 || a.wpb == 2) ? a.wpb : 4u;  // warps per CTA
+  const uint32_t smem = Ly.total * wpb;
   int dev = 0;
   DG_CUDA(cudaGetDevice(&dev));
   LaunchGeometry &G = launch_geometry();
@@ -61,21 +63,22 @@ DgStatus launch_persistent(K kernel, const SearchArgs &a, const WarpLayout &Ly, 
       gr = (int)smem;
     }
     auto &per = G.nb[key];
-    auto n_it = per.find(smem);
+    const uint32_t okey = smem * 8u + wpb;
+    auto n_it = per.find(okey);
     if (n_it == per.end()) {
       int v = 0;
-      DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, 128, smem));
-      n_it = per.emplace(smem, v).first;
+      DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, 32 * (int)wpb, smem));
+      n_it = per.emplace(okey, v).first;
     }
     nb = n_it->second;
   }
   if (nb <= 0) return fail(DG_ENOTSUP, "search kernel cannot be resident on an SM");
   if (a.occ_pct > 0 && a.occ_pct < 100) nb = std::max(1, (int)((nb * a.occ_pct + 99) / 100));
   int grid = nb * sms;
-  const int need = (int)((a.nq + 3) / 4);
+  const int need = (int)((a.nq + wpb - 1) / wpb);
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  kernel<<<grid, 128, smem, st>>>(a, Ly);
+  kernel<<<grid, 32 * wpb, smem, st>>>(a, Ly);
   DG_CUDA(cudaGetLastError());
   if (info) {
     info->grid = grid;

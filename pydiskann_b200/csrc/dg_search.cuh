@@ -79,6 +79,7 @@ struct SearchArgs {
   uint32_t *counter;  // work counter, zero at launch
   const uint32_t *perm;  // order in which the grid takes the queries (null = as given)
   uint32_t occ_pct;      // share of the resident CTAs per SM the grid uses (percent; 0 = all)
+  uint32_t wpb;          // warps per CTA of the launch (1, 2 or 4; 0 = 4), one query per warp
 };
 
 enum TravKind { TRAV_F32 = 0, TRAV_BF16 = 1, TRAV_PQ = 2, TRAV_INT8 = 3, TRAV_RABITQ = 4, TRAV_F16 = 5, TRAV_FP8 = 6 };
@@ -663,7 +664,8 @@ __device__ __forceinline__ float bf16_dot_mma(const uint16_t *__restrict__ rows,
       const int ch = t + 4 * (j0 + u);
       const bool ok = j0 + u < J && ch < nch;
 #pragma unroll
-      for (int h = 0; h < 4; ++h) x[u][h] = (ok && (h < 2 || two)) ? ldg_row<false>(rp[h] + ch) : z;
+      for (int h = 0; h < 4; ++h)  // the first round's loads fetch whole 256-byte blocks into L2
+        x[u][h] = (ok && (h < 2 || two)) ? (j0 == 0 ? ldg_row<true>(rp[h] + ch) : ldg_row<false>(rp[h] + ch)) : z;
       qv[u] = ok && col ? pq[ch] : z;
     }
 #pragma unroll

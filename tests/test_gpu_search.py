@@ -380,7 +380,8 @@ def test_autotune_keeps_results(oracle, small_data, small_graph):
     filt = [FILTERS[i % len(FILTERS)] for i in range(len(Q))]
     want_b = o.search(Q, 10, 48, rerank=24, use_codes=True, per_query_L=beams)
     for env in ({"DG_HBITS": "8"}, {"DG_HBITS": "13"}, {"DG_ORDER": "1"}, {"DG_ORDER": "1", "DG_HBITS": "8"},
-                {"DG_OCC_PCT": "50"}, {"DG_OCC_PCT": "75", "DG_ORDER": "1"}):
+                {"DG_OCC_PCT": "50"}, {"DG_OCC_PCT": "75", "DG_ORDER": "1"}, {"DG_WPB": "1"},
+                {"DG_WPB": "2", "DG_ORDER": "1", "DG_HBITS": "13"}):
         os.environ.update(env)
         try:
             assert_same(q.search_arrays(Q, 10, 48, rerank_size=24), o.search(Q, 10, 48, rerank=24, use_codes=True))
@@ -397,8 +398,8 @@ def test_autotune_keeps_results(oracle, small_data, small_graph):
 
 
 def test_autotune_schedule_axes(oracle, small_data, small_graph):
-    """The tuner's choice covers the three axes (table size, query order,
-    CTAs per SM) and a device-pointer search of 3000 queries after tuning --
+    """The tuner's choice covers the four axes (table size, query order,
+    CTAs per SM, warps per CTA) and a device-pointer search of 3000 queries after tuning --
     ordered or not -- returns the oracle's results."""
     import torch
 
@@ -409,6 +410,7 @@ def test_autotune_schedule_axes(oracle, small_data, small_graph):
     Qb = np.concatenate([Q] * 15)
     t = ix.autotune(Qb, 10, 40, traversal=_lib.TRAVERSE_BF16, rerank_size=40, reps=2)
     assert 8 <= t["hbits"] <= 13 and t["order"] in (0, 1) and t["occ_pct"] in (50, 75, 100)
+    assert t["warps_per_cta"] in (1, 2, 4)
     o = oracle.OracleIndex(X, adj, med)
     o.set_bf16()
     want = o.search(Qb, 10, 40, rerank=40, use_codes=True)
@@ -499,3 +501,37 @@ def test_packed_filters_equal_per_call_programs(small_data, small_graph):
     b = g.search_arrays(Q, 10, 40, filters=dg.pack_filters(fl))
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
     g.close()
+
+
+def test_bf16_after_row_and_adjacency_updates(oracle):
+    """After rows and adjacency rows are rewritten in place
+    (dg_index_update_rows), the BF16 copy and its per-row norms follow: BF16
+    searches (with and without rerank) equal the oracle on the updated index."""
+    from pydiskann_b200 import synth
+
+    X = synth.mixture(4000, 128, 16, seed=52)
+    Q = synth.mixture(300, 128, 16, seed=52, stream=synth.STREAM_QUERY)
+    adj, med = oracle.build_vamana(X, 32, 64, 1.2, seed=8)
+    adj = adj.reshape(len(X), -1).copy()
+    ix = dg.DiskANN.from_graph(X, adj, med)
+    ix.enable_bf16()
+    rng = np.random.default_rng(52)
+    # rows near the queries move (new integer values), other rows get new neighbours
+    rows = np.unique(np.asarray(oracle.OracleIndex(X, adj, med).search(Q[:40], 5, 64)[0]).ravel())
+    rows = rows[rows != med][:60].astype(np.int64)
+    Xn = X.copy()
+    for r in rows:
+        Xn[r] = np.clip(np.round(X[r] + rng.normal(0, 30, X.shape[1])), 0, 255)
+        assert _lib.lib().dg_index_update_rows(ix._h, int(r), 1, _lib.ptr(Xn[r:r + 1]), None, None) == _lib.DG_OK
+    for r in rng.choice(len(X), 80, replace=False):
+        row = adj[r].copy()
+        row[: len(row) // 2] = rng.choice(len(X), len(row) // 2, replace=False)
+        adj[r] = row
+        assert _lib.lib().dg_index_update_rows(ix._h, int(r), 1, None, _lib.ptr(adj[r:r + 1]), None) == _lib.DG_OK
+    o = oracle.OracleIndex(Xn, adj, med)
+    o.set_bf16()
+    for L, rr in ((40, 0), (64, 64)):
+        assert_same(ix.search_arrays(Q, 10, L, traversal=_lib.TRAVERSE_BF16, rerank_size=rr),
+                    o.search(Q, 10, L, rerank=rr, use_codes=True))
+    ix.close()
+
