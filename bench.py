@@ -319,9 +319,9 @@ class Clocks:
 # dram__bytes_write.sum) from one ncu capture of this bench's command on a
 # smaller batch, keyed by (variant, L, base vectors): (queries captured,
 # bytes).  The line scales it to the batch by queries.
-NCU_TRAFFIC = {("bf16_rerank", 40, 1_000_000): (2000, 612.557568e6 + 4.95616e6)}
+NCU_TRAFFIC = {("bf16_rerank", 40, 1_000_000): (2000, 623.473408e6 + 5.54752e6)}
 NCU_TRAFFIC_SOURCE = ("scaled by queries from one ncu --set full capture of a 2000-query launch of the same "
-                      "kernel (python bench.py --nq 2000 --variants bf16_rerank ...)")
+                      "kernel (python bench.py --nq 2000 --beam 40 --no-autotune --variants bf16_rerank ...)")
 
 VARIANTS = {
     # name: (traversal, rerank = L?)
@@ -852,7 +852,8 @@ def filtered_serving(args, dev, full=True):
                     r = {"variant": name, "k": k, "L": L, "offered_rps": rate,
                          "achieved_qps": round(n / (res["wall_us"] / 1e6)), "p50_ms": round(float(np.percentile(lat, 50)), 3),
                          "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                         "recall_at_10": round(float(np.mean(hits)) / K, 4), "visited_table_bits": tune["hbits"]}
+                         "recall_at_10": round(float(np.mean(hits)) / K, 4), "visited_table_bits": tune["hbits"],
+                         "schedule": {a: b for a, b in tune.items() if a != "ms"}}
                     out["runs"].append(r)
                     log(f"[filtered serving] {json.dumps(r)}")
     ix.close()

@@ -59,7 +59,8 @@ static int lanes_per_row(uint32_t chunks) {
 // Grows every call slot's staging buffers for per-call parameters to hold a
 // batch of nq queries with `ops` filter instructions and `pool` IN values, so
 // that later calls of that size reallocate nothing (a reallocation synchronises
-// the device, a latency spike for every batch in flight).  Waits for slots
+// the device, a latency spike for every batch in flight), the scratch of a
+// pivot-ordered launch included, and makes the pivot rows.  Waits for slots
 // whose previous call is still running.
 DgStatus reserve_call_buffers(DgIndex *idx, uint32_t nq, size_t ops, size_t pool) {
   std::lock_guard<std::mutex> lk(idx->mu);
@@ -75,7 +76,13 @@ DgStatus reserve_call_buffers(DgIndex *idx, uint32_t nq, size_t ops, size_t pool
     if ((s = buf_reserve(sl.fpool, pool * 8)) != DG_OK) return s;
     if ((s = buf_reserve(sl.perl, (size_t)nq * 4)) != DG_OK) return s;
     if ((s = buf_reserve(sl.perk, (size_t)nq * 4)) != DG_OK) return s;
+    // query-order scratch (a schedule that groups queries by nearest pivot)
+    if ((s = buf_reserve(sl.sched, ((size_t)2 * nq + (size_t)DgIndex::kPipeChunks * pivot_count(idx->dpad)) * 4)) !=
+        DG_OK)
+      return s;
   }
+  // the pivot rows of that order, copied once
+  if ((size_t)pivot_count(idx->dpad) * idx->d * 4 <= 48 * 1024) return ensure_pivots(idx);
   return DG_OK;
 }
 
@@ -689,7 +696,9 @@ DgStatus dg_search_batch(DgIndex *idx, const DgSearchParams *p, const float *que
   }
   const size_t kq = (size_t)nq * p->k;
   // host calls of many queries: chunks whose copies overlap the other chunks' kernels
-  const uint32_t chunks = devptr || nq < 4096 ? 1u : std::min<uint32_t>(DgIndex::kPipeChunks, nq / 2048);
+  uint32_t chunks = devptr || nq < 4096 ? 1u : std::min<uint32_t>(DgIndex::kPipeChunks, nq / 2048);
+  if (const char *e = std::getenv("DG_PIPE_CHUNKS"); e && chunks > 1)  // override for measurements
+    chunks = (uint32_t)std::max(1, std::min(DgIndex::kPipeChunks, atoi(e)));
   if (devptr) {
     a.Q = queries;
     a.out_ids = out_ids;
