@@ -195,3 +195,36 @@ def test_device_query_checks():
                 call(_AsCuda(torch.zeros((2, 4), dtype=torch.float64)))
     finally:
         s._h = None
+
+
+def test_autotune_reports_every_axis(monkeypatch):
+    """Index.autotune passes the search to dg_index_autotune and returns the
+    schedule dg_index_tuned_schedule reports: table bits, query order, CTAs
+    per SM and warps per CTA, with the per-table timings that fitted."""
+    import ctypes as C
+
+    import pydiskann_b200 as dg
+
+    class FakeLib:
+        def dg_index_autotune(self, h, p, q, nq, reps, best, ms):
+            assert nq == 3 and reps == 2
+            arr = C.cast(ms, C.POINTER(C.c_float))
+            for i in range(6):
+                arr[i] = -1.0 if i == 5 else 1.0 + i
+            best._obj.value = 10
+            return 0
+
+        def dg_index_tuned_schedule(self, h, hb, order, occ, wpb):
+            hb._obj.value, order._obj.value, occ._obj.value, wpb._obj.value = 10, 1, 75, 2
+            return 0
+
+    monkeypatch.setattr(dg, "lib", lambda: FakeLib())
+    ix = object.__new__(dg._Index)
+    ix._X = np.zeros((1, 4), np.float32)
+    ix._h = object()  # stands in for the device index
+    try:
+        t = ix.autotune(np.zeros((3, 4), np.float32), 10, 32, reps=2)
+    finally:
+        ix._h = None
+    assert t == {"hbits": 10, "order": 1, "occ_pct": 75, "warps_per_cta": 2,
+                 "ms": {8: 1.0, 9: 2.0, 10: 3.0, 11: 4.0, 12: 5.0}}
