@@ -109,6 +109,13 @@ struct ServeSlot {
   std::vector<ServeRequest *> batch;
   uint32_t k = 0;       // result row stride: the batch's largest k
   size_t off = 0;       // the batch's arena region
+  // pinned staging of the batch's filter programs (ops, offsets, IN pool),
+  // sized at creation: a copy from pageable memory is staged by the driver
+  // through a shared buffer and can wait behind other streams' kernels
+  DgFilterOp *h_ops = nullptr;
+  uint32_t *h_offs = nullptr;
+  uint64_t *h_pool = nullptr;
+  size_t cap_ops = 0, cap_pool = 0;
 };
 
 }  // namespace dg
@@ -341,6 +348,14 @@ static void dispatch_loop(DgServer *s) {
         p.filter_offsets = offs.data();
         p.filter_pool = pool.data();
         p.filter_pool_len = (uint32_t)pool.size();
+        if (ops.size() <= sl.cap_ops && pool.size() <= sl.cap_pool && sl.h_ops) {
+          std::memcpy(sl.h_ops, ops.data(), ops.size() * sizeof(DgFilterOp));
+          std::memcpy(sl.h_offs, offs.data(), offs.size() * sizeof(uint32_t));
+          if (!pool.empty()) std::memcpy(sl.h_pool, pool.data(), pool.size() * sizeof(uint64_t));
+          p.filter_ops = sl.h_ops;
+          p.filter_offsets = sl.h_offs;
+          p.filter_pool = sl.h_pool;
+        }
       }
       p.flags = DG_FLAG_DEVICE_PTRS | DG_FLAG_STREAM;
       p.stream = sl.stream;
@@ -423,6 +438,8 @@ DgStatus dg_server_destroy(DgServer *s) {
   for (ServeSlot &sl : s->slots) {
     if (sl.stream) cudaStreamSynchronize(sl.stream);
     if (sl.stream) cudaStreamDestroy(sl.stream);
+    for (void *h : {(void *)sl.h_ops, (void *)sl.h_offs, (void *)sl.h_pool})
+      if (h) cudaFreeHost(h);
   }
   if (s->h_arena) cudaFreeHost(s->h_arena);
   if (s->d_arena) cudaFree(s->d_arena);
@@ -466,6 +483,15 @@ DgStatus dg_server_create(DgIndex *idx, const DgServerConfig *cfg, DgServer **ou
     if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess) {
       dg_server_destroy(s);
       return fail(DG_EDEVICE, "server stream creation failed");
+    }
+    if (cfg->max_filter_ops) {
+      sl.cap_ops = sl.cap_pool = (size_t)cfg->max_batch * cfg->max_filter_ops;
+      if (cudaMallocHost((void **)&sl.h_ops, sl.cap_ops * sizeof(DgFilterOp)) != cudaSuccess ||
+          cudaMallocHost((void **)&sl.h_offs, ((size_t)cfg->max_batch + 1) * sizeof(uint32_t)) != cudaSuccess ||
+          cudaMallocHost((void **)&sl.h_pool, sl.cap_pool * sizeof(uint64_t)) != cudaSuccess) {
+        dg_server_destroy(s);
+        return fail(DG_ENOMEM, "server filter staging allocation failed");
+      }
     }
   }
   s->dispatcher = std::thread(dispatch_loop, s);
