@@ -179,10 +179,10 @@ def recall(ids, gt, k=K):
     return hits / (len(gt) * k)
 
 
-def config_of(args, world, L):
+def config_of(args, world, L, variant=HEADLINE):
     """The `config` object both arms print (same workload, variant and beam)."""
     return {"workload": f"pq-1Mx128 M={M} R={R} L_build={L_BUILD} alpha={ALPHA} k={K} nq={args.nq} n={args.n}",
-            "variant": HEADLINE, "L": L, "global_batch": args.nq * world, "parallelism": f"replicas{world}",
+            "variant": variant, "L": L, "global_batch": args.nq * world, "parallelism": f"replicas{world}",
             "l2_policy": "inputs larger than L2 (512 MB f32 + 256 MB bf16 rows + 256 MB adjacency)"}
 
 
@@ -603,7 +603,7 @@ def main():
         "dtype": {"fp32": "f32", "bf16_rerank": "bf16+f32", "int8_rerank": "u8+f32",
                   "fp8_rerank": "e4m3+f32"}.get(head, "u8-pq+f32"),
         "data": "synthetic (seeded 256-centre Gaussian mixture, 1M x 128, 10k queries)",
-        "config": config_of(args, world, results[head]["L"] if head else None),
+        "config": config_of(args, world, results[head]["L"] if head else None, head or HEADLINE),
         "fp32_qps": results["fp32"]["qps"] if "fp32" in results else None,
         "bf16_rerank_over_fp32": (round(results[HEADLINE]["qps"] / results["fp32"]["qps"], 3)
                                   if HEADLINE in results and "fp32" in results else None),
