@@ -1017,10 +1017,13 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
       if (mx > 0.0f) atomicMax(&s_qmax, __float_as_uint(mx));
     }
     __syncthreads();
-    if (threadIdx.x < m) {
+    // query norms: a warp per query, lanes over the coordinates
+    for (uint32_t j = warp; j < m; j += blockDim.x >> 5) {
       float s2 = 0.0f;
-      for (uint32_t i = 0; i < a.d; ++i) s2 = fmaf(qsm[threadIdx.x * dq + i], qsm[threadIdx.x * dq + i], s2);
-      qn[threadIdx.x] = s2;
+      for (uint32_t i = lane; i < a.d; i += 32) s2 = fmaf(qsm[j * dq + i], qsm[j * dq + i], s2);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(kFull, s2, o);
+      if (lane == 0) qn[j] = s2;
     }
     // this warp's queries: j = warp + 8 u (u < 4)
     int cur[4] = {0, 0, 0, 0}, size[4] = {0, 0, 0, 0};
@@ -1062,11 +1065,16 @@ __global__ void __launch_bounds__(256) k_pm_scan_postings(SpfArgs a, const uint4
         if (mx > 0.0f) atomicMax(&s_tmax, __float_as_uint(mx));
       }
       __syncthreads();
-      if (threadIdx.x < ne) {
-        const float *row = tile + threadIdx.x * dt;
+      // entry norms: four lanes per row (8 rows per warp pass), interleaved
+      // coordinates, so a quarter warp reads one row's consecutive words
+      for (uint32_t r0 = 8u * warp; r0 < ne; r0 += 8u * (blockDim.x >> 5)) {
+        const uint32_t r = r0 + (lane >> 2);
         float s2 = 0.0f;
-        for (uint32_t i = 0; i < a.d; ++i) s2 = fmaf(row[i], row[i], s2);
-        xn[threadIdx.x] = s2;
+        if (r < ne)
+          for (uint32_t i = lane & 3; i < a.d; i += 4) s2 = fmaf(tile[r * dt + i], tile[r * dt + i], s2);
+        s2 += __shfl_xor_sync(kFull, s2, 1);
+        s2 += __shfl_xor_sync(kFull, s2, 2);
+        if (r < ne && (lane & 3) == 0) xn[r] = s2;
       }
       const float qm = __uint_as_float(s_qmax), tm = __uint_as_float(s_tmax);
       // (the dot products overwrite the f32 tile, which must hold kPmQ x kPmT floats)
