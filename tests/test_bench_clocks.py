@@ -77,3 +77,21 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     monkeypatch.setenv("RANK", "1")
     assert bench.reference_arm(None) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_bench_flags(monkeypatch):
+    """The default run carries the short filtered-serving grid (--no-filtered-serving
+    drops it, --filtered-serving asks for the whole grid); --beam and --no-autotune
+    are for profiling runs and default off."""
+    import sys
+
+    import bench
+
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse()
+    assert not a.no_filtered_serving and not a.filtered_serving and a.beam == 0 and not a.no_autotune
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--no-filtered-serving", "--beam", "40", "--no-autotune"])
+    a = bench.parse()
+    assert a.no_filtered_serving and a.beam == 40 and a.no_autotune
+    assert bench.config_of(a, 1, 40, "fp32")["variant"] == "fp32"
+    assert bench.config_of(a, 1, 40)["variant"] == bench.HEADLINE
