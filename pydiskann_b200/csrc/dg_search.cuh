@@ -664,7 +664,7 @@ __device__ __forceinline__ float bf16_dot_mma(const uint16_t *__restrict__ rows,
       const int ch = t + 4 * (j0 + u);
       const bool ok = j0 + u < J && ch < nch;
 #pragma unroll
-      for (int h = 0; h < 4; ++h)  // the first round's loads fetch whole 256-byte blocks into L2
+      for (int h = 0; h < 4; ++h)  // loads of a row's first 128 bytes fetch its whole 256-byte block into L2
         x[u][h] = (ok && (h < 2 || two)) ? (j0 == 0 ? ldg_row<true>(rp[h] + ch) : ldg_row<false>(rp[h] + ch)) : z;
       qv[u] = ok && col ? pq[ch] : z;
     }
